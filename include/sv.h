@@ -1,0 +1,196 @@
+/*
+ * sv.h -- C-ABI of the B200 Saint-Venant time step (libsv_b200.so).
+ *
+ * Drop-in boundary for the hot path of oojimaflib/mfcm: the 2-D Saint-Venant explicit
+ * Runge-Kutta time step (face fluxes with wet/dry handling, bed slope, Manning friction,
+ * rainfall = discharge boundary, outflow = head boundary, RK stage combination and the CFL
+ * control number). Plain C types only; no exceptions cross this boundary; every function
+ * returns 0 on success or a negative SV_E* code, with a message in sv_last_error().
+ *
+ * Ownership: an sv_ctx owns all device memory and one CUDA stream; host pointers are
+ * borrowed for the duration of the call; sv_get_field is synchronous on the ctx stream.
+ * Threading: one ctx is used by one host thread at a time (like the reference's single
+ * sycl::queue); separate ctxs are independent.
+ *
+ * Each entry point names the reference interface it replaces (paths are relative to the
+ * reference project's root).
+ */
+#ifndef SV_B200_H
+#define SV_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- error codes ------------------------------------------------------------------- */
+#define SV_OK 0
+#define SV_E_ARG (-1)       /* invalid argument (null pointer, size mismatch, bad id)      */
+#define SV_E_CUDA (-2)      /* CUDA runtime error                                          */
+#define SV_E_NOMEM (-3)     /* device allocation failed                                    */
+#define SV_E_STATE (-4)     /* call not valid in the current state                         */
+#define SV_E_NONFINITE (-5) /* the control number became NaN (state is no longer finite)    */
+#define SV_E_TIMEOUT (-6)   /* a bounded device-side wait gave up                          */
+#define SV_E_LIMIT (-7)     /* size beyond a documented maximum                            */
+
+/* ---- precision --------------------------------------------------------------------- */
+typedef enum {
+  SV_F32 = 1,         /* FP32 state and arithmetic, FP64 reductions                   */
+  SV_F64 = 2,         /* plain FP64: bit-for-bit the reference arithmetic at T=double */
+  SV_F32_DATUM64 = 3  /* FP32 state, bed stored as FP32 offsets from FP64 tile datums   */
+} sv_precision;
+
+/* Mirrors the Cartesian2DMesh configuration (src/Mesh/Cartesian2DMesh.cpp:24-61):
+ * "cell count" = (nx, ny), "cell size" = (dx, dy), "origin"; rotation angle 0 only. */
+typedef struct {
+  uint64_t nx, ny;
+  double dx, dy;
+  double origin_x, origin_y;
+} sv_mesh_desc;
+
+/* Mirrors the scheme configuration read by create_scheme (src/mfcm.cpp:19-36),
+ * RungeKuttaTimeParameters (src/Config/TimeParameters.cpp:21-38) and the solver's
+ * source-term/boundary lists (src/SaintVenant/Solver.cpp:61-67). */
+typedef struct {
+  int precision;        /* sv_precision                                                 */
+  int rk_method;        /* named tableau index, see SV_RK_* (RungeKutta.cpp:54-115)      */
+  double cn_target;     /* control-number target; the reference hard-codes 1.0
+                           (src/TemporalScheme/RungeKutta.cpp:154)                      */
+  double step_duration; /* "step duration seconds" L (TimeParameters.cpp:29-32)         */
+  double initial_dt;    /* "initial timestep seconds" (TimeParameters.cpp:34)           */
+  double max_dt;        /* 0 = no clamp (reference behaviour); > 0 clamps each new dt   */
+  int rain_mode;        /* 0 = reference discharge clamp, 1 = physical clamp            */
+  int manning;          /* 1 = "manning roughness" source term present                  */
+  int head_first;       /* 1 = head boundary listed before discharge in the config      */
+  int flags;            /* SV_FLAG_*                                                     */
+} sv_params;
+
+#define SV_FLAG_NO_TALLIES 1u /* skip the rain/outflow tally partials                    */
+
+/* named Runge-Kutta tableaux, in the order of runge_kutta_named_coefficient_sets_ */
+#define SV_RK_EULER 0
+#define SV_RK_MIDPOINT 1
+#define SV_RK_HEUN2 2
+#define SV_RK_RALSTON2 3
+#define SV_RK_KUTTA3 4
+#define SV_RK_HEUN3 5
+#define SV_RK_WRAY3 6
+#define SV_RK_RALSTON3 7
+#define SV_RK_SSPRK3 8
+#define SV_RK_CLASSIC 9
+#define SV_RK_RALSTON4 10
+#define SV_RK_38RULE 11
+
+/* field ids for sv_set_field / sv_get_field (cell fields are nx*ny, row-major i = y*nx+x;
+ * face fields are (nx+1)*ny vertical faces followed by (ny+1)*nx horizontal faces) */
+#define SV_FIELD_Z 0            /* bed elevation z_bed (Constants.hpp:39)                 */
+#define SV_FIELD_H 1            /* depth h of U_[0] (State.hpp:40)                       */
+#define SV_FIELD_U 2            /* x velocity u of U_[0]                                  */
+#define SV_FIELD_V 3            /* y velocity v of U_[0]                                  */
+#define SV_FIELD_N_SHALLOW 4    /* Manning n_shallow (ManningRoughnessSourceTerm.hpp:111) */
+#define SV_FIELD_N_DEEP 5
+#define SV_FIELD_D_SHALLOW 6
+#define SV_FIELD_D_DEEP 7
+#define SV_FIELD_QBDY0 8        /* discharge xbdy0 (BoundarySourceTerm.hpp:44), m/s       */
+#define SV_FIELD_QBDY1 9        /* discharge xbdy1                                        */
+#define SV_FIELD_HBDY0 10       /* head xbdy0 (NaN = not selected)                        */
+#define SV_FIELD_HBDY1 11
+#define SV_FIELD_RAIN_PATTERN 12 /* per-cell rain pattern P for SV_RAIN_PATTERN            */
+#define SV_FIELD_DHDT 20        /* dUdt_[0] of the last sv_eval_dudt(0, ...)              */
+#define SV_FIELD_DUDT 21
+#define SV_FIELD_DVDT 22
+#define SV_FIELD_DHDX 23        /* dUdx_ / dUdy_ of the last sv_eval_dudt (State.cpp:176) */
+#define SV_FIELD_DUDX 24
+#define SV_FIELD_DVDX 25
+#define SV_FIELD_DHDY 26
+#define SV_FIELD_DUDY 27
+#define SV_FIELD_DVDY 28
+#define SV_FIELD_DZDX 29        /* bed slopes (Constants.cpp:39-40)                       */
+#define SV_FIELD_DZDY 30
+#define SV_FIELD_FLUX_H 40      /* face fluxes of the last sv_eval_dudt (Fluxes.hpp:43-49)*/
+#define SV_FIELD_FLUX_U 41
+#define SV_FIELD_FLUX_V 42
+#define SV_FIELD_FLUX_Z 43
+#define SV_FIELD_FLUX_BRANCH 44 /* wet/dry branch per face: 0,1,2.25,2.75,3,4             */
+#define SV_FIELD_STATE_BASE 100 /* 100 + 3*s + {0,1,2}: h,u,v of U_[s]                    */
+#define SV_FIELD_K_BASE 200     /* 200 + 3*s + {0,1,2}: h,u,v of dUdt_[s]                 */
+
+/* ---- per-step boundary values (DischargeBoundarySourceTerm.hpp:114-146,
+ *      HeadBoundarySourceTerm.hpp:114-146): values at the start (0) and end (1) of the step,
+ *      varying linearly within it. --------------------------------------------------- */
+#define SV_RAIN_NONE 0
+#define SV_RAIN_UNIFORM 1  /* every cell: q0 = rain_q0, q1 = rain_q1 (m/s)                 */
+#define SV_RAIN_FIELDS 2   /* per-cell SV_FIELD_QBDY0/QBDY1, uploaded by the caller        */
+#define SV_RAIN_PATTERN 3  /* q0 = P * rain_q0, q1 = P * rain_q1 with P = RAIN_PATTERN     */
+#define SV_HEAD_NONE 0
+#define SV_HEAD_EDGES 1    /* one-cell strips along the edges in head_edges               */
+#define SV_HEAD_FIELDS 2   /* per-cell SV_FIELD_HBDY0/HBDY1 (NaN = not selected)          */
+#define SV_EDGE_XMIN 1u
+#define SV_EDGE_XMAX 2u
+#define SV_EDGE_YMIN 4u
+#define SV_EDGE_YMAX 8u
+
+typedef struct {
+  int rain_kind;
+  double rain_q0, rain_q1;
+  int head_kind;
+  unsigned head_edges;
+  double head_h0, head_h1;
+} sv_forcing;
+
+typedef struct {
+  uint64_t accepted;  /* accepted timesteps                                              */
+  uint64_t repeated;  /* rejected (repeated) timesteps                                   */
+  double volume;      /* FP64 sum of h * cell area of U_[0]                              */
+  double rain_in;     /* FP64 volume added by the discharge (rain) term                  */
+  double outflow;     /* FP64 volume removed by the head (outflow) assignment            */
+} sv_stats;
+
+typedef struct sv_ctx sv_ctx;
+
+/* SaintVenantSolver constructor (src/SaintVenant/Solver.cpp:32-71) + RungeKuttaSolver
+ * (src/TemporalScheme/RungeKutta.hpp:319-331): allocates U_[0..N], the k stages and the
+ * bed constants on device `device`. */
+int sv_create(const sv_mesh_desc* mesh, const sv_params* params, int device, sv_ctx** out);
+/* ~SaintVenantSolver */
+void sv_destroy(sv_ctx* ctx);
+/* Field<T,Mesh,C> host->device upload (src/Field/Field.hpp:36-251, DataArray.cpp:21-116);
+ * SV_FIELD_Z recomputes dz/dx, dz/dy (Constants.cpp:39-40). Values are converted to the
+ * ctx precision. */
+int sv_set_field(sv_ctx* ctx, int field_id, const double* host, uint64_t n);
+/* Field device->host read (DataArray::move_to_host, DataArray.cpp:95-116) */
+int sv_get_field(sv_ctx* ctx, int field_id, double* host, uint64_t n);
+/* ManningRoughnessSourceTerm "default shallow/deep n/depth" (ManningRoughnessSourceTerm.cpp:99-102);
+ * uniform values (a later sv_set_field of that id makes it per-cell). */
+int sv_set_manning(sv_ctx* ctx, double n_shallow, double n_deep, double d_shallow, double d_deep);
+/* SaintVenantSolver::start_new_step (Solver.cpp:116-129): boundary values for [t, t + L]. */
+int sv_set_forcing(sv_ctx* ctx, const sv_forcing* forcing);
+/* TypedTemporalScheme::dt_ (TemporalScheme.hpp:78) */
+int sv_set_dt(sv_ctx* ctx, double dt);
+int sv_get_dt(sv_ctx* ctx, double* dt);
+/* SaintVenantSolver::update_dUdt (Solver.cpp:73-114): k = dU/dt of U_[state_no] into
+ * dUdt_[state_no], with slopes and face fluxes kept for inspection (debug/parity path). */
+int sv_eval_dudt(sv_ctx* ctx, int state_no, double t_sub, double dt);
+/* RungeKuttaTemporalScheme::do_timestep (RungeKutta.cpp:141-167): all stages, the control
+ * number and the accept/repeat decision; does not accept. */
+int sv_do_timestep(sv_ctx* ctx, double t_local, double dt, double* cn, int* repeat, double* new_dt);
+/* RungeKuttaSolver::accept_timestep (RungeKutta.hpp:428-431) */
+int sv_accept(sv_ctx* ctx);
+/* TypedTemporalScheme::step (TemporalScheme.hpp:112-149): the whole adaptive-dt loop of one
+ * step of length L, run on the device (dt control included) with no host round trip per
+ * timestep. `out` receives this step's counts and the running tallies. */
+int sv_advance(sv_ctx* ctx, sv_stats* out);
+/* SaintVenantVolumeMeasure::get_volume (src/SaintVenant/Measure.hpp:137-156) plus the
+ * running rain/outflow tallies; FP64. */
+int sv_get_stats(sv_ctx* ctx, sv_stats* out);
+/* device time (ms) of the stage kernels of the last sv_advance, or -1 if not recorded */
+int sv_last_advance_ms(sv_ctx* ctx, double* ms);
+/* message of the last failing call on ctx (or of the last failing sv_create if ctx is NULL) */
+const char* sv_last_error(const sv_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SV_B200_H */

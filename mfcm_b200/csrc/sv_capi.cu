@@ -1,0 +1,637 @@
+// sv_capi.cu -- the C-ABI of include/sv.h: device-memory owner, stage schedule and the
+// graph-captured step loop. Host code only; kernels live in sv_f64.cu / sv_f32.cu.
+//
+// Memory layout in HBM (per solver, SoA, row-major i = y*nx + x, value type T):
+//   S[2][h,u,v]  two state buffers; S[cur] holds U_[0], S[cur^1] is the RK accumulator and
+//                receives U_[N]; accepting a timestep flips `cur` (no copy)
+//   Y[2][h,u,v]  ping-pong stage inputs Y_1..Y_{N-1}
+//   z            bed elevation (its slopes are recomputed in-kernel from the tile)
+//   K[s][h,u,v]  stored stage derivatives, only for non-diagonal tableaux
+//   optional per-cell Manning n / depths, rain q0/q1 or pattern, head targets
+//   ctl, forcing  small device structs (controller state, per-step boundary values)
+//   part         per-CTA FP64 partials of the CFL max/min, volume and tallies
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/sv.h"
+#include "sv_launch.h"
+
+using svk::Ctl;
+using svk::DevForcing;
+
+namespace {
+
+thread_local std::string g_create_err;
+
+struct Tableau {
+  std::vector<std::vector<double>> a;
+  int nsteps() const { return int(a.size()) - 1; }
+  double A(int i, int j) const { return a[i - 1][j]; }
+  double b(int i) const { return a[a.size() - 1][i]; }
+  double c(int i) const { return a[i - 1][0]; }
+};
+
+// runge_kutta_named_coefficient_sets_ (src/TemporalScheme/RungeKutta.cpp:54-115)
+bool named_tableau(int id, Tableau& t) {
+  switch (id) {
+    case 0: t.a = {{0.0}, {0.0, 1.0}}; return true;
+    case 1: t.a = {{0.0}, {0.5, 0.5}, {0.0, 0.0, 1.0}}; return true;
+    case 2: t.a = {{0.0}, {1.0, 1.0}, {0.0, 0.5, 0.5}}; return true;
+    case 3: t.a = {{0.0}, {2.0 / 3.0, 2.0 / 3.0}, {0.0, 0.25, 0.75}}; return true;
+    case 4: t.a = {{0.0}, {0.5, 0.5}, {1.0, -1.0, 2.0}, {0.0, 1.0 / 6.0, 2.0 / 3.0, 1.0 / 6.0}}; return true;
+    case 5: t.a = {{0.0}, {1.0 / 3.0, 1.0 / 3.0}, {2.0 / 3.0, 0.0, 2.0 / 3.0}, {0.0, 0.25, 0.0, 0.75}}; return true;
+    case 6: t.a = {{0.0}, {8.0 / 15.0, 8.0 / 15.0}, {2.0 / 3.0, 0.25, 5.0 / 12.0}, {0.0, 0.25, 0.0, 0.75}}; return true;
+    case 7: t.a = {{0.0}, {0.5, 0.5}, {0.75, 0.0, 0.75}, {0.0, 2.0 / 9.0, 1.0 / 3.0, 4.0 / 9.0}}; return true;
+    case 8: t.a = {{0.0}, {1.0, 1.0}, {0.5, 0.25, 0.25}, {0.0, 1.0 / 6.0, 1.0 / 6.0, 2.0 / 3.0}}; return true;
+    case 9:
+      t.a = {{0.0}, {0.5, 0.5}, {0.5, 0.0, 0.5}, {1.0, 0.0, 0.0, 1.0}, {0.0, (1.0 / 6.0), (1.0 / 3.0), (1.0 / 3.0), (1.0 / 6.0)}};
+      return true;
+    case 10:
+      t.a = {{0.0}, {0.4, 0.4}, {0.45573725, 0.29697761, 0.15875964}, {1.0, 0.21810040, -3.05096516, 3.83286476},
+             {0.0, 0.17476028, -0.55148066, 1.20553560, 0.17118478}};
+      return true;
+    case 11:
+      t.a = {{0.0}, {1.0 / 3.0, 1.0 / 3.0}, {2.0 / 3.0, -1.0 / 3.0, 1.0}, {1.0, 1.0, -1.0, 1.0},
+             {0.0, 1.0 / 8.0, 3.0 / 8.0, 3.0 / 8.0, 1.0 / 8.0}};
+      return true;
+  }
+  return false;
+}
+
+// Y_{s+1} depends on k_s alone (every earlier coefficient is zero): the stages can keep a
+// running accumulator instead of storing the k's.
+bool is_diagonal(const Tableau& t) {
+  int N = t.nsteps();
+  for (int s = 0; s + 1 < N; ++s)
+    for (int j = 0; j < s; ++j)
+      if (t.A(s + 2, j + 1) != 0.0) return false;
+  return true;
+}
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct sv_ctx {
+  virtual ~sv_ctx() {}
+  std::string err;
+  int fail(int code, const std::string& m) {
+    err = m;
+    return code;
+  }
+  int cuda_fail(cudaError_t e, const char* where) {
+    err = std::string(where) + ": " + cudaGetErrorString(e);
+    return SV_E_CUDA;
+  }
+  virtual int set_field(int id, const double* host, uint64_t n) = 0;
+  virtual int get_field(int id, double* host, uint64_t n) = 0;
+  virtual int set_manning(double, double, double, double) = 0;
+  virtual int set_forcing(const sv_forcing*) = 0;
+  virtual int set_dt(double) = 0;
+  virtual int get_dt(double*) = 0;
+  virtual int eval_dudt(int, double, double) = 0;
+  virtual int do_timestep(double, double, double*, int*, double*) = 0;
+  virtual int accept() = 0;
+  virtual int advance(sv_stats*) = 0;
+  virtual int get_stats(sv_stats*) = 0;
+  double last_advance_ms = -1.0;
+};
+
+namespace {
+
+#define SV_CUDA(call)                                  \
+  do {                                                 \
+    cudaError_t e_ = (call);                           \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+  } while (0)
+
+template <typename T>
+struct Solver final : public sv_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  sv_mesh_desc mesh{};
+  sv_params prm{};
+  Tableau tab;
+  bool diag = true;
+  int N = 4;
+  int tile = 0;
+  int tx = 32, ty = 8;
+  long long ncells = 0, nfaces = 0, nblk = 0;
+  T* S[2][3] = {};
+  T* Y[2][3] = {};
+  T* K[4][3] = {};
+  T* z = nullptr;
+  T* man[4] = {};
+  double man_s[4] = {0.03, 0.3, 0.1, 0.3};  // ManningRoughnessSourceTerm.cpp:99-102
+  std::vector<double> host_n_shallow;
+  T *q0 = nullptr, *q1 = nullptr, *pat = nullptr, *hb0 = nullptr, *hb1 = nullptr;
+  // debug buffers (per-function parity path)
+  T* dbg_slp[8] = {};
+  T* dbg_face[5] = {};
+  T *dbg_nh = nullptr, *dbg_sf = nullptr;
+  T* dbg_k[3] = {};
+  Ctl* ctl = nullptr;
+  Ctl* dbg_ctl = nullptr;
+  DevForcing* fc = nullptr;
+  double* part = nullptr;
+  double* scalar = nullptr;
+  int cur = 0;  // host mirror of ctl->cur
+  cudaGraphExec_t graph = nullptr;
+  bool graph_dirty = true;
+  int unroll = 8;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<void*> owned;
+
+  ~Solver() override {
+    cudaSetDevice(device);
+    if (graph) cudaGraphExecDestroy(graph);
+    for (void* p : owned) cudaFree(p);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  template <typename U> cudaError_t alloc(U** p, size_t count) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, count * sizeof(U) > 0 ? count * sizeof(U) : 16);
+    if (e != cudaSuccess) return e;
+    owned.push_back(q);
+    *p = static_cast<U*>(q);
+    return cudaSuccess;
+  }
+  cudaError_t alloc_cells(T** p, bool zero = true) {
+    cudaError_t e = alloc(p, size_t(ncells));
+    if (e == cudaSuccess && zero) e = cudaMemsetAsync(*p, 0, size_t(ncells) * sizeof(T), stream);
+    return e;
+  }
+
+  int init(const sv_mesh_desc* m, const sv_params* p, int dev) {
+    mesh = *m;
+    prm = *p;
+    device = dev;
+    if (!named_tableau(p->rk_method, tab)) return fail(SV_E_ARG, "unknown Runge Kutta scheme index");
+    N = tab.nsteps();
+    diag = is_diagonal(tab);
+    if (m->nx == 0 || m->ny == 0) return fail(SV_E_ARG, "empty mesh");
+    if (m->nx > 0x7fffffffull || m->ny > 0x7fffffffull) return fail(SV_E_LIMIT, "mesh side above 2^31-1");
+    if (!(std::fabs(m->dx) > 1e-6) || !(std::fabs(m->dy) > 1e-6)) return fail(SV_E_ARG, "cell size must exceed 1e-6");
+    if (!(p->step_duration > 0.0)) return fail(SV_E_ARG, "step duration must be positive");
+    mesh.dx = std::fabs(m->dx);
+    mesh.dy = std::fabs(m->dy);
+    ncells = (long long)m->nx * (long long)m->ny;
+    nfaces = (long long)(m->nx + 1) * (long long)m->ny + (long long)(m->ny + 1) * (long long)m->nx;
+    tx = svk::kTiles[tile].tx;
+    ty = svk::kTiles[tile].ty;
+    nblk = (long long)((m->nx + tx - 1) / tx) * (long long)((m->ny + ty - 1) / ty);
+    SV_CUDA(cudaSetDevice(dev));
+    SV_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    SV_CUDA(cudaEventCreate(&ev0));
+    SV_CUDA(cudaEventCreate(&ev1));
+    for (int b = 0; b < 2; ++b)
+      for (int f = 0; f < 3; ++f) {
+        SV_CUDA(alloc_cells(&S[b][f]));
+        SV_CUDA(alloc_cells(&Y[b][f], false));
+      }
+    if (!diag)
+      for (int s = 0; s < N - 1; ++s)
+        for (int f = 0; f < 3; ++f) SV_CUDA(alloc_cells(&K[s][f], false));
+    SV_CUDA(alloc_cells(&z));
+    SV_CUDA(alloc(&ctl, 1));
+    SV_CUDA(alloc(&dbg_ctl, 1));
+    SV_CUDA(alloc(&fc, 1));
+    SV_CUDA(alloc(&part, size_t(svk::part_count(nblk, N))));
+    SV_CUDA(alloc(&scalar, 4));
+    Ctl c{};
+    c.dt = p->initial_dt;
+    SV_CUDA(cudaMemcpyAsync(ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, stream));
+    SV_CUDA(cudaMemcpyAsync(dbg_ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, stream));
+    DevForcing f{};
+    SV_CUDA(cudaMemcpyAsync(fc, &f, sizeof(DevForcing), cudaMemcpyHostToDevice, stream));
+    SV_CUDA(cudaStreamSynchronize(stream));
+    return SV_OK;
+  }
+
+  T** field_slot(int id, bool& lazy) {
+    lazy = false;
+    switch (id) {
+      case SV_FIELD_Z: return &z;
+      case SV_FIELD_H: return &S[cur][0];
+      case SV_FIELD_U: return &S[cur][1];
+      case SV_FIELD_V: return &S[cur][2];
+      case SV_FIELD_N_SHALLOW: lazy = true; return &man[0];
+      case SV_FIELD_N_DEEP: lazy = true; return &man[1];
+      case SV_FIELD_D_SHALLOW: lazy = true; return &man[2];
+      case SV_FIELD_D_DEEP: lazy = true; return &man[3];
+      case SV_FIELD_QBDY0: lazy = true; return &q0;
+      case SV_FIELD_QBDY1: lazy = true; return &q1;
+      case SV_FIELD_HBDY0: lazy = true; return &hb0;
+      case SV_FIELD_HBDY1: lazy = true; return &hb1;
+      case SV_FIELD_RAIN_PATTERN: lazy = true; return &pat;
+    }
+    return nullptr;
+  }
+
+  int upload(T* dst, const double* host, uint64_t n) {
+    std::vector<T> tmp(n);
+    for (uint64_t i = 0; i < n; ++i) tmp[i] = T(host[i]);
+    SV_CUDA(cudaMemcpyAsync(dst, tmp.data(), n * sizeof(T), cudaMemcpyHostToDevice, stream));
+    SV_CUDA(cudaStreamSynchronize(stream));
+    return SV_OK;
+  }
+  int download(const T* src, double* host, uint64_t n) {
+    std::vector<T> tmp(n);
+    SV_CUDA(cudaMemcpyAsync(tmp.data(), src, n * sizeof(T), cudaMemcpyDeviceToHost, stream));
+    SV_CUDA(cudaStreamSynchronize(stream));
+    for (uint64_t i = 0; i < n; ++i) host[i] = double(tmp[i]);
+    return SV_OK;
+  }
+
+  int set_field(int id, const double* host, uint64_t n) override {
+    if (!host) return fail(SV_E_ARG, "null host pointer");
+    if ((long long)n != ncells) return fail(SV_E_ARG, "field size mismatch");
+    bool lazy;
+    T** slot = field_slot(id, lazy);
+    if (!slot) return fail(SV_E_ARG, "field id not settable");
+    if (id == SV_FIELD_N_DEEP && man[0] && host_n_shallow.size() == n &&
+        std::memcmp(host_n_shallow.data(), host, n * sizeof(double)) == 0) {
+      man[1] = man[0];  // n_deep identical to n_shallow: read one array
+      graph_dirty = true;
+      return SV_OK;
+    }
+    if (lazy && (*slot == nullptr || (id == SV_FIELD_N_DEEP && man[1] == man[0]))) {
+      SV_CUDA(alloc_cells(slot, false));
+      graph_dirty = true;
+    }
+    if (id == SV_FIELD_N_SHALLOW) {
+      host_n_shallow.assign(host, host + n);
+      if (man[1] == man[0] && man[1] != nullptr) { man[1] = nullptr; graph_dirty = true; }
+    }
+    return upload(*slot, host, n);
+  }
+
+  int debug_ptr(int id, T*& p, long long& count) {
+    count = ncells;
+    p = nullptr;
+    if (id >= SV_FIELD_DHDX && id <= SV_FIELD_DZDY) {
+      static const int map[8] = {0, 1, 2, 4, 5, 6, 3, 7};  // DHDX,DUDX,DVDX,DHDY,DUDY,DVDY,DZDX,DZDY
+      p = dbg_slp[map[id - SV_FIELD_DHDX]];
+    } else if (id >= SV_FIELD_FLUX_H && id <= SV_FIELD_FLUX_BRANCH) {
+      p = dbg_face[id - SV_FIELD_FLUX_H];
+      count = nfaces;
+    } else if (id >= SV_FIELD_DHDT && id <= SV_FIELD_DVDT) {
+      p = dbg_k[id - SV_FIELD_DHDT];
+    }
+    return p ? SV_OK : fail(SV_E_STATE, "field not available: run sv_eval_dudt first");
+  }
+
+  int get_field(int id, double* host, uint64_t n) override {
+    if (!host) return fail(SV_E_ARG, "null host pointer");
+    const T* src = nullptr;
+    long long count = ncells;
+    bool lazy;
+    if (id >= SV_FIELD_STATE_BASE && id < SV_FIELD_STATE_BASE + 3 * (N + 1)) {
+      int s = (id - SV_FIELD_STATE_BASE) / 3, f = (id - SV_FIELD_STATE_BASE) % 3;
+      if (s == 0) src = S[cur][f];
+      else if (s == N) src = S[cur ^ 1][f];
+      else return fail(SV_E_ARG, "intermediate stage states are not stored");
+    } else if (id >= SV_FIELD_K_BASE && id < SV_FIELD_K_BASE + 3 * N) {
+      int s = (id - SV_FIELD_K_BASE) / 3, f = (id - SV_FIELD_K_BASE) % 3;
+      if (s == 0 && dbg_k[f]) src = dbg_k[f];
+      else if (!diag && s < N - 1) src = K[s][f];
+      else return fail(SV_E_ARG, "stage derivative not stored");
+    } else if (id >= 20) {
+      T* p;
+      int r = debug_ptr(id, p, count);
+      if (r) return r;
+      src = p;
+    } else {
+      T** slot = field_slot(id, lazy);
+      if (!slot) return fail(SV_E_ARG, "unknown field id");
+      if (!*slot) return fail(SV_E_STATE, "field was never set");
+      src = *slot;
+    }
+    if ((long long)n != count) return fail(SV_E_ARG, "field size mismatch");
+    return download(src, host, n);
+  }
+
+  int set_manning(double a, double b, double c, double d) override {
+    man_s[0] = a; man_s[1] = b; man_s[2] = c; man_s[3] = d;
+    for (int i = 0; i < 4; ++i) man[i] = nullptr;  // uniform values replace per-cell fields
+    host_n_shallow.clear();
+    graph_dirty = true;
+    return SV_OK;
+  }
+
+  int set_forcing(const sv_forcing* f) override {
+    if (!f) return fail(SV_E_ARG, "null forcing");
+    if (f->rain_kind < 0 || f->rain_kind > 3 || f->head_kind < 0 || f->head_kind > 2)
+      return fail(SV_E_ARG, "bad forcing kind");
+    if (f->rain_kind == SV_RAIN_FIELDS && (!q0 || !q1)) {
+      // the discharge fields start cleared (BoundarySourceTerm::clear_values)
+      if (!q0) { SV_CUDA(alloc_cells(&q0)); graph_dirty = true; }
+      if (!q1) { SV_CUDA(alloc_cells(&q1)); graph_dirty = true; }
+    }
+    if (f->rain_kind == SV_RAIN_PATTERN && !pat) return fail(SV_E_STATE, "rain pattern field not set");
+    if (f->head_kind == SV_HEAD_FIELDS && (!hb0 || !hb1)) return fail(SV_E_STATE, "head fields not set");
+    DevForcing d{};
+    d.rain_kind = f->rain_kind;
+    d.head_kind = f->head_kind;
+    d.head_edges = f->head_edges;
+    d.rq0 = f->rain_q0; d.rq1 = f->rain_q1;
+    d.hh0 = f->head_h0; d.hh1 = f->head_h1;
+    SV_CUDA(cudaMemcpyAsync(fc, &d, sizeof(d), cudaMemcpyHostToDevice, stream));
+    SV_CUDA(cudaStreamSynchronize(stream));
+    return SV_OK;
+  }
+
+  int read_ctl(Ctl& c) {
+    SV_CUDA(cudaMemcpyAsync(&c, ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, stream));
+    SV_CUDA(cudaStreamSynchronize(stream));
+    cur = c.cur;
+    return SV_OK;
+  }
+  int write_ctl_time(double t_local, double dt) {
+    Ctl c;
+    int r = read_ctl(c);
+    if (r) return r;
+    c.t_local = t_local;
+    c.dt = dt;
+    c.done = 0;
+    SV_CUDA(cudaMemcpyAsync(ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, stream));
+    SV_CUDA(cudaStreamSynchronize(stream));
+    return SV_OK;
+  }
+  int set_dt(double dt) override {
+    Ctl c;
+    int r = read_ctl(c);
+    if (r) return r;
+    return write_ctl_time(c.t_local, dt);
+  }
+  int get_dt(double* dt) override {
+    Ctl c;
+    int r = read_ctl(c);
+    if (r) return r;
+    *dt = c.dt;
+    return SV_OK;
+  }
+
+  svk::StageParams<T> base_params() const {
+    svk::StageParams<T> P{};
+    P.nx = int(mesh.nx); P.ny = int(mesh.ny);
+    P.dx = mesh.dx; P.dy = mesh.dy; P.L = prm.step_duration;
+    P.cell_area = mesh.dx * mesh.dy;
+    for (int b = 0; b < 2; ++b)
+      for (int f = 0; f < 3; ++f) P.S[b][f] = S[b][f];
+    P.z = z;
+    for (int i = 0; i < 4; ++i) { P.man_p[i] = man[i]; P.man_s[i] = T(man_s[i]); }
+    P.fc = fc;
+    P.q0p = q0; P.q1p = q1; P.pat = pat; P.hb0p = hb0; P.hb1p = hb1;
+    P.manning = prm.manning; P.rain_mode = prm.rain_mode; P.head_first = prm.head_first;
+    P.nstages = N;
+    P.ctl = ctl;
+    P.part = part;
+    P.nblk = nblk;
+    return P;
+  }
+
+  // Launch the N stages of one timestep and the finalize kernel (RungeKutta.cpp:147-167).
+  int enqueue_timestep(bool auto_mode) {
+    svk::StageParams<T> P = base_params();
+    const bool tally = !(prm.flags & SV_FLAG_NO_TALLIES);
+    for (int s = 0; s < N; ++s) {
+      P.stage = s;
+      P.c_s = tab.c(s + 1);
+      int mode = 0;
+      if (s == 0) mode |= svk::M_FIRST;
+      if (s == N - 1) mode |= svk::M_LAST;
+      if (diag) mode |= svk::M_ACC;
+      else if (s < N - 1) mode |= svk::M_STOREK;
+      if (tally) mode |= svk::M_TALLY;
+      P.mode = mode;
+      for (int j = 0; j < 4; ++j) { P.a_next[j] = 0.0; P.b[j] = 0.0; }
+      if (s < N - 1)
+        for (int j = 0; j <= s; ++j) P.a_next[j] = tab.A(s + 2, j + 1);
+      for (int j = 0; j < N; ++j) P.b[j] = tab.b(j + 1);
+      // stage inputs: U_[0] (s = 0), then Y[0], Y[1], Y[0] ...
+      const int in = (s - 1) & 1, out = s & 1;
+      for (int f = 0; f < 3; ++f) {
+        P.Yin[f] = s > 0 ? Y[in][f] : nullptr;
+        P.Yout[f] = s < N - 1 ? Y[out][f] : nullptr;
+        P.Kout[f] = (!diag && s < N - 1) ? K[s][f] : nullptr;
+        for (int j = 0; j < 4; ++j) P.Kin[j][f] = (!diag && j < N - 1) ? K[j][f] : nullptr;
+      }
+      cudaError_t e = svk::launch_stage<T>(P, tile, stream);
+      if (e != cudaSuccess) return cuda_fail(e, "stage kernel");
+    }
+    svk::FinalizeParams F{};
+    F.ctl = ctl;
+    F.part = part;
+    F.nblk = nblk;
+    F.nstages = N;
+    for (int j = 0; j < 4; ++j) F.b[j] = j < N ? tab.b(j + 1) : 0.0;
+    F.cn_target = prm.cn_target;
+    F.max_dt = prm.max_dt;
+    F.L = prm.step_duration;
+    F.auto_mode = auto_mode ? 1 : 0;
+    F.tally = tally ? 1 : 0;
+    F.is_float = sizeof(T) == 4;
+    cudaError_t e = svk::launch_finalize(F, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "finalize kernel");
+    return SV_OK;
+  }
+
+  int eval_dudt(int state_no, double t_sub, double dt) override {
+    if (state_no != 0) return fail(SV_E_ARG, "only U_[0] is stored between calls");
+    if (!dbg_k[0]) {
+      for (int f = 0; f < 3; ++f) SV_CUDA(alloc_cells(&dbg_k[f]));
+      for (int f = 0; f < 8; ++f) SV_CUDA(alloc_cells(&dbg_slp[f]));
+      for (int f = 0; f < 5; ++f) {
+        SV_CUDA(alloc(&dbg_face[f], size_t(nfaces)));
+        SV_CUDA(cudaMemsetAsync(dbg_face[f], 0, size_t(nfaces) * sizeof(T), stream));
+      }
+      SV_CUDA(alloc_cells(&dbg_nh));
+      SV_CUDA(alloc_cells(&dbg_sf));
+    }
+    Ctl c{};
+    c.t_local = t_sub;
+    c.dt = dt;
+    SV_CUDA(cudaMemcpyAsync(dbg_ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, stream));
+    svk::StageParams<T> P = base_params();
+    P.ctl = dbg_ctl;
+    P.c_s = 0.0;
+    for (int f = 0; f < 3; ++f) P.Kout[f] = dbg_k[f];
+    svk::DebugParams<T> D{};
+    D.nx = int(mesh.nx); D.ny = int(mesh.ny); D.dx = mesh.dx; D.dy = mesh.dy;
+    D.h = S[cur][0]; D.u = S[cur][1]; D.v = S[cur][2]; D.z = z;
+    D.dhdx = dbg_slp[0]; D.dudx = dbg_slp[1]; D.dvdx = dbg_slp[2]; D.dzdx = dbg_slp[3];
+    D.dhdy = dbg_slp[4]; D.dudy = dbg_slp[5]; D.dvdy = dbg_slp[6]; D.dzdy = dbg_slp[7];
+    D.fh = dbg_face[0]; D.fu = dbg_face[1]; D.fv = dbg_face[2]; D.fz = dbg_face[3]; D.fb = dbg_face[4];
+    cudaError_t e = svk::launch_debug<T>(P, D, dbg_nh, dbg_sf, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "debug kernels");
+    SV_CUDA(cudaStreamSynchronize(stream));
+    return SV_OK;
+  }
+
+  int do_timestep(double t_local, double dt, double* cn, int* repeat, double* new_dt) override {
+    int r = write_ctl_time(t_local, dt);
+    if (r) return r;
+    r = enqueue_timestep(false);
+    if (r) return r;
+    Ctl c;
+    r = read_ctl(c);
+    if (r) return r;
+    if (cn) *cn = c.cn;
+    if (repeat) *repeat = c.repeat;
+    if (new_dt) *new_dt = c.new_dt;
+    return SV_OK;
+  }
+
+  int accept() override {
+    cudaError_t e = svk::launch_accept(ctl, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "accept kernel");
+    Ctl c;
+    return read_ctl(c);
+  }
+
+  int build_graph() {
+    if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+    cudaGraph_t g;
+    SV_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < unroll; ++i) {
+      int r = enqueue_timestep(true);
+      if (r) {
+        cudaStreamEndCapture(stream, &g);
+        if (g) cudaGraphDestroy(g);
+        return r;
+      }
+    }
+    SV_CUDA(cudaStreamEndCapture(stream, &g));
+    cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+    graph_dirty = false;
+    return SV_OK;
+  }
+
+  // TypedTemporalScheme::step: timesteps until t_local reaches L, all on the device.
+  int advance(sv_stats* out) override {
+    if (graph_dirty || !graph) {
+      int r = build_graph();
+      if (r) return r;
+    }
+    cudaError_t e = svk::launch_begin_step(ctl, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "begin step");
+    SV_CUDA(cudaEventRecord(ev0, stream));
+    Ctl c;
+    for (long long it = 0;; ++it) {
+      SV_CUDA(cudaGraphLaunch(graph, stream));
+      SV_CUDA(cudaMemcpyAsync(&c, ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, stream));
+      SV_CUDA(cudaStreamSynchronize(stream));
+      if (c.done) break;
+      if (it > 100000000LL / unroll) return fail(SV_E_STATE, "step did not finish");
+    }
+    SV_CUDA(cudaEventRecord(ev1, stream));
+    SV_CUDA(cudaEventSynchronize(ev1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    last_advance_ms = ms;
+    cur = c.cur;
+    if (out) {
+      out->accepted = c.step_accepted;
+      out->repeated = c.step_repeated;
+      out->rain_in = c.rain_in;
+      out->outflow = c.outflow;
+      int r = volume(&out->volume);
+      if (r) return r;
+    }
+    if (c.error) return fail(SV_E_NONFINITE, "time became NaN: the control number was not finite");
+    return SV_OK;
+  }
+
+  int volume(double* v) {
+    cudaError_t e = svk::launch_volume<T>(S[cur][0], int(mesh.nx), int(mesh.ny), mesh.dx * mesh.dy, part, tile, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "volume kernel");
+    e = svk::launch_sum(part, nblk, scalar, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "sum kernel");
+    SV_CUDA(cudaMemcpyAsync(v, scalar, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    SV_CUDA(cudaStreamSynchronize(stream));
+    return SV_OK;
+  }
+
+  int get_stats(sv_stats* out) override {
+    Ctl c;
+    int r = read_ctl(c);
+    if (r) return r;
+    out->accepted = c.accepted;
+    out->repeated = c.repeated;
+    out->rain_in = c.rain_in;
+    out->outflow = c.outflow;
+    return volume(&out->volume);
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+int sv_create(const sv_mesh_desc* mesh, const sv_params* params, int device, sv_ctx** out) {
+  if (!mesh || !params || !out) {
+    g_create_err = "null argument";
+    return SV_E_ARG;
+  }
+  *out = nullptr;
+  sv_ctx* c = nullptr;
+  int r;
+  if (params->precision == SV_F64) {
+    auto* s = new Solver<double>();
+    r = s->init(mesh, params, device);
+    c = s;
+  } else if (params->precision == SV_F32) {
+    auto* s = new Solver<float>();
+    r = s->init(mesh, params, device);
+    c = s;
+  } else {
+    g_create_err = "precision not available";
+    return SV_E_ARG;
+  }
+  if (r != SV_OK) {
+    g_create_err = c->err;
+    delete c;
+    return r;
+  }
+  *out = c;
+  return SV_OK;
+}
+
+void sv_destroy(sv_ctx* ctx) { delete ctx; }
+
+#define SV_CHECK_CTX(ctx) \
+  if (!(ctx)) return SV_E_ARG
+
+int sv_set_field(sv_ctx* ctx, int id, const double* host, uint64_t n) { SV_CHECK_CTX(ctx); return ctx->set_field(id, host, n); }
+int sv_get_field(sv_ctx* ctx, int id, double* host, uint64_t n) { SV_CHECK_CTX(ctx); return ctx->get_field(id, host, n); }
+int sv_set_manning(sv_ctx* ctx, double a, double b, double c, double d) { SV_CHECK_CTX(ctx); return ctx->set_manning(a, b, c, d); }
+int sv_set_forcing(sv_ctx* ctx, const sv_forcing* f) { SV_CHECK_CTX(ctx); return ctx->set_forcing(f); }
+int sv_set_dt(sv_ctx* ctx, double dt) { SV_CHECK_CTX(ctx); return ctx->set_dt(dt); }
+int sv_get_dt(sv_ctx* ctx, double* dt) { SV_CHECK_CTX(ctx); if (!dt) return SV_E_ARG; return ctx->get_dt(dt); }
+int sv_eval_dudt(sv_ctx* ctx, int s, double t, double dt) { SV_CHECK_CTX(ctx); return ctx->eval_dudt(s, t, dt); }
+int sv_do_timestep(sv_ctx* ctx, double t, double dt, double* cn, int* rep, double* nd) {
+  SV_CHECK_CTX(ctx);
+  return ctx->do_timestep(t, dt, cn, rep, nd);
+}
+int sv_accept(sv_ctx* ctx) { SV_CHECK_CTX(ctx); return ctx->accept(); }
+int sv_advance(sv_ctx* ctx, sv_stats* out) { SV_CHECK_CTX(ctx); return ctx->advance(out); }
+int sv_get_stats(sv_ctx* ctx, sv_stats* out) { SV_CHECK_CTX(ctx); if (!out) return SV_E_ARG; return ctx->get_stats(out); }
+int sv_last_advance_ms(sv_ctx* ctx, double* ms) { SV_CHECK_CTX(ctx); if (!ms) return SV_E_ARG; *ms = ctx->last_advance_ms; return SV_OK; }
+const char* sv_last_error(const sv_ctx* ctx) { return ctx ? ctx->err.c_str() : g_create_err.c_str(); }
+
+}  // extern "C"

@@ -1,0 +1,28 @@
+// sv_f64.cu -- FP64 instantiation of the stage kernels. Compiled with -fmad=false: every
+// FP64 multiply and add is rounded separately, as in the reference's CPU arithmetic, which
+// is what makes the FP64 path bit-identical to the oracle. (Explicit fma() calls are kept:
+// they implement the exact constant-divisor division in sv_device.cuh.)
+#define SV_T double
+#define SV_DEFINE_COMMON_KERNELS
+#include "sv_inst.cuh"
+
+namespace svk {
+
+cudaError_t launch_finalize(const FinalizeParams& F, cudaStream_t s) {
+  finalize_kernel<1024><<<1, 1024, 0, s>>>(F);
+  return cudaGetLastError();
+}
+cudaError_t launch_sum(const double* p, long long n, double* out, cudaStream_t s) {
+  sum_kernel<1024><<<1, 1024, 0, s>>>(p, n, out);
+  return cudaGetLastError();
+}
+cudaError_t launch_accept(Ctl* ctl, cudaStream_t s) {
+  accept_kernel<<<1, 1, 0, s>>>(ctl);
+  return cudaGetLastError();
+}
+cudaError_t launch_begin_step(Ctl* ctl, cudaStream_t s) {
+  begin_step_kernel<<<1, 1, 0, s>>>(ctl);
+  return cudaGetLastError();
+}
+
+}  // namespace svk

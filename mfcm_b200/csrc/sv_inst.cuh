@@ -1,0 +1,67 @@
+// sv_inst.cuh -- launcher definitions, included once per value type by sv_f64.cu / sv_f32.cu
+// with SV_T defined to the value type.
+#pragma once
+#include "sv_launch.h"
+
+namespace svk {
+
+template <typename T, int TX, int TY> static cudaError_t launch_stage_t(const StageParams<T>& P, cudaStream_t s) {
+  using SM = StageSmem<T, TX, TY>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(stage_kernel<T, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(sizeof(SM)));
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  dim3 grid((P.nx + TX - 1) / TX, (P.ny + TY - 1) / TY);
+  stage_kernel<T, TX, TY><<<grid, TX * TY, sizeof(SM), s>>>(P);
+  return cudaGetLastError();
+}
+
+template <> size_t stage_smem_bytes<SV_T>(int tile) {
+  switch (tile) {
+    case 0: return sizeof(StageSmem<SV_T, 32, 8>);
+    case 1: return sizeof(StageSmem<SV_T, 32, 4>);
+    case 2: return sizeof(StageSmem<SV_T, 64, 4>);
+    default: return sizeof(StageSmem<SV_T, 32, 16>);
+  }
+}
+
+template <> cudaError_t launch_stage<SV_T>(const StageParams<SV_T>& P, int tile, cudaStream_t s) {
+  switch (tile) {
+    case 0: return launch_stage_t<SV_T, 32, 8>(P, s);
+    case 1: return launch_stage_t<SV_T, 32, 4>(P, s);
+    case 2: return launch_stage_t<SV_T, 64, 4>(P, s);
+    default: return launch_stage_t<SV_T, 32, 16>(P, s);
+  }
+}
+
+template <typename T, int TX, int TY>
+static cudaError_t launch_volume_t(const T* h, int nx, int ny, double area, double* part, cudaStream_t s) {
+  dim3 grid((nx + TX - 1) / TX, (ny + TY - 1) / TY);
+  volume_partials_kernel<T, TX, TY><<<grid, TX * TY, 0, s>>>(h, nx, ny, area, part);
+  return cudaGetLastError();
+}
+
+template <> cudaError_t launch_volume<SV_T>(const SV_T* h, int nx, int ny, double area, double* part, int tile,
+                                            cudaStream_t s) {
+  switch (tile) {
+    case 0: return launch_volume_t<SV_T, 32, 8>(h, nx, ny, area, part, s);
+    case 1: return launch_volume_t<SV_T, 32, 4>(h, nx, ny, area, part, s);
+    case 2: return launch_volume_t<SV_T, 64, 4>(h, nx, ny, area, part, s);
+    default: return launch_volume_t<SV_T, 32, 16>(h, nx, ny, area, part, s);
+  }
+}
+
+template <> cudaError_t launch_debug<SV_T>(const StageParams<SV_T>& P, const DebugParams<SV_T>& D, SV_T* nh,
+                                           SV_T* sf, cudaStream_t s) {
+  long long n = (long long)D.nx * D.ny;
+  long long nf = (long long)(D.nx + 1) * D.ny + (long long)(D.ny + 1) * D.nx;
+  debug_slopes_kernel<SV_T><<<unsigned((n + 255) / 256), 256, 0, s>>>(D);
+  debug_flux_kernel<SV_T><<<unsigned((nf + 255) / 256), 256, 0, s>>>(D);
+  debug_cell_kernel<SV_T><<<unsigned((n + 255) / 256), 256, 0, s>>>(P, D, nh, sf);
+  return cudaGetLastError();
+}
+
+}  // namespace svk

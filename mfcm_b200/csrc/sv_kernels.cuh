@@ -1,0 +1,654 @@
+// sv_kernels.cuh -- kernels of the Saint-Venant RK time step on sm_100a.
+//
+//  stage_kernel   one launch per RK stage. A CTA owns a TX x TY tile of cells, stages the
+//                 tile plus a 2-cell halo of (h, u, v, z) in shared memory, computes the
+//                 Minmod3 slopes of every cell of the tile plus a 1-cell ring, the fluxes of
+//                 every face of the tile, then per cell dU/dt (flux divergence, depth-slope,
+//                 limited bed slope, zflux), Manning friction, rainfall and outflow, and the
+//                 Runge-Kutta combination. Faces and slopes never leave the SM. The last
+//                 stage also reduces the CFL quantity and the FP64 volume per CTA.
+//  finalize_kernel  one CTA: fixed-order reduction of the per-CTA partials, the control
+//                 number, and the dt controller (accept / repeat / new dt / end-of-step
+//                 trimming) in FP64, so a whole step runs without a host round trip.
+//  debug kernels  the same per-face / per-cell functions over global arrays, one reference
+//                 kernel each, for per-function parity tests.
+#pragma once
+#include "sv_device.cuh"
+
+namespace svk {
+using namespace svd;
+
+// Device-resident controller state of one solver (FP64 times, TT = double).
+struct Ctl {
+  double t_local;   // time since the start of the step
+  double dt;        // current timestep
+  double cn;        // control number of the last timestep
+  double new_dt;    // dt suggested by the last timestep
+  int cur;          // parity of the state buffer that holds U_[0]
+  int done;         // 1: the step is complete (auto mode) -- all stage kernels exit
+  int repeat;       // last timestep rejected
+  int error;        // sticky error code (SV_E_NONFINITE ...)
+  unsigned long long accepted, repeated;            // running totals
+  unsigned long long step_accepted, step_repeated;  // in the current step
+  double rain_in, outflow;      // running tallies over accepted timesteps
+  double volume;                // volume of U_[0] after the last accepted timestep
+  double pend_rain, pend_out, pend_vol;  // tallies of the last timestep, applied on accept
+};
+
+// Per-step boundary values, kept in device memory so captured graphs stay valid when
+// start_new_step changes them (DischargeBoundarySourceTerm.hpp:114-146,
+// HeadBoundarySourceTerm.hpp:114-146).
+struct DevForcing {
+  int rain_kind;        // SV_RAIN_*
+  int head_kind;        // SV_HEAD_*
+  unsigned head_edges;  // SV_EDGE_* bits
+  int pad;
+  double rq0, rq1;      // uniform / pattern-scaled rain values at the start / end of the step
+  double hh0, hh1;      // head targets at the start / end of the step
+};
+
+enum StageMode : int {
+  M_FIRST = 1,    // stage 0: input is U_[0]
+  M_LAST = 2,     // last stage: writes U_[N] and the CFL / volume partials
+  M_ACC = 4,      // diagonal tableau: running accumulator instead of stored k's
+  M_STOREK = 8,   // store k_s for later stages (non-diagonal tableaux)
+  M_TALLY = 16,   // rain / outflow partials
+  M_DEBUGK = 32,  // debug: write k_s only (no RK combination)
+};
+
+template <typename T> struct StageParams {
+  int nx, ny;
+  double dx, dy, L;
+  double cell_area;
+  T* S[2][3];            // state parity buffers: S[cur] = U_[0], S[cur^1] = acc / U_[N]
+  const T* Yin[3];       // stage input (ignored on the first stage)
+  T* Yout[3];            // Y_{s+1} (not on the last stage)
+  T* Kout[3];            // k_s (M_STOREK / M_DEBUGK)
+  const T* Kin[4][3];    // stored k_j, j < s (M_STOREK)
+  const T* z;
+  const T* man_p[4];     // per-cell n_shallow, n_deep, d_shallow, d_deep, or nullptr
+  T man_s[4];            // uniform values where man_p is nullptr
+  const DevForcing* fc;  // per-step boundary values
+  const T* q0p; const T* q1p; const T* pat;
+  const T* hb0p; const T* hb1p;
+  int manning, rain_mode, head_first;
+  int stage, nstages, mode;
+  double c_s;            // c of this stage: t_sub = t_local + c_s * dt
+  double a_next[4];      // a(s+2, j+1), j = 0..s: coefficients of Y_{s+1}
+  double b[4];           // b_1..b_N
+  Ctl* ctl;
+  double* part;          // per-CTA partials (see part_* offsets)
+  long long nblk;
+};
+
+// partial layout: [0, nblk) cn max, [nblk, 2nblk) cn min, [2nblk, 3nblk) volume,
+// then rain[s] at (3 + 2s) nblk, outflow[s] at (4 + 2s) nblk.
+__host__ __device__ inline long long part_count(long long nblk, int nstages) { return (3 + 2LL * nstages) * nblk; }
+
+template <typename T> __device__ __forceinline__ T ld(const T* p, long long i) { return __ldg(p + i); }
+
+// NaN-propagating max/min for the CFL reduction
+__device__ __forceinline__ double nmax(double a, double b) { return (a != a || b != b) ? (a + b) : (a > b ? a : b); }
+__device__ __forceinline__ double nmin(double a, double b) { return (a != a || b != b) ? (a + b) : (a < b ? a : b); }
+
+template <int NT> __device__ double block_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < NT / 32; ++i) r += red[i];
+  }
+  return r;
+}
+template <int NT> __device__ double block_max(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v = nmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  double r = v;
+  if (threadIdx.x == 0) {
+    r = red[0];
+    for (int i = 1; i < NT / 32; ++i) r = nmax(r, red[i]);
+  }
+  return r;
+}
+template <int NT> __device__ double block_min(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v = nmin(v, __shfl_down_sync(0xffffffffu, v, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  double r = v;
+  if (threadIdx.x == 0) {
+    r = red[0];
+    for (int i = 1; i < NT / 32; ++i) r = nmin(r, red[i]);
+  }
+  return r;
+}
+
+template <typename T> __device__ __forceinline__ Div<T> mkdiv(double d);
+template <> __device__ __forceinline__ Div<double> mkdiv<double>(double d) { return make_div(d); }
+template <> __device__ __forceinline__ Div<float> mkdiv<float>(double d) { return make_divf(float(d)); }
+
+// Per-cell dU/dt of one stage (TemporalDerivativeKernel.cpp:53-98, then the source terms
+// and boundaries in configuration order, Solver.cpp:97-113). fw/fe/fs/fn are the four face
+// fluxes; returns the rain rate added and the depth rate removed by the head assignment.
+template <typename T>
+__device__ __forceinline__ void cell_dudt(const StageParams<T>& P, const DevForcing& fc, const CellCtx<T>& c,
+                                          long long g, int gx,
+                                          int gy, T h, T u, T v, T dhdx, T dhdy, T dzdx, T dzdy,
+                                          const FaceF<T>& fw, const FaceF<T>& fe, const FaceF<T>& fs,
+                                          const FaceF<T>& fn, T& kh, T& ku, T& kv, double& rain,
+                                          double& removed, T* n_out, T* sf_out) {
+  T dhdt = c.divx(fw.h - fe.h) + c.divy(fs.h - fn.h);
+  T dudt = c.divx(fw.u - fe.u) + c.divy(fs.u - fn.u);
+  T dvdt = c.divx(fw.v - fe.v) + c.divy(fs.v - fn.v);
+  dudt = dudt + dhdx * T(-kG);
+  dvdt = dvdt + dhdy * T(-kG);
+  T hdx = c.divx(h), hdy = c.divy(h);
+  if (sfabs(dzdx) > hdx) dzdx = (dzdx > T(0)) ? hdx : ((dzdx < T(0)) ? -hdx : c.divx(ssign(dzdx) * h));
+  if (sfabs(dzdy) > hdy) dzdy = (dzdy > T(0)) ? hdy : ((dzdy < T(0)) ? -hdy : c.divy(ssign(dzdy) * h));
+  T dudt_bed = T(-kG) * dzdx;
+  T dvdt_bed = T(-kG) * dzdy;
+  dudt = dudt + c.divx(fw.z - fe.z);
+  dvdt = dvdt + c.divy(fs.z - fn.z);
+  dudt = dudt + dudt_bed;
+  dvdt = dvdt + dvdt_bed;
+  if (P.manning) {
+    T ns = P.man_p[0] ? ld(P.man_p[0], g) : P.man_s[0];
+    T nd = P.man_p[1] ? (P.man_p[1] == P.man_p[0] ? ns : ld(P.man_p[1], g)) : P.man_s[1];
+    T ds = P.man_p[2] ? ld(P.man_p[2], g) : P.man_s[2];
+    T dd = P.man_p[3] ? ld(P.man_p[3], g) : P.man_s[3];
+    manning_apply<T>(h, u, v, ns, nd, ds, dd, c, dudt, dvdt, n_out, sf_out);
+  }
+  rain = 0.0;
+  removed = 0.0;
+  // head boundary target values for this cell (NaN = not selected)
+  bool head_sel = false;
+  T h0 = T(0), h1 = T(0);
+  if (fc.head_kind == 1) {
+    head_sel = ((fc.head_edges & 1u) && gx == 0) || ((fc.head_edges & 2u) && gx == P.nx - 1) ||
+               ((fc.head_edges & 4u) && gy == 0) || ((fc.head_edges & 8u) && gy == P.ny - 1);
+    h0 = T(fc.hh0); h1 = T(fc.hh1);
+  } else if (fc.head_kind == 2) {
+    h0 = ld(P.hb0p, g); h1 = ld(P.hb1p, g);
+    head_sel = true;
+  }
+  if (head_sel && !(h0 == h0 && h1 == h1)) head_sel = false;  // NaN = not selected
+  auto do_rain = [&]() {
+    if (fc.rain_kind == 0) return;
+    T q0, q1;
+    if (fc.rain_kind == 1) { q0 = T(fc.rq0); q1 = T(fc.rq1); }
+    else if (fc.rain_kind == 2) { q0 = ld(P.q0p, g); q1 = ld(P.q1p, g); }
+    else { T pp = ld(P.pat, g); q0 = pp * T(fc.rq0); q1 = pp * T(fc.rq1); }
+    bool applied;
+    T dh = discharge_rate<T>(q0, q1, h, c, applied);
+    if (applied) { dhdt = dhdt + dh; rain = double(dh); }
+  };
+  auto do_head = [&]() {
+    if (!head_sel) return;
+    T target = head_target<T>(h0, h1, c);
+    T before = dhdt;
+    dhdt = c.divdt(target - h);
+    removed = double(before) - double(dhdt);
+  };
+  if (P.head_first) { do_head(); do_rain(); }
+  else { do_rain(); do_head(); }
+  kh = dhdt; ku = dudt; kv = dvdt;
+}
+
+template <typename T, int TX, int TY>
+struct StageSmem {
+  static constexpr int RX = TX + 4, RY = TY + 4;  // values with a 2-cell halo
+  static constexpr int SX = TX + 2, SY = TY + 2;  // slopes with a 1-cell ring
+  T val[4][RY][RX];
+  T slp[8][SY][SX];
+  T fxf[4][TY][TX + 1];
+  T fyf[4][TY + 1][TX];
+  double red[TX * TY / 32];
+};
+
+template <typename T, int TX, int TY>
+__global__ void __launch_bounds__(TX * TY) stage_kernel(const StageParams<T> P) {
+  using SM = StageSmem<T, TX, TY>;
+  constexpr int NT = TX * TY;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SM& s = *reinterpret_cast<SM*>(smem_raw);
+
+  const Ctl* ctl = P.ctl;
+  if (ctl->done) return;
+  const int cur = ctl->cur;
+  const double dt_d = ctl->dt;
+  const double tsub = ctl->t_local + P.c_s * dt_d;
+
+  const int tid = threadIdx.x;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const int nx = P.nx, ny = P.ny;
+  const bool first = P.mode & M_FIRST;
+  const T* Yh = first ? P.S[cur][0] : P.Yin[0];
+  const T* Yu = first ? P.S[cur][1] : P.Yin[1];
+  const T* Yv = first ? P.S[cur][2] : P.Yin[2];
+
+  // phase 1: tile + 2-cell halo of h, u, v, z (clamped at the mesh edge; the clamped
+  // copies are never used because edge faces and edge slopes use the cell itself)
+  for (int i = tid; i < SM::RX * SM::RY; i += NT) {
+    int lx = i % SM::RX, ly = i / SM::RX;
+    int gx = min(max(x0 - 2 + lx, 0), nx - 1);
+    int gy = min(max(y0 - 2 + ly, 0), ny - 1);
+    long long g = (long long)gy * nx + gx;
+    s.val[0][ly][lx] = ld(Yh, g);
+    s.val[1][ly][lx] = ld(Yu, g);
+    s.val[2][ly][lx] = ld(Yv, g);
+    s.val[3][ly][lx] = ld(P.z, g);
+  }
+  __syncthreads();
+
+  const Div<T> divx = mkdiv<T>(P.dx), divy = mkdiv<T>(P.dy);
+  // phase 2: Minmod3 slopes (State.cpp:176-193, Constants.cpp:39-40) on the tile + ring
+  for (int i = tid; i < SM::SX * SM::SY; i += NT) {
+    int sx = i % SM::SX, sy = i / SM::SX;
+    if ((sx == 0 || sx == SM::SX - 1) && (sy == 0 || sy == SM::SY - 1)) continue;  // unused corners
+    int gx = x0 - 1 + sx, gy = y0 - 1 + sy;
+    if (gx < 0 || gx >= nx || gy < 0 || gy >= ny) continue;
+    int lx = sx + 1, ly = sy + 1;
+    bool hasW = gx > 0, hasE = gx < nx - 1, hasN = gy < ny - 1, hasS = gy > 0;
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+      s.slp[f][sy][sx] = minmod3<T>(s.val[f][ly][lx - 1], hasW, s.val[f][ly][lx], hasE, s.val[f][ly][lx + 1], divx);
+      // Y axis: north (row + 1) is the left neighbour, south the right
+      s.slp[4 + f][sy][sx] = minmod3<T>(s.val[f][ly + 1][lx], hasN, s.val[f][ly][lx], hasS, s.val[f][ly - 1][lx], divy);
+    }
+  }
+  __syncthreads();
+
+  auto cellv = [&](int gx, int gy) {
+    int sx = gx - (x0 - 1), sy = gy - (y0 - 1);
+    int lx = sx + 1, ly = sy + 1;
+    CellV<T> c;
+    c.h = s.val[0][ly][lx]; c.u = s.val[1][ly][lx]; c.v = s.val[2][ly][lx]; c.z = s.val[3][ly][lx];
+    c.dhdx = s.slp[0][sy][sx]; c.dudx = s.slp[1][sy][sx]; c.dvdx = s.slp[2][sy][sx]; c.dzdx = s.slp[3][sy][sx];
+    c.dhdy = s.slp[4][sy][sx]; c.dudy = s.slp[5][sy][sx]; c.dvdy = s.slp[6][sy][sx]; c.dzdy = s.slp[7][sy][sx];
+    return c;
+  };
+  // phase 3: face fluxes (Fluxes.cpp:44-65)
+  const T hdx = T(0.5) * T(P.dx), hdy = T(0.5) * T(P.dy);
+  for (int i = tid; i < (TX + 1) * TY; i += NT) {
+    int fx = i % (TX + 1), fy = i / (TX + 1);
+    int gfx = x0 + fx, gy = y0 + fy;
+    if (gy >= ny || gfx > nx) continue;
+    int edge = gfx == 0 ? -1 : (gfx == nx ? 1 : 0);
+    int gl = edge == -1 ? 0 : gfx - 1;
+    int gr = edge == 1 ? nx - 1 : gfx;
+    FaceF<T> F;
+    face_flux<T, 0>(cellv(gl, gy), cellv(gr, gy), edge, hdx, divx, F);
+    s.fxf[0][fy][fx] = F.h; s.fxf[1][fy][fx] = F.u; s.fxf[2][fy][fx] = F.v; s.fxf[3][fy][fx] = F.z;
+  }
+  for (int i = tid; i < TX * (TY + 1); i += NT) {
+    int fx = i % TX, fy = i / TX;
+    int gx = x0 + fx, gfy = y0 + fy;
+    if (gx >= nx || gfy > ny) continue;
+    int edge = gfy == 0 ? -1 : (gfy == ny ? 1 : 0);
+    int gl = edge == -1 ? 0 : gfy - 1;
+    int gr = edge == 1 ? ny - 1 : gfy;
+    FaceF<T> F;
+    face_flux<T, 1>(cellv(gx, gl), cellv(gx, gr), edge, hdy, divy, F);
+    s.fyf[0][fy][fx] = F.h; s.fyf[1][fy][fx] = F.u; s.fyf[2][fy][fx] = F.v; s.fyf[3][fy][fx] = F.z;
+  }
+  __syncthreads();
+
+  // phase 4: per cell
+  const int tx = tid % TX, ty = tid / TX;
+  const int gx = x0 + tx, gy = y0 + ty;
+  const bool valid = gx < nx && gy < ny;
+  double rain = 0.0, removed = 0.0, xcfl = 0.0, xcfl_min = 0.0, vol = 0.0;
+  const bool last = P.mode & M_LAST;
+  if (!valid) xcfl_min = 1.0 / 0.0;
+  if (valid) {
+    const long long g = (long long)gy * nx + gx;
+    CellCtx<T> c;
+    c.divx = divx; c.divy = divy;
+    c.divdt = mkdiv<T>(dt_d);
+    c.divL = mkdiv<T>(P.L);
+    c.dt = T(dt_d); c.dt_d = dt_d; c.tsub_d = tsub;
+    c.manning = P.manning; c.rain_mode = P.rain_mode; c.head_first = P.head_first;
+    const int sx = tx + 1, sy = ty + 1, lx = tx + 2, ly = ty + 2;
+    const T h = s.val[0][ly][lx], u = s.val[1][ly][lx], v = s.val[2][ly][lx];
+    FaceF<T> fw{s.fxf[0][ty][tx], s.fxf[1][ty][tx], s.fxf[2][ty][tx], s.fxf[3][ty][tx]};
+    FaceF<T> fe{s.fxf[0][ty][tx + 1], s.fxf[1][ty][tx + 1], s.fxf[2][ty][tx + 1], s.fxf[3][ty][tx + 1]};
+    FaceF<T> fs{s.fyf[0][ty][tx], s.fyf[1][ty][tx], s.fyf[2][ty][tx], s.fyf[3][ty][tx]};
+    FaceF<T> fn{s.fyf[0][ty + 1][tx], s.fyf[1][ty + 1][tx], s.fyf[2][ty + 1][tx], s.fyf[3][ty + 1][tx]};
+    const DevForcing fc = *P.fc;
+    T kh, ku, kv;
+    cell_dudt<T>(P, fc, c, g, gx, gy, h, u, v, s.slp[0][sy][sx], s.slp[4][sy][sx], s.slp[3][sy][sx],
+                 s.slp[7][sy][sx], fw, fe, fs, fn, kh, ku, kv, rain, removed, nullptr, nullptr);
+
+    if (P.mode & (M_STOREK | M_DEBUGK)) {
+      P.Kout[0][g] = kh; P.Kout[1][g] = ku; P.Kout[2][g] = kv;
+    }
+    if (!(P.mode & M_DEBUGK)) {
+      const int st = P.stage;
+      T* A[3] = {P.S[cur ^ 1][0], P.S[cur ^ 1][1], P.S[cur ^ 1][2]};
+      const T* U0[3] = {P.S[cur][0], P.S[cur][1], P.S[cur][2]};
+      T k[3] = {kh, ku, kv};
+      T out[3];
+      if (P.mode & M_ACC) {
+        // diagonal tableau: Y_{s+1} = U0 + k_s*a and acc += k_s*b, in the reference's
+        // left-to-right order (RungeKutta.hpp:377-388); the skipped zero-coefficient terms
+        // k_j*0 (j < s) can only contribute a NaN, which happens exactly when some earlier
+        // k_j is not finite, i.e. when acc is not finite while U0 is.
+        const T cB = T(P.b[st] * dt_d);
+        T u0v[3], accv[3];
+#pragma unroll
+        for (int f = 0; f < 3; ++f) {
+          u0v[f] = first ? (f == 0 ? h : (f == 1 ? u : v)) : ld(U0[f], g);
+          accv[f] = first ? u0v[f] : ld(A[f], g);
+        }
+        if (!last) {
+          const T cA = T(P.a_next[st] * dt_d);
+#pragma unroll
+          for (int f = 0; f < 3; ++f) {
+            T y = u0v[f] + k[f] * cA;
+            if (!first && finite_(u0v[f]) && !finite_(accv[f])) y = Lim<T>::nan();
+            P.Yout[f][g] = y;
+          }
+        }
+#pragma unroll
+        for (int f = 0; f < 3; ++f) {
+          out[f] = accv[f] + k[f] * cB;
+          A[f][g] = out[f];
+        }
+      } else {
+        // general tableau: Y_{s+1} = ((U0 + k_0 c_0) + k_1 c_1) + ... with stored k_j
+        T u0v[3];
+#pragma unroll
+        for (int f = 0; f < 3; ++f) u0v[f] = first ? (f == 0 ? h : (f == 1 ? u : v)) : ld(U0[f], g);
+        const double* coef = last ? P.b : P.a_next;
+#pragma unroll
+        for (int f = 0; f < 3; ++f) {
+          T y = u0v[f];
+          for (int j = 0; j < st; ++j) y = y + ld(P.Kin[j][f], g) * T(coef[j] * dt_d);
+          y = y + k[f] * T(coef[st] * dt_d);
+          out[f] = y;
+          if (last) A[f][g] = y;
+          else P.Yout[f][g] = y;
+        }
+      }
+      if (last) {
+        // SaintVenantState::max_control_number (State.cpp:204-228) on U_[N]: per cell
+        // x = (|u|+c)/dx + (|v|+c)/dy; cn = max(dt*x) = dt*max(x) (rounding is monotone)
+        T hh = sfmax(out[0], T(0));
+        T cc = ssqrt(T(kG) * hh);
+        T xx = divx(sfabs(out[1]) + cc) + divy(sfabs(out[2]) + cc);
+        xcfl = double(xx);
+        xcfl_min = xcfl;
+        vol = double(out[0]) * P.cell_area;
+      }
+    }
+  }
+  if (last && !(P.mode & M_DEBUGK)) {
+    double mx = block_max<NT>(xcfl, s.red);
+    double mn = block_min<NT>(xcfl_min, s.red);
+    double vs = block_sum<NT>(vol, s.red);
+    if (tid == 0) {
+      long long b = (long long)blockIdx.y * gridDim.x + blockIdx.x;
+      P.part[b] = mx;
+      P.part[P.nblk + b] = mn;
+      P.part[2 * P.nblk + b] = vs;
+    }
+  }
+  if (P.mode & M_TALLY) {
+    double rs = block_sum<NT>(rain, s.red);
+    double os = block_sum<NT>(removed, s.red);
+    if (tid == 0) {
+      long long b = (long long)blockIdx.y * gridDim.x + blockIdx.x;
+      P.part[(3 + 2LL * P.stage) * P.nblk + b] = rs;
+      P.part[(4 + 2LL * P.stage) * P.nblk + b] = os;
+    }
+  }
+}
+
+struct FinalizeParams {
+  Ctl* ctl;
+  const double* part;
+  long long nblk;
+  int nstages;
+  double b[4];
+  double cn_target, max_dt, L;
+  int auto_mode;   // 1: accept/repeat, advance t_local, trim dt (TemporalScheme.hpp:119-146)
+  int tally;
+  int is_float;    // control number rounded to T = float
+};
+
+// Fixed-order sum: thread t adds blocks t, t+NT, ... in order, then a fixed tree.
+template <int NT> __device__ double fixed_sum(const double* p, long long n, double* red) {
+  double a = 0.0;
+  for (long long i = threadIdx.x; i < n; i += NT) a += p[i];
+  red[threadIdx.x] = a;
+  __syncthreads();
+  for (int st = NT / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+    __syncthreads();
+  }
+  double r = red[0];
+  __syncthreads();
+  return r;
+}
+
+template <int NT> __global__ void __launch_bounds__(NT) finalize_kernel(const FinalizeParams F) {
+  __shared__ double red[NT];
+  Ctl* ctl = F.ctl;
+  if (ctl->done) return;
+  // CFL max / min (NaN-propagating), order-independent
+  double mx = 0.0, mn = 1.0 / 0.0;
+  for (long long i = threadIdx.x; i < F.nblk; i += NT) {
+    mx = nmax(mx, F.part[i]);
+    mn = nmin(mn, F.part[F.nblk + i]);
+  }
+  red[threadIdx.x] = mx;
+  __syncthreads();
+  for (int st = NT / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st) red[threadIdx.x] = nmax(red[threadIdx.x], red[threadIdx.x + st]);
+    __syncthreads();
+  }
+  mx = red[0];
+  __syncthreads();
+  red[threadIdx.x] = mn;
+  __syncthreads();
+  for (int st = NT / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st) red[threadIdx.x] = nmin(red[threadIdx.x], red[threadIdx.x + st]);
+    __syncthreads();
+  }
+  mn = red[0];
+  __syncthreads();
+  double vol = fixed_sum<NT>(F.part + 2 * F.nblk, F.nblk, red);
+  double rain = 0.0, outf = 0.0;
+  if (F.tally) {
+    for (int s = 0; s < F.nstages; ++s) {
+      double rs = fixed_sum<NT>(F.part + (3 + 2LL * s) * F.nblk, F.nblk, red);
+      double os = fixed_sum<NT>(F.part + (4 + 2LL * s) * F.nblk, F.nblk, red);
+      double w = F.is_float ? double(float(F.b[s] * ctl->dt)) : F.b[s] * ctl->dt;
+      rain += w * rs;
+      outf += w * os;
+    }
+  }
+  if (threadIdx.x != 0) return;
+  const double dt = ctl->dt;
+  // control number: max over cells of dt * x
+  double cn;
+  if (mx != mx || dt != dt) cn = mx + dt;                  // NaN
+  else if (dt == 1.0 / 0.0) cn = (mn == 0.0) ? (0.0 / 0.0) : dt;
+  else cn = dt * mx;
+  if (F.is_float) cn = double(float(cn));
+  // RungeKuttaTemporalScheme::do_timestep (RungeKutta.cpp:154-167), target as parameter
+  const double tgt = F.cn_target;
+  double nd;
+  int rep;
+  if (cn > tgt) {
+    rep = 1;
+    nd = (cn > 5.0 * tgt) ? dt / 5.0 : (dt * tgt) / (cn * 1.1);
+  } else if (cn > 0.9 * tgt) {
+    rep = 0; nd = dt;
+  } else {
+    rep = 0; nd = (dt * tgt) / cn;
+  }
+  if (F.max_dt > 0.0 && nd > F.max_dt) nd = F.max_dt;
+  ctl->cn = cn;
+  ctl->new_dt = nd;
+  ctl->repeat = rep;
+  ctl->pend_rain = rain;
+  ctl->pend_out = outf;
+  ctl->pend_vol = vol;
+  if (!F.auto_mode) return;
+  // TypedTemporalScheme::step (TemporalScheme.hpp:119-146)
+  double t = ctl->t_local;
+  if (rep) {
+    ctl->repeated++; ctl->step_repeated++;
+  } else {
+    ctl->accepted++; ctl->step_accepted++;
+    ctl->rain_in += rain; ctl->outflow += outf; ctl->volume = vol;
+    t = t + dt;
+    ctl->cur ^= 1;
+  }
+  double ndt = nd;
+  const double L = F.L;
+  if (t >= L) {
+    ctl->done = 1;
+  } else if (t + ndt > L) {
+    ndt = L - t;
+  } else if (t + 2.0 * ndt > L) {
+    ndt = (L - t) * 0.4;
+  }
+  if (!(t < L) && !(t >= L)) { ctl->done = 1; ctl->error = -5; }   // t became NaN
+  ctl->t_local = t;
+  ctl->dt = ndt;
+}
+
+#ifdef SV_DEFINE_COMMON_KERNELS
+// Host-API accept (RungeKutta.hpp:428-431): flip the state parity, apply the pending tallies.
+__global__ void accept_kernel(Ctl* ctl) {
+  ctl->cur ^= 1;
+  ctl->accepted++;
+  ctl->rain_in += ctl->pend_rain;
+  ctl->outflow += ctl->pend_out;
+  ctl->volume = ctl->pend_vol;
+}
+__global__ void begin_step_kernel(Ctl* ctl) {
+  ctl->t_local = 0.0;
+  ctl->done = 0;
+  ctl->step_accepted = 0;
+  ctl->step_repeated = 0;
+}
+#endif
+
+// Volume of a cell field: per-CTA FP64 partials (same tiling and reduction as the stage
+// kernel's last stage), then a fixed-order sum.
+template <typename T, int TX, int TY>
+__global__ void __launch_bounds__(TX * TY) volume_partials_kernel(const T* h, int nx, int ny, double area,
+                                                                  double* part) {
+  __shared__ double red[TX * TY / 32];
+  const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
+  const int gx = blockIdx.x * TX + tx, gy = blockIdx.y * TY + ty;
+  double v = 0.0;
+  if (gx < nx && gy < ny) v = double(h[(long long)gy * nx + gx]) * area;
+  double s = block_sum<TX * TY>(v, red);
+  if (threadIdx.x == 0) part[(long long)blockIdx.y * gridDim.x + blockIdx.x] = s;
+}
+template <int NT> __global__ void __launch_bounds__(NT) sum_kernel(const double* p, long long n, double* out) {
+  __shared__ double red[NT];
+  double r = fixed_sum<NT>(p, n, red);
+  if (threadIdx.x == 0) *out = r;
+}
+
+// ------------------------------- debug / per-function kernels -------------------------
+template <typename T> struct DebugParams {
+  int nx, ny;
+  double dx, dy;
+  const T *h, *u, *v, *z;
+  T *dhdx, *dudx, *dvdx, *dzdx, *dhdy, *dudy, *dvdy, *dzdy;
+  T *fh, *fu, *fv, *fz, *fb;
+};
+
+// SpatialDerivativeOperationKernel over global arrays (State.cpp:187-192, Constants.cpp:39-40)
+template <typename T> __global__ void debug_slopes_kernel(const DebugParams<T> D) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = (long long)D.nx * D.ny;
+  if (i >= n) return;
+  int gx = int(i % D.nx), gy = int(i / D.nx);
+  bool hasW = gx > 0, hasE = gx < D.nx - 1, hasN = gy < D.ny - 1, hasS = gy > 0;
+  Div<T> divx = mkdiv<T>(D.dx), divy = mkdiv<T>(D.dy);
+  const T* src[4] = {D.h, D.u, D.v, D.z};
+  T* dx_[4] = {D.dhdx, D.dudx, D.dvdx, D.dzdx};
+  T* dy_[4] = {D.dhdy, D.dudy, D.dvdy, D.dzdy};
+  for (int f = 0; f < 4; ++f) {
+    const T* a = src[f];
+    T c = a[i];
+    T l = hasW ? a[i - 1] : c, r = hasE ? a[i + 1] : c;
+    dx_[f][i] = minmod3<T>(l, hasW, c, hasE, r, divx);
+    T nn = hasN ? a[i + D.nx] : c, ss = hasS ? a[i - D.nx] : c;
+    dy_[f][i] = minmod3<T>(nn, hasN, c, hasS, ss, divy);
+  }
+}
+
+// SaintVenantFluxKernel over all faces (Fluxes.cpp:55-64)
+template <typename T> __global__ void debug_flux_kernel(const DebugParams<T> D) {
+  long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long nvf = (long long)(D.nx + 1) * D.ny;
+  long long nf = nvf + (long long)(D.ny + 1) * D.nx;
+  if (f >= nf) return;
+  auto cell = [&](long long i) {
+    CellV<T> c;
+    c.h = D.h[i]; c.u = D.u[i]; c.v = D.v[i]; c.z = D.z[i];
+    c.dhdx = D.dhdx[i]; c.dudx = D.dudx[i]; c.dvdx = D.dvdx[i]; c.dzdx = D.dzdx[i];
+    c.dhdy = D.dhdy[i]; c.dudy = D.dudy[i]; c.dvdy = D.dvdy[i]; c.dzdy = D.dzdy[i];
+    return c;
+  };
+  FaceF<T> F;
+  T br;
+  if (f < nvf) {
+    long long fx = f % (D.nx + 1), fy = f / (D.nx + 1);
+    int edge = fx == 0 ? -1 : (fx == D.nx ? 1 : 0);
+    long long l = fy * D.nx + (edge == -1 ? 0 : fx - 1);
+    long long r = fy * D.nx + (edge == 1 ? D.nx - 1 : fx);
+    br = face_flux<T, 0>(cell(l), cell(r), edge, T(0.5) * T(D.dx), mkdiv<T>(D.dx), F);
+  } else {
+    long long f2 = f - nvf;
+    long long fx = f2 % D.nx, fy = f2 / D.nx;
+    int edge = fy == 0 ? -1 : (fy == D.ny ? 1 : 0);
+    long long l = (edge == -1 ? 0 : fy - 1) * D.nx + fx;
+    long long r = (edge == 1 ? D.ny - 1 : fy) * D.nx + fx;
+    br = face_flux<T, 1>(cell(l), cell(r), edge, T(0.5) * T(D.dy), mkdiv<T>(D.dy), F);
+  }
+  D.fh[f] = F.h; D.fu[f] = F.u; D.fv[f] = F.v; D.fz[f] = F.z; D.fb[f] = br;
+}
+
+// temporal derivative + sources + boundaries per cell from the global face arrays
+template <typename T>
+__global__ void debug_cell_kernel(const StageParams<T> P, const DebugParams<T> D, T* nh, T* sf) {
+  long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = (long long)P.nx * P.ny;
+  if (g >= n) return;
+  const Ctl* ctl = P.ctl;
+  const double dt_d = ctl->dt;
+  int gx = int(g % P.nx), gy = int(g / P.nx);
+  CellCtx<T> c;
+  c.divx = mkdiv<T>(P.dx); c.divy = mkdiv<T>(P.dy);
+  c.divdt = mkdiv<T>(dt_d); c.divL = mkdiv<T>(P.L);
+  c.dt = T(dt_d); c.dt_d = dt_d; c.tsub_d = ctl->t_local + P.c_s * dt_d;
+  c.manning = P.manning; c.rain_mode = P.rain_mode; c.head_first = P.head_first;
+  long long w = (long long)gy * (P.nx + 1) + gx, e = w + 1;
+  long long sf_ = (long long)(P.nx + 1) * P.ny + (long long)gy * P.nx + gx, nf_ = sf_ + P.nx;
+  FaceF<T> fw{D.fh[w], D.fu[w], D.fv[w], D.fz[w]}, fe{D.fh[e], D.fu[e], D.fv[e], D.fz[e]};
+  FaceF<T> fs{D.fh[sf_], D.fu[sf_], D.fv[sf_], D.fz[sf_]}, fn{D.fh[nf_], D.fu[nf_], D.fv[nf_], D.fz[nf_]};
+  const DevForcing fc = *P.fc;
+  T kh, ku, kv;
+  double rain, removed;
+  cell_dudt<T>(P, fc, c, g, gx, gy, D.h[g], D.u[g], D.v[g], D.dhdx[g], D.dhdy[g], D.dzdx[g], D.dzdy[g], fw, fe, fs,
+               fn, kh, ku, kv, rain, removed, nh + g, sf + g);
+  P.Kout[0][g] = kh; P.Kout[1][g] = ku; P.Kout[2][g] = kv;
+}
+
+}  // namespace svk

@@ -1,0 +1,27 @@
+// sv_launch.h -- host-callable launchers for the kernels in sv_kernels.cuh. They are
+// explicitly instantiated per value type in sv_f64.cu (compiled with -fmad=false so every
+// FP64 operation is separately rounded, as in the reference) and sv_f32.cu.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "sv_kernels.cuh"
+
+namespace svk {
+
+// Tile shapes compiled for the fused stage kernel (TX x TY cells per CTA).
+struct TileShape { int tx, ty; };
+constexpr TileShape kTiles[] = {{32, 8}, {32, 4}, {64, 4}, {32, 16}};
+constexpr int kNumTiles = 4;
+
+template <typename T> size_t stage_smem_bytes(int tile);
+template <typename T> cudaError_t launch_stage(const StageParams<T>& P, int tile, cudaStream_t s);
+template <typename T> cudaError_t launch_volume(const T* h, int nx, int ny, double area, double* part, int tile,
+                                                cudaStream_t s);
+template <typename T> cudaError_t launch_debug(const StageParams<T>& P, const DebugParams<T>& D, T* nh, T* sf,
+                                               cudaStream_t s);
+cudaError_t launch_finalize(const FinalizeParams& F, cudaStream_t s);
+cudaError_t launch_sum(const double* p, long long n, double* out, cudaStream_t s);
+cudaError_t launch_accept(Ctl* ctl, cudaStream_t s);
+cudaError_t launch_begin_step(Ctl* ctl, cudaStream_t s);
+
+}  // namespace svk

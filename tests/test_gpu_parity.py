@@ -1,0 +1,113 @@
+"""Parity of the CUDA path (through the C-ABI) with the CPU oracle, FP64 bit for bit.
+
+Each reference kernel is checked on its own through sv_eval_dudt (slopes, face fluxes and
+branches, dU/dt), then the fused path through whole timesteps and whole steps. Grids that are
+not multiples of the CTA tile, strips, wet/dry fronts, coded-out (NaN bed) cells, every named
+Runge-Kutta tableau and both boundary orders are covered."""
+import numpy as np
+import pytest
+
+from mfcm_b200 import SaintVenantSolver, solve, EDGE_XMAX, EDGE_XMIN, EDGE_YMIN, EDGE_YMAX, RK_METHODS, synth
+from oracle.sv_oracle_py import OracleSolver
+from tests.scenarios import wet_dry_state, setup, rain_series, forcing, same, first_diff
+
+pytestmark = pytest.mark.gpu
+
+SLOPES = ["DHDX", "DUDX", "DVDX", "DHDY", "DUDY", "DVDY", "DZDX", "DZDY"]
+FACES = ["FLUX_H", "FLUX_U", "FLUX_V", "FLUX_Z", "FLUX_BRANCH"]
+KS = ["DHDT", "DUDT", "DVDT"]
+
+
+def pair(nx, ny, dx, **kw):
+    return SaintVenantSolver(nx, ny, dx, **kw), OracleSolver(nx, ny, dx, **kw)
+
+
+def assert_same(g, o, what):
+    d = first_diff(g, o)
+    assert d is None, f"{what}: first mismatch at {d[0]}: gpu {d[1]!r} oracle {d[2]!r} ({d[3]} cells differ)"
+
+
+@pytest.mark.parametrize("shape", [(17, 13), (8, 8), (1, 9), (9, 1), (40, 3), (33, 17)])
+@pytest.mark.parametrize("nan_cells", [0, 5])
+def test_per_function_parity(shape, nan_cells):
+    nx, ny = shape
+    if nan_cells and nx * ny < 20:
+        pytest.skip("too small for coded-out cells")
+    z, h, u, v = wet_dry_state(nx, ny, 3.0, seed=nx * 31 + ny, nan_cells=nan_cells)
+    g, o = pair(nx, ny, 3.0, rain_mode="reference")
+    for b in (g, o):
+        setup(b, z, h, u, v, n=(0.03, 0.05, 0.1, 0.3))
+        b.set_forcing(forcing((2e-5, 1e-5), head=(0.05, 0.0), edges=EDGE_XMAX | EDGE_YMIN))
+        b.eval_dudt(0, 7.5, 0.37)
+    for f in SLOPES + FACES + KS:
+        assert_same(g.get_field(f), o.get_field(f), f)
+
+
+@pytest.mark.parametrize("rk", RK_METHODS)
+def test_one_timestep_every_tableau(rk):
+    nx, ny, dx = 37, 21, 2.0
+    z, h, u, v = wet_dry_state(nx, ny, dx, seed=7)
+    g, o = pair(nx, ny, dx, rk_method=rk)
+    N = g.nstages
+    for b in (g, o):
+        setup(b, z, h, u, v)
+        b.set_forcing(forcing((3e-5, 3e-5), head=(0.0, 0.0), edges=EDGE_XMIN))
+    rg = g.do_timestep(1.25, 0.05)
+    ro = o.do_timestep(1.25, 0.05)
+    assert rg[0] == ro[0] and rg[1] == ro[1] and rg[2] == ro[2], (rg, ro)
+    for f in range(3):
+        assert_same(g.get_field(100 + 3 * N + f), o.get_field(100 + 3 * N + f), f"U_[N] field {f}")
+
+
+@pytest.mark.parametrize("rain_mode,head_first", [("reference", False), ("physical", False), ("physical", True)])
+def test_steps_match(rain_mode, head_first):
+    nx, ny, dx = 45, 30, 4.0
+    z = synth.plane_with_gaussians(nx, ny, dx, seed=3)
+    h = np.full((ny, nx), 1e-3)
+    g, o = pair(nx, ny, dx, cn_target=0.5, rain_mode=rain_mode, head_first=head_first, step_duration=30.0)
+    for b in (g, o):
+        setup(b, z, h, np.zeros_like(h), np.zeros_like(h))
+    rain = rain_series(50.0 * synth.MM_PER_H, stop=60.0)
+    sg = solve(g, 0.0, 120.0, rain=rain, head=0.0, head_edges=synth.lowest_edge(z))
+    so = solve(o, 0.0, 120.0, rain=rain, head=0.0, head_edges=synth.lowest_edge(z))
+    for a, b in zip(sg, so):
+        assert a["accepted"] == b["accepted"] and a["repeated"] == b["repeated"]
+        assert abs(a["volume"] - b["volume"]) <= 1e-12 * abs(b["volume"])
+        assert abs(a["rain_in"] - b["rain_in"]) <= 1e-12 * abs(b["rain_in"]) + 1e-300
+        assert abs(a["outflow"] - b["outflow"]) <= 1e-12 * abs(b["outflow"]) + 1e-300
+    for f in ("H", "U", "V"):
+        assert_same(g.get_field(f), o.get_field(f), f)
+    assert g.get_dt() == o.get_dt()
+
+
+def test_fields_forcing_and_pattern():
+    nx, ny, dx = 50, 34, 2.0
+    z, h, u, v = wet_dry_state(nx, ny, dx, seed=11)
+    rng = np.random.default_rng(5)
+    pat = rng.uniform(0.5, 1.5, size=(ny, nx))
+    nfield = rng.choice([0.02, 0.035, 0.05, 0.1], size=(ny, nx))
+    g, o = pair(nx, ny, dx, rain_mode="physical", step_duration=20.0)
+    for b in (g, o):
+        setup(b, z, h, u, v, n_field=nfield)
+        b.set_field("RAIN_PATTERN", pat)
+        b.set_forcing(forcing((1e-5, 2e-5), rain_kind=3, head=(0.0, 0.0), edges=15))
+        b.advance()
+    for f in ("H", "U", "V"):
+        assert_same(g.get_field(f), o.get_field(f), f)
+
+
+def test_fp32_close_to_fp64_oracle():
+    nx, ny, dx = 64, 48, 5.0
+    z = synth.plane_with_gaussians(nx, ny, dx, seed=1)
+    h = np.full((ny, nx), 1e-3)
+    g = SaintVenantSolver(nx, ny, dx, precision="f32", cn_target=0.5, rain_mode="physical")
+    o = OracleSolver(nx, ny, dx, cn_target=0.5, rain_mode="physical")
+    for b in (g, o):
+        setup(b, z, h, np.zeros_like(h), np.zeros_like(h))
+    rain = rain_series(50.0 * synth.MM_PER_H, stop=600.0)
+    solve(g, 0.0, 240.0, rain=rain, head=0.0, head_edges=synth.lowest_edge(z))
+    solve(o, 0.0, 240.0, rain=rain, head=0.0, head_edges=synth.lowest_edge(z))
+    err = np.max(np.abs(g.get_field("H") - o.get_field("H")))
+    vg, vo = g.stats()["volume"], o.stats()["volume"]
+    assert err <= 1e-3, err
+    assert abs(vg - vo) <= 1e-3 * vo, (vg, vo)
