@@ -184,8 +184,23 @@ int sv_advance(sv_ctx* ctx, sv_stats* out);
 /* SaintVenantVolumeMeasure::get_volume (src/SaintVenant/Measure.hpp:137-156) plus the
  * running rain/outflow tallies; FP64. */
 int sv_get_stats(sv_ctx* ctx, sv_stats* out);
-/* device time (ms) of the stage kernels of the last sv_advance, or -1 if not recorded */
+/* device time (ms) of the last sv_advance, or -1 if not recorded */
 int sv_last_advance_ms(sv_ctx* ctx, double* ms);
+
+typedef struct {
+  double total_ms;        /* device time of the whole call (CUDA events on the ctx stream)  */
+  double stage_ms;        /* summed device time of the stage kernels                       */
+  double finalize_ms;     /* summed device time of the reduction + dt-controller kernel    */
+  uint64_t stage_launches;
+  uint64_t finalize_launches;
+} sv_timing;
+
+/* Part of TypedTemporalScheme::step (TemporalScheme.hpp:119-146): at most `max_timesteps`
+ * device-controlled timesteps (accepted or repeated) of the current step, stopping early when
+ * the step completes (then `*step_done` = 1). `begin` = 1 starts a new step (t_local = 0).
+ * With `timing` != NULL every kernel is bracketed by CUDA events on the ctx stream. */
+int sv_run_timesteps(sv_ctx* ctx, uint64_t max_timesteps, int begin, sv_stats* out, int* step_done,
+                     sv_timing* timing);
 /* message of the last failing call on ctx (or of the last failing sv_create if ctx is NULL) */
 const char* sv_last_error(const sv_ctx* ctx);
 

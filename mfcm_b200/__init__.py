@@ -56,6 +56,9 @@ def load_library(path=None):
     lib.sv_last_error.argtypes = [C.c_void_p]
     lib.sv_last_advance_ms.restype = C.c_int
     lib.sv_last_advance_ms.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+    lib.sv_run_timesteps.restype = C.c_int
+    lib.sv_run_timesteps.argtypes = [C.c_void_p, C.c_uint64, C.c_int, C.POINTER(Stats), C.POINTER(C.c_int),
+                                     C.POINTER(_abi.Timing)]
     if path is None:
         _lib = lib
     return lib
@@ -162,6 +165,18 @@ class SaintVenantSolver(_Backend):
 
     def last_error(self):
         return self._lib.sv_last_error(self._h).decode()
+
+    def run_timesteps(self, max_timesteps, begin=False, timing=False):
+        """Up to `max_timesteps` device-controlled timesteps of the current step (part of
+        TypedTemporalScheme::step); returns (running stats, step finished?, timing or None)."""
+        s = Stats()
+        done = C.c_int()
+        t = _abi.Timing() if timing else None
+        r = self._lib.sv_run_timesteps(self._h, int(max_timesteps), 1 if begin else 0, C.byref(s), C.byref(done),
+                                       C.byref(t) if t is not None else None)
+        if r != 0:
+            raise SvError(r, self.last_error())
+        return s.as_dict(), bool(done.value), (t.as_dict() if t is not None else None)
 
     def last_advance_ms(self):
         v = C.c_double()

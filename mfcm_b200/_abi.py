@@ -58,6 +58,14 @@ class Stats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class Timing(C.Structure):
+    _fields_ = [("total_ms", C.c_double), ("stage_ms", C.c_double), ("finalize_ms", C.c_double),
+                ("stage_launches", C.c_uint64), ("finalize_launches", C.c_uint64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 def declare(lib, prefix, ctx_type=C.c_void_p):
     """Declare the sv_* (or svo_*) prototypes on a loaded library."""
     P = C.POINTER

@@ -103,6 +103,7 @@ struct sv_ctx {
   virtual int accept() = 0;
   virtual int advance(sv_stats*) = 0;
   virtual int get_stats(sv_stats*) = 0;
+  virtual int run_timesteps(uint64_t, int, sv_stats*, int*, sv_timing*) = 0;
   double last_advance_ms = -1.0;
 };
 
@@ -404,7 +405,8 @@ struct Solver final : public sv_ctx {
   }
 
   // Launch the N stages of one timestep and the finalize kernel (RungeKutta.cpp:147-167).
-  int enqueue_timestep(bool auto_mode) {
+  // ev: if non-null, 2*(N+1) events recorded around every kernel (stages, then finalize)
+  int enqueue_timestep(bool auto_mode, cudaEvent_t* ev = nullptr) {
     svk::StageParams<T> P = base_params();
     const bool tally = !(prm.flags & SV_FLAG_NO_TALLIES);
     for (int s = 0; s < N; ++s) {
@@ -429,8 +431,10 @@ struct Solver final : public sv_ctx {
         P.Kout[f] = (!diag && s < N - 1) ? K[s][f] : nullptr;
         for (int j = 0; j < 4; ++j) P.Kin[j][f] = (!diag && j < N - 1) ? K[j][f] : nullptr;
       }
+      if (ev) SV_CUDA(cudaEventRecord(ev[2 * s], stream));
       cudaError_t e = svk::launch_stage<T>(P, tile, stream);
       if (e != cudaSuccess) return cuda_fail(e, "stage kernel");
+      if (ev) SV_CUDA(cudaEventRecord(ev[2 * s + 1], stream));
     }
     svk::FinalizeParams F{};
     F.ctl = ctl;
@@ -441,11 +445,14 @@ struct Solver final : public sv_ctx {
     F.cn_target = prm.cn_target;
     F.max_dt = prm.max_dt;
     F.L = prm.step_duration;
+    F.cell_area = mesh.dx * mesh.dy;
     F.auto_mode = auto_mode ? 1 : 0;
     F.tally = tally ? 1 : 0;
     F.is_float = sizeof(T) == 4;
+    if (ev) SV_CUDA(cudaEventRecord(ev[2 * N], stream));
     cudaError_t e = svk::launch_finalize(F, stream);
     if (e != cudaSuccess) return cuda_fail(e, "finalize kernel");
+    if (ev) SV_CUDA(cudaEventRecord(ev[2 * N + 1], stream));
     return SV_OK;
   }
 
@@ -481,8 +488,13 @@ struct Solver final : public sv_ctx {
     return SV_OK;
   }
 
+  // do_timestep(local_time, dt) is a function of its arguments: the scheme's own t_local and
+  // dt (TemporalScheme.hpp:78) are restored afterwards.
   int do_timestep(double t_local, double dt, double* cn, int* repeat, double* new_dt) override {
-    int r = write_ctl_time(t_local, dt);
+    Ctl saved;
+    int r = read_ctl(saved);
+    if (r) return r;
+    r = write_ctl_time(t_local, dt);
     if (r) return r;
     r = enqueue_timestep(false);
     if (r) return r;
@@ -492,6 +504,11 @@ struct Solver final : public sv_ctx {
     if (cn) *cn = c.cn;
     if (repeat) *repeat = c.repeat;
     if (new_dt) *new_dt = c.new_dt;
+    c.t_local = saved.t_local;
+    c.dt = saved.dt;
+    c.done = saved.done;
+    SV_CUDA(cudaMemcpyAsync(ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, stream));
+    SV_CUDA(cudaStreamSynchronize(stream));
     return SV_OK;
   }
 
@@ -528,7 +545,7 @@ struct Solver final : public sv_ctx {
       int r = build_graph();
       if (r) return r;
     }
-    cudaError_t e = svk::launch_begin_step(ctl, stream);
+    cudaError_t e = svk::launch_begin_step(ctl, 1, 0, stream);
     if (e != cudaSuccess) return cuda_fail(e, "begin step");
     SV_CUDA(cudaEventRecord(ev0, stream));
     Ctl c;
@@ -552,6 +569,56 @@ struct Solver final : public sv_ctx {
       out->outflow = c.outflow;
       int r = volume(&out->volume);
       if (r) return r;
+    }
+    if (c.error) return fail(SV_E_NONFINITE, "time became NaN: the control number was not finite");
+    return SV_OK;
+  }
+
+  // Direct launches (no graph) of up to n device-controlled timesteps; with timing, every
+  // kernel is bracketed by events and the per-kernel durations are summed after one sync.
+  int run_timesteps(uint64_t n, int begin, sv_stats* out, int* step_done, sv_timing* timing) override {
+    if (n == 0) return fail(SV_E_ARG, "max_timesteps must be positive");
+    cudaError_t e = svk::launch_begin_step(ctl, begin ? 1 : 0, (long long)n, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "begin step");
+    std::vector<cudaEvent_t> evs;
+    const int per = 2 * (N + 1);
+    if (timing) {
+      evs.resize(size_t(n) * per);
+      for (auto& x : evs) SV_CUDA(cudaEventCreate(&x));
+    }
+    SV_CUDA(cudaEventRecord(ev0, stream));
+    for (uint64_t i = 0; i < n; ++i) {
+      int r = enqueue_timestep(true, timing ? &evs[size_t(i) * per] : nullptr);
+      if (r) return r;
+    }
+    SV_CUDA(cudaEventRecord(ev1, stream));
+    SV_CUDA(cudaEventSynchronize(ev1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    if (timing) {
+      timing->total_ms = ms;
+      timing->stage_ms = timing->finalize_ms = 0.0;
+      timing->stage_launches = timing->finalize_launches = 0;
+      for (uint64_t i = 0; i < n; ++i) {
+        for (int k = 0; k <= N; ++k) {
+          float d = 0.f;
+          cudaEventElapsedTime(&d, evs[size_t(i) * per + 2 * k], evs[size_t(i) * per + 2 * k + 1]);
+          if (k < N) { timing->stage_ms += d; timing->stage_launches++; }
+          else { timing->finalize_ms += d; timing->finalize_launches++; }
+        }
+      }
+      for (auto& x : evs) cudaEventDestroy(x);
+    }
+    Ctl c;
+    int r = read_ctl(c);
+    if (r) return r;
+    if (step_done) *step_done = (c.done == 1);
+    if (out) {
+      out->accepted = c.accepted;
+      out->repeated = c.repeated;
+      out->rain_in = c.rain_in;
+      out->outflow = c.outflow;
+      out->volume = c.volume;
     }
     if (c.error) return fail(SV_E_NONFINITE, "time became NaN: the control number was not finite");
     return SV_OK;
@@ -631,6 +698,10 @@ int sv_do_timestep(sv_ctx* ctx, double t, double dt, double* cn, int* rep, doubl
 int sv_accept(sv_ctx* ctx) { SV_CHECK_CTX(ctx); return ctx->accept(); }
 int sv_advance(sv_ctx* ctx, sv_stats* out) { SV_CHECK_CTX(ctx); return ctx->advance(out); }
 int sv_get_stats(sv_ctx* ctx, sv_stats* out) { SV_CHECK_CTX(ctx); if (!out) return SV_E_ARG; return ctx->get_stats(out); }
+int sv_run_timesteps(sv_ctx* ctx, uint64_t n, int begin, sv_stats* out, int* step_done, sv_timing* t) {
+  SV_CHECK_CTX(ctx);
+  return ctx->run_timesteps(n, begin, out, step_done, t);
+}
 int sv_last_advance_ms(sv_ctx* ctx, double* ms) { SV_CHECK_CTX(ctx); if (!ms) return SV_E_ARG; *ms = ctx->last_advance_ms; return SV_OK; }
 const char* sv_last_error(const sv_ctx* ctx) { return ctx ? ctx->err.c_str() : g_create_err.c_str(); }
 

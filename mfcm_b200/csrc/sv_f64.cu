@@ -20,8 +20,8 @@ cudaError_t launch_accept(Ctl* ctl, cudaStream_t s) {
   accept_kernel<<<1, 1, 0, s>>>(ctl);
   return cudaGetLastError();
 }
-cudaError_t launch_begin_step(Ctl* ctl, cudaStream_t s) {
-  begin_step_kernel<<<1, 1, 0, s>>>(ctl);
+cudaError_t launch_begin_step(Ctl* ctl, int new_step, long long budget, cudaStream_t s) {
+  begin_step_kernel<<<1, 1, 0, s>>>(ctl, new_step, budget);
   return cudaGetLastError();
 }
 

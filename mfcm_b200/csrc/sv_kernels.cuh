@@ -33,6 +33,7 @@ struct Ctl {
   double rain_in, outflow;      // running tallies over accepted timesteps
   double volume;                // volume of U_[0] after the last accepted timestep
   double pend_rain, pend_out, pend_vol;  // tallies of the last timestep, applied on accept
+  long long budget;             // > 0: timesteps left before the loop pauses (done = 2)
 };
 
 // Per-step boundary values, kept in device memory so captured graphs stay valid when
@@ -418,6 +419,7 @@ struct FinalizeParams {
   int nstages;
   double b[4];
   double cn_target, max_dt, L;
+  double cell_area;
   int auto_mode;   // 1: accept/repeat, advance t_local, trim dt (TemporalScheme.hpp:119-146)
   int tally;
   int is_float;    // control number rounded to T = float
@@ -471,8 +473,8 @@ template <int NT> __global__ void __launch_bounds__(NT) finalize_kernel(const Fi
       double rs = fixed_sum<NT>(F.part + (3 + 2LL * s) * F.nblk, F.nblk, red);
       double os = fixed_sum<NT>(F.part + (4 + 2LL * s) * F.nblk, F.nblk, red);
       double w = F.is_float ? double(float(F.b[s] * ctl->dt)) : F.b[s] * ctl->dt;
-      rain += w * rs;
-      outf += w * os;
+      rain += w * rs * F.cell_area;
+      outf += w * os * F.cell_area;
     }
   }
   if (threadIdx.x != 0) return;
@@ -525,6 +527,7 @@ template <int NT> __global__ void __launch_bounds__(NT) finalize_kernel(const Fi
   if (!(t < L) && !(t >= L)) { ctl->done = 1; ctl->error = -5; }   // t became NaN
   ctl->t_local = t;
   ctl->dt = ndt;
+  if (ctl->budget > 0 && --ctl->budget == 0 && !ctl->done) ctl->done = 2;  // paused, step not over
 }
 
 #ifdef SV_DEFINE_COMMON_KERNELS
@@ -536,11 +539,14 @@ __global__ void accept_kernel(Ctl* ctl) {
   ctl->outflow += ctl->pend_out;
   ctl->volume = ctl->pend_vol;
 }
-__global__ void begin_step_kernel(Ctl* ctl) {
-  ctl->t_local = 0.0;
+__global__ void begin_step_kernel(Ctl* ctl, int new_step, long long budget) {
+  if (new_step) {
+    ctl->t_local = 0.0;
+    ctl->step_accepted = 0;
+    ctl->step_repeated = 0;
+  }
   ctl->done = 0;
-  ctl->step_accepted = 0;
-  ctl->step_repeated = 0;
+  ctl->budget = budget;
 }
 #endif
 

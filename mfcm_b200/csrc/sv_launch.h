@@ -22,6 +22,6 @@ template <typename T> cudaError_t launch_debug(const StageParams<T>& P, const De
 cudaError_t launch_finalize(const FinalizeParams& F, cudaStream_t s);
 cudaError_t launch_sum(const double* p, long long n, double* out, cudaStream_t s);
 cudaError_t launch_accept(Ctl* ctl, cudaStream_t s);
-cudaError_t launch_begin_step(Ctl* ctl, cudaStream_t s);
+cudaError_t launch_begin_step(Ctl* ctl, int new_step, long long budget, cudaStream_t s);
 
 }  // namespace svk
