@@ -50,6 +50,7 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--variant", default="auto", help="stage-kernel variant 0-6, or auto (autotune)")
     return p.parse_args()
 
 
@@ -289,6 +290,11 @@ def main():
     solver = make_solver(w, args.precision, device)
     runner = Runner(solver)
     runner.spinup(args.spinup)
+    if args.variant == "auto":
+        variant = solver.autotune()
+    else:
+        variant = int(args.variant)
+        solver.set_kernel_variant(variant)
     # warm-up timesteps (untimed)
     runner.run(max(3, args.warmup))
 
@@ -351,7 +357,7 @@ def main():
                                        "0.005 slope, lognormal rain field 30 mm/h, Voronoi n, outflow all edges)",
                            "scheme": "classic RK4", "cn_target": 0.5, "precision": args.precision,
                            "spinup_timesteps": args.spinup, "sim_time_s": runner.t_step, "l2": "inputs larger than L2 (each state field 134 MB)",
-                           "parallelism": f"replicas x{world}", "accepted": accepted, "repeated": repeated},
+                           "parallelism": f"replicas x{world}", "kernel_variant": variant, "accepted": accepted, "repeated": repeated},
                 "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "clocks": clocks,
                 "gpu_launches": int(tm["stage_launches"] + tm["finalize_launches"] + tm["begin_launches"])}
         print(json.dumps(line), flush=True)

@@ -201,6 +201,15 @@ typedef struct {
  * With `timing` != NULL every kernel is bracketed by CUDA events on the ctx stream. */
 int sv_run_timesteps(sv_ctx* ctx, uint64_t max_timesteps, int begin, sv_stats* out, int* step_done,
                      sv_timing* timing);
+/* Stage-kernel variant (no reference counterpart: a launch-shape choice of this library):
+ * 0-3 tiled shared-memory kernel (32x8, 32x4, 64x4, 32x16 cells per CTA), 4-6 column-sweep
+ * kernel (16/32/64 rows per warp). Every variant computes bit-identical results. */
+int sv_set_kernel_variant(sv_ctx* ctx, int variant);
+int sv_get_kernel_variant(sv_ctx* ctx, int* variant);
+/* Autotune: times every variant's stage kernel on the current state and keeps the fastest;
+ * `best_out` (may be NULL) receives the chosen variant. The state U_[0] is not modified. */
+int sv_autotune(sv_ctx* ctx, int* best_out);
+
 /* message of the last failing call on ctx (or of the last failing sv_create if ctx is NULL) */
 const char* sv_last_error(const sv_ctx* ctx);
 

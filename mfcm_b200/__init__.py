@@ -56,6 +56,11 @@ def load_library(path=None):
     lib.sv_last_error.argtypes = [C.c_void_p]
     lib.sv_last_advance_ms.restype = C.c_int
     lib.sv_last_advance_ms.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+    lib.sv_set_kernel_variant.restype = C.c_int
+    lib.sv_set_kernel_variant.argtypes = [C.c_void_p, C.c_int]
+    for name in ("sv_get_kernel_variant", "sv_autotune"):
+        getattr(lib, name).restype = C.c_int
+        getattr(lib, name).argtypes = [C.c_void_p, C.POINTER(C.c_int)]
     lib.sv_run_timesteps.restype = C.c_int
     lib.sv_run_timesteps.argtypes = [C.c_void_p, C.c_uint64, C.c_int, C.POINTER(Stats), C.POINTER(C.c_int),
                                      C.POINTER(_abi.Timing)]
@@ -177,6 +182,24 @@ class SaintVenantSolver(_Backend):
         if r != 0:
             raise SvError(r, self.last_error())
         return s.as_dict(), bool(done.value), (t.as_dict() if t is not None else None)
+
+    def set_kernel_variant(self, variant):
+        r = self._lib.sv_set_kernel_variant(self._h, int(variant))
+        if r != 0:
+            raise SvError(r, self.last_error())
+
+    def kernel_variant(self):
+        v = C.c_int()
+        self._lib.sv_get_kernel_variant(self._h, C.byref(v))
+        return v.value
+
+    def autotune(self):
+        """Time every stage-kernel variant on the current state; keep the fastest."""
+        v = C.c_int()
+        r = self._lib.sv_autotune(self._h, C.byref(v))
+        if r != 0:
+            raise SvError(r, self.last_error())
+        return v.value
 
     def last_advance_ms(self):
         v = C.c_double()

@@ -12,6 +12,7 @@
 //   part         per-CTA FP64 partials of the CFL max/min, volume and tallies
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -104,6 +105,9 @@ struct sv_ctx {
   virtual int advance(sv_stats*) = 0;
   virtual int get_stats(sv_stats*) = 0;
   virtual int run_timesteps(uint64_t, int, sv_stats*, int*, sv_timing*) = 0;
+  virtual int set_variant(int) = 0;
+  virtual int get_variant() const = 0;
+  virtual int autotune(int*) = 0;
   double last_advance_ms = -1.0;
 };
 
@@ -124,13 +128,16 @@ struct Solver final : public sv_ctx {
   Tableau tab;
   bool diag = true;
   int N = 4;
-  int tile = 0;
+  int tile = 0;      // tile shape of the volume kernel
+  int variant = 5;   // stage-kernel variant (svk::launch_variant)
+  float tune_ms[svk::kNumVariants] = {};
   int tx = 32, ty = 8;
-  long long ncells = 0, nfaces = 0, nblk = 0;
+  long long ncells = 0, nfaces = 0, nblk = 0, vol_nblk = 0;
   T* S[2][3] = {};
   T* Y[2][3] = {};
   T* K[4][3] = {};
   T* z = nullptr;
+  T *zx = nullptr, *zy = nullptr;  // bed slopes (Constants.cpp:39-40)
   T* man[4] = {};
   double man_s[4] = {0.03, 0.3, 0.1, 0.3};  // ManningRoughnessSourceTerm.cpp:99-102
   std::vector<double> host_n_shallow;
@@ -192,7 +199,8 @@ struct Solver final : public sv_ctx {
     nfaces = (long long)(m->nx + 1) * (long long)m->ny + (long long)(m->ny + 1) * (long long)m->nx;
     tx = svk::kTiles[tile].tx;
     ty = svk::kTiles[tile].ty;
-    nblk = (long long)((m->nx + tx - 1) / tx) * (long long)((m->ny + ty - 1) / ty);
+    nblk = svk::variant_partials(variant, (long long)m->nx, (long long)m->ny);
+    vol_nblk = (long long)((m->nx + tx - 1) / tx) * (long long)((m->ny + ty - 1) / ty);
     SV_CUDA(cudaSetDevice(dev));
     SV_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     SV_CUDA(cudaEventCreate(&ev0));
@@ -206,10 +214,14 @@ struct Solver final : public sv_ctx {
       for (int s = 0; s < N - 1; ++s)
         for (int f = 0; f < 3; ++f) SV_CUDA(alloc_cells(&K[s][f], false));
     SV_CUDA(alloc_cells(&z));
+    SV_CUDA(alloc_cells(&zx));
+    SV_CUDA(alloc_cells(&zy));
     SV_CUDA(alloc(&ctl, 1));
     SV_CUDA(alloc(&dbg_ctl, 1));
     SV_CUDA(alloc(&fc, 1));
-    SV_CUDA(alloc(&part, size_t(svk::part_count(nblk, N))));
+    long long maxp = vol_nblk;
+    for (int v = 0; v < svk::kNumVariants; ++v) maxp = std::max(maxp, svk::variant_partials(v, m->nx, m->ny));
+    SV_CUDA(alloc(&part, size_t(svk::part_count(maxp, N))));
     SV_CUDA(alloc(&scalar, 4));
     Ctl c{};
     c.dt = p->initial_dt;
@@ -276,7 +288,13 @@ struct Solver final : public sv_ctx {
       host_n_shallow.assign(host, host + n);
       if (man[1] == man[0] && man[1] != nullptr) { man[1] = nullptr; graph_dirty = true; }
     }
-    return upload(*slot, host, n);
+    int r = upload(*slot, host, n);
+    if (r == SV_OK && id == SV_FIELD_Z) {
+      cudaError_t e = svk::launch_bed_slopes<T>(z, int(mesh.nx), int(mesh.ny), mesh.dx, mesh.dy, zx, zy, stream);
+      if (e != cudaSuccess) return cuda_fail(e, "bed slopes");
+      SV_CUDA(cudaStreamSynchronize(stream));
+    }
+    return r;
   }
 
   int debug_ptr(int id, T*& p, long long& count) {
@@ -393,6 +411,8 @@ struct Solver final : public sv_ctx {
     for (int b = 0; b < 2; ++b)
       for (int f = 0; f < 3; ++f) P.S[b][f] = S[b][f];
     P.z = z;
+    P.zx = zx;
+    P.zy = zy;
     for (int i = 0; i < 4; ++i) { P.man_p[i] = man[i]; P.man_s[i] = T(man_s[i]); }
     P.fc = fc;
     P.q0p = q0; P.q1p = q1; P.pat = pat; P.hb0p = hb0; P.hb1p = hb1;
@@ -432,7 +452,7 @@ struct Solver final : public sv_ctx {
         for (int j = 0; j < 4; ++j) P.Kin[j][f] = (!diag && j < N - 1) ? K[j][f] : nullptr;
       }
       if (ev) SV_CUDA(cudaEventRecord(ev[2 * s], stream));
-      cudaError_t e = svk::launch_stage<T>(P, tile, stream);
+      cudaError_t e = svk::launch_variant<T>(P, variant, stream);
       if (e != cudaSuccess) return cuda_fail(e, "stage kernel");
       if (ev) SV_CUDA(cudaEventRecord(ev[2 * s + 1], stream));
     }
@@ -624,10 +644,66 @@ struct Solver final : public sv_ctx {
     return SV_OK;
   }
 
+  int set_variant(int v) override {
+    if (v < 0 || v >= svk::kNumVariants) return fail(SV_E_ARG, "unknown kernel variant");
+    variant = v;
+    nblk = svk::variant_partials(variant, (long long)mesh.nx, (long long)mesh.ny);
+    graph_dirty = true;
+    return SV_OK;
+  }
+  int get_variant() const override { return variant; }
+
+  // Time the first-stage kernel of every variant (it reads U_[0] and writes only the stage
+  // and accumulator buffers, so the state is untouched) and keep the fastest.
+  int autotune(int* best_out) override {
+    // time against a copy of the controller with `done` cleared (the live one may hold a
+    // finished or paused step, which makes every stage kernel return at once)
+    Ctl c;
+    int r0 = read_ctl(c);
+    if (r0) return r0;
+    c.done = 0;
+    SV_CUDA(cudaMemcpyAsync(dbg_ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, stream));
+    svk::StageParams<T> P = base_params();
+    P.ctl = dbg_ctl;
+    P.stage = 0;
+    P.c_s = tab.c(1);
+    P.mode = svk::M_FIRST | (N == 1 ? svk::M_LAST : 0) | (diag ? svk::M_ACC : svk::M_STOREK);
+    for (int j = 0; j < 4; ++j) { P.a_next[j] = 0.0; P.b[j] = 0.0; }
+    if (N > 1) P.a_next[0] = tab.A(2, 1);
+    for (int j = 0; j < N; ++j) P.b[j] = tab.b(j + 1);
+    for (int f = 0; f < 3; ++f) {
+      P.Yout[f] = Y[0][f];
+      P.Kout[f] = (!diag && N > 1) ? K[0][f] : nullptr;
+    }
+    int best = variant;
+    float best_ms = 1e30f;
+    for (int v = 0; v < svk::kNumVariants; ++v) {
+      P.nblk = svk::variant_partials(v, (long long)mesh.nx, (long long)mesh.ny);
+      cudaError_t e = svk::launch_variant<T>(P, v, stream);  // warm-up
+      if (e != cudaSuccess) return cuda_fail(e, "autotune launch");
+      SV_CUDA(cudaEventRecord(ev0, stream));
+      const int reps = 3;
+      for (int i = 0; i < reps; ++i) {
+        e = svk::launch_variant<T>(P, v, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "autotune launch");
+      }
+      SV_CUDA(cudaEventRecord(ev1, stream));
+      SV_CUDA(cudaEventSynchronize(ev1));
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev0, ev1);
+      tune_ms[v] = ms / reps;
+      if (ms < best_ms) { best_ms = ms; best = v; }
+    }
+    int r = set_variant(best);
+    if (r) return r;
+    if (best_out) *best_out = best;
+    return SV_OK;
+  }
+
   int volume(double* v) {
     cudaError_t e = svk::launch_volume<T>(S[cur][0], int(mesh.nx), int(mesh.ny), mesh.dx * mesh.dy, part, tile, stream);
     if (e != cudaSuccess) return cuda_fail(e, "volume kernel");
-    e = svk::launch_sum(part, nblk, scalar, stream);
+    e = svk::launch_sum(part, vol_nblk, scalar, stream);
     if (e != cudaSuccess) return cuda_fail(e, "sum kernel");
     SV_CUDA(cudaMemcpyAsync(v, scalar, sizeof(double), cudaMemcpyDeviceToHost, stream));
     SV_CUDA(cudaStreamSynchronize(stream));
@@ -702,6 +778,9 @@ int sv_run_timesteps(sv_ctx* ctx, uint64_t n, int begin, sv_stats* out, int* ste
   SV_CHECK_CTX(ctx);
   return ctx->run_timesteps(n, begin, out, step_done, t);
 }
+int sv_set_kernel_variant(sv_ctx* ctx, int v) { SV_CHECK_CTX(ctx); return ctx->set_variant(v); }
+int sv_get_kernel_variant(sv_ctx* ctx, int* v) { SV_CHECK_CTX(ctx); if (!v) return SV_E_ARG; *v = ctx->get_variant(); return SV_OK; }
+int sv_autotune(sv_ctx* ctx, int* best) { SV_CHECK_CTX(ctx); return ctx->autotune(best); }
 int sv_last_advance_ms(sv_ctx* ctx, double* ms) { SV_CHECK_CTX(ctx); if (!ms) return SV_E_ARG; *ms = ctx->last_advance_ms; return SV_OK; }
 const char* sv_last_error(const sv_ctx* ctx) { return ctx ? ctx->err.c_str() : g_create_err.c_str(); }
 

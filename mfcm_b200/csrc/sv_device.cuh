@@ -33,10 +33,61 @@ template <> struct Lim<float> {
 };
 
 __device__ __forceinline__ bool finite_(double x) {
-  return (__double_as_longlong(x) & 0x7ff0000000000000LL) != 0x7ff0000000000000LL;
+  return (__double2hiint(x) & 0x7ff00000) != 0x7ff00000;
 }
 __device__ __forceinline__ bool finite_(float x) {
   return (__float_as_int(x) & 0x7f800000) != 0x7f800000;
+}
+
+// Bit-pattern helpers: magnitude comparisons, NaN tests and absolute values on the integer
+// pipe (for non-negative, non-NaN IEEE values the bit patterns order like the numbers).
+template <typename T> struct Bits;
+template <> struct Bits<double> {
+  using I = long long;
+  static constexpr I kMag = 0x7fffffffffffffffLL, kInf = 0x7ff0000000000000LL, kSign = (I)0x8000000000000000ULL;
+  __device__ static I of(double x) { return __double_as_longlong(x); }
+  __device__ static double from(I i) { return __longlong_as_double(i); }
+};
+template <> struct Bits<float> {
+  using I = int;
+  static constexpr I kMag = 0x7fffffff, kInf = 0x7f800000, kSign = (I)0x80000000u;
+  __device__ static I of(float x) { return __float_as_int(x); }
+  __device__ static float from(I i) { return __int_as_float(i); }
+};
+// For doubles the tests work on the 32-bit halves (the integer pipe has no 64-bit compare).
+__device__ __forceinline__ bool isnan_b(double x) {
+  unsigned hi = unsigned(__double2hiint(x)) & 0x7fffffffu;
+  return hi > 0x7ff00000u || (hi == 0x7ff00000u && __double2loint(x) != 0);
+}
+__device__ __forceinline__ bool isnan_b(float x) { return (__float_as_int(x) & 0x7fffffff) > 0x7f800000; }
+__device__ __forceinline__ double abs_b(double x) {
+  return __hiloint2double(__double2hiint(x) & 0x7fffffff, __double2loint(x));
+}
+__device__ __forceinline__ float abs_b(float x) { return __int_as_float(__float_as_int(x) & 0x7fffffff); }
+__device__ __forceinline__ bool iszero_b(double x) {
+  return ((__double2hiint(x) & 0x7fffffff) | __double2loint(x)) == 0;
+}
+__device__ __forceinline__ bool iszero_b(float x) { return (__float_as_int(x) & 0x7fffffff) == 0; }
+// fmax(x, 0) up to the sign of a zero result: 0 for negative or NaN x
+__device__ __forceinline__ double max0_b(double x) { return (__double2hiint(x) < 0 || isnan_b(x)) ? 0.0 : x; }
+__device__ __forceinline__ float max0_b(float x) {
+  int i = __float_as_int(x);
+  return (i < 0 || (i & 0x7fffffff) > 0x7f800000) ? 0.0f : x;
+}
+// The reference's minmod pair T(0.5) * (sign(a) + sign(b)) * min(|a|, |b|) for non-NaN a, b:
+// +min when both are positive, -min when both are negative, a zero otherwise.
+__device__ __forceinline__ double mm2(double a, double b) {
+  const int ha = __double2hiint(a), hb = __double2hiint(b);
+  const bool nz = !iszero_b(a) && !iszero_b(b);
+  const double m = fmin(abs_b(a), abs_b(b));
+  const bool same = (ha ^ hb) >= 0;
+  return (same && nz) ? (ha < 0 ? -m : m) : 0.0;
+}
+__device__ __forceinline__ float mm2(float a, float b) {
+  const int ia = __float_as_int(a), ib = __float_as_int(b);
+  const bool nz = (ia & 0x7fffffff) != 0 && (ib & 0x7fffffff) != 0;
+  const float m = fminf(abs_b(a), abs_b(b));
+  return ((ia ^ ib) >= 0 && nz) ? (ia < 0 ? -m : m) : 0.0f;
 }
 
 // sycl::sign: 1, -1, +-0 for +-0, 0 for NaN
@@ -59,29 +110,55 @@ __device__ __forceinline__ float sfabs(float x) { return fabsf(x); }
 template <typename T> __device__ __forceinline__ T add_tangential(T b, T t) {
   return finite_(t) ? b : Lim<T>::nan();
 }
+// Same for t = hd * s without forming the product: for |s| < 2^1000 and hd < 2^20 the
+// product is finite; beyond that (or for a non-finite s) the product decides.
+__device__ __forceinline__ double add_tangential_s(double b, double hd, double s) {
+  const unsigned e = (unsigned(__double2hiint(s)) >> 20) & 0x7ffu;
+  if (e < 1023u + 1000u) return b;
+  return finite_(hd * s) ? b : Lim<double>::nan();
+}
+__device__ __forceinline__ float add_tangential_s(float b, float hd, float s) {
+  return finite_(hd * s) ? b : Lim<float>::nan();
+}
+
+// Out-of-line IEEE division: the rare operands outside the range where the correction below
+// is exact (zero, subnormal, huge, inf, NaN). Kept out of line so the common path is not
+// predicated with a full division sequence.
+static __device__ __noinline__ double div_slow(double x, double d) { return x / d; }
 
 // Division by a launch-constant divisor d with rd = RN(1/d).
 struct DivD {
   double d, rd;
   __device__ __forceinline__ double operator()(double x) const {
-    long long e = (__double_as_longlong(x) >> 52) & 0x7ff;  // biased exponent
-    if (e < 1023 - 900 || e > 1023 + 900) return x / d;     // zero, tiny, huge, inf, NaN
+    const unsigned e = (unsigned(__double2hiint(x)) >> 20) & 0x7ffu;  // biased exponent
+    if (e - (1023u - 900u) > 1800u) return div_slow(x, d);         // outside [2^-900, 2^901)
     double q0 = x * rd;
     double r = fma(-q0, d, x);
     return fma(r, rd, q0);
   }
 };
+// Division by a power of two d = 2^k: x * 2^-k is the same real number as x / 2^k, so the
+// two round identically (subnormal, zero, inf and NaN results included): one multiply.
+struct DivP2 {
+  double rd;
+  __device__ __forceinline__ double operator()(double x) const { return x * rd; }
+};
+// FP32 path (not held to bit parity): multiply by the rounded reciprocal.
 struct DivF {
-  float d, rd;
-  __device__ __forceinline__ float operator()(float x) const { return __fdiv_rn(x, d); }
+  float rd;
+  __device__ __forceinline__ float operator()(float x) const { return x * rd; }
 };
 template <typename T> struct DivC;
 template <> struct DivC<double> { using type = DivD; };
 template <> struct DivC<float> { using type = DivF; };
 template <typename T> using Div = typename DivC<T>::type;
+// divider for the mesh spacing: exact power-of-two multiply when P2, else the general one
+template <typename T, bool P2> struct DivXC { using type = Div<T>; };
+template <> struct DivXC<double, true> { using type = DivP2; };
+template <typename T, bool P2> using DivX = typename DivXC<T, P2>::type;
 
 __device__ __forceinline__ DivD make_div(double d) { return DivD{d, 1.0 / d}; }
-__device__ __forceinline__ DivF make_divf(float d) { return DivF{d, 1.0f / d}; }
+__device__ __forceinline__ DivF make_divf(float d) { return DivF{1.0f / d}; }
 
 // ---------------------------------------------------------------------------------------
 // Minmod3 slope, theta = 2 (src/SpatialDerivative/Minmod3.hpp:22-84) on a uniform axis of
@@ -90,27 +167,38 @@ __device__ __forceinline__ DivF make_divf(float d) { return DivF{d, 1.0f / d}; }
 // theta*(a-b)/d and (r-l)/(2d) are formed as 2*((a-b)/d) and ((r-l)/d)*0.5, which are
 // exact power-of-two rescalings of the same correctly rounded quotient.
 // ---------------------------------------------------------------------------------------
+// Minmod3 from the difference quotients of a uniform axis: qL = (Uc-Ul)/d, qR = (Ur-Uc)/d,
+// qC = (Ur-Ul)/d. Two-sided: lhs = 2 qL, rhs = 2 qR, central = qC/2; one-sided: the missing
+// difference is NaN and the central difference uses U_l = U_c, so central = the present
+// quotient. The pair minmods follow Minmod3.hpp:66-80 including the NaN rules (a NaN outer
+// difference returns the central one; a NaN central one gives sign(outer)/2 * |outer|).
 template <typename T>
-__device__ __forceinline__ T minmod3(T Ul, bool hasL, T Uc, bool hasR, T Ur, const Div<T>& div) {
+__device__ __forceinline__ T minmod3q(T qL, bool hasL, T qR, bool hasR, T qC) {
   T outer, central;
   if (hasL && hasR) {
-    T lhs = T(2) * div(Uc - Ul);
-    T rhs = T(2) * div(Ur - Uc);
-    central = div(Ur - Ul) * T(0.5);
-    if (lhs != lhs) outer = rhs;
-    else if (rhs != rhs) outer = lhs;
-    else outer = T(0.5) * (ssign(lhs) + ssign(rhs)) * smin(sfabs(lhs), sfabs(rhs));
-  } else if (hasR) {  // west/north edge: lhs difference undefined
-    outer = T(2) * div(Ur - Uc);
-    central = div(Ur - Uc);
+    T lhs = T(2) * qL, rhs = T(2) * qR;
+    central = qC * T(0.5);
+    outer = isnan_b(lhs) ? rhs : (isnan_b(rhs) ? lhs : mm2(lhs, rhs));
+  } else if (hasR) {
+    outer = T(2) * qR;
+    central = qR;
   } else if (hasL) {
-    outer = T(2) * div(Uc - Ul);
-    central = div(Uc - Ul);
+    outer = T(2) * qL;
+    central = qL;
   } else {
     return T(0);
   }
-  if (outer != outer) return central;
-  return T(0.5) * (ssign(outer) + ssign(central)) * smin(sfabs(outer), sfabs(central));
+  if (isnan_b(outer)) return central;
+  if (isnan_b(central)) return T(0.5) * outer;
+  return mm2(outer, central);
+}
+
+template <typename T, typename DV>
+__device__ __forceinline__ T minmod3(T Ul, bool hasL, T Uc, bool hasR, T Ur, const DV& div) {
+  T qL = hasL ? div(Uc - Ul) : T(0);
+  T qR = hasR ? div(Ur - Uc) : T(0);
+  T qC = (hasL && hasR) ? div(Ur - Ul) : T(0);
+  return minmod3q<T>(qL, hasL, qR, hasR, qC);
 }
 
 // Cell values and slopes needed by a face.
@@ -127,9 +215,8 @@ template <typename T> struct FaceF { T h, u, v, z; };
 // d = dx or dy; hd = 0.5*d. Returns the branch code (1, 2.25, 2.75, 3, 4, or 0 when the
 // face borders coded-out cells).
 // ---------------------------------------------------------------------------------------
-template <typename T, int DIR>
-__device__ __forceinline__ T face_flux(CellV<T> L, CellV<T> R, int edge, T hd, const Div<T>& divd,
-                                       FaceF<T>& F) {
+template <typename T, int DIR, typename DV>
+__device__ __forceinline__ T face_flux(CellV<T> L, CellV<T> R, int edge, T hd, const DV& divd, FaceF<T>& F) {
   const T g = T(kG);
   const T zb_L0 = L.z, zb_R0 = R.z;
   T zb_L = zb_L0, zb_R = zb_R0;
@@ -178,41 +265,60 @@ __device__ __forceinline__ T face_flux(CellV<T> L, CellV<T> R, int edge, T hd, c
   // MUSCL reconstruction, FluxKernel.cpp:161-187. For DIR 0 the reference adds the
   // normal term then the tangential (*0) term; for DIR 1 the tangential term first. Both
   // orders give b + n (a finite exact zero never changes a non-zero sum).
-  T zb_m = add_tangential(zb_L + hd * dzn_L, hd * dzt_L);
-  T h_m = add_tangential(h_L + hd * dhn_L, hd * dht_L);
-  T un_m = add_tangential(un_L + hd * dunn_L, hd * dunt_L);
-  T ut_m = add_tangential(ut_L + hd * dutn_L, hd * dutt_L);
-  T zb_p = add_tangential(zb_R - hd * dzn_R, hd * dzt_R);
-  T h_p = add_tangential(h_R - hd * dhn_R, hd * dht_R);
-  T un_p = add_tangential(un_R - hd * dunn_R, hd * dunt_R);
-  T ut_p = add_tangential(ut_R - hd * dutn_R, hd * dutt_R);
+  T zb_m = add_tangential_s(zb_L + hd * dzn_L, hd, dzt_L);
+  T h_m = add_tangential_s(h_L + hd * dhn_L, hd, dht_L);
+  T un_m = add_tangential_s(un_L + hd * dunn_L, hd, dunt_L);
+  T ut_m = add_tangential_s(ut_L + hd * dutn_L, hd, dutt_L);
+  T zb_p = add_tangential_s(zb_R - hd * dzn_R, hd, dzt_R);
+  T h_p = add_tangential_s(h_R - hd * dhn_R, hd, dht_R);
+  T un_p = add_tangential_s(un_R - hd * dunn_R, hd, dunt_R);
+  T ut_p = add_tangential_s(ut_R - hd * dutn_R, hd, dutt_R);
 
   T zb_f = sfmax(zb_m, zb_p);
   T y_m = zb_m + h_m;
   T y_p = zb_p + h_p;
-  h_m = sfmax(h_m, T(0));
-  h_p = sfmax(h_p, T(0));
+  h_m = max0_b(h_m);
+  h_p = max0_b(h_p);
   // momentum components: normal gets 0.5*spd and the +-g*h term; tangential gets
   // 1.0*spd and a g*h*0 term (NaN only for infinite h).
+  // The reference's branch chain (FluxKernel.cpp:208-289): 1 if both levels are above the
+  // face bed, else 2 if both are at or below it, else 3 if the left one is above, else 4.
+  // With a NaN level neither comparison holds, which selects branch 4.
+  const bool both = (y_m > zb_f) && (y_p > zb_f);
+  const bool dry2 = !both && (y_m <= zb_f) && (y_p <= zb_f);
+  const bool wm = !both && !dry2 && (y_m > zb_f);  // branch 3: left side only
   T branch;
   T Fn, Ft;
-  if (y_m > zb_f && y_p > zb_f) {
-    branch = T(1);
-    T c_m = ssqrt(g * h_m), c_p = ssqrt(g * h_p);
-    T spd_m = add_tangential(un_m, ut_m), spd_p = add_tangential(un_p, ut_p);
-    T hf_m = h_m * spd_m, hf_p = h_p * spd_p;
-    T gh_m = g * h_m, gh_p = g * h_p;
-    T nf_m = un_m * (T(0.5) * spd_m) + gh_m;
-    T nf_p = un_p * (T(0.5) * spd_p) - gh_p;
-    T tf_m = add_tangential(ut_m * spd_m, gh_m);
-    T tf_p = add_tangential(ut_p * spd_p, gh_p);
-    T a = sfmax(sfabs(spd_p + ssign(spd_p) * c_p), sfabs(spd_m + ssign(spd_m) * c_m));
-    T ha = T(0.5) * a;
-    F.h = T(0.5) * (hf_p + hf_m) - ha * (h_p - h_m);
-    Fn = T(0.5) * (nf_p + nf_m) - ha * (un_p - un_m);
-    Ft = T(0.5) * (tf_p + tf_m) - ha * (ut_p - ut_m);
-    F.z = (zb_m - zb_p) * g;
-  } else if (y_m <= zb_f && y_p <= zb_f) {
+  if (!dry2) {
+    // Branches 1 (both sides above the face bed), 3 (left only) and 4 (right only)
+    // evaluated without divergence: each side's terms, then the branch's own combination of
+    // them selected per face.
+    const T c_m = ssqrt(g * h_m), c_p = ssqrt(g * h_p);
+    const T spd_m = add_tangential(un_m, ut_m), spd_p = add_tangential(un_p, ut_p);
+    const T hf_m = h_m * spd_m, hf_p = h_p * spd_p;
+    const T gh_m = g * h_m, gh_p = g * h_p;
+    const T nf_m = un_m * (T(0.5) * spd_m) + gh_m;
+    const T nf_p = both ? un_p * (T(0.5) * spd_p) - gh_p : un_p * (T(0.5) * spd_p) + gh_p;
+    const T tf_m = add_tangential(ut_m * spd_m, gh_m);
+    const T tf_p = add_tangential(ut_p * spd_p, gh_p);
+    // |spd + sign(spd) c| = |spd| + c, or 0 when spd is an exact zero (sign(0) = 0)
+    const T a_m = iszero_b(spd_m) ? T(0) : abs_b(spd_m) + c_m;
+    const T a_p = iszero_b(spd_p) ? T(0) : abs_b(spd_p) + c_p;
+    const T a = both ? sfmax(a_p, a_m) : (wm ? a_m : a_p);
+    const T ha = T(0.5) * a;
+    const T Sh = both ? hf_p + hf_m : (wm ? hf_m : hf_p);
+    const T Dh = both ? h_p - h_m : (wm ? -h_m : h_p);
+    const T Sn = both ? nf_p + nf_m : (wm ? nf_m : nf_p);
+    const T Dn = both ? un_p - un_m : (wm ? -un_m : un_p);
+    const T St = both ? tf_p + tf_m : (wm ? tf_m : tf_p);
+    const T Dt = both ? ut_p - ut_m : (wm ? -ut_m : ut_p);
+    F.h = T(0.5) * Sh - ha * Dh;
+    Fn = T(0.5) * Sn - ha * Dn;
+    Ft = T(0.5) * St - ha * Dt;
+    F.z = both ? (zb_m - zb_p) * g : divd(wm ? h_p : h_m);
+    branch = both ? T(1) : (wm ? T(3) : T(4));
+  } else {
+    // branch 2: both water levels at or below the face bed (FluxKernel.cpp:235-254)
     F.h = T(0);
     if (zb_p > zb_m) {
       branch = T(2.25);
@@ -227,34 +333,6 @@ __device__ __forceinline__ T face_flux(CellV<T> L, CellV<T> R, int edge, T hd, c
       Ft = T(-0.5) * (gh * T(0));
       F.z = h_p * T(0.5) * g;
     }
-  } else if (y_m > zb_f) {
-    branch = T(3);
-    T c_m = ssqrt(g * h_m);
-    T spd_m = add_tangential(un_m, ut_m);
-    T hf_m = h_m * spd_m;
-    T gh_m = g * h_m;
-    T nf_m = un_m * (T(0.5) * spd_m) + gh_m;
-    T tf_m = add_tangential(ut_m * spd_m, gh_m);
-    T a = sfabs(spd_m + ssign(spd_m) * c_m);
-    T ha = T(0.5) * a;
-    F.h = T(0.5) * hf_m - ha * (-h_m);
-    Fn = T(0.5) * nf_m - ha * (-un_m);
-    Ft = T(0.5) * tf_m - ha * (-ut_m);
-    F.z = divd(h_p);
-  } else {
-    branch = T(4);
-    T c_p = ssqrt(g * h_p);
-    T spd_p = add_tangential(un_p, ut_p);
-    T hf_p = h_p * spd_p;
-    T gh_p = g * h_p;
-    T nf_p = un_p * (T(0.5) * spd_p) + gh_p;
-    T tf_p = add_tangential(ut_p * spd_p, gh_p);
-    T a = sfabs(spd_p + ssign(spd_p) * c_p);
-    T ha = T(0.5) * a;
-    F.h = T(0.5) * hf_p - ha * h_p;
-    Fn = T(0.5) * nf_p - ha * un_p;
-    Ft = T(0.5) * tf_p - ha * ut_p;
-    F.z = divd(h_m);
   }
   if (DIR == 0) { F.u = Fn; F.v = Ft; }
   else { F.u = Ft; F.v = Fn; }
@@ -262,8 +340,9 @@ __device__ __forceinline__ T face_flux(CellV<T> L, CellV<T> R, int edge, T hd, c
 }
 
 // Per-launch scalars of one stage evaluation (update_dUdt arguments and forcing).
-template <typename T> struct CellCtx {
-  Div<T> divx, divy, divdt, divL;
+template <typename T, typename DX = Div<T>> struct CellCtx {
+  DX divx, divy;
+  Div<T> divdt, divL;
   T dt;          // timestep (TT=double for T=double)
   double dt_d, tsub_d;
   int manning, rain_mode, head_first;
@@ -271,8 +350,8 @@ template <typename T> struct CellCtx {
 
 // Depth-rate of the discharge boundary (DischargeBoundarySourceTerm.cpp:47-66) for
 // boundary values q0, q1 at depth h; returns 0 when the cell is skipped.
-template <typename T>
-__device__ __forceinline__ T discharge_rate(T q0, T q1, T h, const CellCtx<T>& c, bool& applied) {
+template <typename T, typename CC>
+__device__ __forceinline__ T discharge_rate(T q0, T q1, T h, const CC& c, bool& applied) {
   applied = false;
   if (q0 != T(0) || q1 != T(0)) {
     applied = true;
@@ -289,8 +368,8 @@ __device__ __forceinline__ T discharge_rate(T q0, T q1, T h, const CellCtx<T>& c
 
 // HeadBoundarySourceKernel (HeadBoundarySourceTerm.cpp:47-65): target depth for the
 // boundary values h0, h1; the caller assigns dhdt = (target - h) / dt.
-template <typename T>
-__device__ __forceinline__ T head_target(T h0, T h1, const CellCtx<T>& c) {
+template <typename T, typename CC>
+__device__ __forceinline__ T head_target(T h0, T h1, const CC& c) {
   T dhb = c.divL(h1 - h0);
   T hnow = h0 + T(c.tsub_d) * dhb;
   T hnext = hnow + c.dt * dhb;
@@ -303,8 +382,8 @@ __device__ __forceinline__ T head_target(T h0, T h1, const CellCtx<T>& c) {
 __device__ __forceinline__ double pow43_(double x) { return sv_math::pow43(x); }
 __device__ __forceinline__ float pow43_(float x) { return x * cbrtf(x); }
 
-template <typename T>
-__device__ __forceinline__ void manning_apply(T h, T u, T v, T ns, T nd, T ds, T dd, const CellCtx<T>& c,
+template <typename T, typename CC>
+__device__ __forceinline__ void manning_apply(T h, T u, T v, T ns, T nd, T ds, T dd, const CC& c,
                                               T& du, T& dv, T* n_out, T* sf_out) {
   T n;
   if (ns == nd) {

@@ -1,22 +1,33 @@
 // sv_inst.cuh -- launcher definitions, included once per value type by sv_f64.cu / sv_f32.cu
 // with SV_T defined to the value type.
 #pragma once
+#include <cmath>
+
 #include "sv_launch.h"
 
 namespace svk {
 
-template <typename T, int TX, int TY> static cudaError_t launch_stage_t(const StageParams<T>& P, cudaStream_t s) {
+// dx and dy both powers of two: the mesh divisions are exact multiplies
+inline bool pow2_mesh(double dx, double dy) {
+  int e;
+  return std::frexp(dx, &e) == 0.5 && std::frexp(dy, &e) == 0.5;
+}
+
+template <typename T, int TX, int TY, bool P2> static cudaError_t launch_stage_p(const StageParams<T>& P, cudaStream_t s) {
   using SM = StageSmem<T, TX, TY>;
   static bool attr_set = false;
   if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(stage_kernel<T, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(stage_kernel<T, TX, TY, P2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          int(sizeof(SM)));
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
   dim3 grid((P.nx + TX - 1) / TX, (P.ny + TY - 1) / TY);
-  stage_kernel<T, TX, TY><<<grid, TX * TY, sizeof(SM), s>>>(P);
+  stage_kernel<T, TX, TY, P2><<<grid, TX * TY, sizeof(SM), s>>>(P);
   return cudaGetLastError();
+}
+template <typename T, int TX, int TY> static cudaError_t launch_stage_t(const StageParams<T>& P, cudaStream_t s) {
+  return pow2_mesh(P.dx, P.dy) ? launch_stage_p<T, TX, TY, true>(P, s) : launch_stage_p<T, TX, TY, false>(P, s);
 }
 
 template <> size_t stage_smem_bytes<SV_T>(int tile) {
@@ -35,6 +46,35 @@ template <> cudaError_t launch_stage<SV_T>(const StageParams<SV_T>& P, int tile,
     case 2: return launch_stage_t<SV_T, 64, 4>(P, s);
     default: return launch_stage_t<SV_T, 32, 16>(P, s);
   }
+}
+
+template <typename T, int TY, int MINB> static cudaError_t launch_sweep_t(const StageParams<T>& P, int variant,
+                                                                          cudaStream_t s) {
+  constexpr int WPB = 4;
+  const long long ntiles = variant_partials(variant, P.nx, P.ny);
+  dim3 block(32, WPB);
+  dim3 grid(unsigned((ntiles + WPB - 1) / WPB));
+  if (pow2_mesh(P.dx, P.dy)) sweep_kernel<T, TY, WPB, MINB, true><<<grid, block, 0, s>>>(P);
+  else sweep_kernel<T, TY, WPB, MINB, false><<<grid, block, 0, s>>>(P);
+  return cudaGetLastError();
+}
+
+template <> cudaError_t launch_variant<SV_T>(const StageParams<SV_T>& P, int variant, cudaStream_t s) {
+  switch (variant) {
+    case 4: return launch_sweep_t<SV_T, 16, 1>(P, variant, s);
+    case 5: return launch_sweep_t<SV_T, 32, 1>(P, variant, s);
+    case 6: return launch_sweep_t<SV_T, 64, 1>(P, variant, s);
+    case 7: return launch_sweep_t<SV_T, 32, 3>(P, variant, s);
+    case 8: return launch_sweep_t<SV_T, 32, 4>(P, variant, s);
+    default: return launch_stage<SV_T>(P, variant, s);
+  }
+}
+
+template <> cudaError_t launch_bed_slopes<SV_T>(const SV_T* z, int nx, int ny, double dx, double dy, SV_T* zx,
+                                                SV_T* zy, cudaStream_t s) {
+  long long n = (long long)nx * ny;
+  bed_slopes_kernel<SV_T><<<unsigned((n + 255) / 256), 256, 0, s>>>(z, nx, ny, dx, dy, zx, zy);
+  return cudaGetLastError();
 }
 
 template <typename T, int TX, int TY>

@@ -67,6 +67,7 @@ template <typename T> struct StageParams {
   T* Kout[3];            // k_s (M_STOREK / M_DEBUGK)
   const T* Kin[4][3];    // stored k_j, j < s (M_STOREK)
   const T* z;
+  const T* zx; const T* zy;   // bed slopes dz/dx, dz/dy (Constants.cpp:39-40), precomputed
   const T* man_p[4];     // per-cell n_shallow, n_deep, d_shallow, d_deep, or nullptr
   T man_s[4];            // uniform values where man_p is nullptr
   const DevForcing* fc;  // per-step boundary values
@@ -134,12 +135,16 @@ template <int NT> __device__ double block_min(double v, double* red) {
 template <typename T> __device__ __forceinline__ Div<T> mkdiv(double d);
 template <> __device__ __forceinline__ Div<double> mkdiv<double>(double d) { return make_div(d); }
 template <> __device__ __forceinline__ Div<float> mkdiv<float>(double d) { return make_divf(float(d)); }
+template <typename DV> struct MkDivX;
+template <> struct MkDivX<DivD> { __device__ static DivD make(double d) { return make_div(d); } };
+template <> struct MkDivX<DivP2> { __device__ static DivP2 make(double d) { return DivP2{1.0 / d}; } };
+template <> struct MkDivX<DivF> { __device__ static DivF make(double d) { return make_divf(float(d)); } };
 
 // Per-cell dU/dt of one stage (TemporalDerivativeKernel.cpp:53-98, then the source terms
 // and boundaries in configuration order, Solver.cpp:97-113). fw/fe/fs/fn are the four face
 // fluxes; returns the rain rate added and the depth rate removed by the head assignment.
-template <typename T>
-__device__ __forceinline__ void cell_dudt(const StageParams<T>& P, const DevForcing& fc, const CellCtx<T>& c,
+template <typename T, typename CC>
+__device__ __forceinline__ void cell_dudt(const StageParams<T>& P, const DevForcing& fc, const CC& c,
                                           long long g, int gx,
                                           int gy, T h, T u, T v, T dhdx, T dhdy, T dzdx, T dzdy,
                                           const FaceF<T>& fw, const FaceF<T>& fe, const FaceF<T>& fs,
@@ -202,6 +207,84 @@ __device__ __forceinline__ void cell_dudt(const StageParams<T>& P, const DevForc
   kh = dhdt; ku = dudt; kv = dvdt;
 }
 
+// One cell of one stage after its four face fluxes are known: dU/dt, then the Runge-Kutta
+// combination (RungeKutta.hpp:377-388) and, on the last stage, the CFL quantity and volume.
+template <typename T, typename CC>
+__device__ __forceinline__ void finish_cell(const StageParams<T>& P, const DevForcing& fc, const CC& c,
+                                            long long g, int gx, int gy, T h, T u, T v, T dhdx, T dhdy, T dzdx,
+                                            T dzdy, const FaceF<T>& fw, const FaceF<T>& fe, const FaceF<T>& fs,
+                                            const FaceF<T>& fn, bool first, bool last, int cur, double dt_d,
+                                            double& rain, double& removed, double& xcfl, double& xcfl_min,
+                                            double& vol) {
+  T kh, ku, kv;
+  double r_, o_;
+  cell_dudt<T>(P, fc, c, g, gx, gy, h, u, v, dhdx, dhdy, dzdx, dzdy, fw, fe, fs, fn, kh, ku, kv, r_, o_,
+               (T*)nullptr, (T*)nullptr);
+  rain += r_;
+  removed += o_;
+  if (P.mode & (M_STOREK | M_DEBUGK)) {
+    P.Kout[0][g] = kh; P.Kout[1][g] = ku; P.Kout[2][g] = kv;
+  }
+  if (P.mode & M_DEBUGK) return;
+  const int st = P.stage;
+  T* A[3] = {P.S[cur ^ 1][0], P.S[cur ^ 1][1], P.S[cur ^ 1][2]};
+  const T* U0[3] = {P.S[cur][0], P.S[cur][1], P.S[cur][2]};
+  T k[3] = {kh, ku, kv};
+  T out[3];
+  if (P.mode & M_ACC) {
+    // diagonal tableau: Y_{s+1} = U0 + k_s*a and acc += k_s*b, in the reference's
+    // left-to-right order (RungeKutta.hpp:377-388); the skipped zero-coefficient terms
+    // k_j*0 (j < s) can only contribute a NaN, which happens exactly when some earlier
+    // k_j is not finite, i.e. when acc is not finite while U0 is.
+    const T cB = T(P.b[st] * dt_d);
+    T u0v[3], accv[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      u0v[f] = first ? (f == 0 ? h : (f == 1 ? u : v)) : ld(U0[f], g);
+      accv[f] = first ? u0v[f] : ld(A[f], g);
+    }
+    if (!last) {
+      const T cA = T(P.a_next[st] * dt_d);
+#pragma unroll
+      for (int f = 0; f < 3; ++f) {
+        T y = u0v[f] + k[f] * cA;
+        if (!first && finite_(u0v[f]) && !finite_(accv[f])) y = Lim<T>::nan();
+        P.Yout[f][g] = y;
+      }
+    }
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      out[f] = accv[f] + k[f] * cB;
+      A[f][g] = out[f];
+    }
+  } else {
+    // general tableau: Y_{s+1} = ((U0 + k_0 c_0) + k_1 c_1) + ... with stored k_j
+    T u0v[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) u0v[f] = first ? (f == 0 ? h : (f == 1 ? u : v)) : ld(U0[f], g);
+    const double* coef = last ? P.b : P.a_next;
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      T y = u0v[f];
+      for (int j = 0; j < st; ++j) y = y + ld(P.Kin[j][f], g) * T(coef[j] * dt_d);
+      y = y + k[f] * T(coef[st] * dt_d);
+      out[f] = y;
+      if (last) A[f][g] = y;
+      else P.Yout[f][g] = y;
+    }
+  }
+  if (last) {
+    // SaintVenantState::max_control_number (State.cpp:204-228) on U_[N]: per cell
+    // x = (|u|+c)/dx + (|v|+c)/dy; cn = max(dt*x) = dt*max(x) (rounding is monotone)
+    T hh = sfmax(out[0], T(0));
+    T cc = ssqrt(T(kG) * hh);
+    T xx = c.divx(sfabs(out[1]) + cc) + c.divy(sfabs(out[2]) + cc);
+    xcfl = nmax(xcfl, double(xx));
+    xcfl_min = nmin(xcfl_min, double(xx));
+    vol += double(out[0]) * P.cell_area;
+  }
+}
+
 template <typename T, int TX, int TY>
 struct StageSmem {
   static constexpr int RX = TX + 4, RY = TY + 4;  // values with a 2-cell halo
@@ -213,8 +296,9 @@ struct StageSmem {
   double red[TX * TY / 32];
 };
 
-template <typename T, int TX, int TY>
+template <typename T, int TX, int TY, bool P2>
 __global__ void __launch_bounds__(TX * TY) stage_kernel(const StageParams<T> P) {
+  using DX = DivX<T, P2>;
   using SM = StageSmem<T, TX, TY>;
   constexpr int NT = TX * TY;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -248,7 +332,7 @@ __global__ void __launch_bounds__(TX * TY) stage_kernel(const StageParams<T> P) 
   }
   __syncthreads();
 
-  const Div<T> divx = mkdiv<T>(P.dx), divy = mkdiv<T>(P.dy);
+  const DX divx = MkDivX<DX>::make(P.dx), divy = MkDivX<DX>::make(P.dy);
   // phase 2: Minmod3 slopes (State.cpp:176-193, Constants.cpp:39-40) on the tile + ring
   for (int i = tid; i < SM::SX * SM::SY; i += NT) {
     int sx = i % SM::SX, sy = i / SM::SX;
@@ -305,12 +389,11 @@ __global__ void __launch_bounds__(TX * TY) stage_kernel(const StageParams<T> P) 
   const int tx = tid % TX, ty = tid / TX;
   const int gx = x0 + tx, gy = y0 + ty;
   const bool valid = gx < nx && gy < ny;
-  double rain = 0.0, removed = 0.0, xcfl = 0.0, xcfl_min = 0.0, vol = 0.0;
+  double rain = 0.0, removed = 0.0, xcfl = 0.0, xcfl_min = 1.0 / 0.0, vol = 0.0;
   const bool last = P.mode & M_LAST;
-  if (!valid) xcfl_min = 1.0 / 0.0;
   if (valid) {
     const long long g = (long long)gy * nx + gx;
-    CellCtx<T> c;
+    CellCtx<T, DX> c;
     c.divx = divx; c.divy = divy;
     c.divdt = mkdiv<T>(dt_d);
     c.divL = mkdiv<T>(P.L);
@@ -323,72 +406,8 @@ __global__ void __launch_bounds__(TX * TY) stage_kernel(const StageParams<T> P) 
     FaceF<T> fs{s.fyf[0][ty][tx], s.fyf[1][ty][tx], s.fyf[2][ty][tx], s.fyf[3][ty][tx]};
     FaceF<T> fn{s.fyf[0][ty + 1][tx], s.fyf[1][ty + 1][tx], s.fyf[2][ty + 1][tx], s.fyf[3][ty + 1][tx]};
     const DevForcing fc = *P.fc;
-    T kh, ku, kv;
-    cell_dudt<T>(P, fc, c, g, gx, gy, h, u, v, s.slp[0][sy][sx], s.slp[4][sy][sx], s.slp[3][sy][sx],
-                 s.slp[7][sy][sx], fw, fe, fs, fn, kh, ku, kv, rain, removed, nullptr, nullptr);
-
-    if (P.mode & (M_STOREK | M_DEBUGK)) {
-      P.Kout[0][g] = kh; P.Kout[1][g] = ku; P.Kout[2][g] = kv;
-    }
-    if (!(P.mode & M_DEBUGK)) {
-      const int st = P.stage;
-      T* A[3] = {P.S[cur ^ 1][0], P.S[cur ^ 1][1], P.S[cur ^ 1][2]};
-      const T* U0[3] = {P.S[cur][0], P.S[cur][1], P.S[cur][2]};
-      T k[3] = {kh, ku, kv};
-      T out[3];
-      if (P.mode & M_ACC) {
-        // diagonal tableau: Y_{s+1} = U0 + k_s*a and acc += k_s*b, in the reference's
-        // left-to-right order (RungeKutta.hpp:377-388); the skipped zero-coefficient terms
-        // k_j*0 (j < s) can only contribute a NaN, which happens exactly when some earlier
-        // k_j is not finite, i.e. when acc is not finite while U0 is.
-        const T cB = T(P.b[st] * dt_d);
-        T u0v[3], accv[3];
-#pragma unroll
-        for (int f = 0; f < 3; ++f) {
-          u0v[f] = first ? (f == 0 ? h : (f == 1 ? u : v)) : ld(U0[f], g);
-          accv[f] = first ? u0v[f] : ld(A[f], g);
-        }
-        if (!last) {
-          const T cA = T(P.a_next[st] * dt_d);
-#pragma unroll
-          for (int f = 0; f < 3; ++f) {
-            T y = u0v[f] + k[f] * cA;
-            if (!first && finite_(u0v[f]) && !finite_(accv[f])) y = Lim<T>::nan();
-            P.Yout[f][g] = y;
-          }
-        }
-#pragma unroll
-        for (int f = 0; f < 3; ++f) {
-          out[f] = accv[f] + k[f] * cB;
-          A[f][g] = out[f];
-        }
-      } else {
-        // general tableau: Y_{s+1} = ((U0 + k_0 c_0) + k_1 c_1) + ... with stored k_j
-        T u0v[3];
-#pragma unroll
-        for (int f = 0; f < 3; ++f) u0v[f] = first ? (f == 0 ? h : (f == 1 ? u : v)) : ld(U0[f], g);
-        const double* coef = last ? P.b : P.a_next;
-#pragma unroll
-        for (int f = 0; f < 3; ++f) {
-          T y = u0v[f];
-          for (int j = 0; j < st; ++j) y = y + ld(P.Kin[j][f], g) * T(coef[j] * dt_d);
-          y = y + k[f] * T(coef[st] * dt_d);
-          out[f] = y;
-          if (last) A[f][g] = y;
-          else P.Yout[f][g] = y;
-        }
-      }
-      if (last) {
-        // SaintVenantState::max_control_number (State.cpp:204-228) on U_[N]: per cell
-        // x = (|u|+c)/dx + (|v|+c)/dy; cn = max(dt*x) = dt*max(x) (rounding is monotone)
-        T hh = sfmax(out[0], T(0));
-        T cc = ssqrt(T(kG) * hh);
-        T xx = divx(sfabs(out[1]) + cc) + divy(sfabs(out[2]) + cc);
-        xcfl = double(xx);
-        xcfl_min = xcfl;
-        vol = double(out[0]) * P.cell_area;
-      }
-    }
+    finish_cell<T>(P, fc, c, g, gx, gy, h, u, v, s.slp[0][sy][sx], s.slp[4][sy][sx], s.slp[3][sy][sx],
+                   s.slp[7][sy][sx], fw, fe, fs, fn, first, last, cur, dt_d, rain, removed, xcfl, xcfl_min, vol);
   }
   if (last && !(P.mode & M_DEBUGK)) {
     double mx = block_max<NT>(xcfl, s.red);
@@ -410,6 +429,220 @@ __global__ void __launch_bounds__(TX * TY) stage_kernel(const StageParams<T> P) 
       P.part[(4 + 2LL * P.stage) * P.nblk + b] = os;
     }
   }
+}
+
+// ---------------------------------------------------------------------------------------
+// Column-sweep stage kernel. One warp owns a strip of 32 columns (28 output columns plus a
+// 2-column halo on each side) and marches down TY output rows. Each lane holds its column's
+// last three rows of (h, u, v, z, dz/dx, dz/dy) and two rows of slopes in registers; x
+// neighbours come from warp shuffles, y neighbours from the rolling window. Every face
+// flux and every difference quotient is computed once and reused by both cells / both
+// slopes that need it, and there is no block-level barrier. The arithmetic per face and
+// per cell is the same function as in the tiled kernel.
+// ---------------------------------------------------------------------------------------
+constexpr unsigned kFull = 0xffffffffu;
+template <typename T> __device__ __forceinline__ T up1(T v) { return __shfl_up_sync(kFull, v, 1); }
+template <typename T> __device__ __forceinline__ T dn1(T v) { return __shfl_down_sync(kFull, v, 1); }
+
+// Minmod3 (Minmod3.hpp:22-84) from difference quotients qL = (Uc-Ul)/d, qR = (Ur-Uc)/d and
+// qC = (Ur-Ul)/d of a uniform axis (see minmod3 in sv_device.cuh for the exactness notes).
+template <typename T>
+__device__ __forceinline__ T minmod3q(T qL, bool hasL, T qR, bool hasR, T qC) {
+  T outer, central;
+  if (hasL && hasR) {
+    T lhs = T(2) * qL, rhs = T(2) * qR;
+    central = qC * T(0.5);
+    if (lhs != lhs) outer = rhs;
+    else if (rhs != rhs) outer = lhs;
+    else outer = T(0.5) * (ssign(lhs) + ssign(rhs)) * smin(sfabs(lhs), sfabs(rhs));
+  } else if (hasR) {
+    outer = T(2) * qR;
+    central = qR;
+  } else if (hasL) {
+    outer = T(2) * qL;
+    central = qL;
+  } else {
+    return T(0);
+  }
+  if (outer != outer) return central;
+  return T(0.5) * (ssign(outer) + ssign(central)) * smin(sfabs(outer), sfabs(central));
+}
+
+template <typename T> struct RowV { T h, u, v, z, zx, zy; };
+template <typename T> struct SlopeV { T hx, ux, vx, hy, uy, vy; };
+
+template <typename T>
+__device__ __forceinline__ CellV<T> mkcell(const RowV<T>& r, const SlopeV<T>& s) {
+  CellV<T> c;
+  c.h = r.h; c.u = r.u; c.v = r.v; c.z = r.z;
+  c.dhdx = s.hx; c.dudx = s.ux; c.dvdx = s.vx; c.dzdx = r.zx;
+  c.dhdy = s.hy; c.dudy = s.uy; c.dvdy = s.vy; c.dzdy = r.zy;
+  return c;
+}
+template <typename T> __device__ __forceinline__ CellV<T> shfl_cell_up(const CellV<T>& a) {
+  CellV<T> c;
+  c.h = up1(a.h); c.u = up1(a.u); c.v = up1(a.v); c.z = up1(a.z);
+  c.dhdx = up1(a.dhdx); c.dudx = up1(a.dudx); c.dvdx = up1(a.dvdx); c.dzdx = up1(a.dzdx);
+  c.dhdy = up1(a.dhdy); c.dudy = up1(a.dudy); c.dvdy = up1(a.dvdy); c.dzdy = up1(a.dzdy);
+  return c;
+}
+template <typename T> __device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFull, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = nmax(v, __shfl_down_sync(kFull, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_min(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = nmin(v, __shfl_down_sync(kFull, v, o));
+  return v;
+}
+
+constexpr int kSweepOut = 28;  // output columns per warp
+
+template <typename T, int TY, int WPB, int MINB, bool P2>
+__global__ void __launch_bounds__(32 * WPB, MINB) sweep_kernel(const StageParams<T> P) {
+  using DX = DivX<T, P2>;
+  const Ctl* ctl = P.ctl;
+  if (ctl->done) return;
+  const int nx = P.nx, ny = P.ny;
+  const int tiles_x = (nx + kSweepOut - 1) / kSweepOut;
+  const long long ntiles = (long long)tiles_x * ((ny + TY - 1) / TY);
+  const long long gw = (long long)blockIdx.x * WPB + threadIdx.y;
+  if (gw >= ntiles) return;  // whole warp: no block-level synchronisation below
+  const int lane = threadIdx.x;
+  const int tile_x = int(gw % tiles_x), tile_y = int(gw / tiles_x);
+  const int gx = tile_x * kSweepOut - 2 + lane;
+  const int gxc = min(max(gx, 0), nx - 1);
+  const bool out_lane = lane >= 2 && lane < 2 + kSweepOut && gx < nx;
+  const bool wface_lane = lane >= 2 && lane <= 2 + kSweepOut && gx <= nx;
+  const bool hasW = gx > 0, hasE = gx < nx - 1;
+  const int y0 = tile_y * TY;
+
+  const int cur = ctl->cur;
+  const double dt_d = ctl->dt;
+  const double tsub = ctl->t_local + P.c_s * dt_d;
+  const bool first = P.mode & M_FIRST, last = P.mode & M_LAST;
+  const T* Yh = first ? P.S[cur][0] : P.Yin[0];
+  const T* Yu = first ? P.S[cur][1] : P.Yin[1];
+  const T* Yv = first ? P.S[cur][2] : P.Yin[2];
+  const DX divx = MkDivX<DX>::make(P.dx), divy = MkDivX<DX>::make(P.dy);
+  const T hdx = T(0.5) * T(P.dx), hdy = T(0.5) * T(P.dy);
+  CellCtx<T, DX> c;
+  c.divx = divx; c.divy = divy;
+  c.divdt = mkdiv<T>(dt_d);
+  c.divL = mkdiv<T>(P.L);
+  c.dt = T(dt_d); c.dt_d = dt_d; c.tsub_d = tsub;
+  c.manning = P.manning; c.rain_mode = P.rain_mode; c.head_first = P.head_first;
+  const DevForcing fc = *P.fc;
+
+  auto load_row = [&](int gy) {
+    const int r = min(max(gy, 0), ny - 1);
+    const long long g = (long long)r * nx + gxc;
+    RowV<T> v;
+    v.h = ld(Yh, g); v.u = ld(Yu, g); v.v = ld(Yv, g);
+    v.z = ld(P.z, g); v.zx = ld(P.zx, g); v.zy = ld(P.zy, g);
+    return v;
+  };
+
+  RowV<T> Rm{}, R0{}, Rp{};   // rows k-2, k-1, k
+  SlopeV<T> Sm{}, S0{};       // slopes of rows k-2, k-1
+  T fyA[3] = {}, fyB[3] = {};  // (U[k-1]-U[k-2])/dy, (U[k]-U[k-1])/dy
+  FaceF<T> FS{}, FN{};
+  double rain = 0.0, removed = 0.0, xcfl = 0.0, xmin = 1.0 / 0.0, vol = 0.0;
+
+  RowV<T> Rnext = load_row(y0 - 2);
+  for (int k = y0 - 2; k <= y0 + TY + 1; ++k) {
+    Rm = R0; R0 = Rp; Rp = Rnext;
+    if (k < y0 + TY + 1) Rnext = load_row(k + 1);  // prefetch the next row
+    Sm = S0;
+    fyA[0] = fyB[0]; fyA[1] = fyB[1]; fyA[2] = fyB[2];
+    // forward y quotients between rows k-1 and k
+    if (k >= y0 - 1) {
+      fyB[0] = divy(Rp.h - R0.h);
+      fyB[1] = divy(Rp.u - R0.u);
+      fyB[2] = divy(Rp.v - R0.v);
+    }
+    // slopes of row k-1 (State.cpp:187-192): Y axis uses north (row k) as the left neighbour
+    if (k >= y0) {
+      const int r = k - 1;
+      const bool hasN = r < ny - 1, hasS = r > 0;
+      S0.hy = minmod3q<T>(-fyB[0], hasN, -fyA[0], hasS, divy(Rm.h - Rp.h));
+      S0.uy = minmod3q<T>(-fyB[1], hasN, -fyA[1], hasS, divy(Rm.u - Rp.u));
+      S0.vy = minmod3q<T>(-fyB[2], hasN, -fyA[2], hasS, divy(Rm.v - Rp.v));
+      {
+        T r_ = dn1(R0.h), l_ = up1(R0.h);
+        T fq = divx(r_ - R0.h);
+        S0.hx = minmod3q<T>(up1(fq), hasW, fq, hasE, divx(r_ - l_));
+      }
+      {
+        T r_ = dn1(R0.u), l_ = up1(R0.u);
+        T fq = divx(r_ - R0.u);
+        S0.ux = minmod3q<T>(up1(fq), hasW, fq, hasE, divx(r_ - l_));
+      }
+      {
+        T r_ = dn1(R0.v), l_ = up1(R0.v);
+        T fq = divx(r_ - R0.v);
+        S0.vx = minmod3q<T>(up1(fq), hasW, fq, hasE, divx(r_ - l_));
+      }
+    }
+    // horizontal face between rows k-2 and k-1 (face row fy = k-1), Fluxes.cpp:55-64
+    if (k >= y0 + 1 && out_lane) {
+      const int fy = k - 1;
+      if (fy <= ny) {
+        const int edge = fy == 0 ? -1 : (fy == ny ? 1 : 0);
+        const CellV<T> lo = mkcell(Rm, Sm), hi = mkcell(R0, S0);
+        face_flux<T, 1>(edge == -1 ? hi : lo, edge == 1 ? lo : hi, edge, hdy, divy, FN);
+      }
+    }
+    // output row k-2
+    if (k >= y0 + 2) {
+      const int r = k - 2;
+      const CellV<T> me = mkcell(Rm, Sm);
+      const CellV<T> lf = shfl_cell_up(me);
+      FaceF<T> FW{T(0), T(0), T(0), T(0)};
+      if (wface_lane && r < ny) {
+        const int edge = gx == 0 ? -1 : (gx == nx ? 1 : 0);
+        face_flux<T, 0>(edge == -1 ? me : lf, edge == 1 ? lf : me, edge, hdx, divx, FW);
+      }
+      const FaceF<T> FE{dn1(FW.h), dn1(FW.u), dn1(FW.v), dn1(FW.z)};
+      if (out_lane && r < ny) {
+        const long long g = (long long)r * nx + gx;
+        finish_cell<T>(P, fc, c, g, gx, r, me.h, me.u, me.v, me.dhdx, me.dhdy, me.dzdx, me.dzdy, FW, FE, FS, FN,
+                       first, last, cur, dt_d, rain, removed, xcfl, xmin, vol);
+      }
+    }
+    FS = FN;
+  }
+  if (last && !(P.mode & M_DEBUGK)) {
+    double mx = warp_max(xcfl), mn = warp_min(xmin), vs = warp_sum<T>(vol);
+    if (lane == 0) {
+      P.part[gw] = mx;
+      P.part[P.nblk + gw] = mn;
+      P.part[2 * P.nblk + gw] = vs;
+    }
+  }
+  if (P.mode & M_TALLY) {
+    double rs = warp_sum<T>(rain), os = warp_sum<T>(removed);
+    if (lane == 0) {
+      P.part[(3 + 2LL * P.stage) * P.nblk + gw] = rs;
+      P.part[(4 + 2LL * P.stage) * P.nblk + gw] = os;
+    }
+  }
+}
+
+// Bed slopes once per bed upload (SaintVenantConstants, Constants.cpp:39-40).
+template <typename T>
+__global__ void bed_slopes_kernel(const T* z, int nx, int ny, double dx, double dy, T* zx, T* zy) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = (long long)nx * ny;
+  if (i >= n) return;
+  int gx = int(i % nx), gy = int(i / nx);
+  bool hasW = gx > 0, hasE = gx < nx - 1, hasN = gy < ny - 1, hasS = gy > 0;
+  T cz = z[i];
+  zx[i] = minmod3<T>(hasW ? z[i - 1] : cz, hasW, cz, hasE, hasE ? z[i + 1] : cz, mkdiv<T>(dx));
+  zy[i] = minmod3<T>(hasN ? z[i + nx] : cz, hasN, cz, hasS, hasS ? z[i - nx] : cz, mkdiv<T>(dy));
 }
 
 struct FinalizeParams {

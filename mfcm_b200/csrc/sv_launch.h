@@ -15,6 +15,22 @@ constexpr int kNumTiles = 4;
 
 template <typename T> size_t stage_smem_bytes(int tile);
 template <typename T> cudaError_t launch_stage(const StageParams<T>& P, int tile, cudaStream_t s);
+
+// Stage-kernel variants: 0..3 the tiled shared-memory kernel with kTiles[v]; 4..8 the
+// column-sweep kernel with 16 / 32 / 64 / 32 / 32 output rows per warp, the last two with
+// register caps for 3 and 4 resident 4-warp blocks per SM.
+constexpr int kNumVariants = 9;
+constexpr int kSweepRows[5] = {16, 32, 64, 32, 32};
+inline bool variant_is_sweep(int v) { return v >= 4; }
+// per-CTA (tiled) or per-warp (sweep) partial count
+inline long long variant_partials(int v, long long nx, long long ny) {
+  if (v < 4) return ((nx + kTiles[v].tx - 1) / kTiles[v].tx) * ((ny + kTiles[v].ty - 1) / kTiles[v].ty);
+  const long long ty = kSweepRows[v - 4];
+  return ((nx + kSweepOut - 1) / kSweepOut) * ((ny + ty - 1) / ty);
+}
+template <typename T> cudaError_t launch_variant(const StageParams<T>& P, int variant, cudaStream_t s);
+template <typename T> cudaError_t launch_bed_slopes(const T* z, int nx, int ny, double dx, double dy, T* zx, T* zy,
+                                                    cudaStream_t s);
 template <typename T> cudaError_t launch_volume(const T* h, int nx, int ny, double area, double* part, int tile,
                                                 cudaStream_t s);
 template <typename T> cudaError_t launch_debug(const StageParams<T>& P, const DebugParams<T>& D, T* nh, T* sf,
