@@ -289,12 +289,16 @@ def main():
     ncells = w["nx"] * w["ny"]
     solver = make_solver(w, args.precision, device)
     runner = Runner(solver)
-    runner.spinup(args.spinup)
     if args.variant == "auto":
+        # tune on a partly spun-up state, then finish the spin-up with the chosen kernel
+        first = min(50, args.spinup)
+        runner.spinup(first)
         variant = solver.autotune()
+        runner.spinup(args.spinup - first)
     else:
         variant = int(args.variant)
         solver.set_kernel_variant(variant)
+        runner.spinup(args.spinup)
     # warm-up timesteps (untimed)
     runner.run(max(3, args.warmup))
 

@@ -202,8 +202,9 @@ typedef struct {
 int sv_run_timesteps(sv_ctx* ctx, uint64_t max_timesteps, int begin, sv_stats* out, int* step_done,
                      sv_timing* timing);
 /* Stage-kernel variant (no reference counterpart: a launch-shape choice of this library):
- * 0-3 tiled shared-memory kernel (32x8, 32x4, 64x4, 32x16 cells per CTA), 4-6 column-sweep
- * kernel (16/32/64 rows per warp). Every variant computes bit-identical results. */
+ * 0-3 tiled shared-memory kernel (32x8, 32x8 at 3 CTAs/SM, 32x4 at 4 CTAs/SM, 64x4 at 3
+ * CTAs/SM), 4-8 column-sweep kernel (16/32/64 rows per warp, then 32 rows capped for 3 and
+ * 4 CTAs/SM). Every variant computes bit-identical results. */
 int sv_set_kernel_variant(sv_ctx* ctx, int variant);
 int sv_get_kernel_variant(sv_ctx* ctx, int* variant);
 /* Autotune: times every variant's stage kernel on the current state and keeps the fastest;

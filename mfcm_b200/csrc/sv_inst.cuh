@@ -13,38 +13,40 @@ inline bool pow2_mesh(double dx, double dy) {
   return std::frexp(dx, &e) == 0.5 && std::frexp(dy, &e) == 0.5;
 }
 
-template <typename T, int TX, int TY, bool P2> static cudaError_t launch_stage_p(const StageParams<T>& P, cudaStream_t s) {
+template <typename T, int TX, int TY, int MINB, bool P2>
+static cudaError_t launch_stage_p(const StageParams<T>& P, cudaStream_t s) {
   using SM = StageSmem<T, TX, TY>;
   static bool attr_set = false;
   if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(stage_kernel<T, TX, TY, P2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         int(sizeof(SM)));
+    cudaError_t e = cudaFuncSetAttribute(stage_kernel<T, TX, TY, MINB, P2>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(SM)));
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
   dim3 grid((P.nx + TX - 1) / TX, (P.ny + TY - 1) / TY);
-  stage_kernel<T, TX, TY, P2><<<grid, TX * TY, sizeof(SM), s>>>(P);
+  stage_kernel<T, TX, TY, MINB, P2><<<grid, TX * TY, sizeof(SM), s>>>(P);
   return cudaGetLastError();
 }
-template <typename T, int TX, int TY> static cudaError_t launch_stage_t(const StageParams<T>& P, cudaStream_t s) {
-  return pow2_mesh(P.dx, P.dy) ? launch_stage_p<T, TX, TY, true>(P, s) : launch_stage_p<T, TX, TY, false>(P, s);
+template <typename T, int TX, int TY, int MINB> static cudaError_t launch_stage_t(const StageParams<T>& P, cudaStream_t s) {
+  return pow2_mesh(P.dx, P.dy) ? launch_stage_p<T, TX, TY, MINB, true>(P, s)
+                               : launch_stage_p<T, TX, TY, MINB, false>(P, s);
 }
 
 template <> size_t stage_smem_bytes<SV_T>(int tile) {
   switch (tile) {
     case 0: return sizeof(StageSmem<SV_T, 32, 8>);
-    case 1: return sizeof(StageSmem<SV_T, 32, 4>);
-    case 2: return sizeof(StageSmem<SV_T, 64, 4>);
-    default: return sizeof(StageSmem<SV_T, 32, 16>);
+    case 1: return sizeof(StageSmem<SV_T, 32, 8>);
+    case 2: return sizeof(StageSmem<SV_T, 32, 4>);
+    default: return sizeof(StageSmem<SV_T, 64, 4>);
   }
 }
 
 template <> cudaError_t launch_stage<SV_T>(const StageParams<SV_T>& P, int tile, cudaStream_t s) {
   switch (tile) {
-    case 0: return launch_stage_t<SV_T, 32, 8>(P, s);
-    case 1: return launch_stage_t<SV_T, 32, 4>(P, s);
-    case 2: return launch_stage_t<SV_T, 64, 4>(P, s);
-    default: return launch_stage_t<SV_T, 32, 16>(P, s);
+    case 0: return launch_stage_t<SV_T, 32, 8, 1>(P, s);
+    case 1: return launch_stage_t<SV_T, 32, 8, 3>(P, s);
+    case 2: return launch_stage_t<SV_T, 32, 4, 4>(P, s);
+    default: return launch_stage_t<SV_T, 64, 4, 3>(P, s);
   }
 }
 
@@ -86,12 +88,8 @@ static cudaError_t launch_volume_t(const T* h, int nx, int ny, double area, doub
 
 template <> cudaError_t launch_volume<SV_T>(const SV_T* h, int nx, int ny, double area, double* part, int tile,
                                             cudaStream_t s) {
-  switch (tile) {
-    case 0: return launch_volume_t<SV_T, 32, 8>(h, nx, ny, area, part, s);
-    case 1: return launch_volume_t<SV_T, 32, 4>(h, nx, ny, area, part, s);
-    case 2: return launch_volume_t<SV_T, 64, 4>(h, nx, ny, area, part, s);
-    default: return launch_volume_t<SV_T, 32, 16>(h, nx, ny, area, part, s);
-  }
+  (void)tile;  // one fixed decomposition: the volume must not depend on the stage-kernel variant
+  return launch_volume_t<SV_T, 32, 8>(h, nx, ny, area, part, s);
 }
 
 template <> cudaError_t launch_debug<SV_T>(const StageParams<SV_T>& P, const DebugParams<SV_T>& D, SV_T* nh,

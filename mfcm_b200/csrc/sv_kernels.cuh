@@ -296,8 +296,8 @@ struct StageSmem {
   double red[TX * TY / 32];
 };
 
-template <typename T, int TX, int TY, bool P2>
-__global__ void __launch_bounds__(TX * TY) stage_kernel(const StageParams<T> P) {
+template <typename T, int TX, int TY, int MINB, bool P2>
+__global__ void __launch_bounds__(TX * TY, MINB) stage_kernel(const StageParams<T> P) {
   using DX = DivX<T, P2>;
   using SM = StageSmem<T, TX, TY>;
   constexpr int NT = TX * TY;
@@ -333,7 +333,8 @@ __global__ void __launch_bounds__(TX * TY) stage_kernel(const StageParams<T> P) 
   __syncthreads();
 
   const DX divx = MkDivX<DX>::make(P.dx), divy = MkDivX<DX>::make(P.dy);
-  // phase 2: Minmod3 slopes (State.cpp:176-193, Constants.cpp:39-40) on the tile + ring
+  // phase 2: Minmod3 slopes of h, u, v (State.cpp:176-193) on the tile + ring; the bed
+  // slopes (Constants.cpp:39-40) are precomputed once per bed and loaded
   for (int i = tid; i < SM::SX * SM::SY; i += NT) {
     int sx = i % SM::SX, sy = i / SM::SX;
     if ((sx == 0 || sx == SM::SX - 1) && (sy == 0 || sy == SM::SY - 1)) continue;  // unused corners
@@ -341,8 +342,11 @@ __global__ void __launch_bounds__(TX * TY) stage_kernel(const StageParams<T> P) 
     if (gx < 0 || gx >= nx || gy < 0 || gy >= ny) continue;
     int lx = sx + 1, ly = sy + 1;
     bool hasW = gx > 0, hasE = gx < nx - 1, hasN = gy < ny - 1, hasS = gy > 0;
+    long long g = (long long)gy * nx + gx;
+    s.slp[3][sy][sx] = ld(P.zx, g);
+    s.slp[7][sy][sx] = ld(P.zy, g);
 #pragma unroll
-    for (int f = 0; f < 4; ++f) {
+    for (int f = 0; f < 3; ++f) {
       s.slp[f][sy][sx] = minmod3<T>(s.val[f][ly][lx - 1], hasW, s.val[f][ly][lx], hasE, s.val[f][ly][lx + 1], divx);
       // Y axis: north (row + 1) is the left neighbour, south the right
       s.slp[4 + f][sy][sx] = minmod3<T>(s.val[f][ly + 1][lx], hasN, s.val[f][ly][lx], hasS, s.val[f][ly - 1][lx], divy);

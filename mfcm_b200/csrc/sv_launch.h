@@ -8,9 +8,10 @@
 
 namespace svk {
 
-// Tile shapes compiled for the fused stage kernel (TX x TY cells per CTA).
-struct TileShape { int tx, ty; };
-constexpr TileShape kTiles[] = {{32, 8}, {32, 4}, {64, 4}, {32, 16}};
+// Tile shapes compiled for the fused stage kernel (TX x TY cells per CTA, MINB resident
+// CTAs per SM requested from the register allocator).
+struct TileShape { int tx, ty, minb; };
+constexpr TileShape kTiles[] = {{32, 8, 1}, {32, 8, 3}, {32, 4, 4}, {64, 4, 3}};
 constexpr int kNumTiles = 4;
 
 template <typename T> size_t stage_smem_bytes(int tile);
