@@ -211,7 +211,34 @@ int sv_get_kernel_variant(sv_ctx* ctx, int* variant);
  * `best_out` (may be NULL) receives the chosen variant. The state U_[0] is not modified. */
 int sv_autotune(sv_ctx* ctx, int* best_out);
 
-/* message of the last failing call on ctx (or of the last failing sv_create if ctx is NULL) */
+/* One FP64 Runge-Kutta timestep -- the stages of do_timestep followed by the control number
+ * -- on device buffers the caller owns, without allocating any device memory. It has no
+ * counterpart in the reference. It is for callers that must not allocate after start-up: a
+ * host framework that owns every device allocation through its own pool and hands the solver
+ * only pre-allocated buffers, or a real-time loop in which a cudaMalloc would synchronise the
+ * device. Working memory is a fixed array inside this library (about 4.9 MB, held by every
+ * GPU that loads the library until the process exits), which limits the mesh to 65536 cells
+ * (256 x 256); larger meshes return SV_E_LIMIT.
+ *   inputs  (device, FP64, nx*ny each): z, h, u, v = U_[0]
+ *   outputs (device, FP64, nx*ny each): h_out, u_out, v_out = U_[N]; they must not alias the
+ *           inputs. result (device, 3 doubles): control number, suggested next dt, 1.0 if the
+ *           timestep must be repeated else 0.0.
+ *   manning: uniform n_shallow, n_deep, d_shallow, d_deep (host array of 4).
+ *   forcing: SV_RAIN_NONE/UNIFORM and SV_HEAD_NONE/EDGES only (there is no field storage).
+ *   params:  precision SV_F64 and a tableau whose stages use only the previous stage (euler,
+ *            midpoint, heun2, ralston2, heun3, ralston3, classic).
+ *   stream:  cudaStream_t to launch on (NULL = legacy default stream); nothing is synchronised.
+ * The first call on each device looks up the array's device address (cudaGetSymbolAddress),
+ * so make that first call before any stream capture. Every call uses the same array and it
+ * keeps the previous call's contents (each call rewrites all of it before reading): calls
+ * that overlap on the GPU -- on different streams, or from different host threads -- race. */
+int sv_timestep_noalloc(const sv_mesh_desc* mesh, const sv_params* params, const double manning[4],
+                        const sv_forcing* forcing, const double* z, const double* h, const double* u,
+                        const double* v, double* h_out, double* u_out, double* v_out, double t_local,
+                        double dt, double* result, void* stream);
+
+/* message of the last failing call on ctx (or, for ctx NULL, of the last failing sv_create or
+ * sv_timestep_noalloc on this thread) */
 const char* sv_last_error(const sv_ctx* ctx);
 
 #ifdef __cplusplus

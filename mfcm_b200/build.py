@@ -21,6 +21,7 @@ UNITS = {
     "sv_f64.cu": ["-fmad=false"],
     "sv_f32.cu": [],
     "sv_capi.cu": [],
+    "sv_noalloc.cu": [],
 }
 
 

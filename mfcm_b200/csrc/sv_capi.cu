@@ -82,6 +82,11 @@ struct DevBuf {
 
 }  // namespace
 
+namespace svh {
+// error message of context-free entry points, read back by sv_last_error(NULL)
+void set_global_error(const std::string& msg) { g_create_err = msg; }
+}  // namespace svh
+
 struct sv_ctx {
   virtual ~sv_ctx() {}
   std::string err;
