@@ -101,6 +101,19 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def reduce_over_ranks(ms, work, dist, device="cpu"):
+    """Replicas only: the job's time is the slowest rank's device time, its work the sum of
+    the ranks' accepted cell-updates. No simulation data crosses ranks."""
+    if dist is None:
+        return ms, work
+    import torch
+    t_max = torch.tensor([ms], dtype=torch.float64, device=device)
+    w_sum = torch.tensor([work], dtype=torch.float64, device=device)
+    dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    dist.all_reduce(w_sum, op=dist.ReduceOp.SUM)
+    return float(t_max.item()), float(w_sum.item())
+
+
 def workload(size):
     from mfcm_b200 import synth
     nx = ny = size
@@ -317,15 +330,7 @@ def main():
     st1 = solver.stats()
     accepted = st1["accepted"] - st0["accepted"]
     repeated = st1["repeated"] - st0["repeated"]
-    ms = tm["total_ms"]
-    ms_t = torch.tensor([ms, float(accepted * ncells)], dtype=torch.float64, device=f"cuda:{device}")
-    if dist is not None:
-        mx = ms_t.clone()
-        dist.all_reduce(mx[0:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(mx[1:2], op=dist.ReduceOp.SUM)
-        ms_max, work = float(mx[0]), float(mx[1])
-    else:
-        ms_max, work = ms, float(accepted * ncells)
+    ms_max, work = reduce_over_ranks(tm["total_ms"], float(accepted * ncells), dist, f"cuda:{device}")
     value = work / (ms_max * 1e-3)
 
     # roofline of the dominant kernel (the fused stage kernel)
