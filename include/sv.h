@@ -211,6 +211,28 @@ int sv_get_kernel_variant(sv_ctx* ctx, int* variant);
  * `best_out` (may be NULL) receives the chosen variant. The state U_[0] is not modified. */
 int sv_autotune(sv_ctx* ctx, int* best_out);
 
+/* ---- batches of independent catchments (no reference counterpart: the reference runs one
+ *      catchment per process). Members are ordinary sv_ctx solvers; per timestep one batched
+ *      launch per RK stage covers every member's tiles and one batched launch runs every
+ *      member's reductions and dt controller, so each member keeps its own dt, step clock and
+ *      tallies and its results are bit-identical to running it alone. All members share the
+ *      batch's precision and a tableau whose stages use only the previous stage. ---------- */
+typedef struct sv_batch sv_batch;
+int sv_batch_create(int precision, int rk_method, int device, sv_batch** out);
+void sv_batch_destroy(sv_batch* batch);
+/* add a catchment (allocates its device memory); *id is its slot, reused after removal */
+int sv_batch_add(sv_batch* batch, const sv_mesh_desc* mesh, const sv_params* params, int* id);
+/* remove a catchment and free its device memory */
+int sv_batch_remove(sv_batch* batch, int id);
+/* the member's context, for sv_set_field / sv_get_field / sv_set_forcing / sv_get_stats
+ * (owned by the batch: do not sv_destroy it); NULL for an empty slot */
+sv_ctx* sv_batch_member(sv_batch* batch, int id);
+/* TypedTemporalScheme::step for every member at once; out[id] (for id < n_out) receives each
+ * member's step counts and running tallies */
+int sv_batch_advance(sv_batch* batch, sv_stats* out, int n_out);
+/* number of members and their total device memory in bytes */
+int sv_batch_size(sv_batch* batch, int* n_members, uint64_t* device_bytes);
+
 /* One FP64 Runge-Kutta timestep -- the stages of do_timestep followed by the control number
  * -- on device buffers the caller owns, without allocating any device memory. It has no
  * counterpart in the reference. It is for callers that must not allocate after start-up: a

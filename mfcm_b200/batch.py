@@ -1,0 +1,115 @@
+"""Batches of independent catchments advanced in shared launches (sv_batch_* in include/sv.h).
+
+The reference runs one catchment per process; here many uneven catchments advance together:
+per timestep one batched launch per RK stage covers every member's tiles and one batched
+launch runs every member's reductions and dt controller. Each member keeps its own dt, step
+clock and tallies, so its results are bit-identical to running it alone.
+"""
+import ctypes as C
+
+from . import _abi, load_library, SvError, _Backend, _precision_code, RK_METHODS, RK_STAGES
+from ._abi import MeshDesc, Params, Stats
+
+
+def _declare(lib):
+    if getattr(lib, "_batch_declared", False):
+        return
+    P = C.POINTER
+    lib.sv_batch_create.restype = C.c_int
+    lib.sv_batch_create.argtypes = [C.c_int, C.c_int, C.c_int, P(C.c_void_p)]
+    lib.sv_batch_destroy.restype = None
+    lib.sv_batch_destroy.argtypes = [C.c_void_p]
+    lib.sv_batch_add.restype = C.c_int
+    lib.sv_batch_add.argtypes = [C.c_void_p, P(MeshDesc), P(Params), P(C.c_int)]
+    lib.sv_batch_remove.restype = C.c_int
+    lib.sv_batch_remove.argtypes = [C.c_void_p, C.c_int]
+    lib.sv_batch_member.restype = C.c_void_p
+    lib.sv_batch_member.argtypes = [C.c_void_p, C.c_int]
+    lib.sv_batch_advance.restype = C.c_int
+    lib.sv_batch_advance.argtypes = [C.c_void_p, P(Stats), C.c_int]
+    lib.sv_batch_size.restype = C.c_int
+    lib.sv_batch_size.argtypes = [C.c_void_p, P(C.c_int), P(C.c_uint64)]
+    lib._batch_declared = True
+
+
+class BatchMember(_Backend):
+    """One catchment of a batch: the usual field / forcing / stats calls on its context."""
+
+    def __init__(self, batch, slot, nx, ny, dx, dy, step_duration, nstages):
+        self._lib = batch._lib
+        self._batch = batch
+        self.slot = slot
+        self._h = C.c_void_p(batch._lib.sv_batch_member(batch._b, slot))
+        self.nx, self.ny, self.dx, self.dy = nx, ny, dx, dy
+        self.ncells = nx * ny
+        self.nfaces = (nx + 1) * ny + (ny + 1) * nx
+        self.step_duration = step_duration
+        self.nstages = nstages
+
+    def last_error(self):
+        return self._lib.sv_last_error(self._h).decode()
+
+
+class SaintVenantBatch:
+    def __init__(self, precision="f64", rk_method="classic", device=0):
+        self._lib = load_library()
+        _declare(self._lib)
+        self.precision = precision
+        self.rk_method = rk_method
+        h = C.c_void_p()
+        r = self._lib.sv_batch_create(_precision_code(precision), RK_METHODS.index(rk_method), int(device), C.byref(h))
+        if r != 0:
+            raise SvError(r, self._lib.sv_last_error(None).decode())
+        self._b = h
+        self.members = {}
+
+    def add(self, nx, ny, dx, dy=None, cn_target=1.0, step_duration=60.0, initial_dt=1.0, max_dt=0.0,
+            rain_mode="reference", manning=True, head_first=False, tallies=True):
+        dy = float(dx if dy is None else dy)
+        m = MeshDesc(int(nx), int(ny), float(dx), dy, 0.0, 0.0)
+        p = Params(_precision_code(self.precision), RK_METHODS.index(self.rk_method), float(cn_target),
+                   float(step_duration), float(initial_dt), float(max_dt), 0 if rain_mode == "reference" else 1,
+                   1 if manning else 0, 1 if head_first else 0, 0 if tallies else _abi.SV_FLAG_NO_TALLIES)
+        slot = C.c_int()
+        r = self._lib.sv_batch_add(self._b, C.byref(m), C.byref(p), C.byref(slot))
+        if r != 0:
+            raise SvError(r, self._lib.sv_last_error(None).decode())
+        mem = BatchMember(self, slot.value, int(nx), int(ny), float(dx), dy, float(step_duration),
+                          RK_STAGES[RK_METHODS.index(self.rk_method)])
+        self.members[slot.value] = mem
+        return mem
+
+    def remove(self, member):
+        r = self._lib.sv_batch_remove(self._b, member.slot)
+        if r != 0:
+            raise SvError(r, self._lib.sv_last_error(None).decode())
+        self.members.pop(member.slot, None)
+        member._h = None
+
+    def advance(self):
+        """One step (of each member's own step length) for every member; returns
+        {slot: stats} with the step's counts and each member's running tallies."""
+        n = max(self.members) + 1 if self.members else 0
+        out = (Stats * max(n, 1))()
+        r = self._lib.sv_batch_advance(self._b, out, n)
+        if r != 0:
+            raise SvError(r, self._lib.sv_last_error(None).decode())
+        return {k: out[k].as_dict() for k in self.members}
+
+    def size(self):
+        n, b = C.c_int(), C.c_uint64()
+        self._lib.sv_batch_size(self._b, C.byref(n), C.byref(b))
+        return n.value, b.value
+
+    def close(self):
+        if getattr(self, "_b", None):
+            for m in self.members.values():
+                m._h = None
+            self._lib.sv_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -160,6 +160,7 @@ struct Solver final : public sv_ctx {
   int cur = 0;  // host mirror of ctl->cur
   cudaGraphExec_t graph = nullptr;
   bool graph_dirty = true;
+  unsigned long long pversion = 0;  // bumped whenever launch parameters change
   int unroll = 8;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<void*> owned;
@@ -173,10 +174,13 @@ struct Solver final : public sv_ctx {
     if (stream) cudaStreamDestroy(stream);
   }
 
+  size_t device_bytes = 0;
   template <typename U> cudaError_t alloc(U** p, size_t count) {
     void* q = nullptr;
-    cudaError_t e = cudaMalloc(&q, count * sizeof(U) > 0 ? count * sizeof(U) : 16);
+    const size_t bytes = count * sizeof(U) > 0 ? count * sizeof(U) : 16;
+    cudaError_t e = cudaMalloc(&q, bytes);
     if (e != cudaSuccess) return e;
+    device_bytes += bytes;
     owned.push_back(q);
     *p = static_cast<U*>(q);
     return cudaSuccess;
@@ -282,16 +286,16 @@ struct Solver final : public sv_ctx {
     if (id == SV_FIELD_N_DEEP && man[0] && host_n_shallow.size() == n &&
         std::memcmp(host_n_shallow.data(), host, n * sizeof(double)) == 0) {
       man[1] = man[0];  // n_deep identical to n_shallow: read one array
-      graph_dirty = true;
+      graph_dirty = true; ++pversion;
       return SV_OK;
     }
     if (lazy && (*slot == nullptr || (id == SV_FIELD_N_DEEP && man[1] == man[0]))) {
       SV_CUDA(alloc_cells(slot, false));
-      graph_dirty = true;
+      graph_dirty = true; ++pversion;
     }
     if (id == SV_FIELD_N_SHALLOW) {
       host_n_shallow.assign(host, host + n);
-      if (man[1] == man[0] && man[1] != nullptr) { man[1] = nullptr; graph_dirty = true; }
+      if (man[1] == man[0] && man[1] != nullptr) { man[1] = nullptr; graph_dirty = true; ++pversion; }
     }
     int r = upload(*slot, host, n);
     if (r == SV_OK && id == SV_FIELD_Z) {
@@ -351,7 +355,7 @@ struct Solver final : public sv_ctx {
     man_s[0] = a; man_s[1] = b; man_s[2] = c; man_s[3] = d;
     for (int i = 0; i < 4; ++i) man[i] = nullptr;  // uniform values replace per-cell fields
     host_n_shallow.clear();
-    graph_dirty = true;
+    graph_dirty = true; ++pversion;
     return SV_OK;
   }
 
@@ -361,8 +365,8 @@ struct Solver final : public sv_ctx {
       return fail(SV_E_ARG, "bad forcing kind");
     if (f->rain_kind == SV_RAIN_FIELDS && (!q0 || !q1)) {
       // the discharge fields start cleared (BoundarySourceTerm::clear_values)
-      if (!q0) { SV_CUDA(alloc_cells(&q0)); graph_dirty = true; }
-      if (!q1) { SV_CUDA(alloc_cells(&q1)); graph_dirty = true; }
+      if (!q0) { SV_CUDA(alloc_cells(&q0)); graph_dirty = true; ++pversion; }
+      if (!q1) { SV_CUDA(alloc_cells(&q1)); graph_dirty = true; ++pversion; }
     }
     if (f->rain_kind == SV_RAIN_PATTERN && !pat) return fail(SV_E_STATE, "rain pattern field not set");
     if (f->head_kind == SV_HEAD_FIELDS && (!hb0 || !hb1)) return fail(SV_E_STATE, "head fields not set");
@@ -430,37 +434,34 @@ struct Solver final : public sv_ctx {
   }
 
   // Launch the N stages of one timestep and the finalize kernel (RungeKutta.cpp:147-167).
-  // ev: if non-null, 2*(N+1) events recorded around every kernel (stages, then finalize)
-  int enqueue_timestep(bool auto_mode, cudaEvent_t* ev = nullptr) {
+  // Stage s of a timestep (RungeKutta.cpp:147-153): mode, RK coefficients and buffers.
+  svk::StageParams<T> stage_params(int st) const {
     svk::StageParams<T> P = base_params();
     const bool tally = !(prm.flags & SV_FLAG_NO_TALLIES);
-    for (int s = 0; s < N; ++s) {
-      P.stage = s;
-      P.c_s = tab.c(s + 1);
-      int mode = 0;
-      if (s == 0) mode |= svk::M_FIRST;
-      if (s == N - 1) mode |= svk::M_LAST;
-      if (diag) mode |= svk::M_ACC;
-      else if (s < N - 1) mode |= svk::M_STOREK;
-      if (tally) mode |= svk::M_TALLY;
-      P.mode = mode;
-      for (int j = 0; j < 4; ++j) { P.a_next[j] = 0.0; P.b[j] = 0.0; }
-      if (s < N - 1)
-        for (int j = 0; j <= s; ++j) P.a_next[j] = tab.A(s + 2, j + 1);
-      for (int j = 0; j < N; ++j) P.b[j] = tab.b(j + 1);
-      // stage inputs: U_[0] (s = 0), then Y[0], Y[1], Y[0] ...
-      const int in = (s - 1) & 1, out = s & 1;
-      for (int f = 0; f < 3; ++f) {
-        P.Yin[f] = s > 0 ? Y[in][f] : nullptr;
-        P.Yout[f] = s < N - 1 ? Y[out][f] : nullptr;
-        P.Kout[f] = (!diag && s < N - 1) ? K[s][f] : nullptr;
-        for (int j = 0; j < 4; ++j) P.Kin[j][f] = (!diag && j < N - 1) ? K[j][f] : nullptr;
-      }
-      if (ev) SV_CUDA(cudaEventRecord(ev[2 * s], stream));
-      cudaError_t e = svk::launch_variant<T>(P, variant, stream);
-      if (e != cudaSuccess) return cuda_fail(e, "stage kernel");
-      if (ev) SV_CUDA(cudaEventRecord(ev[2 * s + 1], stream));
+    P.stage = st;
+    P.c_s = tab.c(st + 1);
+    int mode = 0;
+    if (st == 0) mode |= svk::M_FIRST;
+    if (st == N - 1) mode |= svk::M_LAST;
+    if (diag) mode |= svk::M_ACC;
+    else if (st < N - 1) mode |= svk::M_STOREK;
+    if (tally) mode |= svk::M_TALLY;
+    P.mode = mode;
+    for (int j = 0; j < 4; ++j) { P.a_next[j] = 0.0; P.b[j] = 0.0; }
+    if (st < N - 1)
+      for (int j = 0; j <= st; ++j) P.a_next[j] = tab.A(st + 2, j + 1);
+    for (int j = 0; j < N; ++j) P.b[j] = tab.b(j + 1);
+    // stage inputs: U_[0] (s = 0), then Y[0], Y[1], Y[0] ...
+    const int in = (st - 1) & 1, out = st & 1;
+    for (int f = 0; f < 3; ++f) {
+      P.Yin[f] = st > 0 ? Y[in][f] : nullptr;
+      P.Yout[f] = st < N - 1 ? Y[out][f] : nullptr;
+      P.Kout[f] = (!diag && st < N - 1) ? K[st][f] : nullptr;
+      for (int j = 0; j < 4; ++j) P.Kin[j][f] = (!diag && j < N - 1) ? K[j][f] : nullptr;
     }
+    return P;
+  }
+  svk::FinalizeParams finalize_params(bool auto_mode) const {
     svk::FinalizeParams F{};
     F.ctl = ctl;
     F.part = part;
@@ -472,8 +473,22 @@ struct Solver final : public sv_ctx {
     F.L = prm.step_duration;
     F.cell_area = mesh.dx * mesh.dy;
     F.auto_mode = auto_mode ? 1 : 0;
-    F.tally = tally ? 1 : 0;
+    F.tally = (prm.flags & SV_FLAG_NO_TALLIES) ? 0 : 1;
     F.is_float = sizeof(T) == 4;
+    return F;
+  }
+
+  // Launch the N stages of one timestep and the finalize kernel (RungeKutta.cpp:147-167).
+  // ev: if non-null, 2*(N+1) events recorded around every kernel (stages, then finalize)
+  int enqueue_timestep(bool auto_mode, cudaEvent_t* ev = nullptr) {
+    for (int st = 0; st < N; ++st) {
+      svk::StageParams<T> P = stage_params(st);
+      if (ev) SV_CUDA(cudaEventRecord(ev[2 * st], stream));
+      cudaError_t e = svk::launch_variant<T>(P, variant, stream);
+      if (e != cudaSuccess) return cuda_fail(e, "stage kernel");
+      if (ev) SV_CUDA(cudaEventRecord(ev[2 * st + 1], stream));
+    }
+    svk::FinalizeParams F = finalize_params(auto_mode);
     if (ev) SV_CUDA(cudaEventRecord(ev[2 * N], stream));
     cudaError_t e = svk::launch_finalize(F, stream);
     if (e != cudaSuccess) return cuda_fail(e, "finalize kernel");
@@ -653,7 +668,7 @@ struct Solver final : public sv_ctx {
     if (v < 0 || v >= svk::kNumVariants) return fail(SV_E_ARG, "unknown kernel variant");
     variant = v;
     nblk = svk::variant_partials(variant, (long long)mesh.nx, (long long)mesh.ny);
-    graph_dirty = true;
+    graph_dirty = true; ++pversion;
     return SV_OK;
   }
   int get_variant() const override { return variant; }
@@ -727,7 +742,243 @@ struct Solver final : public sv_ctx {
   }
 };
 
+
+// ------------------------------------------------------------------------------------------
+// Batch of independent catchments advanced together: per timestep one batched launch per RK
+// stage covers every tile of every member, and one batched finalize runs every member's
+// reductions and dt controller. Each member keeps its own state, dt, step clock and tallies,
+// so its results are bit-identical to running it alone.
+// ------------------------------------------------------------------------------------------
+struct sv_batch_base {
+  virtual ~sv_batch_base() {}
+  std::string err;
+  int fail(int code, const std::string& m) {
+    err = m;
+    return code;
+  }
+  virtual int add(const sv_mesh_desc*, const sv_params*, int*) = 0;
+  virtual int remove(int) = 0;
+  virtual sv_ctx* member(int) = 0;
+  virtual int advance(sv_stats*, int) = 0;
+  virtual int size(int*, uint64_t*) = 0;
+};
+
+template <typename T>
+struct Batch final : public sv_batch_base {
+  int device = 0, precision = SV_F64, rk_method = SV_RK_CLASSIC, N = 4;
+  cudaStream_t stream = nullptr;
+  std::vector<Solver<T>*> members;  // slot id -> member (nullptr when removed)
+  // device arrays, rebuilt when membership changes
+  svk::StageParams<T>* d_params = nullptr;  // [N][nact]
+  svk::FinalizeParams* d_fin = nullptr;     // [nact]
+  long long* d_tiles = nullptr;             // [nact + 1]
+  Ctl** d_ctls = nullptr;                   // [nact]
+  int* d_done = nullptr;                    // [nact]
+  int nact = 0, cap = 0;
+  long long total_tiles = 0;
+  bool p2 = true, dirty = true;
+  std::vector<int> active;                  // slot ids in launch order
+  std::vector<unsigned long long> versions; // members' pversion at the last rebuild
+  cudaGraphExec_t graph = nullptr;
+  int unroll = 8;
+
+  ~Batch() override {
+    cudaSetDevice(device);
+    if (graph) cudaGraphExecDestroy(graph);
+    for (auto* m : members) delete m;
+    free_arrays();
+    if (stream) cudaStreamDestroy(stream);
+  }
+  void free_arrays() {
+    cudaFree(d_params); cudaFree(d_fin); cudaFree(d_tiles); cudaFree(d_ctls); cudaFree(d_done);
+    d_params = nullptr; d_fin = nullptr; d_tiles = nullptr; d_ctls = nullptr; d_done = nullptr;
+    cap = 0;
+  }
+  int cuda_fail(cudaError_t e, const char* where) {
+    return fail(SV_E_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+  }
+  int init(int prec, int rk, int dev) {
+    precision = prec; rk_method = rk; device = dev;
+    Tableau t;
+    if (!named_tableau(rk, t)) return fail(SV_E_ARG, "unknown Runge Kutta scheme index");
+    if (!is_diagonal(t)) return fail(SV_E_ARG, "batches need a tableau whose stages use only the previous stage");
+    N = t.nsteps();
+    SV_CUDA(cudaSetDevice(dev));
+    SV_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    return SV_OK;
+  }
+  int add(const sv_mesh_desc* m, const sv_params* p, int* id) override {
+    if (!m || !p) return fail(SV_E_ARG, "null argument");
+    if (p->precision != precision || p->rk_method != rk_method)
+      return fail(SV_E_ARG, "member precision and tableau must match the batch");
+    auto* s = new Solver<T>();
+    int r = s->init(m, p, device);
+    if (r != SV_OK) {
+      err = s->err;
+      delete s;
+      return r;
+    }
+    s->set_variant(svk::kBatchVariant);
+    int slot = -1;
+    for (size_t i = 0; i < members.size(); ++i)
+      if (!members[i]) { slot = int(i); break; }
+    if (slot < 0) { slot = int(members.size()); members.push_back(nullptr); }
+    members[slot] = s;
+    if (id) *id = slot;
+    dirty = true;
+    return SV_OK;
+  }
+  int remove(int id) override {
+    if (id < 0 || id >= int(members.size()) || !members[id]) return fail(SV_E_ARG, "no such batch member");
+    delete members[id];
+    members[id] = nullptr;
+    cudaSetDevice(device);
+    dirty = true;
+    return SV_OK;
+  }
+  sv_ctx* member(int id) override {
+    if (id < 0 || id >= int(members.size()) || !members[id]) return nullptr;
+    return members[id];
+  }
+  int size(int* n, uint64_t* bytes) override {
+    int c = 0;
+    uint64_t b = 0;
+    for (auto* m : members)
+      if (m) { ++c; b += m->device_bytes; }
+    if (n) *n = c;
+    if (bytes) *bytes = b;
+    return SV_OK;
+  }
+
+  int rebuild() {
+    active.clear();
+    for (size_t i = 0; i < members.size(); ++i)
+      if (members[i]) active.push_back(int(i));
+    nact = int(active.size());
+    if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+    if (nact > cap) {
+      free_arrays();
+      int c = std::max(nact, 8);
+      SV_CUDA(cudaMalloc(&d_params, sizeof(svk::StageParams<T>) * size_t(N) * c));
+      SV_CUDA(cudaMalloc(&d_fin, sizeof(svk::FinalizeParams) * c));
+      SV_CUDA(cudaMalloc(&d_tiles, sizeof(long long) * (c + 1)));
+      SV_CUDA(cudaMalloc(&d_ctls, sizeof(Ctl*) * c));
+      SV_CUDA(cudaMalloc(&d_done, sizeof(int) * c));
+      cap = c;
+    }
+    std::vector<svk::StageParams<T>> hp(size_t(N) * std::max(nact, 1));
+    std::vector<svk::FinalizeParams> hf(std::max(nact, 1));
+    std::vector<long long> ht(nact + 1, 0);
+    std::vector<Ctl*> hc(std::max(nact, 1));
+    p2 = true;
+    for (int k = 0; k < nact; ++k) {
+      Solver<T>* m = members[active[k]];
+      ht[k + 1] = ht[k] + m->nblk;
+      int e2;
+      p2 = p2 && std::frexp(m->mesh.dx, &e2) == 0.5 && std::frexp(m->mesh.dy, &e2) == 0.5;
+      for (int st = 0; st < N; ++st) hp[size_t(st) * nact + k] = m->stage_params(st);
+      hf[k] = m->finalize_params(true);
+      hc[k] = m->ctl;
+    }
+    total_tiles = ht[nact];
+    versions.assign(nact, 0);
+    for (int k = 0; k < nact; ++k) versions[k] = members[active[k]]->pversion;
+    if (nact > 0) {
+      SV_CUDA(cudaMemcpyAsync(d_params, hp.data(), sizeof(svk::StageParams<T>) * size_t(N) * nact,
+                              cudaMemcpyHostToDevice, stream));
+      SV_CUDA(cudaMemcpyAsync(d_fin, hf.data(), sizeof(svk::FinalizeParams) * nact, cudaMemcpyHostToDevice, stream));
+      SV_CUDA(cudaMemcpyAsync(d_tiles, ht.data(), sizeof(long long) * (nact + 1), cudaMemcpyHostToDevice, stream));
+      SV_CUDA(cudaMemcpyAsync(d_ctls, hc.data(), sizeof(Ctl*) * nact, cudaMemcpyHostToDevice, stream));
+      SV_CUDA(cudaStreamSynchronize(stream));
+    }
+    dirty = false;
+    return SV_OK;
+  }
+
+  int enqueue_timestep() {
+    for (int st = 0; st < N; ++st) {
+      cudaError_t e = svk::launch_stage_batch<T>(d_params + size_t(st) * nact, d_tiles, nact, total_tiles, p2, stream);
+      if (e != cudaSuccess) return cuda_fail(e, "batched stage kernel");
+    }
+    cudaError_t e = svk::launch_finalize_batch(d_fin, nact, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "batched finalize kernel");
+    return SV_OK;
+  }
+
+  int build_graph() {
+    cudaGraph_t g;
+    SV_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < unroll; ++i) {
+      int r = enqueue_timestep();
+      if (r) {
+        cudaStreamEndCapture(stream, &g);
+        if (g) cudaGraphDestroy(g);
+        return r;
+      }
+    }
+    SV_CUDA(cudaStreamEndCapture(stream, &g));
+    cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+    return SV_OK;
+  }
+
+  // One step (of each member's own length L) for every member, in batched launches.
+  int advance(sv_stats* out, int n_out) override {
+    SV_CUDA(cudaSetDevice(device));
+    for (size_t k = 0; k < active.size() && !dirty; ++k)
+      if (!members[active[k]] || members[active[k]]->pversion != versions[k]) dirty = true;
+    if (dirty) {
+      int r = rebuild();
+      if (r) return r;
+    }
+    if (nact == 0) return SV_OK;
+    // members' own streams may hold pending uploads (set_field/set_forcing synchronise, but
+    // be safe): order them before the batch's work
+    for (int k : active) SV_CUDA(cudaStreamSynchronize(members[k]->stream));
+    if (!graph) {
+      int r = build_graph();
+      if (r) return r;
+    }
+    cudaError_t e = svk::launch_begin_batch(d_ctls, nact, 0, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "begin batch");
+    std::vector<int> done(nact);
+    for (long long it = 0;; ++it) {
+      SV_CUDA(cudaGraphLaunch(graph, stream));
+      e = svk::launch_gather_done(d_ctls, nact, d_done, stream);
+      if (e != cudaSuccess) return cuda_fail(e, "gather done");
+      SV_CUDA(cudaMemcpyAsync(done.data(), d_done, sizeof(int) * nact, cudaMemcpyDeviceToHost, stream));
+      SV_CUDA(cudaStreamSynchronize(stream));
+      bool all = true;
+      for (int d : done) all = all && d != 0;
+      if (all) break;
+      if (it > 100000000LL / unroll) return fail(SV_E_STATE, "batch step did not finish");
+    }
+    int rc = SV_OK;
+    for (int k = 0; k < nact; ++k) {
+      Solver<T>* m = members[active[k]];
+      Ctl c;
+      int r = m->read_ctl(c);
+      if (r) return r;
+      if (c.error) rc = fail(SV_E_NONFINITE, "a member's time became NaN: its control number was not finite");
+      if (out && active[k] < n_out) {
+        sv_stats& o = out[active[k]];
+        o.accepted = c.step_accepted;
+        o.repeated = c.step_repeated;
+        o.rain_in = c.rain_in;
+        o.outflow = c.outflow;
+        o.volume = c.volume;
+      }
+    }
+    return rc;
+  }
+};
+
 }  // namespace
+
+struct sv_batch {
+  std::unique_ptr<sv_batch_base> impl;
+};
 
 extern "C" {
 
@@ -783,6 +1034,55 @@ int sv_run_timesteps(sv_ctx* ctx, uint64_t n, int begin, sv_stats* out, int* ste
   SV_CHECK_CTX(ctx);
   return ctx->run_timesteps(n, begin, out, step_done, t);
 }
+int sv_batch_create(int precision, int rk_method, int device, sv_batch** out) {
+  if (!out) return SV_E_ARG;
+  *out = nullptr;
+  std::unique_ptr<sv_batch_base> b;
+  int r;
+  if (precision == SV_F64) {
+    auto* x = new Batch<double>();
+    b.reset(x);
+    r = x->init(precision, rk_method, device);
+  } else if (precision == SV_F32) {
+    auto* x = new Batch<float>();
+    b.reset(x);
+    r = x->init(precision, rk_method, device);
+  } else {
+    g_create_err = "precision not available";
+    return SV_E_ARG;
+  }
+  if (r != SV_OK) {
+    g_create_err = b->err;
+    return r;
+  }
+  *out = new sv_batch{std::move(b)};
+  return SV_OK;
+}
+void sv_batch_destroy(sv_batch* b) { delete b; }
+int sv_batch_add(sv_batch* b, const sv_mesh_desc* m, const sv_params* p, int* id) {
+  if (!b) return SV_E_ARG;
+  int r = b->impl->add(m, p, id);
+  if (r) g_create_err = b->impl->err;
+  return r;
+}
+int sv_batch_remove(sv_batch* b, int id) {
+  if (!b) return SV_E_ARG;
+  int r = b->impl->remove(id);
+  if (r) g_create_err = b->impl->err;
+  return r;
+}
+sv_ctx* sv_batch_member(sv_batch* b, int id) { return b ? b->impl->member(id) : nullptr; }
+int sv_batch_advance(sv_batch* b, sv_stats* out, int n_out) {
+  if (!b) return SV_E_ARG;
+  int r = b->impl->advance(out, n_out);
+  if (r) g_create_err = b->impl->err;
+  return r;
+}
+int sv_batch_size(sv_batch* b, int* n, uint64_t* bytes) {
+  if (!b) return SV_E_ARG;
+  return b->impl->size(n, bytes);
+}
+
 int sv_set_kernel_variant(sv_ctx* ctx, int v) { SV_CHECK_CTX(ctx); return ctx->set_variant(v); }
 int sv_get_kernel_variant(sv_ctx* ctx, int* v) { SV_CHECK_CTX(ctx); if (!v) return SV_E_ARG; *v = ctx->get_variant(); return SV_OK; }
 int sv_autotune(sv_ctx* ctx, int* best) { SV_CHECK_CTX(ctx); return ctx->autotune(best); }

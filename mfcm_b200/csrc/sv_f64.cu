@@ -12,6 +12,21 @@ cudaError_t launch_finalize(const FinalizeParams& F, cudaStream_t s) {
   finalize_kernel<1024><<<1, 1024, 0, s>>>(F);
   return cudaGetLastError();
 }
+cudaError_t launch_finalize_batch(const FinalizeParams* Fs, int ninst, cudaStream_t s) {
+  if (ninst <= 0) return cudaSuccess;
+  finalize_batch_kernel<1024><<<ninst, 1024, 0, s>>>(Fs);
+  return cudaGetLastError();
+}
+cudaError_t launch_begin_batch(Ctl* const* ctls, int n, long long budget, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  begin_batch_kernel<<<(n + 127) / 128, 128, 0, s>>>(ctls, n, budget);
+  return cudaGetLastError();
+}
+cudaError_t launch_gather_done(Ctl* const* ctls, int n, int* done, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  gather_done_kernel<<<(n + 127) / 128, 128, 0, s>>>(ctls, n, done);
+  return cudaGetLastError();
+}
 cudaError_t launch_sum(const double* p, long long n, double* out, cudaStream_t s) {
   sum_kernel<1024><<<1, 1024, 0, s>>>(p, n, out);
   return cudaGetLastError();

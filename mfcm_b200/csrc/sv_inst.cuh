@@ -79,6 +79,28 @@ template <> cudaError_t launch_bed_slopes<SV_T>(const SV_T* z, int nx, int ny, d
   return cudaGetLastError();
 }
 
+template <typename T, int TX, int TY, int MINB, bool P2>
+static cudaError_t launch_stage_batch_p(const StageParams<T>* Ps, const long long* tile_start, int ninst,
+                                        long long total_tiles, cudaStream_t s) {
+  using SM = StageSmem<T, TX, TY>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(stage_batch_kernel<T, TX, TY, MINB, P2>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(SM)));
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  if (total_tiles <= 0) return cudaSuccess;
+  stage_batch_kernel<T, TX, TY, MINB, P2><<<unsigned(total_tiles), TX * TY, sizeof(SM), s>>>(Ps, tile_start, ninst);
+  return cudaGetLastError();
+}
+
+template <> cudaError_t launch_stage_batch<SV_T>(const StageParams<SV_T>* Ps, const long long* tile_start, int ninst,
+                                                 long long total_tiles, bool p2, cudaStream_t s) {
+  return p2 ? launch_stage_batch_p<SV_T, 32, 8, 3, true>(Ps, tile_start, ninst, total_tiles, s)
+            : launch_stage_batch_p<SV_T, 32, 8, 3, false>(Ps, tile_start, ninst, total_tiles, s);
+}
+
 template <typename T, int TX, int TY>
 static cudaError_t launch_volume_t(const T* h, int nx, int ny, double area, double* part, cudaStream_t s) {
   dim3 grid((nx + TX - 1) / TX, (ny + TY - 1) / TY);

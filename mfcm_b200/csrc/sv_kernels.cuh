@@ -296,13 +296,13 @@ struct StageSmem {
   double red[TX * TY / 32];
 };
 
-template <typename T, int TX, int TY, int MINB, bool P2>
-__global__ void __launch_bounds__(TX * TY, MINB) stage_kernel(const StageParams<T> P) {
+// One TX x TY tile of one stage: bx, by = tile coordinates, blk = partial-sum slot.
+template <typename T, int TX, int TY, bool P2>
+__device__ __forceinline__ void stage_tile(const StageParams<T>& P, int bx, int by, long long blk,
+                                           StageSmem<T, TX, TY>& s) {
   using DX = DivX<T, P2>;
   using SM = StageSmem<T, TX, TY>;
   constexpr int NT = TX * TY;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  SM& s = *reinterpret_cast<SM*>(smem_raw);
 
   const Ctl* ctl = P.ctl;
   if (ctl->done) return;
@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(TX * TY, MINB) stage_kernel(const StageParams<
   const double tsub = ctl->t_local + P.c_s * dt_d;
 
   const int tid = threadIdx.x;
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const int x0 = bx * TX, y0 = by * TY;
   const int nx = P.nx, ny = P.ny;
   const bool first = P.mode & M_FIRST;
   const T* Yh = first ? P.S[cur][0] : P.Yin[0];
@@ -418,21 +418,54 @@ __global__ void __launch_bounds__(TX * TY, MINB) stage_kernel(const StageParams<
     double mn = block_min<NT>(xcfl_min, s.red);
     double vs = block_sum<NT>(vol, s.red);
     if (tid == 0) {
-      long long b = (long long)blockIdx.y * gridDim.x + blockIdx.x;
-      P.part[b] = mx;
-      P.part[P.nblk + b] = mn;
-      P.part[2 * P.nblk + b] = vs;
+      P.part[blk] = mx;
+      P.part[P.nblk + blk] = mn;
+      P.part[2 * P.nblk + blk] = vs;
     }
   }
   if (P.mode & M_TALLY) {
     double rs = block_sum<NT>(rain, s.red);
     double os = block_sum<NT>(removed, s.red);
     if (tid == 0) {
-      long long b = (long long)blockIdx.y * gridDim.x + blockIdx.x;
-      P.part[(3 + 2LL * P.stage) * P.nblk + b] = rs;
-      P.part[(4 + 2LL * P.stage) * P.nblk + b] = os;
+      P.part[(3 + 2LL * P.stage) * P.nblk + blk] = rs;
+      P.part[(4 + 2LL * P.stage) * P.nblk + blk] = os;
     }
   }
+}
+
+template <typename T, int TX, int TY, int MINB, bool P2>
+__global__ void __launch_bounds__(TX * TY, MINB) stage_kernel(const StageParams<T> P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  auto& s = *reinterpret_cast<StageSmem<T, TX, TY>*>(smem_raw);
+  stage_tile<T, TX, TY, P2>(P, blockIdx.x, blockIdx.y, (long long)blockIdx.y * gridDim.x + blockIdx.x, s);
+}
+
+// Batched stage: one launch covers every tile of every instance of a batch. tile_start has
+// ninst + 1 entries (prefix sums of the instances' tile counts); each CTA finds its instance,
+// copies that instance's parameters to shared memory and runs the same tile body. Instances
+// whose step is finished (their controller's done flag) return at once.
+template <typename T, int TX, int TY, int MINB, bool P2>
+__global__ void __launch_bounds__(TX * TY, MINB)
+    stage_batch_kernel(const StageParams<T>* __restrict__ Ps, const long long* __restrict__ tile_start, int ninst) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  auto& s = *reinterpret_cast<StageSmem<T, TX, TY>*>(smem_raw);
+  __shared__ StageParams<T> Psh;
+  __shared__ int inst_sh;
+  const long long tile = blockIdx.x;
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = ninst - 1;  // last instance with tile_start[i] <= tile
+    while (lo < hi) {
+      int mid = (lo + hi + 1) / 2;
+      if (tile_start[mid] <= tile) lo = mid;
+      else hi = mid - 1;
+    }
+    inst_sh = lo;
+    Psh = Ps[lo];
+  }
+  __syncthreads();
+  const long long local = tile - tile_start[inst_sh];
+  const int tiles_x = (Psh.nx + TX - 1) / TX;
+  stage_tile<T, TX, TY, P2>(Psh, int(local % tiles_x), int(local / tiles_x), local, s);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -677,8 +710,7 @@ template <int NT> __device__ double fixed_sum(const double* p, long long n, doub
   return r;
 }
 
-template <int NT> __global__ void __launch_bounds__(NT) finalize_kernel(const FinalizeParams F) {
-  __shared__ double red[NT];
+template <int NT> __device__ __forceinline__ void finalize_body(const FinalizeParams& F, double* red) {
   Ctl* ctl = F.ctl;
   if (ctl->done) return;
   // CFL max / min (NaN-propagating), order-independent
@@ -767,6 +799,20 @@ template <int NT> __global__ void __launch_bounds__(NT) finalize_kernel(const Fi
   if (ctl->budget > 0 && --ctl->budget == 0 && !ctl->done) ctl->done = 2;  // paused, step not over
 }
 
+template <int NT> __global__ void __launch_bounds__(NT) finalize_kernel(const FinalizeParams F) {
+  __shared__ double red[NT];
+  finalize_body<NT>(F, red);
+}
+
+// Batched finalize: one CTA per instance of a batch.
+template <int NT> __global__ void __launch_bounds__(NT) finalize_batch_kernel(const FinalizeParams* __restrict__ Fs) {
+  __shared__ double red[NT];
+  __shared__ FinalizeParams Fsh;
+  if (threadIdx.x == 0) Fsh = Fs[blockIdx.x];
+  __syncthreads();
+  finalize_body<NT>(Fsh, red);
+}
+
 #ifdef SV_DEFINE_COMMON_KERNELS
 // Host-API accept (RungeKutta.hpp:428-431): flip the state parity, apply the pending tallies.
 __global__ void accept_kernel(Ctl* ctl) {
@@ -784,6 +830,23 @@ __global__ void begin_step_kernel(Ctl* ctl, int new_step, long long budget) {
   }
   ctl->done = 0;
   ctl->budget = budget;
+}
+// start a new step on every instance of a batch
+__global__ void begin_batch_kernel(Ctl* const* ctls, int n, long long budget) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Ctl* c = ctls[i];
+  c->t_local = 0.0;
+  c->step_accepted = 0;
+  c->step_repeated = 0;
+  c->done = 0;
+  c->budget = budget;
+}
+// done flags of a batch into one array (1: step complete, nonzero error code: -1)
+__global__ void gather_done_kernel(Ctl* const* ctls, int n, int* done) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  done[i] = ctls[i]->error ? -1 : ctls[i]->done;
 }
 #endif
 

@@ -36,7 +36,15 @@ template <typename T> cudaError_t launch_volume(const T* h, int nx, int ny, doub
                                                 cudaStream_t s);
 template <typename T> cudaError_t launch_debug(const StageParams<T>& P, const DebugParams<T>& D, T* nh, T* sf,
                                                cudaStream_t s);
+// batched launches: every tile of every instance (tiled 32 x 8 kernel, 3 CTAs/SM); p2 when
+// every instance's dx and dy are powers of two
+template <typename T> cudaError_t launch_stage_batch(const StageParams<T>* Ps, const long long* tile_start, int ninst,
+                                                     long long total_tiles, bool p2, cudaStream_t s);
+constexpr int kBatchVariant = 1;
 cudaError_t launch_finalize(const FinalizeParams& F, cudaStream_t s);
+cudaError_t launch_finalize_batch(const FinalizeParams* Fs, int ninst, cudaStream_t s);
+cudaError_t launch_begin_batch(Ctl* const* ctls, int n, long long budget, cudaStream_t s);
+cudaError_t launch_gather_done(Ctl* const* ctls, int n, int* done, cudaStream_t s);
 cudaError_t launch_sum(const double* p, long long n, double* out, cudaStream_t s);
 cudaError_t launch_accept(Ctl* ctl, cudaStream_t s);
 cudaError_t launch_begin_step(Ctl* ctl, int new_step, long long budget, cudaStream_t s);

@@ -1,0 +1,99 @@
+"""Batches: uneven catchments advanced in shared launches give, member by member, the same
+bits as running each catchment alone (and as the oracle), including after members are
+removed and added between steps."""
+import numpy as np
+import pytest
+
+from mfcm_b200 import SaintVenantSolver, synth, start_new_step_forcing, RAIN_UNIFORM, EDGE_XMAX, EDGE_YMIN
+from mfcm_b200.batch import SaintVenantBatch
+from oracle.sv_oracle_py import OracleSolver
+from tests.scenarios import setup, rain_series, same
+
+pytestmark = pytest.mark.gpu
+
+CASES = [  # nx, ny, dx, rain mm/h, head edges, seed
+    (64, 40, 2.0, 60.0, EDGE_XMAX, 1),
+    (37, 91, 5.0, 30.0, EDGE_YMIN, 2),
+    (128, 17, 1.0, 90.0, EDGE_XMAX | EDGE_YMIN, 3),
+]
+
+
+def _init(b, nx, ny, dx, seed):
+    z = synth.plane_with_gaussians(nx, ny, dx, slope=0.01, seed=seed)
+    setup(b, z, np.full((ny, nx), 2e-3), np.zeros((ny, nx)), np.zeros((ny, nx)))
+
+
+def _forcing(t, L, rate, edges):
+    return start_new_step_forcing(t, L, rain=rain_series(rate * synth.MM_PER_H, stop=40.0), rain_kind=RAIN_UNIFORM,
+                                  head=0.0, head_edges=edges)
+
+
+def _run_alone(cls, case, steps, L=20.0):
+    nx, ny, dx, rate, edges, seed = case
+    s = cls(nx, ny, dx, cn_target=0.5, step_duration=L, rain_mode="physical")
+    _init(s, nx, ny, dx, seed)
+    for i in range(steps):
+        s.set_forcing(_forcing(i * L, L, rate, edges))
+        s.advance()
+    return [s.get_field(f) for f in ("H", "U", "V")], s.stats()
+
+
+def test_batch_members_match_solo_runs_and_oracle():
+    L, steps = 20.0, 3
+    batch = SaintVenantBatch("f64")
+    mem = []
+    for c in CASES:
+        m = batch.add(c[0], c[1], c[2], cn_target=0.5, step_duration=L, rain_mode="physical")
+        _init(m, c[0], c[1], c[2], c[5])
+        mem.append(m)
+    for i in range(steps):
+        for m, c in zip(mem, CASES):
+            m.set_forcing(_forcing(i * L, L, c[3], c[4]))
+        batch.advance()
+    for m, c in zip(mem, CASES):
+        solo, _ = _run_alone(SaintVenantSolver, c, steps, L)
+        orc, so = _run_alone(OracleSolver, c, steps, L)
+        for k, f in enumerate(("H", "U", "V")):
+            got = m.get_field(f)
+            assert same(got, solo[k]), f"{c}: {f} differs from the solo run"
+            assert same(got, orc[k]), f"{c}: {f} differs from the oracle"
+        assert abs(m.stats()["volume"] - so["volume"]) <= 1e-12 * so["volume"]
+    batch.close()
+
+
+def test_members_join_and_leave_between_steps():
+    L = 20.0
+    batch = SaintVenantBatch("f64")
+    a = batch.add(*CASES[0][:3], cn_target=0.5, step_duration=L, rain_mode="physical")
+    _init(a, CASES[0][0], CASES[0][1], CASES[0][2], CASES[0][5])
+    b = batch.add(*CASES[1][:3], cn_target=0.5, step_duration=L, rain_mode="physical")
+    _init(b, CASES[1][0], CASES[1][1], CASES[1][2], CASES[1][5])
+    for m, c in ((a, CASES[0]), (b, CASES[1])):
+        m.set_forcing(_forcing(0.0, L, c[3], c[4]))
+    batch.advance()
+    batch.remove(b)
+    c = batch.add(*CASES[2][:3], cn_target=0.5, step_duration=L, rain_mode="physical")
+    _init(c, CASES[2][0], CASES[2][1], CASES[2][2], CASES[2][5])
+    a.set_forcing(_forcing(L, L, CASES[0][3], CASES[0][4]))
+    c.set_forcing(_forcing(0.0, L, CASES[2][3], CASES[2][4]))
+    batch.advance()
+    assert batch.size()[0] == 2
+    solo_a, _ = _run_alone(SaintVenantSolver, CASES[0], 2, L)
+    solo_c, _ = _run_alone(SaintVenantSolver, CASES[2], 1, L)
+    for k, f in enumerate(("H", "U", "V")):
+        assert same(a.get_field(f), solo_a[k])
+        assert same(c.get_field(f), solo_c[k])
+    batch.close()
+
+
+def test_fp32_batch_close_to_fp64():
+    L, steps = 20.0, 2
+    b32 = SaintVenantBatch("f32")
+    m = b32.add(*CASES[0][:3], cn_target=0.5, step_duration=L, rain_mode="physical")
+    _init(m, CASES[0][0], CASES[0][1], CASES[0][2], CASES[0][5])
+    for i in range(steps):
+        m.set_forcing(_forcing(i * L, L, CASES[0][3], CASES[0][4]))
+        b32.advance()
+    ref, _ = _run_alone(OracleSolver, CASES[0], steps, L)
+    assert np.max(np.abs(m.get_field("H") - ref[0])) <= 1e-3
+    b32.close()
