@@ -1,0 +1,158 @@
+"""Continuous-batching flood-solve server.
+
+Requests (a catchment, its rainfall and a simulated horizon) arrive at wall-clock times. Each
+request is admitted into one running batch (mfcm_b200.batch) as soon as a slot and its device
+memory fit under the budget; admission happens at step boundaries, so requests that arrive
+while others are on the GPU join the same launches. A request leaves the batch when its
+horizon is reached, freeing its memory for the queue. Each request's results are
+bit-identical whether it runs alone or in the mix (members never share state).
+
+The reference has no serving layer; this is the north-star production pattern built on the
+same step (one `step()` of TypedTemporalScheme per batch advance, per member).
+"""
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import synth, TimeSeries, start_new_step_forcing, RAIN_UNIFORM
+from .batch import SaintVenantBatch
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float          # seconds after the server starts
+    nx: int
+    ny: int
+    dx: float
+    z: np.ndarray
+    rain: TimeSeries        # m/s, uniform over the catchment
+    horizon: float          # simulated seconds
+    n: float = 0.035
+    head_edges: int = 15    # outflow on every edge
+    # filled in by the server
+    admitted: float = math.nan
+    finished: float = math.nan
+    cell_updates: int = 0
+    steps: int = 0
+    result_h: np.ndarray = None
+    stats: dict = field(default_factory=dict)
+
+    @property
+    def latency(self):
+        return self.finished - self.arrival
+
+
+def triangular_hyetograph(peak_mm_h, duration_s, end=1e9):
+    """Rain rate rising linearly to peak at duration/2 and back to zero at duration."""
+    p = peak_mm_h * synth.MM_PER_H
+    return TimeSeries([0.0, duration_s / 2.0, duration_s, end], [0.0, p, 0.0, 0.0])
+
+
+def make_requests(rate, count, seed=0, side=(64, 512), dxs=(1.0, 2.0, 5.0), horizon=(120.0, 600.0),
+                  relief=(10.0, 150.0), peak=(20.0, 120.0), duration=(900.0, 7200.0), hurst=0.8):
+    """Poisson arrivals at `rate` requests/s; mesh side log-uniform on `side`; fractal beds."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(count):
+        t += rng.exponential(1.0 / rate)
+        s = int(round(math.exp(rng.uniform(math.log(side[0]), math.log(side[1])))))
+        dx = float(rng.choice(dxs))
+        z = synth.diamond_square(s, s, hurst, float(rng.uniform(*relief)), seed=seed * 100003 + i)
+        rain = triangular_hyetograph(float(rng.uniform(*peak)), float(rng.uniform(*duration)))
+        out.append(Request(i, t, s, s, dx, z, rain, float(rng.uniform(*horizon))))
+    return out
+
+
+class FloodServer:
+    def __init__(self, budget_bytes=150e9, max_slots=512, precision="f32", step_duration=60.0, cn_target=0.5,
+                 device=0):
+        self.batch = SaintVenantBatch(precision, "classic", device)
+        self.budget = float(budget_bytes)
+        self.max_slots = int(max_slots)
+        self.L = float(step_duration)
+        self.cn_target = float(cn_target)
+        self.value_bytes = 4 if precision == "f32" else 8
+
+    def estimate_bytes(self, req):
+        """Device memory of one member: 15 cell fields (two states, two stage buffers, bed and
+        its slopes), the per-cell Manning field, and the per-tile partial sums."""
+        cells = req.nx * req.ny
+        tiles = math.ceil(req.nx / 32) * math.ceil(req.ny / 8)
+        return cells * self.value_bytes * 16 + tiles * 11 * 8 + 4096
+
+    def _admit(self, req, now):
+        m = self.batch.add(req.nx, req.ny, req.dx, cn_target=self.cn_target, step_duration=self.L,
+                           rain_mode="physical")
+        m.set_field("Z", req.z)
+        zero = np.zeros((req.ny, req.nx))
+        m.set_field("H", zero)
+        m.set_field("U", zero)
+        m.set_field("V", zero)
+        m.set_manning(req.n, req.n, 0.1, 0.3)
+        req.admitted = now
+        return m
+
+    def run(self, requests, time_limit=None):
+        """Serve `requests` (sorted by arrival). Returns a summary dict; the requests carry
+        their own timings and results."""
+        pending = sorted(requests, key=lambda r: r.arrival)
+        active = {}   # slot -> (request, member, simulated time)
+        used = 0.0
+        t0 = time.perf_counter()
+        total_updates = 0
+        max_active = 0
+        while pending or active:
+            now = time.perf_counter() - t0
+            if time_limit is not None and now > time_limit:
+                break
+            while pending and pending[0].arrival <= now and len(active) < self.max_slots:
+                need = self.estimate_bytes(pending[0])
+                if used + need > self.budget and active:
+                    break  # wait for memory to free up
+                req = pending.pop(0)
+                m = self._admit(req, now)
+                active[m.slot] = [req, m, 0.0]
+                used += need
+            max_active = max(max_active, len(active))
+            if not active:
+                time.sleep(max(0.0, min(0.05, pending[0].arrival - now)))
+                continue
+            for slot, (req, m, t) in active.items():
+                m.set_forcing(start_new_step_forcing(t, self.L, rain=req.rain, rain_kind=RAIN_UNIFORM, head=0.0,
+                                                     head_edges=req.head_edges))
+            stats = self.batch.advance()
+            now = time.perf_counter() - t0
+            done = []
+            for slot, entry in active.items():
+                req, m, t = entry
+                st = stats[slot]
+                req.cell_updates += st["accepted"] * req.nx * req.ny
+                total_updates += st["accepted"] * req.nx * req.ny
+                req.steps += 1
+                entry[2] = t + self.L
+                if entry[2] >= req.horizon - 1e-9:
+                    req.result_h = m.get_field("H")
+                    req.stats = m.stats()
+                    req.finished = time.perf_counter() - t0
+                    done.append(slot)
+            for slot in done:
+                req, m, _ = active.pop(slot)
+                self.batch.remove(m)
+                used -= self.estimate_bytes(req)
+        wall = time.perf_counter() - t0
+        lat = np.array([r.latency for r in requests if not math.isnan(r.finished)])
+        return {
+            "requests": len(requests), "completed": int(lat.size), "wall_s": wall,
+            "p50_s": float(np.percentile(lat, 50)) if lat.size else None,
+            "p95_s": float(np.percentile(lat, 95)) if lat.size else None,
+            "p99_s": float(np.percentile(lat, 99)) if lat.size else None,
+            "cell_updates_per_s": total_updates / wall if wall > 0 else 0.0,
+            "max_concurrent": max_active,
+        }
+
+    def close(self):
+        self.batch.close()
