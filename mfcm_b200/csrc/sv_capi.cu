@@ -141,8 +141,12 @@ struct Solver final : public sv_ctx {
   T* S[2][3] = {};
   T* Y[2][3] = {};
   T* K[4][3] = {};
-  T* z = nullptr;
+  T* z = nullptr;                  // bed (FP32-with-datum mode: offset from the tile datum)
   T *zx = nullptr, *zy = nullptr;  // bed slopes (Constants.cpp:39-40)
+  bool datum = false;              // SV_F32_DATUM64
+  double* zdat = nullptr;          // per datum tile FP64 datum
+  int dtiles_x = 0, dtiles_y = 0;
+  std::vector<double> host_datum;
   T* man[4] = {};
   double man_s[4] = {0.03, 0.3, 0.1, 0.3};  // ManningRoughnessSourceTerm.cpp:99-102
   std::vector<double> host_n_shallow;
@@ -225,6 +229,14 @@ struct Solver final : public sv_ctx {
     SV_CUDA(alloc_cells(&z));
     SV_CUDA(alloc_cells(&zx));
     SV_CUDA(alloc_cells(&zy));
+    datum = (p->precision == SV_F32_DATUM64);
+    if (datum) {
+      dtiles_x = int((m->nx + svk::kDatumTX - 1) / svk::kDatumTX);
+      dtiles_y = int((m->ny + svk::kDatumTY - 1) / svk::kDatumTY);
+      SV_CUDA(alloc(&zdat, size_t(dtiles_x) * dtiles_y));
+      SV_CUDA(cudaMemsetAsync(zdat, 0, sizeof(double) * size_t(dtiles_x) * dtiles_y, stream));
+      host_datum.assign(size_t(dtiles_x) * dtiles_y, 0.0);
+    }
     SV_CUDA(alloc(&ctl, 1));
     SV_CUDA(alloc(&dbg_ctl, 1));
     SV_CUDA(alloc(&fc, 1));
@@ -297,6 +309,7 @@ struct Solver final : public sv_ctx {
       host_n_shallow.assign(host, host + n);
       if (man[1] == man[0] && man[1] != nullptr) { man[1] = nullptr; graph_dirty = true; ++pversion; }
     }
+    if (id == SV_FIELD_Z && datum) return set_bed_with_datum(host, n);
     int r = upload(*slot, host, n);
     if (r == SV_OK && id == SV_FIELD_Z) {
       cudaError_t e = svk::launch_bed_slopes<T>(z, int(mesh.nx), int(mesh.ny), mesh.dx, mesh.dy, zx, zy, stream);
@@ -304,6 +317,49 @@ struct Solver final : public sv_ctx {
       SV_CUDA(cudaStreamSynchronize(stream));
     }
     return r;
+  }
+
+  // FP32-with-datum bed: per 32 x 8 tile datum = the tile's lowest bed rounded down to a
+  // multiple of 2^-10 m (datum differences are then exact in FP64); stored bed = FP32
+  // offset from it; bed slopes from the FP64 bed (Minmod3 in FP64, rounded once).
+  int set_bed_with_datum(const double* host, uint64_t n) {
+    std::vector<double> dat(size_t(dtiles_x) * dtiles_y, 0.0);
+    std::vector<char> seen(dat.size(), 0);
+    for (uint64_t i = 0; i < n; ++i) {
+      double v = host[i];
+      if (v != v) continue;
+      int gx = int(i % mesh.nx), gy = int(i / mesh.nx);
+      size_t t = size_t(svk::datum_tile(gx, gy, dtiles_x));
+      if (!seen[t] || v < dat[t]) { dat[t] = v; seen[t] = 1; }
+    }
+    for (double& d : dat) d = std::floor(d * 1024.0) / 1024.0;
+    std::vector<T> off(n);
+    for (uint64_t i = 0; i < n; ++i) {
+      int gx = int(i % mesh.nx), gy = int(i / mesh.nx);
+      off[i] = T(host[i] - dat[size_t(svk::datum_tile(gx, gy, dtiles_x))]);
+    }
+    host_datum = dat;
+    SV_CUDA(cudaMemcpyAsync(z, off.data(), n * sizeof(T), cudaMemcpyHostToDevice, stream));
+    SV_CUDA(cudaMemcpyAsync(zdat, dat.data(), dat.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+    // FP64 slopes on a temporary device copy of the FP64 bed
+    double *dz = nullptr, *dzx = nullptr, *dzy = nullptr;
+    SV_CUDA(cudaMalloc(&dz, n * sizeof(double)));
+    SV_CUDA(cudaMalloc(&dzx, n * sizeof(double)));
+    SV_CUDA(cudaMalloc(&dzy, n * sizeof(double)));
+    SV_CUDA(cudaMemcpyAsync(dz, host, n * sizeof(double), cudaMemcpyHostToDevice, stream));
+    cudaError_t e = svk::launch_bed_slopes<double>(dz, int(mesh.nx), int(mesh.ny), mesh.dx, mesh.dy, dzx, dzy, stream);
+    std::vector<double> hx(n), hy(n);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hx.data(), dzx, n * sizeof(double), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hy.data(), dzy, n * sizeof(double), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    cudaFree(dz); cudaFree(dzx); cudaFree(dzy);
+    if (e != cudaSuccess) return cuda_fail(e, "datum bed slopes");
+    std::vector<T> fx(n), fy(n);
+    for (uint64_t i = 0; i < n; ++i) { fx[i] = T(hx[i]); fy[i] = T(hy[i]); }
+    SV_CUDA(cudaMemcpyAsync(zx, fx.data(), n * sizeof(T), cudaMemcpyHostToDevice, stream));
+    SV_CUDA(cudaMemcpyAsync(zy, fy.data(), n * sizeof(T), cudaMemcpyHostToDevice, stream));
+    SV_CUDA(cudaStreamSynchronize(stream));
+    return SV_OK;
   }
 
   int debug_ptr(int id, T*& p, long long& count) {
@@ -348,7 +404,11 @@ struct Solver final : public sv_ctx {
       src = *slot;
     }
     if ((long long)n != count) return fail(SV_E_ARG, "field size mismatch");
-    return download(src, host, n);
+    int r = download(src, host, n);
+    if (r == SV_OK && datum && id == SV_FIELD_Z)
+      for (uint64_t i = 0; i < n; ++i)
+        host[i] += host_datum[size_t(svk::datum_tile(int(i % mesh.nx), int(i / mesh.nx), dtiles_x))];
+    return r;
   }
 
   int set_manning(double a, double b, double c, double d) override {
@@ -422,6 +482,8 @@ struct Solver final : public sv_ctx {
     P.z = z;
     P.zx = zx;
     P.zy = zy;
+    P.zdat = datum ? zdat : nullptr;
+    P.dtiles_x = dtiles_x;
     for (int i = 0; i < 4; ++i) { P.man_p[i] = man[i]; P.man_s[i] = T(man_s[i]); }
     P.fc = fc;
     P.q0p = q0; P.q1p = q1; P.pat = pat; P.hb0p = hb0; P.hb1p = hb1;
@@ -498,6 +560,7 @@ struct Solver final : public sv_ctx {
 
   int eval_dudt(int state_no, double t_sub, double dt) override {
     if (state_no != 0) return fail(SV_E_ARG, "only U_[0] is stored between calls");
+    if (datum) return fail(SV_E_STATE, "per-function evaluation is not available with tile datums");
     if (!dbg_k[0]) {
       for (int f = 0; f < 3; ++f) SV_CUDA(alloc_cells(&dbg_k[f]));
       for (int f = 0; f < 8; ++f) SV_CUDA(alloc_cells(&dbg_slp[f]));
@@ -994,7 +1057,7 @@ int sv_create(const sv_mesh_desc* mesh, const sv_params* params, int device, sv_
     auto* s = new Solver<double>();
     r = s->init(mesh, params, device);
     c = s;
-  } else if (params->precision == SV_F32) {
+  } else if (params->precision == SV_F32 || params->precision == SV_F32_DATUM64) {
     auto* s = new Solver<float>();
     r = s->init(mesh, params, device);
     c = s;
@@ -1043,7 +1106,7 @@ int sv_batch_create(int precision, int rk_method, int device, sv_batch** out) {
     auto* x = new Batch<double>();
     b.reset(x);
     r = x->init(precision, rk_method, device);
-  } else if (precision == SV_F32) {
+  } else if (precision == SV_F32 || precision == SV_F32_DATUM64) {
     auto* x = new Batch<float>();
     b.reset(x);
     r = x->init(precision, rk_method, device);

@@ -68,6 +68,8 @@ template <typename T> struct StageParams {
   const T* Kin[4][3];    // stored k_j, j < s (M_STOREK)
   const T* z;
   const T* zx; const T* zy;   // bed slopes dz/dx, dz/dy (Constants.cpp:39-40), precomputed
+  const double* zdat;         // FP32-with-datum mode: per datum tile FP64 datum (z = datum + z_off)
+  int dtiles_x;               // datum tiles per row
   const T* man_p[4];     // per-cell n_shallow, n_deep, d_shallow, d_deep, or nullptr
   T man_s[4];            // uniform values where man_p is nullptr
   const DevForcing* fc;  // per-step boundary values
@@ -88,6 +90,24 @@ template <typename T> struct StageParams {
 __host__ __device__ inline long long part_count(long long nblk, int nstages) { return (3 + 2LL * nstages) * nblk; }
 
 template <typename T> __device__ __forceinline__ T ld(const T* p, long long i) { return __ldg(p + i); }
+
+// Datum tiles of the FP32-with-datum mode: 32 x 8 cells, each with an FP64 datum; the stored
+// bed is the FP32 offset from its tile's datum.
+constexpr int kDatumTX = 32, kDatumTY = 8;
+__host__ __device__ inline long long datum_tile(int gx, int gy, int dtiles_x) {
+  return (long long)(gy / kDatumTY) * dtiles_x + gx / kDatumTX;
+}
+// Bed of cell (gx, gy) in the frame of datum tile `ref`: the stored value itself, or, for a
+// cell of another datum tile, its offset moved by the FP64 datum difference and rounded once.
+template <typename T>
+__device__ __forceinline__ T load_bed(const T* z, const double* zdat, int dtiles_x, long long g, int gx, int gy,
+                                      long long ref) {
+  const T zo = __ldg(z + g);
+  if (!zdat) return zo;
+  const long long t = datum_tile(gx, gy, dtiles_x);
+  if (t == ref) return zo;
+  return T(double(zo) + (__ldg(zdat + t) - __ldg(zdat + ref)));
+}
 
 // NaN-propagating max/min for the CFL reduction
 __device__ __forceinline__ double nmax(double a, double b) { return (a != a || b != b) ? (a + b) : (a > b ? a : b); }
@@ -320,6 +340,7 @@ __device__ __forceinline__ void stage_tile(const StageParams<T>& P, int bx, int 
 
   // phase 1: tile + 2-cell halo of h, u, v, z (clamped at the mesh edge; the clamped
   // copies are never used because edge faces and edge slopes use the cell itself)
+  const long long zref = P.zdat ? datum_tile(x0, y0, P.dtiles_x) : 0;
   for (int i = tid; i < SM::RX * SM::RY; i += NT) {
     int lx = i % SM::RX, ly = i / SM::RX;
     int gx = min(max(x0 - 2 + lx, 0), nx - 1);
@@ -328,7 +349,7 @@ __device__ __forceinline__ void stage_tile(const StageParams<T>& P, int bx, int 
     s.val[0][ly][lx] = ld(Yh, g);
     s.val[1][ly][lx] = ld(Yu, g);
     s.val[2][ly][lx] = ld(Yv, g);
-    s.val[3][ly][lx] = ld(P.z, g);
+    s.val[3][ly][lx] = load_bed(P.z, P.zdat, P.dtiles_x, g, gx, gy, zref);
   }
   __syncthreads();
 
@@ -574,12 +595,14 @@ __global__ void __launch_bounds__(32 * WPB, MINB) sweep_kernel(const StageParams
   c.manning = P.manning; c.rain_mode = P.rain_mode; c.head_first = P.head_first;
   const DevForcing fc = *P.fc;
 
+  const long long zref = P.zdat ? datum_tile(min(tile_x * kSweepOut, nx - 1), y0, P.dtiles_x) : 0;
   auto load_row = [&](int gy) {
     const int r = min(max(gy, 0), ny - 1);
     const long long g = (long long)r * nx + gxc;
     RowV<T> v;
     v.h = ld(Yh, g); v.u = ld(Yu, g); v.v = ld(Yv, g);
-    v.z = ld(P.z, g); v.zx = ld(P.zx, g); v.zy = ld(P.zy, g);
+    v.z = load_bed(P.z, P.zdat, P.dtiles_x, g, gxc, r, zref);
+    v.zx = ld(P.zx, g); v.zy = ld(P.zy, g);
     return v;
   };
 
