@@ -1,24 +1,39 @@
 #!/usr/bin/env python
-"""Throughput of the B200 Saint-Venant RK time step on the single large catchment:
-4096 x 4096 cells, dx = 2 m, diamond-square bed (Hurst 0.8, 100 m relief) + 0.005 slope,
-lognormal rainfall field (mean 30 mm/h) for 1800 s, Voronoi Manning classes, outflow on
-every edge, classic RK4, CFL target 0.5.
+"""Throughput of the B200 Saint-Venant RK time step.
 
-One "step" of this benchmark is one accepted RK4 timestep of the whole grid; the metric is
-cell-updates/s (cells x accepted timesteps / device seconds). Inputs are seeded synthetic
-fields with the workload's shapes and statistics. Before timing, the catchment is spun up
-from dry for --spinup timesteps so the timed timesteps see wet/dry fronts and channel
-flow. Every state field (134 MB in FP64) is larger than the 126 MB L2.
+Workload: the single large catchment. It is 4096 x 4096 cells at dx = 2 m, with a
+diamond-square bed (Hurst 0.8, 100 m relief) plus a 0.005 regional slope. Rainfall is a
+lognormal field (mean 30 mm/h, sigma_log 0.5, smoothed over 200 m) for 1800 s. Manning n comes
+from Voronoi land classes, and every edge is an outflow. The scheme is classic RK4 at CFL 0.5.
+
+The metric: batched FP32 vs plain FP64 cell-updates/s at <= 1 mm depth error, with p50/p99
+latency.
+
+- `value` is the FP32 path (FP32 state and arithmetic, bed as FP32 offsets from FP64 tile
+  datums, FP64 reductions and dt control). It counts cell-updates/s: cells x accepted
+  timesteps per device second.
+- `fp64` is the plain FP64 path, which is bit-identical to the reference arithmetic.
+- `precision` gives the FP32 paths' max depth error against FP64 on a dam break over a 350 m
+  bed (the wet/dry-front precision study).
+- `serving` gives p50/p95/p99 latency of a continuous-batching run.
+- `batched` gives the throughput of an ensemble of uneven catchments advancing in shared
+  launches.
+
+One "step" is one accepted RK4 timestep of the whole grid. Inputs are seeded synthetic fields
+with the workload's shapes and statistics. Before timing, each precision is spun up from dry
+for --spinup timesteps. Every FP64 state field (134 MB) is larger than the 126 MB L2.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-Under torchrun each rank runs an independent replica on its own GPU (replicas only: one
-catchment never spans GPUs); timing is the max over ranks, value sums the ranks' work.
---impl reference times the CPU oracle (the reference's arithmetic restated in C++, OpenMP on
-all host cores) on a bounded sample of the same workload; rank 0 alone runs it.
+Under torchrun each rank runs an independent replica on its own GPU: one catchment never
+spans GPUs. The time is the max over ranks, and the value sums the ranks' work.
+--impl reference times the CPU oracle on a bounded window of the same workload, with OpenMP
+on all host cores. The oracle restates the reference's arithmetic in C++ at the reference's
+shipped FP32 precision. Rank 0 alone runs it.
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -33,24 +48,26 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Batched FP32 vs plain FP64 cell-updates/s at ≤1mm depth err; p50/p99 latency"
 UNIT = "cell-updates/s"
-# algorithmic HBM bytes per cell-update, one pass per RK stage (classic RK4):
-# 52 values (state in/out, accumulator, bed) + 4 (per-cell n) + 4 (per-cell rain pattern)
+# algorithmic HBM values per cell-update, one pass per RK stage (classic RK4):
+# 52 (state in/out, accumulator, bed) + 4 (per-cell Manning n) + 4 (per-cell rain pattern)
 VALUES_PER_CELL_UPDATE = 60
 
 
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=200)
-    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--steps", type=int, default=100)
+    p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--precision", default="f64", choices=["f64", "f32"])
+    p.add_argument("--precision", default="f32_datum64", choices=["f32_datum64", "f32", "f64"],
+                   help="precision of the headline value")
     p.add_argument("--size", type=int, default=4096)
     p.add_argument("--spinup", type=int, default=600, help="timesteps run from dry before timing")
-    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--variant", default="auto", help="stage-kernel variant 0-6, or auto (autotune)")
+    p.add_argument("--no-extras", action="store_true", help="skip the fp64, precision, serving, batched parts")
+    p.add_argument("--variant", default="auto", help="stage-kernel variant 0-8, or auto (autotune)")
     return p.parse_args()
 
 
@@ -116,34 +133,27 @@ def reduce_over_ranks(ms, work, dist, device="cpu"):
 
 def workload(size):
     from mfcm_b200 import synth
-    nx = ny = size
-    w = synth.config2(nx, ny, 2.0, seed=2)
-    return w
+    return synth.config2(size, size, 2.0, seed=2)
 
 
 def rain_series():
     from mfcm_b200 import TimeSeries
-    # uniform time profile of the spatial field: on for the first 1800 s
+    # uniform time profile of the spatial rain field: on for the first 1800 s
     return TimeSeries([0.0, 1800.0, 1800.001, 1e7], [1.0, 1.0, 0.0, 0.0])
 
 
-def make_solver(w, precision, device):
+def make_solver(w, precision, device, **kw):
     from mfcm_b200 import SaintVenantSolver
     s = SaintVenantSolver(w["nx"], w["ny"], w["dx"], precision=precision, cn_target=0.5,
-                          rain_mode="physical", step_duration=60.0, initial_dt=1.0, device=device)
-    upload(s, w)
-    return s
-
-
-def upload(s, w):
+                          rain_mode="physical", step_duration=60.0, initial_dt=1.0, device=device, **kw)
     zeros = np.zeros((w["ny"], w["nx"]))
     s.set_field("Z", w["z"])
-    s.set_field("H", zeros)
-    s.set_field("U", zeros)
-    s.set_field("V", zeros)
+    for f in ("H", "U", "V"):
+        s.set_field(f, zeros)
     s.set_field("N_SHALLOW", w["n"])
     s.set_field("N_DEEP", w["n"])
     s.set_field("RAIN_PATTERN", w["rain"])
+    return s
 
 
 def forcing_at(t, L):
@@ -165,9 +175,8 @@ class Runner:
         """Run n timesteps (accepted or repeated), crossing step boundaries as needed."""
         tot = {"total_ms": 0.0, "stage_ms": 0.0, "finalize_ms": 0.0, "stage_launches": 0, "finalize_launches": 0,
                "begin_launches": 0, "timesteps": 0}
-        st0 = self.s.stats()
+        last = self.s.stats()
         done_so_far = 0
-        last = st0
         while done_so_far < n:
             if self.need_begin:
                 self.s.set_forcing(forcing_at(self.t_step, self.L))
@@ -195,13 +204,10 @@ class Runner:
             self.run(timesteps)
 
 
-def roofline_traffic(precision):
-    """Per-launch DRAM bytes of the stage kernel from the committed ncu capture, scaled to
-    the 4096^2 grid (None when no capture was committed)."""
-    p = os.path.join(ROOT, "profiles", f"stage_kernel_{precision}_traffic.json")
+def profile_traffic(name):
+    """Per-launch DRAM bytes per cell of a stage kernel from a committed ncu capture."""
     try:
-        d = json.load(open(p))
-        return d["bytes_per_cell_per_launch"]
+        return json.load(open(os.path.join(ROOT, "profiles", name)))["bytes_per_cell_per_launch"]
     except Exception:
         return None
 
@@ -214,9 +220,151 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def cpu_baseline(w, state, cpu_seconds, precision="f64"):
-    """The oracle (reference arithmetic restated in C++, OpenMP, all host threads) on a
-    1024 x 1024 window of the spun-up catchment; timed over whole accepted timesteps."""
+def timed_run(w, precision, args, device, barrier, dist):
+    """Spin up, pick the kernel, then time args.steps timesteps with per-kernel events."""
+    solver = make_solver(w, precision, device)
+    runner = Runner(solver)
+    if args.variant == "auto":
+        first = min(50, args.spinup)
+        runner.spinup(first)
+        variant = solver.autotune()
+        runner.spinup(args.spinup - first)
+    else:
+        variant = int(args.variant)
+        solver.set_kernel_variant(variant)
+        runner.spinup(args.spinup)
+    runner.run(max(3, args.warmup))
+    st0 = solver.stats()
+    barrier()
+    sampler = ClockSampler(device)
+    sampler.start()
+    _, tm = runner.run(args.steps, timing=True)
+    barrier()
+    clocks = sampler.stop()
+    st1 = solver.stats()
+    ncells = w["nx"] * w["ny"]
+    accepted = st1["accepted"] - st0["accepted"]
+    repeated = st1["repeated"] - st0["repeated"]
+    ms_max, work = reduce_over_ranks(tm["total_ms"], float(accepted * ncells), dist, f"cuda:{device}")
+    bpv = 8 if precision == "f64" else 4
+    alg_bytes_launch = VALUES_PER_CELL_UPDATE / 4.0 * bpv * ncells
+    stage_avg_s = tm["stage_ms"] * 1e-3 / max(1, solver.nstages * tm["timesteps"])
+    achieved = alg_bytes_launch / stage_avg_s / 1e9
+    peak, peak_kind = measured_peaks()
+    kernel = "stage_kernel" if variant < 4 else "sweep_kernel"
+    traffic_pc = profile_traffic(f"{kernel}_{'f64' if precision == 'f64' else 'f32'}_2048_traffic.json")
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": (traffic_pc * ncells if traffic_pc else None), "peak_kind": peak_kind,
+            "kernel": f"{kernel} (variant {variant})", "alg_bytes_per_launch": alg_bytes_launch,
+            "stage_launch_ms": stage_avg_s * 1e3, "stage_share_of_step": tm["stage_ms"] / max(1e-9, tm["total_ms"])}
+    res = {"value": work / (ms_max * 1e-3), "ms": ms_max, "accepted": accepted, "repeated": repeated,
+           "variant": variant, "roofline": roof, "clocks": clocks, "timesteps": tm["timesteps"],
+           "sim_time_s": runner.t_step,
+           "launches": int(tm["stage_launches"] + tm["finalize_launches"] + tm["begin_launches"])}
+    return solver, res
+
+
+def precision_study(device, nx=2048, ny=256, dx=0.5, seconds=20.0):
+    """Dam break on a flat bed at 350 m (h = 1 m upstream, dry downstream, frictionless):
+    max depth error and relative volume error of the FP32 paths against FP64, and the front
+    position against Ritter's 2 sqrt(g h0) t."""
+    from mfcm_b200 import SaintVenantSolver, synth
+    z, h = synth.dam_break(nx, ny, 350.0, 1.0)
+    out = {}
+    for prec in ("f64", "f32", "f32_datum64"):
+        s = SaintVenantSolver(nx, ny, dx, precision=prec, cn_target=0.5, step_duration=seconds, manning=False,
+                              initial_dt=0.01, device=device)
+        s.set_field("Z", z)
+        s.set_field("H", h)
+        s.advance()
+        out[prec] = (s.get_field("H"), s.stats()["volume"])
+        s.close()
+    h64, v64 = out["f64"]
+    mid = nx // 2
+    wet = np.where(h64[ny // 2, mid:] > 1e-3)[0]
+    front = (wet.max() + 1) * dx if wet.size else 0.0
+    res = {"case": f"dam break {nx}x{ny}, dx={dx} m, bed 350 m, {seconds:.0f} s",
+           "front_m": front, "ritter_front_m": 2.0 * math.sqrt(9.81 * 1.0) * seconds}
+    for prec in ("f32", "f32_datum64"):
+        hp, vp = out[prec]
+        res[prec] = {"max_depth_err_m": float(np.max(np.abs(hp - h64))), "rel_volume_err": abs(vp - v64) / v64}
+    return res
+
+
+def serving_run(device, rate=20.0, count=40, precision="f32_datum64"):
+    from mfcm_b200.serving import FloodServer, make_requests
+    reqs = make_requests(rate, count, seed=11, side=(128, 512), horizon=(120.0, 600.0))
+    srv = FloodServer(budget_bytes=150e9, precision=precision, device=device)
+    summary = srv.run(reqs, time_limit=120.0)
+    srv.close()
+    summary.update({"arrival_rate_per_s": rate, "mesh_side": [128, 512], "horizon_s": [120, 600]})
+    return summary
+
+
+def batched_run(device, count=24, steps=20, precision="f32_datum64"):
+    """An ensemble of uneven catchments (sides log-uniform on [256, 1024], rounded to 32,
+    aspect U(0.5, 2), catchment beds with 0.5-3 % regional slope, uniform rain) advanced in
+    shared launches. Only members that complete a step count toward the throughput."""
+    from mfcm_b200 import synth, start_new_step_forcing, RAIN_UNIFORM
+    from mfcm_b200.batch import SaintVenantBatch
+    from mfcm_b200.serving import catchment_bed
+    rng = np.random.default_rng(13)
+    b = SaintVenantBatch(precision, device=device)
+    b.set_step_limit(20000)
+    mem = []
+    for i in range(count):
+        side = math.exp(rng.uniform(math.log(256), math.log(1024)))
+        asp = rng.uniform(0.5, 2.0)
+        nx = max(32, int(round(side * math.sqrt(asp) / 32)) * 32)
+        ny = max(32, int(round(side / math.sqrt(asp) / 32)) * 32)
+        m = b.add(nx, ny, 2.0, cn_target=0.5, step_duration=10.0, rain_mode="physical")
+        z = catchment_bed(nx, ny, 2.0, rng.uniform(0.005, 0.03), rng.uniform(0.01, 0.03), 1000 + i)
+        m.set_field("Z", z)
+        m.set_field("H", np.full((ny, nx), 0.01))
+        m.set_manning(*(2 * [rng.uniform(0.02, 0.08)]), 0.1, 0.3)
+        rate = rng.uniform(10, 100) * synth.MM_PER_H
+        mem.append((m, rate, nx * ny))
+    import torch
+    for m, rate, _ in mem:
+        m.set_forcing(start_new_step_forcing(0.0, 10.0, rain=rate, rain_kind=RAIN_UNIFORM, head=0.0, head_edges=15))
+    cells = sum(n for _, _, n in mem)
+    failed = 0
+    st = b.advance(raise_on_error=False)  # warm-up step
+    live = []
+    for m, rate, n in mem:
+        if st[m.slot]["status"] != 0:
+            failed += 1
+            b.remove(m)
+        else:
+            live.append((m, rate, n))
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    work = 0
+    for k in range(1, steps + 1):
+        for m, rate, _ in live:
+            m.set_forcing(start_new_step_forcing(10.0 * k, 10.0, rain=rate, rain_kind=RAIN_UNIFORM, head=0.0,
+                                                 head_edges=15))
+        st = b.advance(raise_on_error=False)
+        keep = []
+        for m, rate, n in live:
+            if st[m.slot]["status"] != 0:   # blown up: leaves the ensemble, its work is not counted
+                failed += 1
+                b.remove(m)
+            else:
+                work += st[m.slot]["accepted"] * n
+                keep.append((m, rate, n))
+        live = keep
+    torch.cuda.synchronize(device)
+    el = time.perf_counter() - t0
+    b.close()
+    return {"catchments": count, "cells": cells, "steps": steps, "step_s": 10.0, "cell_updates_per_s": work / el,
+            "seconds": el, "failed_members": failed}
+
+
+def cpu_baseline(w, state, cpu_seconds, precision):
+    """The oracle (the reference's arithmetic restated in C++, OpenMP, all host threads) on a
+    1024 x 1024 window of the catchment, at the given state; timed over whole accepted
+    timesteps."""
     from oracle.sv_oracle_py import OracleSolver, threads_available
     threads = os.cpu_count() or 1
     n = min(1024, w["nx"])
@@ -231,10 +379,8 @@ def cpu_baseline(w, state, cpu_seconds, precision="f64"):
     o.set_field("N_DEEP", w["n"][sl])
     o.set_field("RAIN_PATTERN", w["rain"][sl])
     o.set_forcing(forcing_at(600.0, 60.0))
-    o.set_dt(state["dt"])
-    t_local, dt = 0.0, state["dt"]
-    # one untimed warm-up timestep, then whole accepted timesteps until the budget is used
-    cn, rep, nd = o.do_timestep(t_local, dt)
+    dt = state["dt"]
+    cn, rep, nd = o.do_timestep(0.0, dt)  # one untimed warm-up timestep
     if not rep:
         o.accept()
     dt = nd
@@ -249,149 +395,58 @@ def cpu_baseline(w, state, cpu_seconds, precision="f64"):
     el = time.perf_counter() - t0
     used = threads_available(True)
     return {"value": acc * n * n / el, "unit": UNIT, "cores": used, "kind": "port",
-            "sample": f"{acc} accepted RK4 timesteps of a {n}x{n} window of the spun-up 4096^2 catchment "
-                      f"({precision}, {el:.1f} s, OpenMP {used} threads)"}
+            "sample": f"{acc} accepted RK4 timesteps of a {n}x{n} window of the {w['nx']}x{w['ny']} catchment "
+                      f"(oracle {precision}, {el:.1f} s, OpenMP {used} threads)"}
+
+
+def oracle_precision(p):
+    return "f64" if p == "f64" else "f32"
 
 
 def run_reference(args):
     rank, _, world = dist_env()
     if rank != 0:
         return 0
-    w = workload(min(args.size, 1024))
+    w = workload(args.size)
     zeros = np.zeros((w["ny"], w["nx"]))
-    # state: a thin film stands in for the spun-up state (no GPU on this arm)
+    # state: a 2 cm film stands in for the spun-up state (this arm has no GPU spin-up)
     state = {"h": zeros + 0.02, "u": zeros, "v": zeros, "dt": 0.5}
-    per_step = max(2.0, args.cpu_seconds / max(1, args.steps))
+    prec = oracle_precision(args.precision)
+    # each step is a bounded sample (about 1 s of CPU work; at least one whole timestep)
+    per_step = max(0.6, min(2.0, 120.0 / max(1, args.steps)))
     vals = []
-    for _ in range(args.warmup if args.warmup < 2 else 1):
-        cpu_baseline(w, state, min(per_step, 2.0), args.precision)
+    cpu_baseline(w, state, per_step, prec)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        vals.append(cpu_baseline(w, state, per_step, args.precision))
+        vals.append(cpu_baseline(w, state, per_step, prec))
     el = time.perf_counter() - t0
     v = statistics.median([x["value"] for x in vals])
     cb = dict(vals[-1])
     cb["value"] = v
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * el / max(1, args.steps), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
-            "impl": "reference", "cpu_baseline": cb,
+            "vs_baseline": None, "dtype": prec, "data": "synthetic", "impl": "reference", "cpu_baseline": cb,
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "config": {"workload": f"{w['nx']}x{w['ny']} window of the 4096x4096 dx=2 m catchment (oracle port, "
-                                   "reference not buildable here)", "scheme": "classic RK4", "cn_target": 0.5}}
+            "config": {"workload": f"1024x1024 window of the {w['nx']}x{w['ny']} dx=2 m catchment, oracle port of "
+                                   "the reference arithmetic (the reference itself does not build here)",
+                       "scheme": "classic RK4", "cn_target": 0.5}}
     print(json.dumps(line), flush=True)
     return 0
 
 
-def main():
-    args = parse()
-    if args.impl == "reference":
-        return run_reference(args)
-    rank, local_rank, world = dist_env()
-    import torch
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        torch.cuda.set_device(local_rank)
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
-    device = local_rank
-    torch.cuda.set_device(device)
-
-    w = workload(args.size)
-    ncells = w["nx"] * w["ny"]
-    solver = make_solver(w, args.precision, device)
-    runner = Runner(solver)
-    if args.variant == "auto":
-        # tune on a partly spun-up state, then finish the spin-up with the chosen kernel
-        first = min(50, args.spinup)
-        runner.spinup(first)
-        variant = solver.autotune()
-        runner.spinup(args.spinup - first)
-    else:
-        variant = int(args.variant)
-        solver.set_kernel_variant(variant)
-        runner.spinup(args.spinup)
-    # warm-up timesteps (untimed)
-    runner.run(max(3, args.warmup))
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize(device)
-
-    sampler = ClockSampler(device)
-    barrier()
-    st0 = solver.stats()
-    sampler.start()
-    last, tm = runner.run(args.steps, timing=True)
-    barrier()
-    clocks = sampler.stop()
-    st1 = solver.stats()
-    accepted = st1["accepted"] - st0["accepted"]
-    repeated = st1["repeated"] - st0["repeated"]
-    ms_max, work = reduce_over_ranks(tm["total_ms"], float(accepted * ncells), dist, f"cuda:{device}")
-    value = work / (ms_max * 1e-3)
-
-    # roofline of the dominant kernel (the fused stage kernel)
-    bpv = 8 if args.precision == "f64" else 4
-    alg_bytes_launch = VALUES_PER_CELL_UPDATE / 4.0 * bpv * ncells
-    real_stage_launches = solver.nstages * tm["timesteps"]
-    stage_avg_s = tm["stage_ms"] * 1e-3 / max(1, real_stage_launches)
-    achieved = alg_bytes_launch / stage_avg_s / 1e9
-    peak, peak_kind = measured_peaks()
-    traffic_pc = roofline_traffic(args.precision)
-    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": (traffic_pc * ncells if traffic_pc else None), "peak_kind": peak_kind,
-            "alg_bytes_per_launch": alg_bytes_launch, "stage_launch_ms": stage_avg_s * 1e3,
-            "stage_share_of_step": tm["stage_ms"] / max(1e-9, tm["total_ms"])}
-
-    state = None
-    if rank == 0 and (not args.no_cpu or not args.no_e2e):
-        state = {"h": solver.get_field("H"), "u": solver.get_field("U"), "v": solver.get_field("V"),
-                 "dt": solver.get_dt()}
-
-    e2e = None
-    if not args.no_e2e:
-        e2e = measure_e2e(w, args, device, state)
-    cb = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        cb = cpu_baseline(w, state, args.cpu_seconds, args.precision)
-
-    if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms_max / max(1, args.steps), "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
-                "config": {"workload": f"single catchment {w['nx']}x{w['ny']}, dx=2 m (diamond-square H0.8 100 m + "
-                                       "0.005 slope, lognormal rain field 30 mm/h, Voronoi n, outflow all edges)",
-                           "scheme": "classic RK4", "cn_target": 0.5, "precision": args.precision,
-                           "spinup_timesteps": args.spinup, "sim_time_s": runner.t_step, "l2": "inputs larger than L2 (each state field 134 MB)",
-                           "parallelism": f"replicas x{world}", "kernel_variant": variant, "accepted": accepted, "repeated": repeated},
-                "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "clocks": clocks,
-                "gpu_launches": int(tm["stage_launches"] + tm["finalize_launches"] + tm["begin_launches"])}
-        print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
-    solver.close()
-    return 0
-
-
-def measure_e2e(w, args, device, state):
+def measure_e2e(w, args, device, state, variant, precision):
     """End to end through the public API from host arrays: upload the inputs (bed, state,
     Manning n, rain pattern) from pinned host memory, run the same number of timesteps, read
     the state back; wall clock with the device synchronised on both sides."""
     import torch
     from mfcm_b200 import SaintVenantSolver
     pinned = {}
-    for k, a in (("z", w["z"]), ("n", w["n"]), ("rain", w["rain"]),
-                 ("h", state["h"] if state else np.zeros_like(w["z"])),
-                 ("u", state["u"] if state else np.zeros_like(w["z"])),
-                 ("v", state["v"] if state else np.zeros_like(w["z"]))):
-        t = torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).pin_memory()
-        pinned[k] = t.numpy()
-    s = SaintVenantSolver(w["nx"], w["ny"], w["dx"], precision=args.precision, cn_target=0.5, rain_mode="physical",
-                          step_duration=60.0, initial_dt=state["dt"] if state else 1.0, device=device)
+    for k, a in (("z", w["z"]), ("n", w["n"]), ("rain", w["rain"]), ("h", state["h"]), ("u", state["u"]),
+                 ("v", state["v"])):
+        pinned[k] = torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).pin_memory().numpy()
+    s = SaintVenantSolver(w["nx"], w["ny"], w["dx"], precision=precision, cn_target=0.5, rain_mode="physical",
+                          step_duration=60.0, initial_dt=state["dt"], device=device)
+    s.set_kernel_variant(variant)
     torch.cuda.synchronize(device)
     t0 = time.perf_counter()
     s.set_field("Z", pinned["z"])
@@ -404,20 +459,85 @@ def measure_e2e(w, args, device, state):
     r = Runner(s, t0=600.0)
     r.run(args.steps)
     st = s.stats()
-    out_h = s.get_field("H")
-    out_u = s.get_field("U")
-    out_v = s.get_field("V")
+    out = [s.get_field(f) for f in ("H", "U", "V")]
     torch.cuda.synchronize(device)
     el = time.perf_counter() - t0
     ncells = w["nx"] * w["ny"]
-    h2d = 6 * ncells * 8
-    d2h = 3 * ncells * 8 + 40
     s.close()
-    del out_h, out_u, out_v
+    del out
     return {"value": st["accepted"] * ncells / el, "unit": UNIT,
-            "h2d_bytes_per_step": h2d / max(1, args.steps), "d2h_bytes_per_step": d2h / max(1, args.steps),
+            "h2d_bytes_per_step": 6 * ncells * 8 / max(1, args.steps),
+            "d2h_bytes_per_step": (3 * ncells * 8 + 40) / max(1, args.steps),
             "seconds": el, "accepted": st["accepted"],
-            "what": "upload bed/state/n/rain from pinned host memory, run the timesteps, read h/u/v back"}
+            "what": "upload bed/state/n/rain (FP64 host arrays) from pinned memory, run the timesteps, read h/u/v back"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    rank, local_rank, world = dist_env()
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    device = local_rank
+    torch.cuda.set_device(device)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(device)
+
+    w = workload(args.size)
+    solver, main_res = timed_run(w, args.precision, args, device, barrier, dist)
+    state = None
+    if rank == 0 and (not args.no_cpu or not args.no_e2e):
+        state = {"h": solver.get_field("H"), "u": solver.get_field("U"), "v": solver.get_field("V"),
+                 "dt": solver.get_dt()}
+    solver.close()
+    extras = {}
+    if not args.no_extras and args.precision != "f64":
+        s64, r64 = timed_run(w, "f64", args, device, barrier, dist)
+        s64.close()
+        extras["fp64"] = {"value": r64["value"], "ms_per_step": r64["ms"] / max(1, args.steps),
+                          "accepted": r64["accepted"], "repeated": r64["repeated"], "kernel_variant": r64["variant"],
+                          "roofline": r64["roofline"], "clocks": r64["clocks"]}
+        extras["fp32_over_fp64"] = main_res["value"] / r64["value"]
+    if rank == 0 and not args.no_extras:
+        extras["precision"] = precision_study(device)
+        extras["serving"] = serving_run(device)
+        extras["batched"] = batched_run(device)
+    e2e = None
+    if rank == 0 and not args.no_e2e:
+        e2e = measure_e2e(w, args, device, state, main_res["variant"], args.precision)
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cb = cpu_baseline(w, state, args.cpu_seconds, oracle_precision(args.precision))
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": main_res["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": main_res["ms"] / max(1, args.steps), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "f64" else "f32",
+                "data": "synthetic",
+                "config": {"workload": f"single catchment {w['nx']}x{w['ny']}, dx=2 m (diamond-square H0.8 100 m + "
+                                       "0.005 slope, lognormal rain field 30 mm/h, Voronoi n, outflow all edges)",
+                           "scheme": "classic RK4", "cn_target": 0.5, "precision": args.precision,
+                           "spinup_timesteps": args.spinup, "sim_time_s": main_res["sim_time_s"],
+                           "l2": "inputs larger than L2 (each FP64 state field 134 MB; FP32 67 MB x 13 fields)",
+                           "parallelism": f"replicas x{world}", "kernel_variant": main_res["variant"],
+                           "accepted": main_res["accepted"], "repeated": main_res["repeated"]},
+                "roofline": main_res["roofline"], "cpu_baseline": cb, "e2e": e2e, "clocks": main_res["clocks"],
+                "gpu_launches": main_res["launches"]}
+        line.update(extras)
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
 
 
 if __name__ == "__main__":

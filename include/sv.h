@@ -228,8 +228,20 @@ int sv_batch_remove(sv_batch* batch, int id);
  * (owned by the batch: do not sv_destroy it); NULL for an empty slot */
 sv_ctx* sv_batch_member(sv_batch* batch, int id);
 /* TypedTemporalScheme::step for every member at once; out[id] (for id < n_out) receives each
- * member's step counts and running tallies */
+ * member's step counts and running tallies. A member that fails does not stop the others:
+ * every member still completes (or fails) its own step, out[] is filled for all of them, and
+ * the call returns SV_E_NONFINITE (some member's time became NaN) or SV_E_LIMIT (some member
+ * reached the step limit) -- sv_batch_status says which. */
 int sv_batch_advance(sv_batch* batch, sv_stats* out, int n_out);
+/* Cap on the timesteps one member may take within one step (0, the default: no cap). The
+ * reference's velocity formulation can blow up in thin films on steep beds, where dt shrinks
+ * without bound and the step never ends; the cap turns that member into an SV_E_LIMIT
+ * status, part-way through its step, instead of stalling the whole batch. */
+int sv_batch_set_step_limit(sv_batch* batch, long long max_timesteps);
+/* status[id] (for id < n) receives each slot's outcome of the last sv_batch_advance: SV_OK,
+ * SV_E_NONFINITE (its state is no longer usable) or SV_E_LIMIT (left part-way through the
+ * step); SV_OK for empty slots */
+int sv_batch_status(sv_batch* batch, int* status, int n);
 /* number of members and their total device memory in bytes */
 int sv_batch_size(sv_batch* batch, int* n_members, uint64_t* device_bytes);
 

@@ -27,6 +27,10 @@ def _declare(lib):
     lib.sv_batch_member.argtypes = [C.c_void_p, C.c_int]
     lib.sv_batch_advance.restype = C.c_int
     lib.sv_batch_advance.argtypes = [C.c_void_p, P(Stats), C.c_int]
+    lib.sv_batch_set_step_limit.restype = C.c_int
+    lib.sv_batch_set_step_limit.argtypes = [C.c_void_p, C.c_longlong]
+    lib.sv_batch_status.restype = C.c_int
+    lib.sv_batch_status.argtypes = [C.c_void_p, P(C.c_int), C.c_int]
     lib.sv_batch_size.restype = C.c_int
     lib.sv_batch_size.argtypes = [C.c_void_p, P(C.c_int), P(C.c_uint64)]
     lib._batch_declared = True
@@ -86,15 +90,32 @@ class SaintVenantBatch:
         self.members.pop(member.slot, None)
         member._h = None
 
-    def advance(self):
+    def set_step_limit(self, max_timesteps):
+        """Cap the timesteps one member may take within one step (0: no cap). A member that
+        reaches it leaves the step part-way with status SV_E_LIMIT; the others go on."""
+        r = self._lib.sv_batch_set_step_limit(self._b, int(max_timesteps))
+        if r != 0:
+            raise SvError(r, self._lib.sv_last_error(None).decode())
+
+    def advance(self, raise_on_error=True):
         """One step (of each member's own step length) for every member; returns
-        {slot: stats} with the step's counts and each member's running tallies."""
+        {slot: stats} with the step's counts, each member's running tallies and its
+        "status" (0, SV_E_NONFINITE or SV_E_LIMIT). A failing member does not stop the
+        others; with raise_on_error (the default) its failure still raises SvError after
+        the step, otherwise it is only reported in its status."""
         n = max(self.members) + 1 if self.members else 0
         out = (Stats * max(n, 1))()
         r = self._lib.sv_batch_advance(self._b, out, n)
-        if r != 0:
+        if r != 0 and (raise_on_error or r not in (_abi.SV_E_NONFINITE, _abi.SV_E_LIMIT)):
             raise SvError(r, self._lib.sv_last_error(None).decode())
-        return {k: out[k].as_dict() for k in self.members}
+        status = (C.c_int * max(n, 1))()
+        self._lib.sv_batch_status(self._b, status, n)
+        res = {}
+        for k in self.members:
+            d = out[k].as_dict()
+            d["status"] = status[k]
+            res[k] = d
+        return res
 
     def size(self):
         n, b = C.c_int(), C.c_uint64()

@@ -824,6 +824,8 @@ struct sv_batch_base {
   virtual sv_ctx* member(int) = 0;
   virtual int advance(sv_stats*, int) = 0;
   virtual int size(int*, uint64_t*) = 0;
+  virtual int set_step_limit(long long) = 0;
+  virtual int status(int*, int) = 0;
 };
 
 template <typename T>
@@ -844,6 +846,8 @@ struct Batch final : public sv_batch_base {
   std::vector<unsigned long long> versions; // members' pversion at the last rebuild
   cudaGraphExec_t graph = nullptr;
   int unroll = 8;
+  long long step_limit = 0;                 // timesteps per member per step (0: no limit)
+  std::vector<int> last_status;             // slot id -> outcome of the last advance
 
   ~Batch() override {
     cudaSetDevice(device);
@@ -1003,7 +1007,7 @@ struct Batch final : public sv_batch_base {
       int r = build_graph();
       if (r) return r;
     }
-    cudaError_t e = svk::launch_begin_batch(d_ctls, nact, 0, stream);
+    cudaError_t e = svk::launch_begin_batch(d_ctls, nact, step_limit, stream);
     if (e != cudaSuccess) return cuda_fail(e, "begin batch");
     std::vector<int> done(nact);
     for (long long it = 0;; ++it) {
@@ -1017,13 +1021,22 @@ struct Batch final : public sv_batch_base {
       if (all) break;
       if (it > 100000000LL / unroll) return fail(SV_E_STATE, "batch step did not finish");
     }
-    int rc = SV_OK;
+    // a failing member does not hold up the others: each finished (or failed) on its own
+    // controller; the outcome of every slot is kept for sv_batch_status
+    int rc = SV_OK, n_nan = 0, n_limit = 0;
+    last_status.assign(members.size(), SV_OK);
     for (int k = 0; k < nact; ++k) {
       Solver<T>* m = members[active[k]];
       Ctl c;
       int r = m->read_ctl(c);
       if (r) return r;
-      if (c.error) rc = fail(SV_E_NONFINITE, "a member's time became NaN: its control number was not finite");
+      if (c.error) {
+        last_status[active[k]] = SV_E_NONFINITE;
+        ++n_nan;
+      } else if (c.done == 2) {
+        last_status[active[k]] = SV_E_LIMIT;
+        ++n_limit;
+      }
       if (out && active[k] < n_out) {
         sv_stats& o = out[active[k]];
         o.accepted = c.step_accepted;
@@ -1033,7 +1046,25 @@ struct Batch final : public sv_batch_base {
         o.volume = c.volume;
       }
     }
+    if (n_nan)
+      rc = fail(SV_E_NONFINITE, std::to_string(n_nan) + " member(s)' time became NaN: the control number was not "
+                                "finite (sv_batch_status names them; the other members completed the step)");
+    else if (n_limit)
+      rc = fail(SV_E_LIMIT, std::to_string(n_limit) + " member(s) reached the step limit of " +
+                                std::to_string(step_limit) + " timesteps before the end of the step "
+                                "(sv_batch_status names them; the other members completed the step)");
     return rc;
+  }
+
+  int set_step_limit(long long n) override {
+    if (n < 0) return fail(SV_E_ARG, "step limit must be >= 0");
+    step_limit = n;
+    return SV_OK;
+  }
+  int status(int* out, int n) override {
+    if (!out || n < 0) return fail(SV_E_ARG, "null status array");
+    for (int i = 0; i < n; ++i) out[i] = i < int(last_status.size()) ? last_status[i] : SV_OK;
+    return SV_OK;
   }
 };
 
@@ -1138,6 +1169,18 @@ sv_ctx* sv_batch_member(sv_batch* b, int id) { return b ? b->impl->member(id) : 
 int sv_batch_advance(sv_batch* b, sv_stats* out, int n_out) {
   if (!b) return SV_E_ARG;
   int r = b->impl->advance(out, n_out);
+  if (r) g_create_err = b->impl->err;
+  return r;
+}
+int sv_batch_set_step_limit(sv_batch* b, long long max_timesteps) {
+  if (!b) return SV_E_ARG;
+  int r = b->impl->set_step_limit(max_timesteps);
+  if (r) g_create_err = b->impl->err;
+  return r;
+}
+int sv_batch_status(sv_batch* b, int* status, int n) {
+  if (!b) return SV_E_ARG;
+  int r = b->impl->status(status, n);
   if (r) g_create_err = b->impl->err;
   return r;
 }

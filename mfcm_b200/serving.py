@@ -7,8 +7,13 @@ while others are on the GPU join the same launches. A request leaves the batch w
 horizon is reached, freeing its memory for the queue. Each request's results are
 bit-identical whether it runs alone or in the mix (members never share state).
 
-The reference has no serving layer; this is the north-star production pattern built on the
-same step (one `step()` of TypedTemporalScheme per batch advance, per member).
+A request whose solve fails is failed alone: a member whose time turns NaN, or which takes
+more than `step_limit` timesteps within one step (the reference's thin-film velocity
+blow-up on steep beds, where dt shrinks without bound), is removed with its reason recorded
+while the rest of the batch completes the same step.
+
+The reference has no serving layer; this is a production serving pattern built on the same
+step (one `step()` of TypedTemporalScheme per batch advance, per member).
 """
 import math
 import time
@@ -18,6 +23,7 @@ import numpy as np
 
 from . import synth, TimeSeries, start_new_step_forcing, RAIN_UNIFORM
 from .batch import SaintVenantBatch
+from ._abi import SV_E_NONFINITE
 
 
 @dataclass
@@ -35,6 +41,7 @@ class Request:
     # filled in by the server
     admitted: float = math.nan
     finished: float = math.nan
+    error: str = None       # why the solve failed (None: completed)
     cell_updates: int = 0
     steps: int = 0
     result_h: np.ndarray = None
@@ -51,9 +58,20 @@ def triangular_hyetograph(peak_mm_h, duration_s, end=1e9):
     return TimeSeries([0.0, duration_s / 2.0, duration_s, end], [0.0, p, 0.0, 0.0])
 
 
+def catchment_bed(nx, ny, dx, slope, relief_frac, seed, hurst=0.8, smooth_m=10.0):
+    """A catchment bed: a regional `slope` toward +x plus fractal relief of `relief_frac`
+    times the catchment's longer side, smoothed over `smooth_m` metres (bed slopes of a few
+    to twenty-odd percent, like gridded terrain at metre resolution)."""
+    r = relief_frac * max(nx, ny) * dx
+    z = synth.gaussian_smooth(synth.diamond_square(nx, ny, hurst, r, seed=seed), smooth_m / dx)
+    return z + synth.regional_slope(nx, ny, dx, slope)
+
+
 def make_requests(rate, count, seed=0, side=(64, 512), dxs=(1.0, 2.0, 5.0), horizon=(120.0, 600.0),
-                  relief=(10.0, 150.0), peak=(20.0, 120.0), duration=(900.0, 7200.0), hurst=0.8):
-    """Poisson arrivals at `rate` requests/s; mesh side log-uniform on `side`; fractal beds."""
+                  slope=(0.005, 0.03), relief=(0.01, 0.03), peak=(20.0, 120.0), duration=(900.0, 7200.0),
+                  hurst=0.8):
+    """Poisson arrivals at `rate` requests/s; mesh side log-uniform on `side`; beds from
+    `catchment_bed` with regional slope U(`slope`) and relief U(`relief`) x length."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
@@ -61,7 +79,7 @@ def make_requests(rate, count, seed=0, side=(64, 512), dxs=(1.0, 2.0, 5.0), hori
         t += rng.exponential(1.0 / rate)
         s = int(round(math.exp(rng.uniform(math.log(side[0]), math.log(side[1])))))
         dx = float(rng.choice(dxs))
-        z = synth.diamond_square(s, s, hurst, float(rng.uniform(*relief)), seed=seed * 100003 + i)
+        z = catchment_bed(s, s, dx, float(rng.uniform(*slope)), float(rng.uniform(*relief)), seed * 100003 + i, hurst)
         rain = triangular_hyetograph(float(rng.uniform(*peak)), float(rng.uniform(*duration)))
         out.append(Request(i, t, s, s, dx, z, rain, float(rng.uniform(*horizon))))
     return out
@@ -69,13 +87,14 @@ def make_requests(rate, count, seed=0, side=(64, 512), dxs=(1.0, 2.0, 5.0), hori
 
 class FloodServer:
     def __init__(self, budget_bytes=150e9, max_slots=512, precision="f32", step_duration=60.0, cn_target=0.5,
-                 device=0):
+                 device=0, step_limit=20000):
         self.batch = SaintVenantBatch(precision, "classic", device)
+        self.batch.set_step_limit(step_limit)
         self.budget = float(budget_bytes)
         self.max_slots = int(max_slots)
         self.L = float(step_duration)
         self.cn_target = float(cn_target)
-        self.value_bytes = 4 if precision == "f32" else 8
+        self.value_bytes = 8 if precision == "f64" else 4
 
     def estimate_bytes(self, req):
         """Device memory of one member: 15 cell fields (two states, two stage buffers, bed and
@@ -124,7 +143,7 @@ class FloodServer:
             for slot, (req, m, t) in active.items():
                 m.set_forcing(start_new_step_forcing(t, self.L, rain=req.rain, rain_kind=RAIN_UNIFORM, head=0.0,
                                                      head_edges=req.head_edges))
-            stats = self.batch.advance()
+            stats = self.batch.advance(raise_on_error=False)
             now = time.perf_counter() - t0
             done = []
             for slot, entry in active.items():
@@ -134,7 +153,13 @@ class FloodServer:
                 total_updates += st["accepted"] * req.nx * req.ny
                 req.steps += 1
                 entry[2] = t + self.L
-                if entry[2] >= req.horizon - 1e-9:
+                if st["status"] != 0:
+                    req.error = ("time became NaN" if st["status"] == SV_E_NONFINITE else
+                                 "step limit reached (dt collapsed)")
+                    req.stats = m.stats()
+                    req.finished = time.perf_counter() - t0
+                    done.append(slot)
+                elif entry[2] >= req.horizon - 1e-9:
                     req.result_h = m.get_field("H")
                     req.stats = m.stats()
                     req.finished = time.perf_counter() - t0
@@ -144,9 +169,10 @@ class FloodServer:
                 self.batch.remove(m)
                 used -= self.estimate_bytes(req)
         wall = time.perf_counter() - t0
-        lat = np.array([r.latency for r in requests if not math.isnan(r.finished)])
+        lat = np.array([r.latency for r in requests if not math.isnan(r.finished) and r.error is None])
         return {
-            "requests": len(requests), "completed": int(lat.size), "wall_s": wall,
+            "requests": len(requests), "completed": int(lat.size),
+            "failed": sum(1 for r in requests if r.error is not None), "wall_s": wall,
             "p50_s": float(np.percentile(lat, 50)) if lat.size else None,
             "p95_s": float(np.percentile(lat, 95)) if lat.size else None,
             "p99_s": float(np.percentile(lat, 99)) if lat.size else None,

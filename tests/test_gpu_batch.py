@@ -4,7 +4,8 @@ removed and added between steps."""
 import numpy as np
 import pytest
 
-from mfcm_b200 import SaintVenantSolver, synth, start_new_step_forcing, RAIN_UNIFORM, EDGE_XMAX, EDGE_YMIN
+from mfcm_b200 import SaintVenantSolver, SvError, synth, start_new_step_forcing, RAIN_UNIFORM, EDGE_XMAX, EDGE_YMIN
+from mfcm_b200._abi import SV_E_NONFINITE, SV_E_LIMIT
 from mfcm_b200.batch import SaintVenantBatch
 from oracle.sv_oracle_py import OracleSolver
 from tests.scenarios import setup, rain_series, same
@@ -97,3 +98,54 @@ def test_fp32_batch_close_to_fp64():
     ref, _ = _run_alone(OracleSolver, CASES[0], steps, L)
     assert np.max(np.abs(m.get_field("H") - ref[0])) <= 1e-3
     b32.close()
+
+
+def test_a_failing_member_does_not_stop_the_others():
+    """One member's time turns NaN (its dt is set to NaN): it alone is reported, and the other
+    members complete the same steps with the bits of their solo runs."""
+    L, steps = 20.0, 2
+    batch = SaintVenantBatch("f64")
+    mem = []
+    for c in CASES:
+        m = batch.add(c[0], c[1], c[2], cn_target=0.5, step_duration=L, rain_mode="physical")
+        _init(m, c[0], c[1], c[2], c[5])
+        mem.append(m)
+    mem[1].set_dt(float("nan"))
+    for i in range(steps):
+        for m, c in zip(mem, CASES):
+            m.set_forcing(_forcing(i * L, L, c[3], c[4]))
+        st = batch.advance(raise_on_error=False)
+        assert [st[m.slot]["status"] for m in mem] == [0, SV_E_NONFINITE, 0]
+    for j in (0, 2):
+        solo, _ = _run_alone(SaintVenantSolver, CASES[j], steps, L)
+        for k, f in enumerate(("H", "U", "V")):
+            assert same(mem[j].get_field(f), solo[k]), f"{CASES[j]}: {f} differs from the solo run"
+    with pytest.raises(SvError) as e:
+        batch.advance()
+    assert e.value.code == SV_E_NONFINITE
+    batch.close()
+
+
+def test_step_limit_leaves_members_part_way():
+    """With a cap of 2 timesteps per step every member (each needs more) stops after exactly
+    2 timesteps with status SV_E_LIMIT; by default advance raises SV_E_LIMIT."""
+    L = 20.0
+    batch = SaintVenantBatch("f64")
+    mem = []
+    for c in CASES:
+        m = batch.add(c[0], c[1], c[2], cn_target=0.5, step_duration=L, rain_mode="physical")
+        _init(m, c[0], c[1], c[2], c[5])
+        m.set_forcing(_forcing(0.0, L, c[3], c[4]))
+        mem.append(m)
+    batch.set_step_limit(2)
+    st = batch.advance(raise_on_error=False)
+    for m in mem:
+        assert st[m.slot]["status"] == SV_E_LIMIT
+        assert st[m.slot]["accepted"] + st[m.slot]["repeated"] == 2
+    with pytest.raises(SvError) as e:
+        batch.advance()
+    assert e.value.code == SV_E_LIMIT
+    batch.set_step_limit(0)
+    st = batch.advance()
+    assert all(st[m.slot]["status"] == 0 for m in mem)
+    batch.close()
