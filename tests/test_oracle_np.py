@@ -1,0 +1,119 @@
+"""The C++ oracle against the independent numpy restatement of the same reference lines
+(oracle/sv_oracle_np.py): slopes, face fluxes and branches, and dU/dt with roughness and both
+boundaries must agree bit for bit (up to the sign of an exact zero), on wet/dry states with
+coded-out cells, ragged and one-cell-wide grids, dx != dy, both rain clamps and both
+boundary orders. No GPU is needed."""
+import numpy as np
+import pytest
+
+from mfcm_b200 import EDGE_XMAX, EDGE_XMIN, EDGE_YMAX, EDGE_YMIN
+from oracle import sv_oracle_np as onp
+from oracle.sv_oracle_py import OracleSolver
+from tests.scenarios import wet_dry_state, forcing, same, first_diff
+
+SLOPES = {"DHDX": "dhdx", "DUDX": "dudx", "DVDX": "dvdx", "DHDY": "dhdy", "DUDY": "dudy", "DVDY": "dvdy",
+          "DZDX": "dzdx", "DZDY": "dzdy"}
+FACES = {"FLUX_H": "flux_h", "FLUX_U": "flux_u", "FLUX_V": "flux_v", "FLUX_Z": "flux_z",
+         "FLUX_BRANCH": "flux_branch"}
+KS = {"DHDT": "dhdt", "DUDT": "dudt", "DVDT": "dvdt"}
+
+
+def _check(o, ref, fields):
+    for name, key in fields.items():
+        got = o.get_field(name)
+        want = ref[key].reshape(got.shape)
+        d = first_diff(got, want)
+        assert d is None, f"{name}: first mismatch at {d[0]}: oracle {d[1]!r} numpy {d[2]!r} ({d[3]} differ)"
+
+
+CASES = [  # nx, ny, dx, dy, nan cells, seed
+    (17, 13, 3.0, 3.0, 0, 1),
+    (33, 17, 2.0, 5.0, 6, 2),
+    (1, 9, 3.0, 3.0, 0, 3),
+    (9, 1, 3.0, 3.0, 0, 4),
+    (40, 3, 0.5, 0.5, 4, 5),
+    (24, 24, 4.0, 1.0, 10, 6),
+]
+
+
+@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("rain_mode,head_first", [("reference", False), ("physical", False), ("physical", True)])
+def test_oracle_matches_numpy_restatement(case, rain_mode, head_first):
+    nx, ny, dx, dy, nan_cells, seed = case
+    z, h, u, v = wet_dry_state(nx, ny, dx, seed=seed, nan_cells=nan_cells if nx * ny >= 20 else 0)
+    n = (0.03, 0.05, 0.1, 0.3)
+    q = (2e-5, 1e-5)
+    head, edges = (0.05, 0.0), EDGE_XMAX | EDGE_YMIN
+    t_now, ts, L = 7.5, 0.37, 60.0
+    o = OracleSolver(nx, ny, dx, dy, rain_mode=rain_mode, head_first=head_first, step_duration=L)
+    o.set_field("Z", z)
+    o.set_field("H", h)
+    o.set_field("U", u)
+    o.set_field("V", v)
+    o.set_manning(*n)
+    o.set_forcing(forcing(q, head=head, edges=edges))
+    o.eval_dudt(0, t_now, ts)
+    shape = (ny, nx)
+    hb = onp.edge_strips(nx, ny, edges, *head)
+    assert same(o.get_field("HBDY0"), hb[0]) and same(o.get_field("HBDY1"), hb[1])
+    ref = onp.update_dudt(h, u, v, z, dx, dy, manning=tuple(np.full(shape, x) for x in n),
+                          qbdy=(np.full(shape, q[0]), np.full(shape, q[1])), hbdy=hb, time_now=t_now, timestep=ts,
+                          step_length=L, rain_mode=rain_mode, head_first=head_first)
+    _check(o, ref, SLOPES)
+    _check(o, ref, FACES)
+    _check(o, ref, KS)
+
+
+def test_numpy_restatement_sees_every_branch():
+    """The wet/dry scenario drives all four flux branches (both step cases of branch 2)."""
+    nx, ny, dx = 33, 17, 2.0
+    z, h, u, v = wet_dry_state(nx, ny, dx, seed=2)
+    ref = onp.update_dudt(h, u, v, z, dx, dx)
+    assert {1.0, 2.25, 2.75, 3.0, 4.0} <= set(np.unique(ref["flux_branch"]).tolist())
+
+
+def test_numpy_pow43_matches_the_shared_routine():
+    from oracle.sv_oracle_py import pow43
+    rng = np.random.default_rng(1)
+    x = np.exp(rng.uniform(np.log(1e-9), np.log(1e4), 5000))
+    assert np.array_equal(onp.pow43(x), np.array([pow43(t) for t in x]))
+
+
+def test_mirror_in_y_is_not_a_symmetry_of_the_reference_slopes():
+    """The y slope takes the north (row + 1) neighbour as its left operand, so dU/dy is
+    minus the row-wise derivative: a linear ramp rising with the row index has a negative
+    reference slope."""
+    ny, nx = 6, 4
+    f = np.tile(np.arange(ny, dtype=float)[:, None], (1, nx))
+    s = onp.slope_y(f, 1.0)
+    assert np.all(s[1:-1] == -1.0)
+
+
+@pytest.mark.parametrize("method", ["classic", "ralston4", "3/8rule"])
+@pytest.mark.parametrize("case", CASES[:2] + CASES[4:5])
+def test_oracle_timestep_matches_numpy_restatement(method, case):
+    """A whole timestep: every stage, the left-to-right stage combination, the control number
+    and the dt controller."""
+    nx, ny, dx, dy, nan_cells, seed = case
+    z, h, u, v = wet_dry_state(nx, ny, dx, seed=seed + 50, nan_cells=0)
+    n = (0.03, 0.05, 0.1, 0.3)
+    q = (2e-5, 3e-5)
+    head, edges = (0.02, 0.01), EDGE_XMIN | EDGE_YMAX
+    t0, dt, L, tgt = 4.0, 0.05, 30.0, 0.5
+    o = OracleSolver(nx, ny, dx, dy, rk_method=method, cn_target=tgt, rain_mode="physical", step_duration=L)
+    for name, a in (("Z", z), ("H", h), ("U", u), ("V", v)):
+        o.set_field(name, a)
+    o.set_manning(*n)
+    o.set_forcing(forcing(q, head=head, edges=edges))
+    cn, rep, nd = o.do_timestep(t0, dt)
+    shape = (ny, nx)
+    (hN, uN, vN), cn2, rep2, nd2 = onp.do_timestep(
+        h, u, v, z, dx, dy, t0, dt, method=method, cn_target=tgt,
+        manning=tuple(np.full(shape, x) for x in n), qbdy=(np.full(shape, q[0]), np.full(shape, q[1])),
+        hbdy=onp.edge_strips(nx, ny, edges, *head), step_length=L, rain_mode="physical")
+    assert cn == cn2 and bool(rep) == rep2 and nd == nd2, ((cn, rep, nd), (cn2, rep2, nd2))
+    N = o.nstages
+    for k, want in enumerate((hN, uN, vN)):
+        got = o.get_field(100 + 3 * N + k)
+        d = first_diff(got, want)
+        assert d is None, f"U_[N] field {k}: first mismatch at {d[0]}: oracle {d[1]!r} numpy {d[2]!r}"
