@@ -252,9 +252,11 @@ def timed_run(w, precision, args, device, barrier, dist):
     achieved = alg_bytes_launch / stage_avg_s / 1e9
     peak, peak_kind = measured_peaks()
     kernel = "stage_kernel" if variant < 4 else "sweep_kernel"
-    traffic_pc = profile_traffic(f"{kernel}_{'f64' if precision == 'f64' else 'f32'}_2048_traffic.json")
+    traffic_pc = profile_traffic(f"{kernel}_{precision}_2048_traffic.json")
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": (traffic_pc * ncells if traffic_pc else None), "peak_kind": peak_kind,
+            "traffic_source": (f"profiles/{kernel}_{precision}_2048_traffic.json scaled to {w['nx']}x{w['ny']} cells"
+                               if traffic_pc else None),
             "kernel": f"{kernel} (variant {variant})", "alg_bytes_per_launch": alg_bytes_launch,
             "stage_launch_ms": stage_avg_s * 1e3, "stage_share_of_step": tm["stage_ms"] / max(1e-9, tm["total_ms"])}
     res = {"value": work / (ms_max * 1e-3), "ms": ms_max, "accepted": accepted, "repeated": repeated,
@@ -264,30 +266,42 @@ def timed_run(w, precision, args, device, barrier, dist):
     return solver, res
 
 
-def precision_study(device, nx=2048, ny=256, dx=0.5, seconds=20.0):
-    """Dam break on a flat bed at 350 m (h = 1 m upstream, dry downstream, frictionless):
-    max depth error and relative volume error of the FP32 paths against FP64, and the front
-    position against Ritter's 2 sqrt(g h0) t."""
+def precision_study(device, nx=8192, ny=1024, dx=0.5, seconds=60.0):
+    """Dam break on a flat bed at 350 m (8192 x 1024 cells, dx = 0.5 m, h = 1 m for x below the
+    centre, dry beyond, frictionless, no rain, 60 s): max depth error and relative volume
+    error of the FP32 paths against FP64, the front position of each against Ritter's
+    2 sqrt(g h0) t, and the depth and velocity at the dam against Ritter's 4/9 h0 and
+    2/3 sqrt(g h0)."""
     from mfcm_b200 import SaintVenantSolver, synth
     z, h = synth.dam_break(nx, ny, 350.0, 1.0)
     out = {}
+    mid = nx // 2
     for prec in ("f64", "f32", "f32_datum64"):
         s = SaintVenantSolver(nx, ny, dx, precision=prec, cn_target=0.5, step_duration=seconds, manning=False,
                               initial_dt=0.01, device=device)
         s.set_field("Z", z)
         s.set_field("H", h)
-        s.advance()
-        out[prec] = (s.get_field("H"), s.stats()["volume"])
+        t0 = time.perf_counter()
+        st = s.advance()
+        el = time.perf_counter() - t0
+        hf, uf = s.get_field("H"), s.get_field("U")
+        wet = np.where(hf[ny // 2, mid:] > 1e-3)[0]
+        out[prec] = {"h": hf, "volume": s.stats()["volume"], "front_m": (wet.max() + 1) * dx if wet.size else 0.0,
+                     "h_dam": float(hf[ny // 2, mid]), "u_dam": float(uf[ny // 2, mid]), "accepted": st["accepted"],
+                     "repeated": st["repeated"], "seconds": el}
         s.close()
-    h64, v64 = out["f64"]
-    mid = nx // 2
-    wet = np.where(h64[ny // 2, mid:] > 1e-3)[0]
-    front = (wet.max() + 1) * dx if wet.size else 0.0
-    res = {"case": f"dam break {nx}x{ny}, dx={dx} m, bed 350 m, {seconds:.0f} s",
-           "front_m": front, "ritter_front_m": 2.0 * math.sqrt(9.81 * 1.0) * seconds}
-    for prec in ("f32", "f32_datum64"):
-        hp, vp = out[prec]
-        res[prec] = {"max_depth_err_m": float(np.max(np.abs(hp - h64))), "rel_volume_err": abs(vp - v64) / v64}
+    h64, v64 = out["f64"]["h"], out["f64"]["volume"]
+    c0 = math.sqrt(9.81 * 1.0)
+    res = {"case": f"dam break {nx}x{ny}, dx={dx} m, bed 350 m, {seconds:.0f} s, no friction",
+           "ritter_front_m": 2.0 * c0 * seconds, "ritter_h_dam": 4.0 / 9.0, "ritter_u_dam": 2.0 / 3.0 * c0}
+    for prec in ("f64", "f32", "f32_datum64"):
+        o = out[prec]
+        r = {k: o[k] for k in ("front_m", "h_dam", "u_dam", "accepted", "repeated", "seconds")}
+        if prec != "f64":
+            r["max_depth_err_m"] = float(np.max(np.abs(o["h"] - h64)))
+            r["rel_volume_err"] = abs(o["volume"] - v64) / v64
+            r["within_1mm"] = r["max_depth_err_m"] <= 1e-3
+        res[prec] = r
     return res
 
 
@@ -310,7 +324,7 @@ def batched_run(device, count=24, steps=20, precision="f32_datum64"):
     from mfcm_b200.serving import catchment_bed
     rng = np.random.default_rng(13)
     b = SaintVenantBatch(precision, device=device)
-    b.set_step_limit(20000)
+    b.set_step_limit(2000)   # 10-s steps: a member whose dt falls below 5 ms has blown up
     mem = []
     for i in range(count):
         side = math.exp(rng.uniform(math.log(256), math.log(1024)))
@@ -502,11 +516,18 @@ def main():
     extras = {}
     if not args.no_extras and args.precision != "f64":
         s64, r64 = timed_run(w, "f64", args, device, barrier, dist)
+        s64_state = None
+        if rank == 0 and world == 1 and not args.no_cpu:
+            s64_state = {"h": s64.get_field("H"), "u": s64.get_field("U"), "v": s64.get_field("V"),
+                         "dt": s64.get_dt()}
         s64.close()
         extras["fp64"] = {"value": r64["value"], "ms_per_step": r64["ms"] / max(1, args.steps),
                           "accepted": r64["accepted"], "repeated": r64["repeated"], "kernel_variant": r64["variant"],
                           "roofline": r64["roofline"], "clocks": r64["clocks"]}
         extras["fp32_over_fp64"] = main_res["value"] / r64["value"]
+        if rank == 0 and world == 1 and not args.no_cpu:
+            st64 = {"h": s64_state["h"], "u": s64_state["u"], "v": s64_state["v"], "dt": s64_state["dt"]}
+            extras["fp64"]["cpu_baseline"] = cpu_baseline(w, st64, args.cpu_seconds, "f64")
     if rank == 0 and not args.no_extras:
         extras["precision"] = precision_study(device)
         extras["serving"] = serving_run(device)
