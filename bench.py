@@ -343,36 +343,40 @@ def batched_run(device, count=24, steps=20, precision="f32_datum64"):
         m.set_forcing(start_new_step_forcing(0.0, 10.0, rain=rate, rain_kind=RAIN_UNIFORM, head=0.0, head_edges=15))
     cells = sum(n for _, _, n in mem)
     failed = 0
-    st = b.advance(raise_on_error=False)  # warm-up step
-    live = []
-    for m, rate, n in mem:
-        if st[m.slot]["status"] != 0:
-            failed += 1
-            b.remove(m)
-        else:
-            live.append((m, rate, n))
-    torch.cuda.synchronize(device)
-    t0 = time.perf_counter()
-    work = 0
-    for k in range(1, steps + 1):
-        for m, rate, _ in live:
-            m.set_forcing(start_new_step_forcing(10.0 * k, 10.0, rain=rate, rain_kind=RAIN_UNIFORM, head=0.0,
-                                                 head_edges=15))
-        st = b.advance(raise_on_error=False)
-        keep = []
+    live = mem
+    k0 = 0
+
+    def run(nsteps):
+        """nsteps queued steps per member; failed members leave, their work is not counted."""
+        nonlocal live, k0, failed
+        res = b.advance_steps({m: [start_new_step_forcing(10.0 * (k0 + i), 10.0, rain=rate, rain_kind=RAIN_UNIFORM,
+                                                          head=0.0, head_edges=15) for i in range(nsteps)]
+                               for m, rate, _ in live}, raise_on_error=False)
+        k0 += nsteps
+        keep, work = [], 0
         for m, rate, n in live:
-            if st[m.slot]["status"] != 0:   # blown up: leaves the ensemble, its work is not counted
+            r = res[m.slot]
+            if r["status"] != 0:
                 failed += 1
                 b.remove(m)
             else:
-                work += st[m.slot]["accepted"] * n
+                work += sum(st["accepted"] for st in r["steps"]) * n
                 keep.append((m, rate, n))
         live = keep
+        return work
+
+    run(1)  # warm-up step (builds the launch graph)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    work = 0
+    per_call = 5
+    for _ in range(steps // per_call):
+        work += run(per_call)
     torch.cuda.synchronize(device)
     el = time.perf_counter() - t0
     b.close()
-    return {"catchments": count, "cells": cells, "steps": steps, "step_s": 10.0, "cell_updates_per_s": work / el,
-            "seconds": el, "failed_members": failed}
+    return {"catchments": count, "cells": cells, "steps": steps, "step_s": 10.0, "steps_per_call": per_call,
+            "cell_updates_per_s": work / el, "seconds": el, "failed_members": failed}
 
 
 def cpu_baseline(w, state, cpu_seconds, precision):

@@ -233,6 +233,18 @@ sv_ctx* sv_batch_member(sv_batch* batch, int id);
  * the call returns SV_E_NONFINITE (some member's time became NaN) or SV_E_LIMIT (some member
  * reached the step limit) -- sv_batch_status says which. */
 int sv_batch_advance(sv_batch* batch, sv_stats* out, int n_out);
+/* Several steps per call (TypedTemporalScheme::solve over up to SV_BATCH_MAX_STEPS steps):
+ * member `id` (for id < n) runs nsteps[id] steps back to back, step s with the boundary values
+ * forcing[id * max_steps + s]; members with id >= n or nsteps[id] = 0 sit the call out. Each
+ * member moves to its next step on the device as soon as its current one ends, so members
+ * with long timesteps do not wait for the slowest member at every step; results are
+ * bit-identical to nsteps[id] calls of sv_batch_advance. out[id * max_steps + s] receives
+ * step s's counts and the running tallies at its end (zeros for steps not run). A member
+ * that fails stops alone (status via sv_batch_status, return code as sv_batch_advance).
+ * SV_RAIN_FIELDS and SV_HEAD_FIELDS steps use the member's fields as they stand. */
+#define SV_BATCH_MAX_STEPS 16
+int sv_batch_advance_steps(sv_batch* batch, int max_steps, const int* nsteps, const sv_forcing* forcing,
+                           sv_stats* out, int n);
 /* Cap on the timesteps one member may take within one step (0, the default: no cap). The
  * reference's velocity formulation can blow up in thin films on steep beds, where dt shrinks
  * without bound and the step never ends; the cap turns that member into an SV_E_LIMIT
@@ -242,6 +254,9 @@ int sv_batch_set_step_limit(sv_batch* batch, long long max_timesteps);
  * SV_E_NONFINITE (its state is no longer usable) or SV_E_LIMIT (left part-way through the
  * step); SV_OK for empty slots */
 int sv_batch_status(sv_batch* batch, int* status, int n);
+/* the stage-kernel variant every member of the batch runs (FP32 results are reproducible
+ * per variant: a solo run with this variant gives a member's bits) */
+int sv_batch_kernel_variant(sv_batch* batch, int* variant);
 /* number of members and their total device memory in bytes */
 int sv_batch_size(sv_batch* batch, int* n_members, uint64_t* device_bytes);
 

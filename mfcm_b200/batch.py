@@ -29,6 +29,10 @@ def _declare(lib):
     lib.sv_batch_advance.argtypes = [C.c_void_p, P(Stats), C.c_int]
     lib.sv_batch_set_step_limit.restype = C.c_int
     lib.sv_batch_set_step_limit.argtypes = [C.c_void_p, C.c_longlong]
+    lib.sv_batch_advance_steps.restype = C.c_int
+    lib.sv_batch_advance_steps.argtypes = [C.c_void_p, C.c_int, P(C.c_int), P(_abi.Forcing), P(Stats), C.c_int]
+    lib.sv_batch_kernel_variant.restype = C.c_int
+    lib.sv_batch_kernel_variant.argtypes = [C.c_void_p, P(C.c_int)]
     lib.sv_batch_status.restype = C.c_int
     lib.sv_batch_status.argtypes = [C.c_void_p, P(C.c_int), C.c_int]
     lib.sv_batch_size.restype = C.c_int
@@ -52,6 +56,9 @@ class BatchMember(_Backend):
 
     def last_error(self):
         return self._lib.sv_last_error(self._h).decode()
+
+
+MAX_STEPS = 16  # SV_BATCH_MAX_STEPS
 
 
 class SaintVenantBatch:
@@ -116,6 +123,51 @@ class SaintVenantBatch:
             d["status"] = status[k]
             res[k] = d
         return res
+
+    def advance_steps(self, forcings, raise_on_error=True):
+        """Several steps per call. `forcings` maps a member (or its slot) to the list of its
+        steps' boundary values (Forcing, at most MAX_STEPS); members not listed sit the call
+        out. Each member runs its steps back to back at its own pace, bit-identical to one
+        advance() per step. Returns {slot: {"steps": [stats per step run], "status": s}}
+        where a failed member's last entry is the step it failed in."""
+        slots = {}
+        for key, fl in forcings.items():
+            slot = key.slot if isinstance(key, BatchMember) else int(key)
+            if slot not in self.members:
+                raise SvError(_abi.SV_E_ARG, f"no batch member in slot {slot}")
+            slots[slot] = list(fl)
+        n = max(self.members) + 1 if self.members else 0
+        ms = max([len(v) for v in slots.values()] + [1])
+        if ms > MAX_STEPS:
+            raise SvError(_abi.SV_E_LIMIT, f"at most {MAX_STEPS} steps per batched advance")
+        counts = (C.c_int * max(n, 1))()
+        fa = (_abi.Forcing * (max(n, 1) * ms))()
+        for slot, fl in slots.items():
+            counts[slot] = len(fl)
+            for k, f in enumerate(fl):
+                fa[slot * ms + k] = f
+        out = (Stats * (max(n, 1) * ms))()
+        r = self._lib.sv_batch_advance_steps(self._b, ms, counts, fa, out, n)
+        if r != 0 and (raise_on_error or r not in (_abi.SV_E_NONFINITE, _abi.SV_E_LIMIT)):
+            raise SvError(r, self._lib.sv_last_error(None).decode())
+        status = (C.c_int * max(n, 1))()
+        self._lib.sv_batch_status(self._b, status, n)
+        res = {}
+        for slot in self.members:
+            k = counts[slot] if slot < n else 0
+            steps = [out[slot * ms + j].as_dict() for j in range(k)]
+            if status[slot] != 0:  # the steps run, the last being the one it failed in
+                while steps and steps[-1]["accepted"] == 0 and steps[-1]["repeated"] == 0:
+                    steps.pop()
+            res[slot] = {"steps": steps, "status": status[slot]}
+        return res
+
+    def kernel_variant(self):
+        """The stage-kernel variant every member runs; a solo SaintVenantSolver with this
+        variant reproduces a member's FP32 bits."""
+        v = C.c_int()
+        self._lib.sv_batch_kernel_variant(self._b, C.byref(v))
+        return v.value
 
     def size(self):
         n, b = C.c_int(), C.c_uint64()

@@ -419,23 +419,33 @@ struct Solver final : public sv_ctx {
     return SV_OK;
   }
 
-  int set_forcing(const sv_forcing* f) override {
+  // Checks one step's boundary values against the fields this solver holds and converts
+  // them to the device form. `may_alloc`: allocate the (cleared) discharge fields that
+  // SV_RAIN_FIELDS needs (BoundarySourceTerm::clear_values); a queued batch step may not.
+  int make_forcing(const sv_forcing* f, DevForcing* d, bool may_alloc) {
     if (!f) return fail(SV_E_ARG, "null forcing");
     if (f->rain_kind < 0 || f->rain_kind > 3 || f->head_kind < 0 || f->head_kind > 2)
       return fail(SV_E_ARG, "bad forcing kind");
     if (f->rain_kind == SV_RAIN_FIELDS && (!q0 || !q1)) {
-      // the discharge fields start cleared (BoundarySourceTerm::clear_values)
+      if (!may_alloc) return fail(SV_E_STATE, "discharge fields not set");
       if (!q0) { SV_CUDA(alloc_cells(&q0)); graph_dirty = true; ++pversion; }
       if (!q1) { SV_CUDA(alloc_cells(&q1)); graph_dirty = true; ++pversion; }
     }
     if (f->rain_kind == SV_RAIN_PATTERN && !pat) return fail(SV_E_STATE, "rain pattern field not set");
     if (f->head_kind == SV_HEAD_FIELDS && (!hb0 || !hb1)) return fail(SV_E_STATE, "head fields not set");
-    DevForcing d{};
-    d.rain_kind = f->rain_kind;
-    d.head_kind = f->head_kind;
-    d.head_edges = f->head_edges;
-    d.rq0 = f->rain_q0; d.rq1 = f->rain_q1;
-    d.hh0 = f->head_h0; d.hh1 = f->head_h1;
+    *d = DevForcing{};
+    d->rain_kind = f->rain_kind;
+    d->head_kind = f->head_kind;
+    d->head_edges = f->head_edges;
+    d->rq0 = f->rain_q0; d->rq1 = f->rain_q1;
+    d->hh0 = f->head_h0; d->hh1 = f->head_h1;
+    return SV_OK;
+  }
+
+  int set_forcing(const sv_forcing* f) override {
+    DevForcing d;
+    int r = make_forcing(f, &d, true);
+    if (r) return r;
     SV_CUDA(cudaMemcpyAsync(fc, &d, sizeof(d), cudaMemcpyHostToDevice, stream));
     SV_CUDA(cudaStreamSynchronize(stream));
     return SV_OK;
@@ -826,6 +836,8 @@ struct sv_batch_base {
   virtual int size(int*, uint64_t*) = 0;
   virtual int set_step_limit(long long) = 0;
   virtual int status(int*, int) = 0;
+  virtual int advance_steps(int, const int*, const sv_forcing*, sv_stats*, int) = 0;
+  virtual int kernel_variant() const = 0;
 };
 
 template <typename T>
@@ -839,6 +851,7 @@ struct Batch final : public sv_batch_base {
   long long* d_tiles = nullptr;             // [nact + 1]
   Ctl** d_ctls = nullptr;                   // [nact]
   int* d_done = nullptr;                    // [nact]
+  svk::StepQueue* d_queue = nullptr;        // [nact] steps queued by the current advance
   int nact = 0, cap = 0;
   long long total_tiles = 0;
   bool p2 = true, dirty = true;
@@ -857,8 +870,8 @@ struct Batch final : public sv_batch_base {
     if (stream) cudaStreamDestroy(stream);
   }
   void free_arrays() {
-    cudaFree(d_params); cudaFree(d_fin); cudaFree(d_tiles); cudaFree(d_ctls); cudaFree(d_done);
-    d_params = nullptr; d_fin = nullptr; d_tiles = nullptr; d_ctls = nullptr; d_done = nullptr;
+    cudaFree(d_params); cudaFree(d_fin); cudaFree(d_tiles); cudaFree(d_ctls); cudaFree(d_done); cudaFree(d_queue);
+    d_params = nullptr; d_fin = nullptr; d_tiles = nullptr; d_ctls = nullptr; d_done = nullptr; d_queue = nullptr;
     cap = 0;
   }
   int cuda_fail(cudaError_t e, const char* where) {
@@ -885,7 +898,7 @@ struct Batch final : public sv_batch_base {
       delete s;
       return r;
     }
-    s->set_variant(svk::kBatchVariant);
+    s->set_variant(svk::batch_variant<T>());
     int slot = -1;
     for (size_t i = 0; i < members.size(); ++i)
       if (!members[i]) { slot = int(i); break; }
@@ -931,6 +944,7 @@ struct Batch final : public sv_batch_base {
       SV_CUDA(cudaMalloc(&d_tiles, sizeof(long long) * (c + 1)));
       SV_CUDA(cudaMalloc(&d_ctls, sizeof(Ctl*) * c));
       SV_CUDA(cudaMalloc(&d_done, sizeof(int) * c));
+      SV_CUDA(cudaMalloc(&d_queue, sizeof(svk::StepQueue) * c));
       cap = c;
     }
     std::vector<svk::StageParams<T>> hp(size_t(N) * std::max(nact, 1));
@@ -940,11 +954,15 @@ struct Batch final : public sv_batch_base {
     p2 = true;
     for (int k = 0; k < nact; ++k) {
       Solver<T>* m = members[active[k]];
+      // the tile prefix and the partials follow the batch kernel's decomposition
+      if (m->variant != svk::batch_variant<T>()) m->set_variant(svk::batch_variant<T>());
       ht[k + 1] = ht[k] + m->nblk;
       int e2;
       p2 = p2 && std::frexp(m->mesh.dx, &e2) == 0.5 && std::frexp(m->mesh.dy, &e2) == 0.5;
       for (int st = 0; st < N; ++st) hp[size_t(st) * nact + k] = m->stage_params(st);
       hf[k] = m->finalize_params(true);
+      hf[k].q = d_queue + k;
+      hf[k].fc = m->fc;
       hc[k] = m->ctl;
     }
     total_tiles = ht[nact];
@@ -964,7 +982,9 @@ struct Batch final : public sv_batch_base {
 
   int enqueue_timestep() {
     for (int st = 0; st < N; ++st) {
-      cudaError_t e = svk::launch_stage_batch<T>(d_params + size_t(st) * nact, d_tiles, nact, total_tiles, p2, stream);
+      cudaError_t e = svk::variant_is_sweep(svk::batch_variant<T>())
+                          ? svk::launch_sweep_batch<T>(d_params + size_t(st) * nact, d_tiles, nact, total_tiles, p2, stream)
+                          : svk::launch_stage_batch<T>(d_params + size_t(st) * nact, d_tiles, nact, total_tiles, p2, stream);
       if (e != cudaSuccess) return cuda_fail(e, "batched stage kernel");
     }
     cudaError_t e = svk::launch_finalize_batch(d_fin, nact, stream);
@@ -990,8 +1010,8 @@ struct Batch final : public sv_batch_base {
     return SV_OK;
   }
 
-  // One step (of each member's own length L) for every member, in batched launches.
-  int advance(sv_stats* out, int n_out) override {
+  // Brings the launch arrays and the graph up to date with the membership.
+  int prepare() {
     SV_CUDA(cudaSetDevice(device));
     for (size_t k = 0; k < active.size() && !dirty; ++k)
       if (!members[active[k]] || members[active[k]]->pversion != versions[k]) dirty = true;
@@ -1007,8 +1027,17 @@ struct Batch final : public sv_batch_base {
       int r = build_graph();
       if (r) return r;
     }
-    cudaError_t e = svk::launch_begin_batch(d_ctls, nact, step_limit, stream);
-    if (e != cudaSuccess) return cuda_fail(e, "begin batch");
+    return SV_OK;
+  }
+
+  // Runs the queued steps of every member (hq[k] for active member k) to completion: one
+  // upload of the queues, graph launches of `unroll` timesteps until every member is done,
+  // one read-back. Each member runs its steps back to back at its own pace; a failing
+  // member stops alone. hq receives the per-step results; last_status each slot's outcome.
+  int run_queue(std::vector<svk::StepQueue>& hq) {
+    SV_CUDA(cudaMemcpyAsync(d_queue, hq.data(), sizeof(svk::StepQueue) * nact, cudaMemcpyHostToDevice, stream));
+    cudaError_t e = svk::launch_begin_queue(d_fin, nact, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "begin queued steps");
     std::vector<int> done(nact);
     for (long long it = 0;; ++it) {
       SV_CUDA(cudaGraphLaunch(graph, stream));
@@ -1021,40 +1050,91 @@ struct Batch final : public sv_batch_base {
       if (all) break;
       if (it > 100000000LL / unroll) return fail(SV_E_STATE, "batch step did not finish");
     }
-    // a failing member does not hold up the others: each finished (or failed) on its own
-    // controller; the outcome of every slot is kept for sv_batch_status
-    int rc = SV_OK, n_nan = 0, n_limit = 0;
+    SV_CUDA(cudaMemcpyAsync(hq.data(), d_queue, sizeof(svk::StepQueue) * nact, cudaMemcpyDeviceToHost, stream));
+    SV_CUDA(cudaStreamSynchronize(stream));
+    int n_nan = 0, n_limit = 0;
     last_status.assign(members.size(), SV_OK);
     for (int k = 0; k < nact; ++k) {
-      Solver<T>* m = members[active[k]];
-      Ctl c;
-      int r = m->read_ctl(c);
-      if (r) return r;
-      if (c.error) {
-        last_status[active[k]] = SV_E_NONFINITE;
-        ++n_nan;
-      } else if (c.done == 2) {
-        last_status[active[k]] = SV_E_LIMIT;
-        ++n_limit;
-      }
-      if (out && active[k] < n_out) {
-        sv_stats& o = out[active[k]];
-        o.accepted = c.step_accepted;
-        o.repeated = c.step_repeated;
-        o.rain_in = c.rain_in;
-        o.outflow = c.outflow;
-        o.volume = c.volume;
-      }
+      members[active[k]]->cur = hq[k].cur;  // the state parity moved on the device
+      last_status[active[k]] = hq[k].status;
+      n_nan += hq[k].status == SV_E_NONFINITE;
+      n_limit += hq[k].status == SV_E_LIMIT;
     }
     if (n_nan)
-      rc = fail(SV_E_NONFINITE, std::to_string(n_nan) + " member(s)' time became NaN: the control number was not "
-                                "finite (sv_batch_status names them; the other members completed the step)");
-    else if (n_limit)
-      rc = fail(SV_E_LIMIT, std::to_string(n_limit) + " member(s) reached the step limit of " +
-                                std::to_string(step_limit) + " timesteps before the end of the step "
-                                "(sv_batch_status names them; the other members completed the step)");
+      return fail(SV_E_NONFINITE, std::to_string(n_nan) + " member(s)' time became NaN: the control number was not "
+                                  "finite (sv_batch_status names them; the other members completed their steps)");
+    if (n_limit)
+      return fail(SV_E_LIMIT, std::to_string(n_limit) + " member(s) reached the step limit of " +
+                                  std::to_string(step_limit) + " timesteps before the end of a step "
+                                  "(sv_batch_status names them; the other members completed their steps)");
+    return SV_OK;
+  }
+
+  static void step_stats(const svk::StepQueue& q, int s, sv_stats& o) {
+    o.accepted = q.acc[s];
+    o.repeated = q.rep[s];
+    o.rain_in = q.rain[s];
+    o.outflow = q.outflow[s];
+    o.volume = q.volume[s];
+  }
+
+  // One step (of each member's own length L) for every member, with the forcing each member
+  // holds, in batched launches.
+  int advance(sv_stats* out, int n_out) override {
+    int r = prepare();
+    if (r || nact == 0) return r;
+    std::vector<svk::StepQueue> hq(nact);
+    for (auto& q : hq) {
+      q = svk::StepQueue{};
+      q.n = 1;
+      q.keep_first = 1;
+      q.limit = step_limit;
+    }
+    int rc = run_queue(hq);
+    if (rc == SV_E_CUDA || rc == SV_E_STATE) return rc;
+    for (int k = 0; k < nact; ++k)
+      if (out && active[k] < n_out) step_stats(hq[k], 0, out[active[k]]);
     return rc;
   }
+
+  // Up to kMaxQueuedSteps steps per member in one call (TypedTemporalScheme::solve over
+  // several steps): member id runs nsteps[id] steps with forcing[id * max_steps + s].
+  int advance_steps(int max_steps, const int* nsteps, const sv_forcing* forcing, sv_stats* out, int n) override {
+    if (max_steps < 1 || max_steps > svk::kMaxQueuedSteps)
+      return fail(SV_E_LIMIT, "at most " + std::to_string(svk::kMaxQueuedSteps) + " steps per batched advance");
+    if (n < 0 || (n > 0 && (!nsteps || !forcing))) return fail(SV_E_ARG, "null step counts or forcing");
+    int r = prepare();
+    if (r || nact == 0) return r;
+    std::vector<svk::StepQueue> hq(nact);
+    for (int k = 0; k < nact; ++k) {
+      svk::StepQueue& q = hq[k];
+      q = svk::StepQueue{};
+      q.limit = step_limit;
+      const int id = active[k];
+      const int ns = id < n ? nsteps[id] : 0;
+      if (ns < 0 || ns > max_steps) return fail(SV_E_ARG, "step count of member " + std::to_string(id) + " out of range");
+      q.n = ns;
+      for (int st = 0; st < ns; ++st) {
+        int e = members[id]->make_forcing(&forcing[size_t(id) * max_steps + st], &q.f[st], false);
+        if (e) return fail(e, "member " + std::to_string(id) + ", step " + std::to_string(st) + ": " + members[id]->err);
+      }
+    }
+    int rc = run_queue(hq);
+    if (rc == SV_E_CUDA || rc == SV_E_STATE) return rc;
+    if (out)
+      for (int k = 0; k < nact; ++k) {
+        const int id = active[k];
+        if (id >= n) continue;
+        for (int st = 0; st < max_steps; ++st) {
+          sv_stats& o = out[size_t(id) * max_steps + st];
+          o = sv_stats{};
+          if (st < hq[k].n && st <= hq[k].k && (st < hq[k].k || hq[k].status != 0)) step_stats(hq[k], st, o);
+        }
+      }
+    return rc;
+  }
+
+  int kernel_variant() const override { return svk::batch_variant<T>(); }
 
   int set_step_limit(long long n) override {
     if (n < 0) return fail(SV_E_ARG, "step limit must be >= 0");
@@ -1177,6 +1257,18 @@ int sv_batch_set_step_limit(sv_batch* b, long long max_timesteps) {
   int r = b->impl->set_step_limit(max_timesteps);
   if (r) g_create_err = b->impl->err;
   return r;
+}
+int sv_batch_advance_steps(sv_batch* b, int max_steps, const int* nsteps, const sv_forcing* forcing, sv_stats* out,
+                           int n) {
+  if (!b) return SV_E_ARG;
+  int r = b->impl->advance_steps(max_steps, nsteps, forcing, out, n);
+  if (r) g_create_err = b->impl->err;
+  return r;
+}
+int sv_batch_kernel_variant(sv_batch* b, int* variant) {
+  if (!b || !variant) return SV_E_ARG;
+  *variant = b->impl->kernel_variant();
+  return SV_OK;
 }
 int sv_batch_status(sv_batch* b, int* status, int n) {
   if (!b) return SV_E_ARG;

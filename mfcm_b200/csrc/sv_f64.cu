@@ -17,9 +17,9 @@ cudaError_t launch_finalize_batch(const FinalizeParams* Fs, int ninst, cudaStrea
   finalize_batch_kernel<1024><<<ninst, 1024, 0, s>>>(Fs);
   return cudaGetLastError();
 }
-cudaError_t launch_begin_batch(Ctl* const* ctls, int n, long long budget, cudaStream_t s) {
+cudaError_t launch_begin_queue(const FinalizeParams* Fs, int n, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
-  begin_batch_kernel<<<(n + 127) / 128, 128, 0, s>>>(ctls, n, budget);
+  begin_queue_kernel<<<(n + 127) / 128, 128, 0, s>>>(Fs, n);
   return cudaGetLastError();
 }
 cudaError_t launch_gather_done(Ctl* const* ctls, int n, int* done, cudaStream_t s) {

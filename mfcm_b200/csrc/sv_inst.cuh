@@ -101,6 +101,17 @@ template <> cudaError_t launch_stage_batch<SV_T>(const StageParams<SV_T>* Ps, co
             : launch_stage_batch_p<SV_T, 32, 8, 3, false>(Ps, tile_start, ninst, total_tiles, s);
 }
 
+template <> cudaError_t launch_sweep_batch<SV_T>(const StageParams<SV_T>* Ps, const long long* warp_start, int ninst,
+                                                 long long total_warps, bool p2, cudaStream_t s) {
+  constexpr int WPB = 4, TY = 32, MINB = 4;  // variant 8
+  if (total_warps <= 0) return cudaSuccess;
+  dim3 block(32, WPB);
+  dim3 grid(unsigned((total_warps + WPB - 1) / WPB));
+  if (p2) sweep_batch_kernel<SV_T, TY, WPB, MINB, true><<<grid, block, 0, s>>>(Ps, warp_start, ninst);
+  else sweep_batch_kernel<SV_T, TY, WPB, MINB, false><<<grid, block, 0, s>>>(Ps, warp_start, ninst);
+  return cudaGetLastError();
+}
+
 template <typename T, int TX, int TY>
 static cudaError_t launch_volume_t(const T* h, int nx, int ny, double area, double* part, cudaStream_t s) {
   dim3 grid((nx + TX - 1) / TX, (ny + TY - 1) / TY);

@@ -559,16 +559,15 @@ __device__ __forceinline__ double warp_min(double v) {
 
 constexpr int kSweepOut = 28;  // output columns per warp
 
-template <typename T, int TY, int WPB, int MINB, bool P2>
-__global__ void __launch_bounds__(32 * WPB, MINB) sweep_kernel(const StageParams<T> P) {
+// One warp's strip `gw` (row-major over strips of kSweepOut columns x TY rows) of one
+// solver's stage. Called by the single-solver kernel (P in parameter space) and by the
+// batched kernel (P in shared memory).
+template <typename T, int TY, bool P2>
+__device__ __forceinline__ void sweep_strip(const StageParams<T>& P, long long gw) {
   using DX = DivX<T, P2>;
   const Ctl* ctl = P.ctl;
-  if (ctl->done) return;
   const int nx = P.nx, ny = P.ny;
   const int tiles_x = (nx + kSweepOut - 1) / kSweepOut;
-  const long long ntiles = (long long)tiles_x * ((ny + TY - 1) / TY);
-  const long long gw = (long long)blockIdx.x * WPB + threadIdx.y;
-  if (gw >= ntiles) return;  // whole warp: no block-level synchronisation below
   const int lane = threadIdx.x;
   const int tile_x = int(gw % tiles_x), tile_y = int(gw / tiles_x);
   const int gx = tile_x * kSweepOut - 2 + lane;
@@ -692,6 +691,46 @@ __global__ void __launch_bounds__(32 * WPB, MINB) sweep_kernel(const StageParams
   }
 }
 
+template <typename T, int TY, int WPB, int MINB, bool P2>
+__global__ void __launch_bounds__(32 * WPB, MINB) sweep_kernel(const __grid_constant__ StageParams<T> P) {
+  if (P.ctl->done) return;
+  const int tiles_x = (P.nx + kSweepOut - 1) / kSweepOut;
+  const long long ntiles = (long long)tiles_x * ((P.ny + TY - 1) / TY);
+  const long long gw = (long long)blockIdx.x * WPB + threadIdx.y;
+  if (gw >= ntiles) return;  // whole warp: no block-level synchronisation below
+  sweep_strip<T, TY, P2>(P, gw);
+}
+
+// Batched column sweep: the strips of every instance of a batch, warp_start[i] being the
+// first global warp of instance i. Each warp finds its instance, stages its parameters in
+// shared memory and sweeps its strip; instances whose step is finished return at once.
+template <typename T, int TY, int WPB, int MINB, bool P2>
+__global__ void __launch_bounds__(32 * WPB, MINB)
+    sweep_batch_kernel(const StageParams<T>* __restrict__ Ps, const long long* __restrict__ warp_start, int ninst) {
+  __shared__ __align__(16) StageParams<T> Psh[WPB];
+  const long long gw = (long long)blockIdx.x * WPB + threadIdx.y;
+  if (gw >= warp_start[ninst]) return;  // whole warp
+  int inst = 0;
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = ninst - 1;  // last instance with warp_start[i] <= gw
+    while (lo < hi) {
+      int mid = (lo + hi + 1) / 2;
+      if (warp_start[mid] <= gw) lo = mid;
+      else hi = mid - 1;
+    }
+    inst = lo;
+  }
+  inst = __shfl_sync(kFull, inst, 0);
+  static_assert(sizeof(StageParams<T>) % 4 == 0, "parameter block copied as 32-bit words");
+  const unsigned* src = reinterpret_cast<const unsigned*>(Ps + inst);
+  unsigned* dst = reinterpret_cast<unsigned*>(&Psh[threadIdx.y]);
+  for (int i = threadIdx.x; i < int(sizeof(StageParams<T>) / 4); i += 32) dst[i] = src[i];
+  __syncwarp();
+  const StageParams<T>& P = Psh[threadIdx.y];
+  if (P.ctl->done) return;
+  sweep_strip<T, TY, P2>(P, gw - warp_start[inst]);
+}
+
 // Bed slopes once per bed upload (SaintVenantConstants, Constants.cpp:39-40).
 template <typename T>
 __global__ void bed_slopes_kernel(const T* z, int nx, int ny, double dx, double dy, T* zx, T* zy) {
@@ -705,8 +744,28 @@ __global__ void bed_slopes_kernel(const T* z, int nx, int ny, double dx, double 
   zy[i] = minmod3<T>(hasN ? z[i + nx] : cz, hasN, cz, hasS, hasS ? z[i - nx] : cz, mkdiv<T>(dy));
 }
 
+// Steps queued for one batch member by one batched advance. The member runs them back to
+// back at its own pace: when a step ends, the controller records it and starts the next one
+// on the device (TypedTemporalScheme::solve's loop, TemporalScheme.hpp:244-276, moved onto
+// the GPU), so members with large timesteps do not wait for the slowest one at every step.
+constexpr int kMaxQueuedSteps = 16;
+struct StepQueue {
+  int n;           // steps queued (0: the member sits this advance out)
+  int k;           // steps completed so far
+  int status;      // 0, or -5 (time became NaN) / -7 (step limit reached) in step k
+  int keep_first;  // 1: step 0 uses the forcing already in place (f[0] unused)
+  int cur;         // the member's state parity when the advance ended (host mirror)
+  int pad;
+  long long limit; // timesteps allowed per step (0: no limit)
+  DevForcing f[kMaxQueuedSteps];                             // forcing of each queued step
+  unsigned long long acc[kMaxQueuedSteps], rep[kMaxQueuedSteps];   // per-step counts
+  double rain[kMaxQueuedSteps], outflow[kMaxQueuedSteps], volume[kMaxQueuedSteps];  // running, at step end
+};
+
 struct FinalizeParams {
   Ctl* ctl;
+  StepQueue* q;      // batch members: the step queue (null for a solver on its own)
+  DevForcing* fc;    // batch members: the member's forcing slot read by its stage kernels
   const double* part;
   long long nblk;
   int nstages;
@@ -820,6 +879,27 @@ template <int NT> __device__ __forceinline__ void finalize_body(const FinalizePa
   ctl->t_local = t;
   ctl->dt = ndt;
   if (ctl->budget > 0 && --ctl->budget == 0 && !ctl->done) ctl->done = 2;  // paused, step not over
+  if (F.q == nullptr || !ctl->done) return;
+  // batch member: record the step that ended (or failed); start the next queued one
+  StepQueue* q = F.q;
+  const int k = q->k;
+  q->acc[k] = ctl->step_accepted;
+  q->rep[k] = ctl->step_repeated;
+  q->rain[k] = ctl->rain_in;
+  q->outflow[k] = ctl->outflow;
+  q->volume[k] = ctl->volume;
+  q->cur = ctl->cur;
+  if (ctl->error) { q->status = -5; return; }
+  if (ctl->done == 2) { q->status = -7; return; }
+  q->k = k + 1;
+  if (k + 1 < q->n) {  // start_new_step of the next queued step; dt carries over as in step()
+    *F.fc = q->f[k + 1];
+    ctl->t_local = 0.0;
+    ctl->step_accepted = 0;
+    ctl->step_repeated = 0;
+    ctl->budget = q->limit;
+    ctl->done = 0;
+  }
 }
 
 template <int NT> __global__ void __launch_bounds__(NT) finalize_kernel(const FinalizeParams F) {
@@ -854,16 +934,29 @@ __global__ void begin_step_kernel(Ctl* ctl, int new_step, long long budget) {
   ctl->done = 0;
   ctl->budget = budget;
 }
-// start a new step on every instance of a batch
-__global__ void begin_batch_kernel(Ctl* const* ctls, int n, long long budget) {
+// start a batched advance of queued steps: each member's first step (or, with no steps
+// queued or a member that already failed, nothing: done at once)
+__global__ void begin_queue_kernel(const FinalizeParams* Fs, int n) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  Ctl* c = ctls[i];
+  Ctl* c = Fs[i].ctl;
+  StepQueue* q = Fs[i].q;
   c->t_local = 0.0;
   c->step_accepted = 0;
   c->step_repeated = 0;
-  c->done = 0;
-  c->budget = budget;
+  c->budget = q->limit;
+  q->k = 0;
+  q->status = 0;
+  q->cur = c->cur;
+  if (c->error) {
+    q->status = -5;
+    c->done = 1;
+  } else if (q->n <= 0) {
+    c->done = 1;
+  } else {
+    if (!q->keep_first) *Fs[i].fc = q->f[0];
+    c->done = 0;
+  }
 }
 // done flags of a batch into one array (1: step complete, nonzero error code: -1)
 __global__ void gather_done_kernel(Ctl* const* ctls, int n, int* done) {

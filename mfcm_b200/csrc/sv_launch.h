@@ -40,10 +40,14 @@ template <typename T> cudaError_t launch_debug(const StageParams<T>& P, const De
 // every instance's dx and dy are powers of two
 template <typename T> cudaError_t launch_stage_batch(const StageParams<T>* Ps, const long long* tile_start, int ninst,
                                                      long long total_tiles, bool p2, cudaStream_t s);
-constexpr int kBatchVariant = 1;
+// batches of FP64 instances use the tiled variant 1; FP32 batches the column sweep of
+// variant 8 (launch_sweep_batch), the fastest single-solver kernels of each precision
+template <typename T> constexpr int batch_variant() { return sizeof(T) == 8 ? 1 : 8; }
+template <typename T> cudaError_t launch_sweep_batch(const StageParams<T>* Ps, const long long* warp_start, int ninst,
+                                                     long long total_warps, bool p2, cudaStream_t s);
 cudaError_t launch_finalize(const FinalizeParams& F, cudaStream_t s);
 cudaError_t launch_finalize_batch(const FinalizeParams* Fs, int ninst, cudaStream_t s);
-cudaError_t launch_begin_batch(Ctl* const* ctls, int n, long long budget, cudaStream_t s);
+cudaError_t launch_begin_queue(const FinalizeParams* Fs, int n, cudaStream_t s);
 cudaError_t launch_gather_done(Ctl* const* ctls, int n, int* done, cudaStream_t s);
 cudaError_t launch_sum(const double* p, long long n, double* out, cudaStream_t s);
 cudaError_t launch_accept(Ctl* ctl, cudaStream_t s);

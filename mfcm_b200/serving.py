@@ -2,8 +2,9 @@
 
 Requests (a catchment, its rainfall and a simulated horizon) arrive at wall-clock times. Each
 request is admitted into one running batch (mfcm_b200.batch) as soon as a slot and its device
-memory fit under the budget; admission happens at step boundaries, so requests that arrive
-while others are on the GPU join the same launches. A request leaves the batch when its
+memory fit under the budget. The batch advances every running request by a few steps per
+call (`steps_per_advance`), each request at its own pace; admission happens between calls,
+so requests that arrive while others are on the GPU join the same launches. A request leaves the batch when its
 horizon is reached, freeing its memory for the queue. Each request's results are
 bit-identical whether it runs alone or in the mix (members never share state).
 
@@ -87,9 +88,12 @@ def make_requests(rate, count, seed=0, side=(64, 512), dxs=(1.0, 2.0, 5.0), hori
 
 class FloodServer:
     def __init__(self, budget_bytes=150e9, max_slots=512, precision="f32", step_duration=60.0, cn_target=0.5,
-                 device=0, step_limit=20000):
+                 device=0, step_limit=20000, steps_per_advance=4):
         self.batch = SaintVenantBatch(precision, "classic", device)
         self.batch.set_step_limit(step_limit)
+        # steps each running request advances per batched launch sequence: members run them
+        # back to back at their own pace; new arrivals are admitted between sequences
+        self.steps_per_advance = int(steps_per_advance)
         self.budget = float(budget_bytes)
         self.max_slots = int(max_slots)
         self.L = float(step_duration)
@@ -140,21 +144,25 @@ class FloodServer:
             if not active:
                 time.sleep(max(0.0, min(0.05, pending[0].arrival - now)))
                 continue
+            queued = {}
             for slot, (req, m, t) in active.items():
-                m.set_forcing(start_new_step_forcing(t, self.L, rain=req.rain, rain_kind=RAIN_UNIFORM, head=0.0,
-                                                     head_edges=req.head_edges))
-            stats = self.batch.advance(raise_on_error=False)
+                left = max(1, math.ceil((req.horizon - t) / self.L - 1e-9))
+                queued[m] = [start_new_step_forcing(t + i * self.L, self.L, rain=req.rain, rain_kind=RAIN_UNIFORM,
+                                                    head=0.0, head_edges=req.head_edges)
+                             for i in range(min(self.steps_per_advance, left))]
+            res = self.batch.advance_steps(queued, raise_on_error=False)
             now = time.perf_counter() - t0
             done = []
             for slot, entry in active.items():
                 req, m, t = entry
-                st = stats[slot]
-                req.cell_updates += st["accepted"] * req.nx * req.ny
-                total_updates += st["accepted"] * req.nx * req.ny
-                req.steps += 1
-                entry[2] = t + self.L
-                if st["status"] != 0:
-                    req.error = ("time became NaN" if st["status"] == SV_E_NONFINITE else
+                r = res[slot]
+                for st in r["steps"]:
+                    req.cell_updates += st["accepted"] * req.nx * req.ny
+                    total_updates += st["accepted"] * req.nx * req.ny
+                req.steps += len(r["steps"])
+                entry[2] = t + self.L * len(r["steps"])
+                if r["status"] != 0:
+                    req.error = ("time became NaN" if r["status"] == SV_E_NONFINITE else
                                  "step limit reached (dt collapsed)")
                     req.stats = m.stats()
                     req.finished = time.perf_counter() - t0

@@ -149,3 +149,67 @@ def test_step_limit_leaves_members_part_way():
     st = batch.advance()
     assert all(st[m.slot]["status"] == 0 for m in mem)
     batch.close()
+
+
+def test_queued_steps_equal_single_steps():
+    """advance_steps runs each member's steps back to back at its own pace; the results are
+    bit-identical to one advance() per step, and members with fewer steps queued stop early."""
+    L, steps = 20.0, 4
+    runs = []
+    for queued in (False, True):
+        batch = SaintVenantBatch("f64")
+        mem = []
+        for c in CASES:
+            m = batch.add(c[0], c[1], c[2], cn_target=0.5, step_duration=L, rain_mode="physical")
+            _init(m, c[0], c[1], c[2], c[5])
+            mem.append(m)
+        nsteps = [steps, steps - 1, steps]
+        per_step = []
+        if queued:
+            res = batch.advance_steps({m: [_forcing(i * L, L, c[3], c[4]) for i in range(ns)]
+                                       for m, c, ns in zip(mem, CASES, nsteps)})
+            for m, ns in zip(mem, nsteps):
+                assert res[m.slot]["status"] == 0 and len(res[m.slot]["steps"]) == ns
+            per_step = [[(s["accepted"], s["repeated"], s["volume"]) for s in res[m.slot]["steps"]] for m in mem]
+        else:
+            per_step = [[] for _ in mem]
+            for i in range(steps):
+                for j, (m, c) in enumerate(zip(mem, CASES)):
+                    if i == nsteps[j]:
+                        batch.remove(m)  # its steps are over: it leaves the batch
+                    elif i < nsteps[j]:
+                        m.set_forcing(_forcing(i * L, L, c[3], c[4]))
+                st = batch.advance()
+                for j, m in enumerate(mem):
+                    if i < nsteps[j]:
+                        s = st[m.slot]
+                        per_step[j].append((s["accepted"], s["repeated"], s["volume"]))
+        fields = [[m.get_field(f) for f in ("H", "U", "V")] if m.slot in batch.members else None for m in mem]
+        runs.append((per_step, fields))
+        batch.close()
+    (ps_a, f_a), (ps_b, f_b) = runs
+    assert ps_a == ps_b
+    for j in (0, 2):
+        for k in range(3):
+            assert same(f_a[j][k], f_b[j][k])
+    solo, _ = _run_alone(SaintVenantSolver, CASES[1], steps - 1, L)
+    for k in range(3):
+        assert same(f_b[1][k], solo[k])
+
+
+def test_queued_steps_isolate_a_failing_member():
+    L = 20.0
+    batch = SaintVenantBatch("f64")
+    mem = []
+    for c in CASES:
+        m = batch.add(c[0], c[1], c[2], cn_target=0.5, step_duration=L, rain_mode="physical")
+        _init(m, c[0], c[1], c[2], c[5])
+        mem.append(m)
+    mem[2].set_dt(float("nan"))
+    res = batch.advance_steps({m: [_forcing(i * L, L, c[3], c[4]) for i in range(3)] for m, c in zip(mem, CASES)},
+                              raise_on_error=False)
+    assert [res[m.slot]["status"] for m in mem] == [0, 0, SV_E_NONFINITE]
+    assert len(res[mem[0].slot]["steps"]) == 3 and len(res[mem[2].slot]["steps"]) == 1
+    solo, _ = _run_alone(SaintVenantSolver, CASES[0], 3, L)
+    assert same(mem[0].get_field("H"), solo[0])
+    batch.close()

@@ -52,7 +52,7 @@ def test_datum_members_in_a_batch():
     b.advance()
     ref = SaintVenantSolver(128, 16, 0.5, precision="f32_datum64", cn_target=0.5, step_duration=2.0, manning=False,
                             initial_dt=0.01)
-    ref.set_kernel_variant(1)
+    ref.set_kernel_variant(b.kernel_variant())
     ref.set_field("Z", z)
     ref.set_field("H", h)
     ref.advance()

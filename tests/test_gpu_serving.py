@@ -10,12 +10,12 @@ from tests.scenarios import same
 pytestmark = pytest.mark.gpu
 
 
-def _alone(req, L=60.0, precision="f32"):
+def _alone(req, variant, L=60.0, precision="f32"):
     """The request solved on its own, with the kernel variant batches use (FP32 arithmetic is
     contracted per kernel, so FP32 bits are reproducible per variant)."""
     s = SaintVenantSolver(req.nx, req.ny, req.dx, precision=precision, cn_target=0.5, step_duration=L,
                           rain_mode="physical")
-    s.set_kernel_variant(1)
+    s.set_kernel_variant(variant)
     s.set_field("Z", req.z)
     z0 = np.zeros((req.ny, req.nx))
     for f in ("H", "U", "V"):
@@ -36,12 +36,13 @@ def test_requests_overlap_and_match_their_solo_runs():
     reqs = make_requests(rate=50.0, count=12, seed=5, side=(32, 96), horizon=(120.0, 300.0))
     server = FloodServer(budget_bytes=2e9, precision="f32")
     summary = server.run(reqs, time_limit=300)
+    variant = server.batch.kernel_variant()
     server.close()
     assert summary["completed"] == len(reqs)
     assert summary["max_concurrent"] >= 2          # work of different requests overlapped
     assert summary["p50_s"] <= summary["p99_s"]
     for r in reqs[:4]:
-        assert same(r.result_h, _alone(r)), f"request {r.rid} differs from its solo run"
+        assert same(r.result_h, _alone(r, variant)), f"request {r.rid} differs from its solo run"
 
 
 def test_memory_budget_queues_requests():
