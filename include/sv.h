@@ -203,13 +203,16 @@ int sv_run_timesteps(sv_ctx* ctx, uint64_t max_timesteps, int begin, sv_stats* o
                      sv_timing* timing);
 /* Stage-kernel variant (no reference counterpart: a launch-shape choice of this library):
  * 0-3 tiled shared-memory kernel (32x8, 32x8 at 3 CTAs/SM, 32x4 at 4 CTAs/SM, 64x4 at 3
- * CTAs/SM), 4-8 column-sweep kernel (16/32/64 rows per warp, then 32 rows capped for 3 and
- * 4 CTAs/SM). Every variant computes bit-identical results. */
+ * CTAs/SM), 4-10 column-sweep kernel (16/32/64 rows per warp, then 32 rows capped for 3, 4,
+ * 5 and 6 CTAs/SM). Every variant computes bit-identical FP64 results; FP32 results are
+ * reproducible per variant. */
 int sv_set_kernel_variant(sv_ctx* ctx, int variant);
 int sv_get_kernel_variant(sv_ctx* ctx, int* variant);
 /* Autotune: times every variant's stage kernel on the current state and keeps the fastest;
  * `best_out` (may be NULL) receives the chosen variant. The state U_[0] is not modified. */
 int sv_autotune(sv_ctx* ctx, int* best_out);
+/* per-variant stage-kernel times (ms) measured by the last sv_autotune; ms[v] for v < n */
+int sv_get_autotune_ms(sv_ctx* ctx, float* ms, int n);
 
 /* ---- batches of independent catchments (no reference counterpart: the reference runs one
  *      catchment per process). Members are ordinary sv_ctx solvers; per timestep one batched

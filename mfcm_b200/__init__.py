@@ -61,6 +61,8 @@ def load_library(path=None):
     for name in ("sv_get_kernel_variant", "sv_autotune"):
         getattr(lib, name).restype = C.c_int
         getattr(lib, name).argtypes = [C.c_void_p, C.POINTER(C.c_int)]
+    lib.sv_get_autotune_ms.restype = C.c_int
+    lib.sv_get_autotune_ms.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_int]
     lib.sv_run_timesteps.restype = C.c_int
     lib.sv_run_timesteps.argtypes = [C.c_void_p, C.c_uint64, C.c_int, C.POINTER(Stats), C.POINTER(C.c_int),
                                      C.POINTER(_abi.Timing)]
@@ -200,6 +202,12 @@ class SaintVenantSolver(_Backend):
         if r != 0:
             raise SvError(r, self.last_error())
         return v.value
+
+    def autotune_ms(self, n=16):
+        """Per-variant stage-kernel times (ms) measured by the last autotune (0 = untimed)."""
+        a = (C.c_float * n)()
+        self._lib.sv_get_autotune_ms(self._h, a, n)
+        return {v: float(a[v]) for v in range(n) if a[v] > 0}
 
     def last_advance_ms(self):
         v = C.c_double()

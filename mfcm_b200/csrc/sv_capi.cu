@@ -113,6 +113,7 @@ struct sv_ctx {
   virtual int set_variant(int) = 0;
   virtual int get_variant() const = 0;
   virtual int autotune(int*) = 0;
+  virtual float autotune_ms(int v) const = 0;
   double last_advance_ms = -1.0;
 };
 
@@ -136,6 +137,7 @@ struct Solver final : public sv_ctx {
   int tile = 0;      // tile shape of the volume kernel
   int variant = 5;   // stage-kernel variant (svk::launch_variant)
   float tune_ms[svk::kNumVariants] = {};
+  float autotune_ms(int v) const override { return v >= 0 && v < svk::kNumVariants ? tune_ms[v] : 0.0f; }
   int tx = 32, ty = 8;
   long long ncells = 0, nfaces = 0, nblk = 0, vol_nblk = 0;
   T* S[2][3] = {};
@@ -1284,6 +1286,12 @@ int sv_batch_size(sv_batch* b, int* n, uint64_t* bytes) {
 int sv_set_kernel_variant(sv_ctx* ctx, int v) { SV_CHECK_CTX(ctx); return ctx->set_variant(v); }
 int sv_get_kernel_variant(sv_ctx* ctx, int* v) { SV_CHECK_CTX(ctx); if (!v) return SV_E_ARG; *v = ctx->get_variant(); return SV_OK; }
 int sv_autotune(sv_ctx* ctx, int* best) { SV_CHECK_CTX(ctx); return ctx->autotune(best); }
+int sv_get_autotune_ms(sv_ctx* ctx, float* ms, int n) {
+  SV_CHECK_CTX(ctx);
+  if (!ms || n < 0) return SV_E_ARG;
+  for (int v = 0; v < n; ++v) ms[v] = ctx->autotune_ms(v);
+  return SV_OK;
+}
 int sv_last_advance_ms(sv_ctx* ctx, double* ms) { SV_CHECK_CTX(ctx); if (!ms) return SV_E_ARG; *ms = ctx->last_advance_ms; return SV_OK; }
 const char* sv_last_error(const sv_ctx* ctx) { return ctx ? ctx->err.c_str() : g_create_err.c_str(); }
 

@@ -102,7 +102,10 @@ __device__ __forceinline__ float sfmax(float x, float y) { return fmaxf(x, y); }
 __device__ __forceinline__ double sfmin(double x, double y) { return fmin(x, y); }
 __device__ __forceinline__ float sfmin(float x, float y) { return fminf(x, y); }
 __device__ __forceinline__ double ssqrt(double x) { return sqrt(x); }
-__device__ __forceinline__ float ssqrt(float x) { return sqrtf(x); }
+// FP32 path: the hardware reciprocal square root (about 2 ulp) instead of the correctly
+// rounded square root; 0, infinity and NaN pass through unchanged. The FP32 path is held to
+// a depth tolerance, not to bit parity, and this saves about 8 instructions per root.
+__device__ __forceinline__ float ssqrt(float x) { return (x > 0.0f && x < INFINITY) ? x * rsqrtf(x) : x; }
 __device__ __forceinline__ double sfabs(double x) { return fabs(x); }
 __device__ __forceinline__ float sfabs(float x) { return fabsf(x); }
 
@@ -380,7 +383,13 @@ __device__ __forceinline__ T head_target(T h0, T h1, const CC& c) {
 
 // Manning friction (ManningRoughnessSourceTerm.cpp:53-87): adds to du, dv.
 __device__ __forceinline__ double pow43_(double x) { return sv_math::pow43(x); }
-__device__ __forceinline__ float pow43_(float x) { return x * cbrtf(x); }
+// FP32 path: x^(4/3) = 2^(4/3 log2 x) on the special-function unit (relative error about
+// 1e-6 over the range of 1/h here); 0 gives 0, infinity infinity, NaN NaN.
+__device__ __forceinline__ float pow43_(float x) { return __powf(x, 4.0f / 3.0f); }
+// h / (h^2 + 1e-3) of the roughness term: IEEE division in FP64, the fast reciprocal form
+// in FP32
+__device__ __forceinline__ double manning_inv_h(double h) { return h / (h * h + 1e-3); }
+__device__ __forceinline__ float manning_inv_h(float h) { return __fdividef(h, h * h + 1e-3f); }
 
 template <typename T, typename CC>
 __device__ __forceinline__ void manning_apply(T h, T u, T v, T ns, T nd, T ds, T dd, const CC& c,
@@ -395,7 +404,7 @@ __device__ __forceinline__ void manning_apply(T h, T u, T v, T ns, T nd, T ds, T
   }
   if (n_out) *n_out = n;
   if (h > T(1e-6)) {
-    T inv_h = h / (h * h + T(1e-3));
+    T inv_h = manning_inv_h(h);
     T sf = n * n * ssqrt(u * u + v * v) * pow43_(inv_h);
     if (sf_out) *sf_out = sf;
     T fu = -T(kG) * sf * u;

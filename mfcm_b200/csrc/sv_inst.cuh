@@ -68,6 +68,8 @@ template <> cudaError_t launch_variant<SV_T>(const StageParams<SV_T>& P, int var
     case 6: return launch_sweep_t<SV_T, 64, 1>(P, variant, s);
     case 7: return launch_sweep_t<SV_T, 32, 3>(P, variant, s);
     case 8: return launch_sweep_t<SV_T, 32, 4>(P, variant, s);
+    case 9: return launch_sweep_t<SV_T, 32, 5>(P, variant, s);
+    case 10: return launch_sweep_t<SV_T, 32, 6>(P, variant, s);
     default: return launch_stage<SV_T>(P, variant, s);
   }
 }

@@ -17,11 +17,11 @@ constexpr int kNumTiles = 4;
 template <typename T> size_t stage_smem_bytes(int tile);
 template <typename T> cudaError_t launch_stage(const StageParams<T>& P, int tile, cudaStream_t s);
 
-// Stage-kernel variants: 0..3 the tiled shared-memory kernel with kTiles[v]; 4..8 the
-// column-sweep kernel with 16 / 32 / 64 / 32 / 32 output rows per warp, the last two with
-// register caps for 3 and 4 resident 4-warp blocks per SM.
-constexpr int kNumVariants = 9;
-constexpr int kSweepRows[5] = {16, 32, 64, 32, 32};
+// Stage-kernel variants: 0..3 the tiled shared-memory kernel with kTiles[v]; 4..10 the
+// column-sweep kernel with 16 / 32 / 64 / 32 / 32 / 32 / 32 output rows per warp, the last
+// four with register caps for 3, 4, 5 and 6 resident 4-warp blocks per SM.
+constexpr int kNumVariants = 11;
+constexpr int kSweepRows[7] = {16, 32, 64, 32, 32, 32, 32};
 inline bool variant_is_sweep(int v) { return v >= 4; }
 // per-CTA (tiled) or per-warp (sweep) partial count
 inline long long variant_partials(int v, long long nx, long long ny) {

@@ -113,7 +113,7 @@ def test_fp32_close_to_fp64_oracle():
     assert abs(vg - vo) <= 1e-3 * vo, (vg, vo)
 
 
-@pytest.mark.parametrize("variant", range(9))
+@pytest.mark.parametrize("variant", range(11))
 @pytest.mark.parametrize("shape", [(61, 45), (29, 70), (3, 5)])
 def test_every_kernel_variant(variant, shape):
     """All stage-kernel variants (tiled and column sweep, every tile height) give the same
