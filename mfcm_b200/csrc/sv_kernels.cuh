@@ -558,6 +558,12 @@ __device__ __forceinline__ double warp_min(double v) {
 }
 
 constexpr int kSweepOut = 28;  // output columns per warp
+// Rows the column sweep prefetches into L1 ahead of use: the window fields of row k+1+2 and
+// the per-cell fields of output row k-2+4 at iteration k. A warp marches its rows in order,
+// so without these hints each row's loads wait a full memory latency with only one row in
+// flight.
+constexpr int kSweepPfWindow = 2, kSweepPfCell = 4;
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
 
 // One warp's strip `gw` (row-major over strips of kSweepOut columns x TY rows) of one
 // solver's stage. Called by the single-solver kernel (P in parameter space) and by the
@@ -611,8 +617,31 @@ __device__ __forceinline__ void sweep_strip(const StageParams<T>& P, long long g
   FaceF<T> FS{}, FN{};
   double rain = 0.0, removed = 0.0, xcfl = 0.0, xmin = 1.0 / 0.0, vol = 0.0;
 
+  // L1 prefetch of rows ahead (addresses clamped into the mesh, like the loads)
+  auto prefetch_rows = [&](int k) {
+    {
+      const int r = min(max(k + 1 + kSweepPfWindow, 0), ny - 1);
+      const long long g = (long long)r * nx + gxc;
+      prefetch_l1(Yh + g); prefetch_l1(Yu + g); prefetch_l1(Yv + g);
+      prefetch_l1(P.z + g); prefetch_l1(P.zx + g); prefetch_l1(P.zy + g);
+    }
+    const int r = min(max(k - 2 + kSweepPfCell, 0), ny - 1);
+    const long long g = (long long)r * nx + gxc;
+    if (!first) {
+      for (int f = 0; f < 3; ++f) { prefetch_l1(P.S[cur][f] + g); prefetch_l1(P.S[cur ^ 1][f] + g); }
+    }
+    if (P.manning) {
+      for (int f = 0; f < 4; ++f)
+        if (P.man_p[f]) prefetch_l1(P.man_p[f] + g);
+    }
+    if (fc.rain_kind == 3) prefetch_l1(P.pat + g);
+    if (fc.rain_kind == 2) { prefetch_l1(P.q0p + g); prefetch_l1(P.q1p + g); }
+    if (fc.head_kind == 2) { prefetch_l1(P.hb0p + g); prefetch_l1(P.hb1p + g); }
+  };
+
   RowV<T> Rnext = load_row(y0 - 2);
   for (int k = y0 - 2; k <= y0 + TY + 1; ++k) {
+    prefetch_rows(k);
     Rm = R0; R0 = Rp; Rp = Rnext;
     if (k < y0 + TY + 1) Rnext = load_row(k + 1);  // prefetch the next row
     Sm = S0;
