@@ -67,6 +67,9 @@ typedef struct {
 } sv_params;
 
 #define SV_FLAG_NO_TALLIES 1u /* skip the rain/outflow tally partials                    */
+#define SV_FLAG_ELOSS_FIRST 2u /* energy loss listed before Manning roughness in the config:
+                                  both add to du/dt and dv/dt, so their order sets the
+                                  rounding; infiltration (dh/dt only) commutes with both   */
 
 /* named Runge-Kutta tableaux, in the order of runge_kutta_named_coefficient_sets_ */
 #define SV_RK_EULER 0
@@ -97,6 +100,11 @@ typedef struct {
 #define SV_FIELD_HBDY0 10       /* head xbdy0 (NaN = not selected)                        */
 #define SV_FIELD_HBDY1 11
 #define SV_FIELD_RAIN_PATTERN 12 /* per-cell rain pattern P for SV_RAIN_PATTERN            */
+#define SV_FIELD_INFIL_RATE 13  /* infiltration rate, m/s (InfiltrationSourceTerm.hpp:106)   */
+#define SV_FIELD_INFIL_CAP 14   /* remaining infiltration capacity, m; consumed at every
+                                   stage evaluation as in InfiltrationSourceTerm.cpp:61      */
+#define SV_FIELD_ELOSS_FX 15    /* energy-loss coefficient fx/m (EnergyLossSourceTerm.hpp:199)*/
+#define SV_FIELD_ELOSS_FY 16    /* energy-loss coefficient fy/m                              */
 #define SV_FIELD_DHDT 20        /* dUdt_[0] of the last sv_eval_dudt(0, ...)              */
 #define SV_FIELD_DUDT 21
 #define SV_FIELD_DVDT 22
@@ -126,6 +134,10 @@ typedef struct {
 #define SV_HEAD_NONE 0
 #define SV_HEAD_EDGES 1    /* one-cell strips along the edges in head_edges               */
 #define SV_HEAD_FIELDS 2   /* per-cell SV_FIELD_HBDY0/HBDY1 (NaN = not selected)          */
+/* stage boundary (StageBoundarySourceTerm.cpp:39-69): targets are water levels, the depth
+ * target being level - bed; it takes the head boundary's place in the boundary order */
+#define SV_STAGE_EDGES 3   /* one-cell strips along head_edges, levels head_h0/head_h1     */
+#define SV_STAGE_FIELDS 4  /* per-cell levels in SV_FIELD_HBDY0/HBDY1 (NaN = not selected)*/
 #define SV_EDGE_XMIN 1u
 #define SV_EDGE_XMAX 2u
 #define SV_EDGE_YMIN 4u

@@ -18,13 +18,13 @@ import numpy as np
 from . import _abi
 from ._abi import (FIELD, FACE_FIELDS, RK_METHODS, RK_STAGES, Forcing, MeshDesc, Params, Stats,
                    RAIN_NONE, RAIN_UNIFORM, RAIN_FIELDS, RAIN_PATTERN, HEAD_NONE, HEAD_EDGES,
-                   HEAD_FIELDS, EDGE_XMIN, EDGE_XMAX, EDGE_YMIN, EDGE_YMAX, SV_F32, SV_F64,
-                   SV_F32_DATUM64)
+                   HEAD_FIELDS, STAGE_EDGES, STAGE_FIELDS, EDGE_XMIN, EDGE_XMAX, EDGE_YMIN, EDGE_YMAX,
+                   SV_F32, SV_F64, SV_F32_DATUM64)
 
 __all__ = ["SaintVenantSolver", "SvError", "TimeSeries", "solve", "num_steps", "load_library",
            "FIELD", "Forcing", "RK_METHODS", "RAIN_NONE", "RAIN_UNIFORM", "RAIN_FIELDS",
-           "RAIN_PATTERN", "HEAD_NONE", "HEAD_EDGES", "HEAD_FIELDS", "EDGE_XMIN", "EDGE_XMAX",
-           "EDGE_YMIN", "EDGE_YMAX"]
+           "RAIN_PATTERN", "HEAD_NONE", "HEAD_EDGES", "HEAD_FIELDS", "STAGE_EDGES", "STAGE_FIELDS",
+           "EDGE_XMIN", "EDGE_XMAX", "EDGE_YMIN", "EDGE_YMAX"]
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libsv_b200.so")
 _lib = None
@@ -148,7 +148,7 @@ class SaintVenantSolver(_Backend):
 
     def __init__(self, nx, ny, dx, dy=None, precision="f64", rk_method="classic", cn_target=1.0,
                  step_duration=60.0, initial_dt=1.0, max_dt=0.0, rain_mode="reference", manning=True,
-                 head_first=False, tallies=True, device=0):
+                 head_first=False, tallies=True, device=0, eloss_first=False):
         self._lib = load_library()
         self.nx, self.ny = int(nx), int(ny)
         self.dx = float(dx)
@@ -163,7 +163,7 @@ class SaintVenantSolver(_Backend):
         p = Params(_precision_code(precision), RK_METHODS.index(rk_method), float(cn_target),
                    self.step_duration, float(initial_dt), float(max_dt),
                    0 if rain_mode == "reference" else 1, 1 if manning else 0, 1 if head_first else 0,
-                   0 if tallies else _abi.SV_FLAG_NO_TALLIES)
+                   _flags(tallies, eloss_first))
         h = C.c_void_p()
         r = self._lib.sv_create(C.byref(m), C.byref(p), int(device), C.byref(h))
         if r != 0:
@@ -266,16 +266,22 @@ def num_steps(start_time, end_time, step_duration):
     return n + 1
 
 
-def start_new_step_forcing(t, L, rain=None, rain_kind=RAIN_UNIFORM, head=None, head_edges=0):
+def _flags(tallies=True, eloss_first=False):
+    return (0 if tallies else _abi.SV_FLAG_NO_TALLIES) | (_abi.SV_FLAG_ELOSS_FIRST if eloss_first else 0)
+
+
+def start_new_step_forcing(t, L, rain=None, rain_kind=RAIN_UNIFORM, head=None, head_edges=0,
+                           head_kind=HEAD_EDGES):
     """Boundary values for [t, t + L] (DischargeBoundarySourceTerm.hpp:114-146,
-    HeadBoundarySourceTerm.hpp:114-146): rain / head are TimeSeries, constants or None."""
+    HeadBoundarySourceTerm.hpp:114-146): rain / head are TimeSeries, constants or None;
+    head_kind STAGE_EDGES reads `head` as water levels (a stage boundary)."""
     f = Forcing()
     if rain is not None:
         q0, q1 = (rain.at(t), rain.at(t + L)) if isinstance(rain, TimeSeries) else (float(rain), float(rain))
         f.rain_kind, f.rain_q0, f.rain_q1 = rain_kind, q0, q1
     if head is not None:
         h0, h1 = (head.at(t), head.at(t + L)) if isinstance(head, TimeSeries) else (float(head), float(head))
-        f.head_kind, f.head_edges, f.head_h0, f.head_h1 = HEAD_EDGES, head_edges, h0, h1
+        f.head_kind, f.head_edges, f.head_h0, f.head_h1 = head_kind, head_edges, h0, h1
     return f
 
 

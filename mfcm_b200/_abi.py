@@ -15,6 +15,7 @@ SV_F64 = 2
 SV_F32_DATUM64 = 3
 
 SV_FLAG_NO_TALLIES = 1
+SV_FLAG_ELOSS_FIRST = 2
 
 RK_METHODS = ["euler", "midpoint", "heun2", "ralston2", "kutta3", "heun3", "wray3", "ralston3",
               "ssprk3", "classic", "ralston4", "3/8rule"]
@@ -22,14 +23,14 @@ RK_STAGES = [1, 2, 2, 2, 3, 3, 3, 3, 3, 4, 4, 4]
 
 FIELD = dict(
     Z=0, H=1, U=2, V=3, N_SHALLOW=4, N_DEEP=5, D_SHALLOW=6, D_DEEP=7, QBDY0=8, QBDY1=9,
-    HBDY0=10, HBDY1=11, RAIN_PATTERN=12, DHDT=20, DUDT=21, DVDT=22, DHDX=23, DUDX=24, DVDX=25,
+    HBDY0=10, HBDY1=11, RAIN_PATTERN=12, INFIL_RATE=13, INFIL_CAP=14, ELOSS_FX=15, ELOSS_FY=16, DHDT=20, DUDT=21, DVDT=22, DHDX=23, DUDX=24, DVDX=25,
     DHDY=26, DUDY=27, DVDY=28, DZDX=29, DZDY=30, FLUX_H=40, FLUX_U=41, FLUX_V=42, FLUX_Z=43,
     FLUX_BRANCH=44, STATE_BASE=100, K_BASE=200,
 )
 FACE_FIELDS = {40, 41, 42, 43, 44}
 
 RAIN_NONE, RAIN_UNIFORM, RAIN_FIELDS, RAIN_PATTERN = 0, 1, 2, 3
-HEAD_NONE, HEAD_EDGES, HEAD_FIELDS = 0, 1, 2
+HEAD_NONE, HEAD_EDGES, HEAD_FIELDS, STAGE_EDGES, STAGE_FIELDS = 0, 1, 2, 3, 4
 EDGE_XMIN, EDGE_XMAX, EDGE_YMIN, EDGE_YMAX = 1, 2, 4, 8
 
 

@@ -7,7 +7,7 @@ clock and tallies, so its results are bit-identical to running it alone.
 """
 import ctypes as C
 
-from . import _abi, load_library, SvError, _Backend, _precision_code, RK_METHODS, RK_STAGES
+from . import _abi, load_library, SvError, _Backend, _precision_code, _flags, RK_METHODS, RK_STAGES
 from ._abi import MeshDesc, Params, Stats
 
 
@@ -75,12 +75,12 @@ class SaintVenantBatch:
         self.members = {}
 
     def add(self, nx, ny, dx, dy=None, cn_target=1.0, step_duration=60.0, initial_dt=1.0, max_dt=0.0,
-            rain_mode="reference", manning=True, head_first=False, tallies=True):
+            rain_mode="reference", manning=True, head_first=False, tallies=True, eloss_first=False):
         dy = float(dx if dy is None else dy)
         m = MeshDesc(int(nx), int(ny), float(dx), dy, 0.0, 0.0)
         p = Params(_precision_code(self.precision), RK_METHODS.index(self.rk_method), float(cn_target),
                    float(step_duration), float(initial_dt), float(max_dt), 0 if rain_mode == "reference" else 1,
-                   1 if manning else 0, 1 if head_first else 0, 0 if tallies else _abi.SV_FLAG_NO_TALLIES)
+                   1 if manning else 0, 1 if head_first else 0, _flags(tallies, eloss_first))
         slot = C.c_int()
         r = self._lib.sv_batch_add(self._b, C.byref(m), C.byref(p), C.byref(slot))
         if r != 0:

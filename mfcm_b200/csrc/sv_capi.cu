@@ -153,6 +153,8 @@ struct Solver final : public sv_ctx {
   double man_s[4] = {0.03, 0.3, 0.1, 0.3};  // ManningRoughnessSourceTerm.cpp:99-102
   std::vector<double> host_n_shallow;
   T *q0 = nullptr, *q1 = nullptr, *pat = nullptr, *hb0 = nullptr, *hb1 = nullptr;
+  T *irate = nullptr, *icap = nullptr;  // InfiltrationSourceTerm fields (.hpp:106-109)
+  T *efx = nullptr, *efy = nullptr;     // EnergyLossSourceTerm fields (.hpp:199-202)
   // debug buffers (per-function parity path)
   T* dbg_slp[8] = {};
   T* dbg_face[5] = {};
@@ -272,6 +274,10 @@ struct Solver final : public sv_ctx {
       case SV_FIELD_HBDY0: lazy = true; return &hb0;
       case SV_FIELD_HBDY1: lazy = true; return &hb1;
       case SV_FIELD_RAIN_PATTERN: lazy = true; return &pat;
+      case SV_FIELD_INFIL_RATE: lazy = true; return &irate;
+      case SV_FIELD_INFIL_CAP: lazy = true; return &icap;
+      case SV_FIELD_ELOSS_FX: lazy = true; return &efx;
+      case SV_FIELD_ELOSS_FY: lazy = true; return &efy;
     }
     return nullptr;
   }
@@ -426,7 +432,7 @@ struct Solver final : public sv_ctx {
   // SV_RAIN_FIELDS needs (BoundarySourceTerm::clear_values); a queued batch step may not.
   int make_forcing(const sv_forcing* f, DevForcing* d, bool may_alloc) {
     if (!f) return fail(SV_E_ARG, "null forcing");
-    if (f->rain_kind < 0 || f->rain_kind > 3 || f->head_kind < 0 || f->head_kind > 2)
+    if (f->rain_kind < 0 || f->rain_kind > 3 || f->head_kind < 0 || f->head_kind > 4)
       return fail(SV_E_ARG, "bad forcing kind");
     if (f->rain_kind == SV_RAIN_FIELDS && (!q0 || !q1)) {
       if (!may_alloc) return fail(SV_E_STATE, "discharge fields not set");
@@ -434,7 +440,8 @@ struct Solver final : public sv_ctx {
       if (!q1) { SV_CUDA(alloc_cells(&q1)); graph_dirty = true; ++pversion; }
     }
     if (f->rain_kind == SV_RAIN_PATTERN && !pat) return fail(SV_E_STATE, "rain pattern field not set");
-    if (f->head_kind == SV_HEAD_FIELDS && (!hb0 || !hb1)) return fail(SV_E_STATE, "head fields not set");
+    if ((f->head_kind == SV_HEAD_FIELDS || f->head_kind == SV_STAGE_FIELDS) && (!hb0 || !hb1))
+      return fail(SV_E_STATE, "head fields not set");
     *d = DevForcing{};
     d->rain_kind = f->rain_kind;
     d->head_kind = f->head_kind;
@@ -499,6 +506,13 @@ struct Solver final : public sv_ctx {
     for (int i = 0; i < 4; ++i) { P.man_p[i] = man[i]; P.man_s[i] = T(man_s[i]); }
     P.fc = fc;
     P.q0p = q0; P.q1p = q1; P.pat = pat; P.hb0p = hb0; P.hb1p = hb1;
+    // a source term runs once both of its fields are set (the reference builds each with
+    // both fields, ...SourceTerm::create_source_term)
+    P.irate = (irate && icap) ? irate : nullptr;
+    P.icap = (irate && icap) ? icap : nullptr;
+    P.efx = (efx && efy) ? efx : nullptr;
+    P.efy = (efx && efy) ? efy : nullptr;
+    P.eloss_first = (prm.flags & SV_FLAG_ELOSS_FIRST) ? 1 : 0;
     P.manning = prm.manning; P.rain_mode = prm.rain_mode; P.head_first = prm.head_first;
     P.nstages = N;
     P.ctl = ctl;
@@ -770,6 +784,17 @@ struct Solver final : public sv_ctx {
       P.Yout[f] = Y[0][f];
       P.Kout[f] = (!diag && N > 1) ? K[0][f] : nullptr;
     }
+    // the timing launches consume infiltration capacity: give them a copy
+    T* cap_copy = nullptr;
+    if (P.icap) {
+      SV_CUDA(cudaMalloc(&cap_copy, size_t(ncells) * sizeof(T)));
+      SV_CUDA(cudaMemcpyAsync(cap_copy, icap, size_t(ncells) * sizeof(T), cudaMemcpyDeviceToDevice, stream));
+      P.icap = cap_copy;
+    }
+    struct FreeOnExit {
+      T* p;
+      ~FreeOnExit() { if (p) cudaFree(p); }
+    } cap_guard{cap_copy};
     int best = variant;
     float best_ms = 1e30f;
     for (int v = 0; v < svk::kNumVariants; ++v) {

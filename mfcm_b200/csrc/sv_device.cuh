@@ -419,4 +419,29 @@ __device__ __forceinline__ void manning_apply(T h, T u, T v, T ns, T nd, T ds, T
   }
 }
 
+// Energy loss (EnergyLossSourceTerm.cpp:64-87): du = -0.5 u fx |U|, dv = -0.5 v fy |U| on
+// cells deeper than 1e-6 m, capped like the roughness term; adds to du, dv.
+template <typename T, typename CC>
+__device__ __forceinline__ void energy_loss_apply(T h, T u, T v, T fx, T fy, const CC& c, T& du, T& dv) {
+  if (!(h > T(1e-6))) return;
+  T hyp = ssqrt(u * u + v * v);
+  T eu = T(-0.5) * u * fx * hyp;
+  T ev = T(-0.5) * v * fy * hyp;
+  T eudt = eu * c.dt, evdt = ev * c.dt;
+  if (sfabs(eudt) > sfabs(u) && ssign(eudt) != ssign(u)) eu = -c.divdt(u);
+  if (sfabs(evdt) > sfabs(v) && ssign(evdt) != ssign(v)) ev = -c.divdt(v);
+  du = du + eu;
+  dv = dv + ev;
+}
+
+// Infiltration (InfiltrationSourceTerm.cpp:43-62): the depth taken this evaluation,
+// rate * dt limited by the water present and by the remaining soil capacity.
+template <typename T, typename CC>
+__device__ __forceinline__ T infiltration_depth(T h, T rate, T cap, const CC& c) {
+  T dh = rate * c.dt;
+  if (dh > h) dh = h;
+  if (dh > cap) dh = cap;
+  return dh;
+}
+
 }  // namespace svd

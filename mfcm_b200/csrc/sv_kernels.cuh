@@ -75,7 +75,10 @@ template <typename T> struct StageParams {
   const DevForcing* fc;  // per-step boundary values
   const T* q0p; const T* q1p; const T* pat;
   const T* hb0p; const T* hb1p;
+  const T* irate; T* icap;   // infiltration rate (m/s) and remaining capacity (m), or nullptr
+  const T* efx; const T* efy;  // energy-loss coefficients fx/m, fy/m, or nullptr
   int manning, rain_mode, head_first;
+  int eloss_first;       // energy loss applied before roughness (configuration order)
   int stage, nstages, mode;
   double c_s;            // c of this stage: t_sub = t_local + c_s * dt
   double a_next[4];      // a(s+2, j+1), j = 0..s: coefficients of Y_{s+1}
@@ -184,25 +187,50 @@ __device__ __forceinline__ void cell_dudt(const StageParams<T>& P, const DevForc
   dvdt = dvdt + c.divy(fs.z - fn.z);
   dudt = dudt + dudt_bed;
   dvdt = dvdt + dvdt_bed;
-  if (P.manning) {
+  // source terms in configuration order (Solver.cpp:98-104): roughness and energy loss both
+  // add to du/dt, dv/dt, so only their relative order changes the rounding
+  auto do_manning = [&]() {
+    if (!P.manning) return;
     T ns = P.man_p[0] ? ld(P.man_p[0], g) : P.man_s[0];
     T nd = P.man_p[1] ? (P.man_p[1] == P.man_p[0] ? ns : ld(P.man_p[1], g)) : P.man_s[1];
     T ds = P.man_p[2] ? ld(P.man_p[2], g) : P.man_s[2];
     T dd = P.man_p[3] ? ld(P.man_p[3], g) : P.man_s[3];
     manning_apply<T>(h, u, v, ns, nd, ds, dd, c, dudt, dvdt, n_out, sf_out);
+  };
+  auto do_eloss = [&]() {
+    if (P.efx) energy_loss_apply<T>(h, u, v, ld(P.efx, g), ld(P.efy, g), c, dudt, dvdt);
+  };
+  if (P.eloss_first) { do_eloss(); do_manning(); }
+  else { do_manning(); do_eloss(); }
+  if (P.irate) {  // infiltration (InfiltrationSourceTerm.cpp:43-62), capacity consumed in place
+    T cap = P.icap[g];
+    T dh = infiltration_depth<T>(h, ld(P.irate, g), cap, c);
+    dhdt = dhdt - c.divdt(dh);
+    P.icap[g] = cap - dh;
   }
   rain = 0.0;
   removed = 0.0;
-  // head boundary target values for this cell (NaN = not selected)
+  // head boundary target values for this cell (NaN = not selected); a stage boundary
+  // (StageBoundarySourceTerm.cpp:48-52) gives water levels, from which the bed is subtracted
   bool head_sel = false;
   T h0 = T(0), h1 = T(0);
-  if (fc.head_kind == 1) {
+  const int hk = fc.head_kind;
+  if (hk == 1 || hk == 3) {
     head_sel = ((fc.head_edges & 1u) && gx == 0) || ((fc.head_edges & 2u) && gx == P.nx - 1) ||
                ((fc.head_edges & 4u) && gy == 0) || ((fc.head_edges & 8u) && gy == P.ny - 1);
     h0 = T(fc.hh0); h1 = T(fc.hh1);
-  } else if (fc.head_kind == 2) {
+  } else if (hk == 2 || hk == 4) {
     h0 = ld(P.hb0p, g); h1 = ld(P.hb1p, g);
     head_sel = true;
+  }
+  if (head_sel && hk >= 3) {
+    if (P.zdat) {  // absolute bed = FP64 datum + FP32 offset; levels minus bed in FP64
+      const double zb = P.zdat[datum_tile(gx, gy, P.dtiles_x)] + double(ld(P.z, g));
+      h0 = T(double(h0) - zb); h1 = T(double(h1) - zb);
+    } else {
+      const T zb = ld(P.z, g);
+      h0 = h0 - zb; h1 = h1 - zb;
+    }
   }
   if (head_sel && !(h0 == h0 && h1 == h1)) head_sel = false;  // NaN = not selected
   auto do_rain = [&]() {
@@ -634,6 +662,8 @@ __device__ __forceinline__ void sweep_strip(const StageParams<T>& P, long long g
       for (int f = 0; f < 4; ++f)
         if (P.man_p[f]) prefetch_l1(P.man_p[f] + g);
     }
+    if (P.irate) { prefetch_l1(P.irate + g); prefetch_l1(P.icap + g); }
+    if (P.efx) { prefetch_l1(P.efx + g); prefetch_l1(P.efy + g); }
     if (fc.rain_kind == 3) prefetch_l1(P.pat + g);
     if (fc.rain_kind == 2) { prefetch_l1(P.q0p + g); prefetch_l1(P.q1p + g); }
     if (fc.head_kind == 2) { prefetch_l1(P.hb0p + g); prefetch_l1(P.hb1p + g); }

@@ -225,11 +225,13 @@ struct Params {
   int rain_mode = 0;          // 0 = reference clamp, 1 = physical (sign-corrected) clamp
   int manning = 1;            // Manning source term present
   int head_first = 0;         // boundary order: 0 = discharge then head, 1 = head then discharge
+  int eloss_first = 0;        // source order: 1 = energy loss listed before Manning roughness
 };
 
 enum Field : int {
   F_Z = 0, F_H = 1, F_U = 2, F_V = 3, F_N_SHALLOW = 4, F_N_DEEP = 5, F_D_SHALLOW = 6, F_D_DEEP = 7,
   F_QBDY0 = 8, F_QBDY1 = 9, F_HBDY0 = 10, F_HBDY1 = 11, F_RAIN_PATTERN = 12,
+  F_INFIL_RATE = 13, F_INFIL_CAP = 14, F_ELOSS_FX = 15, F_ELOSS_FY = 16,
   F_DHDT = 20, F_DUDT = 21, F_DVDT = 22, F_DHDX = 23, F_DUDX = 24, F_DVDX = 25,
   F_DHDY = 26, F_DUDY = 27, F_DVDY = 28, F_DZDX = 29, F_DZDY = 30, F_NH = 31, F_SF = 32,
   F_FLUX_H = 40, F_FLUX_U = 41, F_FLUX_V = 42, F_FLUX_Z = 43, F_FLUX_BRANCH = 44,
@@ -302,6 +304,9 @@ class Solver final : public SolverBase {
   Vec fh, fu, fv, fz, fb;               // SaintVenantFluxes (Fluxes.cpp:24-42)
   Vec ns, nd, ds, dd, nh, Sf;           // ManningRoughnessSourceTerm (ManningRoughnessSourceTerm.hpp:111-117)
   Vec qb0, qb1, hb0, hb1, pattern;      // boundary xbdy0/xbdy1 (BoundarySourceTerm.hpp:44-45)
+  Vec irate, icap;                      // InfiltrationSourceTerm (InfiltrationSourceTerm.hpp:106-109)
+  Vec efx, efy;                         // EnergyLossSourceTerm (EnergyLossSourceTerm.hpp:199-202)
+  unsigned present = 0;                 // which of those four fields were set (bits 0-3)
   Forcing forcing;
   TT dt_;
   Stats st_;
@@ -324,6 +329,7 @@ class Solver final : public SolverBase {
     qb0.assign(n, T(0)); qb1.assign(n, T(0));
     hb0.assign(n, std::numeric_limits<T>::quiet_NaN()); hb1.assign(n, std::numeric_limits<T>::quiet_NaN());
     pattern.assign(n, T(0));
+    irate.assign(n, T(0)); icap.assign(n, T(0)); efx.assign(n, T(0)); efy.assign(n, T(0));
     dt_ = TT(p.initial_dt);
     rain_sum_.assign(N, 0.0); out_sum_.assign(N, 0.0);
     update_constants();
@@ -346,6 +352,8 @@ class Solver final : public SolverBase {
       case F_N_SHALLOW: return &ns; case F_N_DEEP: return &nd; case F_D_SHALLOW: return &ds;
       case F_D_DEEP: return &dd; case F_QBDY0: return &qb0; case F_QBDY1: return &qb1;
       case F_HBDY0: return &hb0; case F_HBDY1: return &hb1; case F_RAIN_PATTERN: return &pattern;
+      case F_INFIL_RATE: return &irate; case F_INFIL_CAP: return &icap;
+      case F_ELOSS_FX: return &efx; case F_ELOSS_FY: return &efy;
       case F_DHDT: return &K[0].h; case F_DUDT: return &K[0].u; case F_DVDT: return &K[0].v;
       case F_DHDX: return &dUdx.h; case F_DUDX: return &dUdx.u; case F_DVDX: return &dUdx.v;
       case F_DHDY: return &dUdy.h; case F_DUDY: return &dUdy.u; case F_DVDY: return &dUdy.v;
@@ -372,6 +380,7 @@ class Solver final : public SolverBase {
     if (n != f->size()) throw std::runtime_error("field size mismatch");
     for (size_t i = 0; i < n; ++i) (*f)[i] = T(src[i]);
     if (id == F_Z) update_constants();
+    if (id >= F_INFIL_RATE && id <= F_ELOSS_FY) present |= 1u << (id - F_INFIL_RATE);
   }
   void get_field(int id, double* dst, size_t n) const override {
     const Vec* f = field_ptr(id);
@@ -403,7 +412,9 @@ class Solver final : public SolverBase {
       for (size_t i = 0; i < n; ++i) { qb0[i] += pattern[i] * a; qb1[i] += pattern[i] * b; }
     }
     // rain_kind == 2: the caller uploads QBDY0/QBDY1 after this call
-    if (f.head_kind == 1) {
+    // head_kind 3 is a stage boundary on edge strips (StageBoundarySourceTerm): the same
+    // selection and values, read as water levels by stage_cell
+    if (f.head_kind == 1 || f.head_kind == 3) {
       for (size_t i = 0; i < n; ++i) { hb0[i] = hb0[i] * T(0.0) + T(0.0); hb1[i] = hb1[i] * T(0.0) + T(0.0); }
       T a = T(f.head_h0), b = T(f.head_h1);
       for (size_t i = 0; i < n; ++i) {
@@ -581,6 +592,31 @@ class Solver final : public SolverBase {
     }
   }
 
+  // EnergyLossSourceKernel::operator() (EnergyLossSourceTerm.cpp:56-88)
+  void eloss_cell(size_t c, const State& S, State& D, double timestep) {
+    T h = S.h[c], u = S.u[c], v = S.v[c];
+    if (h > 1e-6) {
+      T hyp = std::sqrt(u * u + v * v);
+      T dudt = -T(0.5) * u * efx[c] * hyp;
+      T dvdt = -T(0.5) * v * efy[c] * hyp;
+      if (std::fabs(dudt * timestep) > std::fabs(u) && ssign(dudt * timestep) != ssign(u)) dudt = -u / timestep;
+      if (std::fabs(dvdt * timestep) > std::fabs(v) && ssign(dvdt * timestep) != ssign(v)) dvdt = -v / timestep;
+      D.u[c] += dudt;
+      D.v[c] += dvdt;
+    }
+  }
+
+  // InfiltrationSourceKernel::operator() (InfiltrationSourceTerm.cpp:43-62): the capacity
+  // field is consumed at every evaluation, repeated timesteps included.
+  void infiltration_cell(size_t c, const State& S, State& D, double timestep) {
+    T h = S.h[c];
+    T dh = irate[c] * timestep;
+    if (dh > h) dh = h;
+    if (dh > icap[c]) dh = icap[c];
+    D.h[c] -= dh / timestep;
+    icap[c] -= dh;
+  }
+
   // DischargeBoundarySourceKernel::operator() (DischargeBoundarySourceTerm.cpp:39-69);
   // returns the depth rate added (0 when skipped).
   T discharge_cell(size_t c, const State& S, State& D, double timestep, double time_now, double step_length) {
@@ -606,6 +642,11 @@ class Solver final : public SolverBase {
   // true when the cell's dh/dt was assigned.
   bool head_cell(size_t c, const State& S, State& D, double timestep, double time_now, double step_length) {
     T h0 = hb0[c], h1 = hb1[c];
+    if (forcing.head_kind >= 3) {  // StageBoundarySourceKernel (StageBoundarySourceTerm.cpp:48-52)
+      T zc = z[c];
+      h0 = hb0[c] - zc;
+      h1 = hb1[c] - zc;
+    }
     if (!(h0 != h0) && !(h1 != h1)) {
       T h = S.h[c];
       T dhbdydt = (h1 - h0) / step_length;
@@ -646,9 +687,24 @@ class Solver final : public SolverBase {
 #pragma omp parallel for schedule(static)
     for (size_t c = 0; c < n; ++c) temporal_derivative(c, S, D);
     // source terms (Solver.cpp:98-104)
-    if (p.manning) {
+    // (energy loss and infiltration run when both of their fields were set, as the
+    // reference constructs each with both fields; Manning and energy loss in their
+    // configuration order, infiltration touches dh/dt only)
+    auto run_manning = [&]() {
+      if (!p.manning) return;
 #pragma omp parallel for schedule(static)
       for (size_t c = 0; c < n; ++c) manning_cell(c, S, D, double(timestep));
+    };
+    auto run_eloss = [&]() {
+      if ((present & 12u) != 12u) return;
+#pragma omp parallel for schedule(static)
+      for (size_t c = 0; c < n; ++c) eloss_cell(c, S, D, double(timestep));
+    };
+    if (p.eloss_first) { run_eloss(); run_manning(); }
+    else { run_manning(); run_eloss(); }
+    if ((present & 3u) == 3u) {
+#pragma omp parallel for schedule(static)
+      for (size_t c = 0; c < n; ++c) infiltration_cell(c, S, D, double(timestep));
     }
     // boundaries in configuration order (Solver.cpp:107-113); the tallies record the rain
     // depth rate added and the depth rate removed by the head assignment.

@@ -34,6 +34,7 @@ svo::Params to_params(const sv_params* p) {
   q.rain_mode = p->rain_mode;
   q.manning = p->manning;
   q.head_first = p->head_first;
+  q.eloss_first = (p->flags & SV_FLAG_ELOSS_FIRST) ? 1 : 0;
   return q;
 }
 }  // namespace

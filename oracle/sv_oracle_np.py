@@ -18,6 +18,9 @@ Reference lines followed:
   Manning roughness             src/SaintVenant/SourceTerms/ManningRoughnessSourceTerm.cpp:44-88
   discharge (rain) boundary     src/SaintVenant/Boundaries/DischargeBoundarySourceTerm.cpp:39-69
   head (outflow) boundary       src/SaintVenant/Boundaries/HeadBoundarySourceTerm.cpp:39-67
+  stage boundary                src/SaintVenant/Boundaries/StageBoundarySourceTerm.cpp:39-69
+  energy loss                   src/SaintVenant/SourceTerms/EnergyLossSourceTerm.cpp:56-88
+  infiltration                  src/SaintVenant/SourceTerms/InfiltrationSourceTerm.cpp:38-64
   update_dUdt order             src/SaintVenant/Solver.cpp:73-114
   tableaux                      src/TemporalScheme/RungeKutta.cpp:83-115
   timestep and controller       src/TemporalScheme/RungeKutta.cpp:141-167
@@ -224,11 +227,14 @@ def face_fluxes(h, u, v, z, sl, nx, ny, dx, dy):
 
 
 def update_dudt(h, u, v, z, dx, dy, *, manning=None, qbdy=None, hbdy=None, time_now=0.0, timestep=1.0,
-                step_length=60.0, rain_mode="reference", head_first=False):
+                step_length=60.0, rain_mode="reference", head_first=False, eloss=None, eloss_first=False,
+                infil=None, stage=False):
     """dU/dt of one state (SaintVenantSolver::update_dUdt, Solver.cpp:73-114). Arrays are
     (ny, nx). manning = (n_shallow, n_deep, d_shallow, d_deep) per-cell arrays or None (no
-    roughness term); qbdy = (q0, q1) and hbdy = (h0, h1) per-cell boundary values or None.
-    Returns a dict of slopes, face fields and dhdt/dudt/dvdt."""
+    roughness term); eloss = (fx, fy) energy-loss coefficients or None; infil = (rate,
+    capacity) or None; qbdy = (q0, q1) and hbdy = (h0, h1) per-cell boundary values or None,
+    hbdy holding water levels when `stage` (a stage boundary). Returns a dict of slopes, face
+    fields, dhdt/dudt/dvdt and, with infiltration, the capacity left ("infil_cap")."""
     ny, nx = h.shape
     sl = {"dhdx": slope_x(h, dx), "dudx": slope_x(u, dx), "dvdx": slope_x(v, dx),
           "dhdy": slope_y(h, dy), "dudy": slope_y(u, dy), "dvdy": slope_y(v, dy),
@@ -253,7 +259,9 @@ def update_dudt(h, u, v, z, dx, dy, *, manning=None, qbdy=None, hbdy=None, time_
         dvdt = dvdt + (fz[s] - fz[n]) / dy
         dudt = dudt + (-G) * zx
         dvdt = dvdt + (-G) * zy
-        if manning is not None:
+        def roughness(dudt, dvdt):
+            if manning is None:
+                return dudt, dvdt
             ns, nd, ds, dd = manning
             t = np.fmin(np.fmax((h - ds) / (dd - ds), 0.0), 1.0)
             nman = ns + (nd - ns) * ((t * t) * (3.0 - 2.0 * t))
@@ -266,8 +274,38 @@ def update_dudt(h, u, v, z, dx, dy, *, manning=None, qbdy=None, hbdy=None, time_
             capv = (np.abs(fv_ * timestep) > np.abs(v)) & (sign(fv_ * timestep) != sign(v))
             fu_ = np.where(capu, -u / timestep, fu_)
             fv_ = np.where(capv, -v / timestep, fv_)
-            dudt = np.where(wet, dudt + fu_, dudt)
-            dvdt = np.where(wet, dvdt + fv_, dvdt)
+            return np.where(wet, dudt + fu_, dudt), np.where(wet, dvdt + fv_, dvdt)
+
+        def energy_loss(dudt, dvdt):
+            # EnergyLossSourceKernel::operator() (EnergyLossSourceTerm.cpp:64-87)
+            if eloss is None:
+                return dudt, dvdt
+            fx, fy = eloss
+            wet = h > 1e-6
+            hyp = np.sqrt(u * u + v * v)
+            eu = (((-0.5) * u) * fx) * hyp
+            ev = (((-0.5) * v) * fy) * hyp
+            capu = (np.abs(eu * timestep) > np.abs(u)) & (sign(eu * timestep) != sign(u))
+            capv = (np.abs(ev * timestep) > np.abs(v)) & (sign(ev * timestep) != sign(v))
+            eu = np.where(capu, -u / timestep, eu)
+            ev = np.where(capv, -v / timestep, ev)
+            return np.where(wet, dudt + eu, dudt), np.where(wet, dvdt + ev, dvdt)
+
+        if eloss_first:
+            dudt, dvdt = energy_loss(dudt, dvdt)
+            dudt, dvdt = roughness(dudt, dvdt)
+        else:
+            dudt, dvdt = roughness(dudt, dvdt)
+            dudt, dvdt = energy_loss(dudt, dvdt)
+        cap_left = None
+        if infil is not None:
+            # InfiltrationSourceKernel::operator() (InfiltrationSourceTerm.cpp:43-62)
+            rate, cap = infil
+            dh = rate * timestep
+            dh = np.where(dh > h, h, dh)
+            dh = np.where(dh > cap, cap, dh)
+            dhdt = dhdt - dh / timestep
+            cap_left = cap - dh
 
         def discharge(dh):
             if qbdy is None:
@@ -288,6 +326,8 @@ def update_dudt(h, u, v, z, dx, dy, *, manning=None, qbdy=None, hbdy=None, time_
             if hbdy is None:
                 return dh
             h0, h1 = hbdy
+            if stage:  # StageBoundarySourceKernel (StageBoundarySourceTerm.cpp:48-52)
+                h0, h1 = h0 - z, h1 - z
             on = ~np.isnan(h0) & ~np.isnan(h1)
             slope = (h1 - h0) / step_length
             now = h0 + time_now * slope
@@ -299,7 +339,7 @@ def update_dudt(h, u, v, z, dx, dy, *, manning=None, qbdy=None, hbdy=None, time_
         dhdt = discharge(head(dhdt)) if head_first else head(discharge(dhdt))
     out = dict(sl)
     out.update({"flux_h": fh, "flux_u": fu, "flux_v": fv, "flux_z": fz, "flux_branch": fb,
-                "dhdt": dhdt, "dudt": dudt, "dvdt": dvdt})
+                "dhdt": dhdt, "dudt": dudt, "dvdt": dvdt, "infil_cap": cap_left})
     return out
 
 
@@ -338,7 +378,7 @@ def control_number(h, u, v, dx, dy, timestep):
     return float(np.max(cn))
 
 
-def do_timestep(h, u, v, z, dx, dy, local_time, dt, method="classic", cn_target=1.0, **terms):
+def do_timestep(h, u, v, z, dx, dy, local_time, dt, method="classic", cn_target=1.0, terms_out=None, **terms):
     """RungeKuttaTemporalScheme::do_timestep (RungeKutta.cpp:141-167) with the stage
     combination of RungeKuttaSolver::update_y (RungeKutta.hpp:371-405): stage s evaluates
     dU/dt of state s-1 at local_time + c_s dt, then state s = U0 + sum_j k_j (a(s+1, j) dt),
@@ -348,10 +388,13 @@ def do_timestep(h, u, v, z, dx, dy, local_time, dt, method="classic", cn_target=
     N = len(rows) - 1
     states = [(h, u, v)]
     ks = []
+    terms = dict(terms)
     for s in range(1, N + 1):
         t_sub = local_time + rows[s - 1][0] * dt
         y = states[s - 1]
         r = update_dudt(y[0], y[1], y[2], z, dx, dy, time_now=t_sub, timestep=dt, **terms)
+        if r["infil_cap"] is not None:  # the capacity is consumed by every stage evaluation
+            terms["infil"] = (terms["infil"][0], r["infil_cap"])
         ks.append((r["dhdt"], r["dudt"], r["dvdt"]))
         acc = [a.copy() for a in states[0]]
         with np.errstate(all="ignore"):
@@ -359,6 +402,8 @@ def do_timestep(h, u, v, z, dx, dy, local_time, dt, method="classic", cn_target=
                 coef = rows[s][col + 1] * dt
                 acc = [acc[k] + ks[col][k] * coef for k in range(3)]
         states.append(tuple(acc))
+    if terms_out is not None:
+        terms_out.update(terms)
     hN, uN, vN = states[N]
     cn = control_number(hN, uN, vN, dx, dy, dt)
     if cn > cn_target:

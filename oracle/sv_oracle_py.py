@@ -54,7 +54,7 @@ class OracleSolver(_Backend):
 
     def __init__(self, nx, ny, dx, dy=None, precision="f64", rk_method="classic", cn_target=1.0,
                  step_duration=60.0, initial_dt=1.0, max_dt=0.0, rain_mode="reference", manning=True,
-                 head_first=False, tallies=True, openmp=False, threads=0):
+                 head_first=False, tallies=True, openmp=False, threads=0, eloss_first=False):
         self._lib = load(openmp)
         if openmp and threads:
             self._lib.svo_set_threads(int(threads))
@@ -69,7 +69,8 @@ class OracleSolver(_Backend):
         p = _abi.Params(_precision_code(precision), RK_METHODS.index(rk_method), float(cn_target),
                         self.step_duration, float(initial_dt), float(max_dt),
                         0 if rain_mode == "reference" else 1, 1 if manning else 0, 1 if head_first else 0,
-                        0 if tallies else _abi.SV_FLAG_NO_TALLIES)
+                        (0 if tallies else _abi.SV_FLAG_NO_TALLIES) |
+                        (_abi.SV_FLAG_ELOSS_FIRST if eloss_first else 0))
         h = C.c_void_p()
         r = self._lib.svo_create(C.byref(m), C.byref(p), C.byref(h))
         if r != 0:

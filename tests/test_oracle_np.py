@@ -6,7 +6,7 @@ boundary orders. No GPU is needed."""
 import numpy as np
 import pytest
 
-from mfcm_b200 import EDGE_XMAX, EDGE_XMIN, EDGE_YMAX, EDGE_YMIN
+from mfcm_b200 import EDGE_XMAX, EDGE_XMIN, EDGE_YMAX, EDGE_YMIN, STAGE_EDGES
 from oracle import sv_oracle_np as onp
 from oracle.sv_oracle_py import OracleSolver
 from tests.scenarios import wet_dry_state, forcing, same, first_diff
@@ -117,3 +117,58 @@ def test_oracle_timestep_matches_numpy_restatement(method, case):
         got = o.get_field(100 + 3 * N + k)
         d = first_diff(got, want)
         assert d is None, f"U_[N] field {k}: first mismatch at {d[0]}: oracle {d[1]!r} numpy {d[2]!r}"
+
+
+@pytest.mark.parametrize("case", CASES[:2] + CASES[5:])
+@pytest.mark.parametrize("eloss_first", [False, True])
+def test_oracle_source_terms_match_numpy(case, eloss_first):
+    """Energy loss (either side of the roughness term), infiltration with its in-place
+    capacity, and a stage boundary on edge strips, against the numpy restatement."""
+    nx, ny, dx, dy, nan_cells, seed = case
+    z, h, u, v = wet_dry_state(nx, ny, dx, seed=seed + 11, nan_cells=0)
+    rng = np.random.default_rng(seed)
+    shape = (ny, nx)
+    fx, fy = rng.uniform(0.0, 0.5, shape), rng.uniform(0.0, 0.5, shape)
+    rate, cap = rng.uniform(0.0, 2e-3, shape), rng.uniform(0.0, 1e-3, shape)
+    n = (0.03, 0.05, 0.1, 0.3)
+    q = (2e-5, 1e-5)
+    level, edges = (float(np.median(z)) + 0.05, float(np.median(z))), EDGE_XMAX | EDGE_YMIN
+    t_now, ts, L = 7.5, 0.37, 60.0
+    o = OracleSolver(nx, ny, dx, dy, rain_mode="physical", step_duration=L, eloss_first=eloss_first)
+    for name, a in (("Z", z), ("H", h), ("U", u), ("V", v), ("ELOSS_FX", fx), ("ELOSS_FY", fy),
+                    ("INFIL_RATE", rate), ("INFIL_CAP", cap)):
+        o.set_field(name, a)
+    o.set_manning(*n)
+    f = forcing(q, head=level, edges=edges)
+    f.head_kind = STAGE_EDGES
+    o.set_forcing(f)
+    o.eval_dudt(0, t_now, ts)
+    ref = onp.update_dudt(h, u, v, z, dx, dy, manning=tuple(np.full(shape, x) for x in n),
+                          qbdy=(np.full(shape, q[0]), np.full(shape, q[1])),
+                          hbdy=onp.edge_strips(nx, ny, edges, *level), stage=True, time_now=t_now, timestep=ts,
+                          step_length=L, rain_mode="physical", eloss=(fx, fy), eloss_first=eloss_first,
+                          infil=(rate, cap))
+    _check(o, ref, KS)
+    assert same(o.get_field("INFIL_CAP"), ref["infil_cap"])
+
+
+def test_infiltration_capacity_is_consumed_by_every_stage():
+    nx, ny, dx, dy = 24, 18, 2.0, 2.0
+    z, h, u, v = wet_dry_state(nx, ny, dx, seed=4)
+    shape = (ny, nx)
+    rate, cap = np.full(shape, 1e-3), np.full(shape, 5e-4)
+    o = OracleSolver(nx, ny, dx, rain_mode="physical", cn_target=0.5)
+    for name, a in (("Z", z), ("H", h), ("U", u), ("V", v), ("INFIL_RATE", rate), ("INFIL_CAP", cap)):
+        o.set_field(name, a)
+    cn, rep, nd = o.do_timestep(0.0, 0.2)
+    out = {}
+    (hN, uN, vN), cn2, rep2, nd2 = onp.do_timestep(h, u, v, z, dx, dy, 0.0, 0.2, cn_target=0.5,
+                                                   manning=tuple(np.full(shape, x) for x in (0.03, 0.3, 0.1, 0.3)),
+                                                   infil=(rate, cap), rain_mode="physical", terms_out=out)
+    assert (cn, bool(rep), nd) == (cn2, rep2, nd2)
+    assert same(o.get_field(100 + 3 * o.nstages), hN)
+    assert same(o.get_field("INFIL_CAP"), out["infil"][1])
+    # the four classic RK stages each took up to rate * dt = 2e-4 m: more than one stage's
+    # worth is gone, and deep cells emptied their 5e-4 m capacity
+    taken = cap - o.get_field("INFIL_CAP")
+    assert taken.max() > 2e-4 and np.any(o.get_field("INFIL_CAP") == 0.0)
