@@ -458,6 +458,34 @@ def cpu_baseline(w, state, cpu_seconds, precision):
                       f"(oracle {precision}, {el:.1f} s, OpenMP {used} threads)"}
 
 
+def source_terms_cost(w, state, precision, variant, device, timesteps=20):
+    """Stage-kernel time on the spun-up catchment with and without the energy-loss and
+    infiltration terms (per-cell fx, fy, rate and a capacity read and written each stage:
+    5 more values per cell per stage)."""
+    ncells = w["nx"] * w["ny"]
+    out = {}
+    for on in (False, True):
+        s = make_solver(w, precision, device)
+        s.set_kernel_variant(variant)
+        for f in ("H", "U", "V"):
+            s.set_field(f, state[f.lower()])
+        s.set_dt(state["dt"])
+        if on:
+            for name, val in (("ELOSS_FX", 0.05), ("ELOSS_FY", 0.05), ("INFIL_RATE", 2e-6), ("INFIL_CAP", 0.05)):
+                s.set_field(name, np.full((w["ny"], w["nx"]), val))
+        r = Runner(s, t0=600.0)
+        r.run(3)
+        _, tm = r.run(timesteps, timing=True)
+        out["with" if on else "without"] = tm["stage_ms"] / max(1, tm["stage_launches"])
+        s.close()
+    bpv = 8 if precision == "f64" else 4
+    alg = (VALUES_PER_CELL_UPDATE + 4 * 5) / 4.0 * bpv * ncells
+    peak, _ = measured_peaks()
+    return {"terms": "energy loss + infiltration", "stage_ms_without": out["without"], "stage_ms_with": out["with"],
+            "extra_values_per_cell_stage": 5,
+            "roofline_frac_with": alg / (out["with"] * 1e-3) / 1e9 / peak}
+
+
 def oracle_precision(p):
     return "f64" if p == "f64" else "f32"
 
@@ -581,6 +609,8 @@ def main():
     e2e = None
     if rank == 0 and not args.no_e2e:
         e2e = measure_e2e(w, args, device, state, main_res["variant"], args.precision)
+    if rank == 0 and not args.no_extras:
+        extras["source_terms"] = source_terms_cost(w, state, args.precision, main_res["variant"], device)
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_baseline(w, state, args.cpu_seconds, oracle_precision(args.precision))
