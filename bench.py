@@ -253,7 +253,9 @@ def timed_run(w, precision, args, device, barrier, dist):
     stage_avg_s = tm["stage_ms"] * 1e-3 / max(1, solver.nstages * tm["timesteps"])
     achieved = alg_bytes_launch / stage_avg_s / 1e9
     peak, peak_kind = measured_peaks()
-    kernel = "stage_kernel" if variant < 4 else "sweep_kernel"
+    # FP32 with the batches' variant runs the batched column sweep as a batch of one
+    kernel = "stage_kernel" if variant < 4 else ("sweep_batch_kernel" if precision != "f64" and variant == 8
+                                                  else "sweep_kernel")
     traffic_pc = profile_traffic(f"{kernel}_{precision}_2048_traffic.json")
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": (traffic_pc * ncells if traffic_pc else None), "peak_kind": peak_kind,
@@ -387,8 +389,8 @@ def batched_run(device, members, precision, steps=10, per_call=5, step_s=10.0):
     final = {}
     for i, m in live:
         st = m.stats()
-        # mass balance of the whole run: V_end - (V_0 + rain in - outflow), FP64 tallies
-        closure = (st["volume"] - (v0[i] + st["rain_in"] - st["outflow"])) / st["volume"]
+        # mass balance of the whole run: V_end - (V_0 + rain in - outflow + wall flow), FP64
+        closure = (st["volume"] - (v0[i] + st["rain_in"] - st["outflow"] + st["wall_in"])) / st["volume"]
         final[i] = (m.get_field("H"), st["volume"], closure)
     b.close()
     return ({"precision": precision, "catchments": len(members), "cells": cells, "steps": steps + 1,

@@ -157,6 +157,9 @@ typedef struct {
   double volume;      /* FP64 sum of h * cell area of U_[0]                              */
   double rain_in;     /* FP64 volume added by the discharge (rain) term                  */
   double outflow;     /* FP64 volume removed by the head (outflow) assignment            */
+  double wall_in;     /* FP64 volume that entered through the mesh-edge faces (negative:
+                         left); the reference's walls pass flow through their one-sided
+                         flux branches, so volume = initial + rain_in - outflow + wall_in  */
 } sv_stats;
 
 typedef struct sv_ctx sv_ctx;
@@ -196,6 +199,10 @@ int sv_advance(sv_ctx* ctx, sv_stats* out);
 /* SaintVenantVolumeMeasure::get_volume (src/SaintVenant/Measure.hpp:137-156) plus the
  * running rain/outflow tallies; FP64. */
 int sv_get_stats(sv_ctx* ctx, sv_stats* out);
+/* restore the running counters and FP64 tallies of sv_get_stats (accepted, repeated,
+ * rain_in, outflow; volume is recomputed from the state) -- used to resume from a checkpoint
+ * of the state, dt and stats; no reference counterpart (the reference has no restart) */
+int sv_set_stats(sv_ctx* ctx, const sv_stats* stats);
 /* device time (ms) of the last sv_advance, or -1 if not recorded */
 int sv_last_advance_ms(sv_ctx* ctx, double* ms);
 
@@ -280,7 +287,7 @@ int sv_batch_size(sv_batch* batch, int* n_members, uint64_t* device_bytes);
  * counterpart in the reference. It is for callers that must not allocate after start-up: a
  * host framework that owns every device allocation through its own pool and hands the solver
  * only pre-allocated buffers, or a real-time loop in which a cudaMalloc would synchronise the
- * device. Working memory is a fixed array inside this library (about 4.9 MB, held by every
+ * device. Working memory is a fixed array inside this library (about 5.2 MB, held by every
  * GPU that loads the library until the process exits), which limits the mesh to 65536 cells
  * (256 x 256); larger meshes return SV_E_LIMIT.
  *   inputs  (device, FP64, nx*ny each): z, h, u, v = U_[0]

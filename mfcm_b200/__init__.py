@@ -136,6 +136,12 @@ class _Backend:
         self._call("get_stats", C.byref(s))
         return s.as_dict()
 
+    def set_stats(self, st):
+        """Restore the running counters and tallies (a checkpoint's); volume is recomputed."""
+        s = Stats(int(st["accepted"]), int(st["repeated"]), 0.0, float(st["rain_in"]), float(st["outflow"]),
+                  float(st.get("wall_in", 0.0)))
+        self._call("set_stats", C.byref(s))
+
 
 class SaintVenantSolver(_Backend):
     """One catchment on one GPU: SaintVenantSolver + RungeKuttaSolver behind the C-ABI.

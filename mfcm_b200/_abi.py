@@ -53,7 +53,7 @@ class Forcing(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [("accepted", C.c_uint64), ("repeated", C.c_uint64), ("volume", C.c_double),
-                ("rain_in", C.c_double), ("outflow", C.c_double)]
+                ("rain_in", C.c_double), ("outflow", C.c_double), ("wall_in", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -83,6 +83,7 @@ def declare(lib, prefix, ctx_type=C.c_void_p):
         "accept": (C.c_int, [ctx_type]),
         "advance": (C.c_int, [ctx_type, P(Stats)]),
         "get_stats": (C.c_int, [ctx_type, P(Stats)]),
+        "set_stats": (C.c_int, [ctx_type, P(Stats)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, prefix + name)

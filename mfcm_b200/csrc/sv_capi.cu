@@ -109,6 +109,7 @@ struct sv_ctx {
   virtual int accept() = 0;
   virtual int advance(sv_stats*) = 0;
   virtual int get_stats(sv_stats*) = 0;
+  virtual int set_stats(const sv_stats*) = 0;
   virtual int run_timesteps(uint64_t, int, sv_stats*, int*, sv_timing*) = 0;
   virtual int set_variant(int) = 0;
   virtual int get_variant() const = 0;
@@ -155,6 +156,12 @@ struct Solver final : public sv_ctx {
   T *q0 = nullptr, *q1 = nullptr, *pat = nullptr, *hb0 = nullptr, *hb1 = nullptr;
   T *irate = nullptr, *icap = nullptr;  // InfiltrationSourceTerm fields (.hpp:106-109)
   T *efx = nullptr, *efy = nullptr;     // EnergyLossSourceTerm fields (.hpp:199-202)
+  // FP32 with the batches' variant runs the batched column sweep as a batch of one, so a
+  // solver on its own and a batch member execute the same machine code and give the same
+  // bits (FP32 is contracted per kernel); that kernel reads its parameters from device memory
+  svk::StageParams<T>* d_sp = nullptr;  // [N] stage parameters + [1] for the autotuner
+  long long* d_ws = nullptr;            // warp starts: {0, nblk} and, for the autotuner, {0, n}
+  unsigned long long sp_version = ~0ull;
   // debug buffers (per-function parity path)
   T* dbg_slp[8] = {};
   T* dbg_face[5] = {};
@@ -566,13 +573,47 @@ struct Solver final : public sv_ctx {
     return F;
   }
 
+  bool batch_path(int v) const { return sizeof(T) == 4 && v == svk::batch_variant<T>(); }
+  bool pow2_mesh() const {
+    int e;
+    return std::frexp(mesh.dx, &e) == 0.5 && std::frexp(mesh.dy, &e) == 0.5;
+  }
+  // Device copy of the stage parameters for the batch-of-one path (outside stream capture).
+  int ensure_dev_params() {
+    if (!batch_path(variant) || sp_version == pversion) return SV_OK;
+    if (!d_sp) {
+      SV_CUDA(alloc(&d_sp, size_t(N + 1)));
+      SV_CUDA(alloc(&d_ws, size_t(4)));
+    }
+    std::vector<svk::StageParams<T>> hp(N);
+    for (int st = 0; st < N; ++st) hp[st] = stage_params(st);
+    long long ws[2] = {0, nblk};
+    SV_CUDA(cudaMemcpyAsync(d_sp, hp.data(), sizeof(svk::StageParams<T>) * N, cudaMemcpyHostToDevice, stream));
+    SV_CUDA(cudaMemcpyAsync(d_ws, ws, sizeof(ws), cudaMemcpyHostToDevice, stream));
+    SV_CUDA(cudaStreamSynchronize(stream));
+    sp_version = pversion;
+    return SV_OK;
+  }
+  cudaError_t launch_stage_kernel(const svk::StageParams<T>& P, int st) {
+    if (batch_path(variant)) return svk::launch_sweep_batch<T>(d_sp + st, d_ws, 1, nblk, pow2_mesh(), stream);
+    return svk::launch_variant<T>(P, variant, stream);
+  }
+
   // Launch the N stages of one timestep and the finalize kernel (RungeKutta.cpp:147-167).
   // ev: if non-null, 2*(N+1) events recorded around every kernel (stages, then finalize)
   int enqueue_timestep(bool auto_mode, cudaEvent_t* ev = nullptr) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    SV_CUDA(cudaStreamIsCapturing(stream, &cs));
+    if (cs == cudaStreamCaptureStatusNone) {
+      int r = ensure_dev_params();
+      if (r) return r;
+    } else if (batch_path(variant) && sp_version != pversion) {
+      return fail(SV_E_STATE, "stage parameters not on the device before capture");
+    }
     for (int st = 0; st < N; ++st) {
       svk::StageParams<T> P = stage_params(st);
       if (ev) SV_CUDA(cudaEventRecord(ev[2 * st], stream));
-      cudaError_t e = svk::launch_variant<T>(P, variant, stream);
+      cudaError_t e = launch_stage_kernel(P, st);
       if (e != cudaSuccess) return cuda_fail(e, "stage kernel");
       if (ev) SV_CUDA(cudaEventRecord(ev[2 * st + 1], stream));
     }
@@ -650,6 +691,8 @@ struct Solver final : public sv_ctx {
 
   int build_graph() {
     if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+    int r0 = ensure_dev_params();
+    if (r0) return r0;
     cudaGraph_t g;
     SV_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     for (int i = 0; i < unroll; ++i) {
@@ -696,6 +739,7 @@ struct Solver final : public sv_ctx {
       out->repeated = c.step_repeated;
       out->rain_in = c.rain_in;
       out->outflow = c.outflow;
+      out->wall_in = c.wall_in;
       int r = volume(&out->volume);
       if (r) return r;
     }
@@ -747,6 +791,7 @@ struct Solver final : public sv_ctx {
       out->repeated = c.repeated;
       out->rain_in = c.rain_in;
       out->outflow = c.outflow;
+      out->wall_in = c.wall_in;
       out->volume = c.volume;
     }
     if (c.error) return fail(SV_E_NONFINITE, "time became NaN: the control number was not finite");
@@ -799,12 +844,27 @@ struct Solver final : public sv_ctx {
     float best_ms = 1e30f;
     for (int v = 0; v < svk::kNumVariants; ++v) {
       P.nblk = svk::variant_partials(v, (long long)mesh.nx, (long long)mesh.ny);
-      cudaError_t e = svk::launch_variant<T>(P, v, stream);  // warm-up
+      // the batch variant runs as the batched kernel (see launch_stage_kernel): time that one
+      auto launch = [&]() -> cudaError_t {
+        if (!batch_path(v)) return svk::launch_variant<T>(P, v, stream);
+        return svk::launch_sweep_batch<T>(d_sp + N, d_ws + 2, 1, P.nblk, pow2_mesh(), stream);
+      };
+      if (batch_path(v)) {
+        if (!d_sp) {
+          SV_CUDA(alloc(&d_sp, size_t(N + 1)));
+          SV_CUDA(alloc(&d_ws, size_t(4)));
+        }
+        long long ws[2] = {0, P.nblk};
+        SV_CUDA(cudaMemcpyAsync(d_sp + N, &P, sizeof(P), cudaMemcpyHostToDevice, stream));
+        SV_CUDA(cudaMemcpyAsync(d_ws + 2, ws, sizeof(ws), cudaMemcpyHostToDevice, stream));
+        SV_CUDA(cudaStreamSynchronize(stream));
+      }
+      cudaError_t e = launch();  // warm-up
       if (e != cudaSuccess) return cuda_fail(e, "autotune launch");
       SV_CUDA(cudaEventRecord(ev0, stream));
       const int reps = 3;
       for (int i = 0; i < reps; ++i) {
-        e = svk::launch_variant<T>(P, v, stream);
+        e = launch();
         if (e != cudaSuccess) return cuda_fail(e, "autotune launch");
       }
       SV_CUDA(cudaEventRecord(ev1, stream));
@@ -830,6 +890,20 @@ struct Solver final : public sv_ctx {
     return SV_OK;
   }
 
+  int set_stats(const sv_stats* in) override {
+    if (!in) return fail(SV_E_ARG, "null stats");
+    Ctl c;
+    int r = read_ctl(c);
+    if (r) return r;
+    c.accepted = in->accepted;
+    c.repeated = in->repeated;
+    c.rain_in = in->rain_in;
+    c.outflow = in->outflow;
+    c.wall_in = in->wall_in;
+    SV_CUDA(cudaMemcpyAsync(ctl, &c, sizeof(Ctl), cudaMemcpyHostToDevice, stream));
+    SV_CUDA(cudaStreamSynchronize(stream));
+    return SV_OK;
+  }
   int get_stats(sv_stats* out) override {
     Ctl c;
     int r = read_ctl(c);
@@ -838,6 +912,7 @@ struct Solver final : public sv_ctx {
     out->repeated = c.repeated;
     out->rain_in = c.rain_in;
     out->outflow = c.outflow;
+    out->wall_in = c.wall_in;
     return volume(&out->volume);
   }
 };
@@ -1102,6 +1177,7 @@ struct Batch final : public sv_batch_base {
     o.repeated = q.rep[s];
     o.rain_in = q.rain[s];
     o.outflow = q.outflow[s];
+    o.wall_in = q.wall[s];
     o.volume = q.volume[s];
   }
 
@@ -1231,6 +1307,7 @@ int sv_do_timestep(sv_ctx* ctx, double t, double dt, double* cn, int* rep, doubl
 int sv_accept(sv_ctx* ctx) { SV_CHECK_CTX(ctx); return ctx->accept(); }
 int sv_advance(sv_ctx* ctx, sv_stats* out) { SV_CHECK_CTX(ctx); return ctx->advance(out); }
 int sv_get_stats(sv_ctx* ctx, sv_stats* out) { SV_CHECK_CTX(ctx); if (!out) return SV_E_ARG; return ctx->get_stats(out); }
+int sv_set_stats(sv_ctx* ctx, const sv_stats* in) { SV_CHECK_CTX(ctx); return ctx->set_stats(in); }
 int sv_run_timesteps(sv_ctx* ctx, uint64_t n, int begin, sv_stats* out, int* step_done, sv_timing* t) {
   SV_CHECK_CTX(ctx);
   return ctx->run_timesteps(n, begin, out, step_done, t);

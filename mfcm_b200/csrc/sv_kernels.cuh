@@ -31,8 +31,10 @@ struct Ctl {
   unsigned long long accepted, repeated;            // running totals
   unsigned long long step_accepted, step_repeated;  // in the current step
   double rain_in, outflow;      // running tallies over accepted timesteps
+  double wall_in;               // running tally of the flow through the mesh-edge faces
   double volume;                // volume of U_[0] after the last accepted timestep
   double pend_rain, pend_out, pend_vol;  // tallies of the last timestep, applied on accept
+  double pend_wall;
   long long budget;             // > 0: timesteps left before the loop pauses (done = 2)
 };
 
@@ -89,8 +91,8 @@ template <typename T> struct StageParams {
 };
 
 // partial layout: [0, nblk) cn max, [nblk, 2nblk) cn min, [2nblk, 3nblk) volume,
-// then rain[s] at (3 + 2s) nblk, outflow[s] at (4 + 2s) nblk.
-__host__ __device__ inline long long part_count(long long nblk, int nstages) { return (3 + 2LL * nstages) * nblk; }
+// then rain[s] at (3 + 3s) nblk, outflow[s] at (4 + 3s) nblk, wall flow[s] at (5 + 3s) nblk.
+__host__ __device__ inline long long part_count(long long nblk, int nstages) { return (3 + 3LL * nstages) * nblk; }
 
 template <typename T> __device__ __forceinline__ T ld(const T* p, long long i) { return __ldg(p + i); }
 
@@ -165,14 +167,16 @@ template <> struct MkDivX<DivF> { __device__ static DivF make(double d) { return
 
 // Per-cell dU/dt of one stage (TemporalDerivativeKernel.cpp:53-98, then the source terms
 // and boundaries in configuration order, Solver.cpp:97-113). fw/fe/fs/fn are the four face
-// fluxes; returns the rain rate added and the depth rate removed by the head assignment.
+// fluxes; returns the rain rate added, the depth rate removed by the head assignment and the
+// depth rate that entered through mesh-edge faces (the reference's walls pass flow through
+// their one-sided branches; taken before any boundary assignment).
 template <typename T, typename CC>
 __device__ __forceinline__ void cell_dudt(const StageParams<T>& P, const DevForcing& fc, const CC& c,
                                           long long g, int gx,
                                           int gy, T h, T u, T v, T dhdx, T dhdy, T dzdx, T dzdy,
                                           const FaceF<T>& fw, const FaceF<T>& fe, const FaceF<T>& fs,
                                           const FaceF<T>& fn, T& kh, T& ku, T& kv, double& rain,
-                                          double& removed, T* n_out, T* sf_out) {
+                                          double& removed, double& wall, T* n_out, T* sf_out) {
   T dhdt = c.divx(fw.h - fe.h) + c.divy(fs.h - fn.h);
   T dudt = c.divx(fw.u - fe.u) + c.divy(fs.u - fn.u);
   T dvdt = c.divx(fw.v - fe.v) + c.divy(fs.v - fn.v);
@@ -210,6 +214,11 @@ __device__ __forceinline__ void cell_dudt(const StageParams<T>& P, const DevForc
   }
   rain = 0.0;
   removed = 0.0;
+  wall = 0.0;
+  if (gx == 0) wall += double(c.divx(fw.h));
+  if (gx == P.nx - 1) wall -= double(c.divx(fe.h));
+  if (gy == 0) wall += double(c.divy(fs.h));
+  if (gy == P.ny - 1) wall -= double(c.divy(fn.h));
   // head boundary target values for this cell (NaN = not selected); a stage boundary
   // (StageBoundarySourceTerm.cpp:48-52) gives water levels, from which the bed is subtracted
   bool head_sel = false;
@@ -262,14 +271,15 @@ __device__ __forceinline__ void finish_cell(const StageParams<T>& P, const DevFo
                                             long long g, int gx, int gy, T h, T u, T v, T dhdx, T dhdy, T dzdx,
                                             T dzdy, const FaceF<T>& fw, const FaceF<T>& fe, const FaceF<T>& fs,
                                             const FaceF<T>& fn, bool first, bool last, int cur, double dt_d,
-                                            double& rain, double& removed, double& xcfl, double& xcfl_min,
-                                            double& vol) {
+                                            double& rain, double& removed, double& walls, double& xcfl,
+                                            double& xcfl_min, double& vol) {
   T kh, ku, kv;
-  double r_, o_;
-  cell_dudt<T>(P, fc, c, g, gx, gy, h, u, v, dhdx, dhdy, dzdx, dzdy, fw, fe, fs, fn, kh, ku, kv, r_, o_,
+  double r_, o_, w_;
+  cell_dudt<T>(P, fc, c, g, gx, gy, h, u, v, dhdx, dhdy, dzdx, dzdy, fw, fe, fs, fn, kh, ku, kv, r_, o_, w_,
                (T*)nullptr, (T*)nullptr);
   rain += r_;
   removed += o_;
+  walls += w_;
   if (P.mode & (M_STOREK | M_DEBUGK)) {
     P.Kout[0][g] = kh; P.Kout[1][g] = ku; P.Kout[2][g] = kv;
   }
@@ -442,7 +452,7 @@ __device__ __forceinline__ void stage_tile(const StageParams<T>& P, int bx, int 
   const int tx = tid % TX, ty = tid / TX;
   const int gx = x0 + tx, gy = y0 + ty;
   const bool valid = gx < nx && gy < ny;
-  double rain = 0.0, removed = 0.0, xcfl = 0.0, xcfl_min = 1.0 / 0.0, vol = 0.0;
+  double rain = 0.0, removed = 0.0, walls = 0.0, xcfl = 0.0, xcfl_min = 1.0 / 0.0, vol = 0.0;
   const bool last = P.mode & M_LAST;
   if (valid) {
     const long long g = (long long)gy * nx + gx;
@@ -460,7 +470,7 @@ __device__ __forceinline__ void stage_tile(const StageParams<T>& P, int bx, int 
     FaceF<T> fn{s.fyf[0][ty + 1][tx], s.fyf[1][ty + 1][tx], s.fyf[2][ty + 1][tx], s.fyf[3][ty + 1][tx]};
     const DevForcing fc = *P.fc;
     finish_cell<T>(P, fc, c, g, gx, gy, h, u, v, s.slp[0][sy][sx], s.slp[4][sy][sx], s.slp[3][sy][sx],
-                   s.slp[7][sy][sx], fw, fe, fs, fn, first, last, cur, dt_d, rain, removed, xcfl, xcfl_min, vol);
+                   s.slp[7][sy][sx], fw, fe, fs, fn, first, last, cur, dt_d, rain, removed, walls, xcfl, xcfl_min, vol);
   }
   if (last && !(P.mode & M_DEBUGK)) {
     double mx = block_max<NT>(xcfl, s.red);
@@ -475,9 +485,11 @@ __device__ __forceinline__ void stage_tile(const StageParams<T>& P, int bx, int 
   if (P.mode & M_TALLY) {
     double rs = block_sum<NT>(rain, s.red);
     double os = block_sum<NT>(removed, s.red);
+    double ws = block_sum<NT>(walls, s.red);
     if (tid == 0) {
-      P.part[(3 + 2LL * P.stage) * P.nblk + blk] = rs;
-      P.part[(4 + 2LL * P.stage) * P.nblk + blk] = os;
+      P.part[(3 + 3LL * P.stage) * P.nblk + blk] = rs;
+      P.part[(4 + 3LL * P.stage) * P.nblk + blk] = os;
+      P.part[(5 + 3LL * P.stage) * P.nblk + blk] = ws;
     }
   }
 }
@@ -643,7 +655,7 @@ __device__ __forceinline__ void sweep_strip(const StageParams<T>& P, long long g
   SlopeV<T> Sm{}, S0{};       // slopes of rows k-2, k-1
   T fyA[3] = {}, fyB[3] = {};  // (U[k-1]-U[k-2])/dy, (U[k]-U[k-1])/dy
   FaceF<T> FS{}, FN{};
-  double rain = 0.0, removed = 0.0, xcfl = 0.0, xmin = 1.0 / 0.0, vol = 0.0;
+  double rain = 0.0, removed = 0.0, walls = 0.0, xcfl = 0.0, xmin = 1.0 / 0.0, vol = 0.0;
 
   // L1 prefetch of rows ahead (addresses clamped into the mesh, like the loads)
   auto prefetch_rows = [&](int k) {
@@ -728,7 +740,7 @@ __device__ __forceinline__ void sweep_strip(const StageParams<T>& P, long long g
       if (out_lane && r < ny) {
         const long long g = (long long)r * nx + gx;
         finish_cell<T>(P, fc, c, g, gx, r, me.h, me.u, me.v, me.dhdx, me.dhdy, me.dzdx, me.dzdy, FW, FE, FS, FN,
-                       first, last, cur, dt_d, rain, removed, xcfl, xmin, vol);
+                       first, last, cur, dt_d, rain, removed, walls, xcfl, xmin, vol);
       }
     }
     FS = FN;
@@ -742,10 +754,11 @@ __device__ __forceinline__ void sweep_strip(const StageParams<T>& P, long long g
     }
   }
   if (P.mode & M_TALLY) {
-    double rs = warp_sum<T>(rain), os = warp_sum<T>(removed);
+    double rs = warp_sum<T>(rain), os = warp_sum<T>(removed), ws = warp_sum<T>(walls);
     if (lane == 0) {
-      P.part[(3 + 2LL * P.stage) * P.nblk + gw] = rs;
-      P.part[(4 + 2LL * P.stage) * P.nblk + gw] = os;
+      P.part[(3 + 3LL * P.stage) * P.nblk + gw] = rs;
+      P.part[(4 + 3LL * P.stage) * P.nblk + gw] = os;
+      P.part[(5 + 3LL * P.stage) * P.nblk + gw] = ws;
     }
   }
 }
@@ -819,6 +832,7 @@ struct StepQueue {
   DevForcing f[kMaxQueuedSteps];                             // forcing of each queued step
   unsigned long long acc[kMaxQueuedSteps], rep[kMaxQueuedSteps];   // per-step counts
   double rain[kMaxQueuedSteps], outflow[kMaxQueuedSteps], volume[kMaxQueuedSteps];  // running, at step end
+  double wall[kMaxQueuedSteps];
 };
 
 struct FinalizeParams {
@@ -877,14 +891,16 @@ template <int NT> __device__ __forceinline__ void finalize_body(const FinalizePa
   mn = red[0];
   __syncthreads();
   double vol = fixed_sum<NT>(F.part + 2 * F.nblk, F.nblk, red);
-  double rain = 0.0, outf = 0.0;
+  double rain = 0.0, outf = 0.0, wall = 0.0;
   if (F.tally) {
     for (int s = 0; s < F.nstages; ++s) {
-      double rs = fixed_sum<NT>(F.part + (3 + 2LL * s) * F.nblk, F.nblk, red);
-      double os = fixed_sum<NT>(F.part + (4 + 2LL * s) * F.nblk, F.nblk, red);
+      double rs = fixed_sum<NT>(F.part + (3 + 3LL * s) * F.nblk, F.nblk, red);
+      double os = fixed_sum<NT>(F.part + (4 + 3LL * s) * F.nblk, F.nblk, red);
+      double ws = fixed_sum<NT>(F.part + (5 + 3LL * s) * F.nblk, F.nblk, red);
       double w = F.is_float ? double(float(F.b[s] * ctl->dt)) : F.b[s] * ctl->dt;
       rain += w * rs * F.cell_area;
       outf += w * os * F.cell_area;
+      wall += w * ws * F.cell_area;
     }
   }
   if (threadIdx.x != 0) return;
@@ -913,6 +929,7 @@ template <int NT> __device__ __forceinline__ void finalize_body(const FinalizePa
   ctl->repeat = rep;
   ctl->pend_rain = rain;
   ctl->pend_out = outf;
+  ctl->pend_wall = wall;
   ctl->pend_vol = vol;
   if (!F.auto_mode) return;
   // TypedTemporalScheme::step (TemporalScheme.hpp:119-146)
@@ -921,7 +938,7 @@ template <int NT> __device__ __forceinline__ void finalize_body(const FinalizePa
     ctl->repeated++; ctl->step_repeated++;
   } else {
     ctl->accepted++; ctl->step_accepted++;
-    ctl->rain_in += rain; ctl->outflow += outf; ctl->volume = vol;
+    ctl->rain_in += rain; ctl->outflow += outf; ctl->wall_in += wall; ctl->volume = vol;
     t = t + dt;
     ctl->cur ^= 1;
   }
@@ -946,6 +963,7 @@ template <int NT> __device__ __forceinline__ void finalize_body(const FinalizePa
   q->rep[k] = ctl->step_repeated;
   q->rain[k] = ctl->rain_in;
   q->outflow[k] = ctl->outflow;
+  q->wall[k] = ctl->wall_in;
   q->volume[k] = ctl->volume;
   q->cur = ctl->cur;
   if (ctl->error) { q->status = -5; return; }
@@ -982,6 +1000,7 @@ __global__ void accept_kernel(Ctl* ctl) {
   ctl->accepted++;
   ctl->rain_in += ctl->pend_rain;
   ctl->outflow += ctl->pend_out;
+  ctl->wall_in += ctl->pend_wall;
   ctl->volume = ctl->pend_vol;
 }
 __global__ void begin_step_kernel(Ctl* ctl, int new_step, long long budget) {
@@ -1126,9 +1145,9 @@ __global__ void debug_cell_kernel(const StageParams<T> P, const DebugParams<T> D
   FaceF<T> fs{D.fh[sf_], D.fu[sf_], D.fv[sf_], D.fz[sf_]}, fn{D.fh[nf_], D.fu[nf_], D.fv[nf_], D.fz[nf_]};
   const DevForcing fc = *P.fc;
   T kh, ku, kv;
-  double rain, removed;
+  double rain, removed, wall;
   cell_dudt<T>(P, fc, c, g, gx, gy, D.h[g], D.u[g], D.v[g], D.dhdx[g], D.dhdy[g], D.dzdx[g], D.dzdy[g], fw, fe, fs,
-               fn, kh, ku, kv, rain, removed, nh + g, sf + g);
+               fn, kh, ku, kv, rain, removed, wall, nh + g, sf + g);
   P.Kout[0][g] = kh; P.Kout[1][g] = ku; P.Kout[2][g] = kv;
 }
 

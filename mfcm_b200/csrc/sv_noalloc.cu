@@ -27,7 +27,7 @@ namespace {
 
 constexpr long long kMaxCells = 65536;  // 256 x 256
 // partial-sum slots of the 32 x 8 tiled stage kernel: at most 8192 CTAs for any mesh of at
-// most kMaxCells cells (reached by a 1-cell-wide strip), times 3 + 2 * 4 stages
+// most kMaxCells cells (reached by a 1-cell-wide strip), times 3 + 3 * 4 stages
 constexpr long long kMaxBlocks = 8192;
 constexpr int kVariant = 1;  // tiled stage kernel, 32 x 8 cells per CTA
 constexpr size_t kFieldBytes = size_t(kMaxCells) * sizeof(double);
@@ -35,7 +35,7 @@ constexpr size_t kYOffset = 0;                           // Y[2][3]: stage input
 constexpr size_t kZxOffset = kYOffset + 6 * kFieldBytes;  // bed slopes dz/dx, dz/dy
 constexpr size_t kZyOffset = kZxOffset + kFieldBytes;
 constexpr size_t kPartOffset = kZyOffset + kFieldBytes;
-constexpr size_t kPartBytes = size_t(3 + 2 * 4) * size_t(kMaxBlocks) * sizeof(double);
+constexpr size_t kPartBytes = size_t(3 + 3 * 4) * size_t(kMaxBlocks) * sizeof(double);
 constexpr size_t kCtlOffset = kPartOffset + kPartBytes;
 constexpr size_t kFcOffset = kCtlOffset + 256;
 constexpr size_t kScratchBytes = kFcOffset + 256;

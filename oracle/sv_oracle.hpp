@@ -251,7 +251,7 @@ struct Forcing {
 
 struct Stats {
   uint64_t accepted = 0, repeated = 0;
-  double volume = 0, rain_in = 0, outflow = 0;
+  double volume = 0, rain_in = 0, outflow = 0, wall_in = 0;
 };
 
 // Fixed-order compensated (Neumaier) sum: deterministic and accurate to ~1 ulp of the
@@ -285,6 +285,7 @@ class SolverBase {
   virtual void step(Stats* st) = 0;
   virtual double volume() const = 0;
   virtual Stats stats() const = 0;
+  virtual void set_stats(const Stats& s) = 0;
   virtual size_t state_count() const = 0;
   virtual void set_track_tallies(bool on) = 0;
 };
@@ -312,7 +313,7 @@ class Solver final : public SolverBase {
   Stats st_;
   // tallies of the last evaluated stages, per state_no: sum over cells of the rain term
   // and of the head-boundary removal (k before head assignment minus k after)
-  std::vector<double> rain_sum_, out_sum_;
+  std::vector<double> rain_sum_, out_sum_, wall_sum_;
   bool track_tallies = true;  // off for the timed CPU baseline (the reference keeps no tallies)
 
   Solver(const Mesh& mesh, const Params& prm) : m(mesh), p(prm), tab(named_tableau(prm.rk_method)) {
@@ -331,7 +332,7 @@ class Solver final : public SolverBase {
     pattern.assign(n, T(0));
     irate.assign(n, T(0)); icap.assign(n, T(0)); efx.assign(n, T(0)); efy.assign(n, T(0));
     dt_ = TT(p.initial_dt);
-    rain_sum_.assign(N, 0.0); out_sum_.assign(N, 0.0);
+    rain_sum_.assign(N, 0.0); out_sum_.assign(N, 0.0); wall_sum_.assign(N, 0.0);
     update_constants();
   }
 
@@ -394,6 +395,10 @@ class Solver final : public SolverBase {
   void set_dt(double dt) override { dt_ = TT(dt); }
   double get_dt() const override { return double(dt_); }
   Stats stats() const override { Stats s = st_; s.volume = volume(); return s; }
+  void set_stats(const Stats& s) override {
+    st_.accepted = s.accepted; st_.repeated = s.repeated; st_.rain_in = s.rain_in; st_.outflow = s.outflow;
+    st_.wall_in = s.wall_in;
+  }
 
   // start_new_step for the discharge and head boundaries
   // (DischargeBoundarySourceTerm.hpp:114-146, HeadBoundarySourceTerm.hpp:114-146): clear,
@@ -722,7 +727,19 @@ class Solver final : public SolverBase {
       else { run_discharge(); run_head(); }
       return;
     }
-    std::vector<double> rain(n, 0.0), removed(n, 0.0);
+    std::vector<double> rain(n, 0.0), removed(n, 0.0), wall(n, 0.0);
+    // flow through the mesh-edge faces (before any boundary assignment)
+#pragma omp parallel for schedule(static)
+    for (size_t c = 0; c < n; ++c) {
+      auto f = m.adjacent_faces(c);
+      size_t x = c % m.nx, y = c / m.nx;
+      double w = 0.0;
+      if (x == 0) w += double(T(fh[f.w] / f.dx));
+      if (x == m.nx - 1) w -= double(T(fh[f.e] / f.dx));
+      if (y == 0) w += double(T(fh[f.s] / f.dy));
+      if (y == m.ny - 1) w -= double(T(fh[f.n] / f.dy));
+      wall[c] = w;
+    }
     auto run_discharge = [&]() {
 #pragma omp parallel for schedule(static)
       for (size_t c = 0; c < n; ++c) rain[c] = double(discharge_cell(c, S, D, double(timestep), double(time_now), L));
@@ -738,6 +755,7 @@ class Solver final : public SolverBase {
     else { run_discharge(); run_head(); }
     rain_sum_[state_no] = neumaier_sum(rain.data(), n);
     out_sum_[state_no] = neumaier_sum(removed.data(), n);
+    wall_sum_[state_no] = neumaier_sum(wall.data(), n);
   }
 
   // RungeKuttaSolver::update_y (src/TemporalScheme/RungeKutta.hpp:371-405)
@@ -831,6 +849,7 @@ class Solver final : public SolverBase {
       double w = double(T(tab.b(s + 1) * dt));
       st_.rain_in += w * rain_sum_[s] * area;
       st_.outflow += w * out_sum_[s] * area;
+      st_.wall_in += w * wall_sum_[s] * area;
     }
   }
 

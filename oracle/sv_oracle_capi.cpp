@@ -94,14 +94,21 @@ int svo_advance(void* h, sv_stats* out) {
   static_cast<svo::SolverBase*>(h)->step(&st);
   if (out) {
     out->accepted = st.accepted; out->repeated = st.repeated; out->volume = st.volume;
-    out->rain_in = st.rain_in; out->outflow = st.outflow;
+    out->rain_in = st.rain_in; out->outflow = st.outflow; out->wall_in = st.wall_in;
   }
   return 0;
 }
 int svo_get_stats(void* h, sv_stats* out) {
   svo::Stats st = static_cast<svo::SolverBase*>(h)->stats();
   out->accepted = st.accepted; out->repeated = st.repeated; out->volume = st.volume;
-  out->rain_in = st.rain_in; out->outflow = st.outflow;
+  out->rain_in = st.rain_in; out->outflow = st.outflow; out->wall_in = st.wall_in;
+  return 0;
+}
+int svo_set_stats(void* h, const sv_stats* in) {
+  svo::Stats st{};
+  st.accepted = in->accepted; st.repeated = in->repeated; st.rain_in = in->rain_in; st.outflow = in->outflow;
+  st.wall_in = in->wall_in;
+  static_cast<svo::SolverBase*>(h)->set_stats(st);
   return 0;
 }
 int svo_set_threads(int n) {

@@ -62,6 +62,7 @@ class OracleSolver(_Backend):
         self.dx = float(dx)
         self.dy = float(dx if dy is None else dy)
         self.ncells = self.nx * self.ny
+        self.precision = precision
         self.nfaces = (self.nx + 1) * self.ny + (self.ny + 1) * self.nx
         self.step_duration = float(step_duration)
         self.nstages = RK_STAGES[RK_METHODS.index(rk_method)]

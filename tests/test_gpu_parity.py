@@ -168,3 +168,29 @@ def test_autotune_keeps_state_and_bits():
     g.advance(); o.advance()
     for f in ("H", "U", "V"):
         assert_same(g.get_field(f), o.get_field(f), f)
+
+
+@pytest.mark.parametrize("precision,tol", [("f64", 1e-12), ("f32", 1e-6), ("f32_datum64", 1e-6)])
+def test_mass_balance_closure_and_tallies(precision, tol):
+    """The FP64 tallies (rain in, outflow, flow through the walls) close the volume balance
+    to rounding in every precision, and in FP64 match the oracle's."""
+    nx, ny, dx = 45, 30, 4.0
+    z = synth.plane_with_gaussians(nx, ny, dx, seed=3)
+    res = []
+    for cls in (SaintVenantSolver, OracleSolver):
+        b = cls(nx, ny, dx, cn_target=0.5, step_duration=20.0, rain_mode="physical",
+                **({"precision": precision} if cls is SaintVenantSolver else {}))
+        setup(b, z, np.full((ny, nx), 1e-3), np.zeros((ny, nx)), np.zeros((ny, nx)))
+        v0 = b.stats()["volume"]
+        solve(b, 0.0, 60.0, rain=rain_series(50 * synth.MM_PER_H, stop=1e4), head=0.0, head_edges=EDGE_XMAX)
+        s = b.stats()
+        res.append((s, v0))
+        if cls is SaintVenantSolver and precision != "f64":
+            break
+    s, v0 = res[0]
+    closure = s["volume"] - (v0 + s["rain_in"] - s["outflow"] + s["wall_in"])
+    assert abs(closure) <= tol * s["volume"], closure
+    if precision == "f64":
+        so = res[1][0]
+        for k in ("rain_in", "outflow", "wall_in"):
+            assert abs(s[k] - so[k]) <= 1e-12 * max(abs(so[k]), 1e-300), (k, s[k], so[k])

@@ -166,3 +166,21 @@ def test_num_steps():
     assert num_steps(0.0, 3600.0, 60.0) == 60
     assert num_steps(0.0, 3600.0000001, 60.0) == 60
     assert num_steps(0.0, 3601.0, 60.0) == 61
+
+
+def test_mass_balance_closes_with_the_wall_tally():
+    """Volume = initial + rain in - outflow + wall flow, to rounding: the wall tally counts
+    what the reference's y-walls let through (closed box, no outflow boundary) and what
+    crosses the edge faces of head-boundary strips."""
+    nx, ny, dx = 30, 24, 2.0
+    for edges in (0, EDGE_XMAX):
+        o = OracleSolver(nx, ny, dx, cn_target=0.5, step_duration=10.0, rain_mode="physical")
+        setup(o, synth.plane_with_gaussians(nx, ny, dx, seed=8), np.full((ny, nx), 1e-3), np.zeros((ny, nx)),
+              np.zeros((ny, nx)))
+        v0 = o.stats()["volume"]
+        solve(o, 0.0, 60.0, rain=rain_series(40 * synth.MM_PER_H, stop=1e4), head=0.0 if edges else None,
+              head_edges=edges)
+        s = o.stats()
+        assert s["wall_in"] < 0.0                     # water left through the walls
+        closure = s["volume"] - (v0 + s["rain_in"] - s["outflow"] + s["wall_in"])
+        assert abs(closure) <= 1e-12 * s["volume"], closure
