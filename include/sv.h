@@ -105,6 +105,9 @@ typedef struct {
                                    stage evaluation as in InfiltrationSourceTerm.cpp:61      */
 #define SV_FIELD_ELOSS_FX 15    /* energy-loss coefficient fx/m (EnergyLossSourceTerm.hpp:199)*/
 #define SV_FIELD_ELOSS_FY 16    /* energy-loss coefficient fy/m                              */
+#define SV_FIELD_H_COMP 17      /* FP32 solvers: compensation carried by the depth update
+                                   (part of the state for a bit-exact restart; zeroed
+                                   whenever SV_FIELD_H is set)                              */
 #define SV_FIELD_DHDT 20        /* dUdt_[0] of the last sv_eval_dudt(0, ...)              */
 #define SV_FIELD_DUDT 21
 #define SV_FIELD_DVDT 22
@@ -224,7 +227,7 @@ int sv_run_timesteps(sv_ctx* ctx, uint64_t max_timesteps, int begin, sv_stats* o
  * 0-3 tiled shared-memory kernel (32x8, 32x8 at 3 CTAs/SM, 32x4 at 4 CTAs/SM, 64x4 at 3
  * CTAs/SM), 4-10 column-sweep kernel (16/32/64 rows per warp, then 32 rows capped for 3, 4,
  * 5 and 6 CTAs/SM). Every variant computes bit-identical FP64 results; FP32 results are
- * reproducible per variant. */
+ * reproducible per variant. SV_F32_DATUM64 solvers take the column-sweep variants only. */
 int sv_set_kernel_variant(sv_ctx* ctx, int variant);
 int sv_get_kernel_variant(sv_ctx* ctx, int* variant);
 /* Autotune: times every variant's stage kernel on the current state and keeps the fastest;

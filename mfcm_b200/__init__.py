@@ -163,6 +163,7 @@ class SaintVenantSolver(_Backend):
         self.nfaces = (self.nx + 1) * self.ny + (self.ny + 1) * self.nx
         self.step_duration = float(step_duration)
         self.precision = precision
+        self.depth_compensation = precision != "f64"  # FP32 depth updates carry a compensation
         self.rk_method = rk_method
         self.nstages = RK_STAGES[RK_METHODS.index(rk_method)]
         m = MeshDesc(self.nx, self.ny, self.dx, self.dy, 0.0, 0.0)

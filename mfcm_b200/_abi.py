@@ -23,7 +23,7 @@ RK_STAGES = [1, 2, 2, 2, 3, 3, 3, 3, 3, 4, 4, 4]
 
 FIELD = dict(
     Z=0, H=1, U=2, V=3, N_SHALLOW=4, N_DEEP=5, D_SHALLOW=6, D_DEEP=7, QBDY0=8, QBDY1=9,
-    HBDY0=10, HBDY1=11, RAIN_PATTERN=12, INFIL_RATE=13, INFIL_CAP=14, ELOSS_FX=15, ELOSS_FY=16, DHDT=20, DUDT=21, DVDT=22, DHDX=23, DUDX=24, DVDX=25,
+    HBDY0=10, HBDY1=11, RAIN_PATTERN=12, INFIL_RATE=13, INFIL_CAP=14, ELOSS_FX=15, ELOSS_FY=16, H_COMP=17, DHDT=20, DUDT=21, DVDT=22, DHDX=23, DUDX=24, DVDX=25,
     DHDY=26, DUDY=27, DVDY=28, DZDX=29, DZDY=30, FLUX_H=40, FLUX_U=41, FLUX_V=42, FLUX_Z=43,
     FLUX_BRANCH=44, STATE_BASE=100, K_BASE=200,
 )

@@ -156,6 +156,7 @@ struct Solver final : public sv_ctx {
   T *q0 = nullptr, *q1 = nullptr, *pat = nullptr, *hb0 = nullptr, *hb1 = nullptr;
   T *irate = nullptr, *icap = nullptr;  // InfiltrationSourceTerm fields (.hpp:106-109)
   T *efx = nullptr, *efy = nullptr;     // EnergyLossSourceTerm fields (.hpp:199-202)
+  T* hcomp[2] = {};                     // FP32: compensation of the depth update, per state parity
   // FP32 with the batches' variant runs the batched column sweep as a batch of one, so a
   // solver on its own and a batch member execute the same machine code and give the same
   // bits (FP32 is contracted per kernel); that kernel reads its parameters from device memory
@@ -240,6 +241,10 @@ struct Solver final : public sv_ctx {
     SV_CUDA(alloc_cells(&z));
     SV_CUDA(alloc_cells(&zx));
     SV_CUDA(alloc_cells(&zy));
+    if (sizeof(T) == 4) {  // zero compensation: a new state carries none
+      SV_CUDA(alloc_cells(&hcomp[0]));
+      SV_CUDA(alloc_cells(&hcomp[1]));
+    }
     datum = (p->precision == SV_F32_DATUM64);
     if (datum) {
       dtiles_x = int((m->nx + svk::kDatumTX - 1) / svk::kDatumTX);
@@ -285,6 +290,7 @@ struct Solver final : public sv_ctx {
       case SV_FIELD_INFIL_CAP: lazy = true; return &icap;
       case SV_FIELD_ELOSS_FX: lazy = true; return &efx;
       case SV_FIELD_ELOSS_FY: lazy = true; return &efy;
+      case SV_FIELD_H_COMP: return hcomp[cur] ? &hcomp[cur] : nullptr;
     }
     return nullptr;
   }
@@ -326,6 +332,11 @@ struct Solver final : public sv_ctx {
     }
     if (id == SV_FIELD_Z && datum) return set_bed_with_datum(host, n);
     int r = upload(*slot, host, n);
+    if (r == SV_OK && id == SV_FIELD_H && hcomp[0]) {  // a new depth field carries no compensation
+      SV_CUDA(cudaMemsetAsync(hcomp[0], 0, size_t(ncells) * sizeof(T), stream));
+      SV_CUDA(cudaMemsetAsync(hcomp[1], 0, size_t(ncells) * sizeof(T), stream));
+      SV_CUDA(cudaStreamSynchronize(stream));
+    }
     if (r == SV_OK && id == SV_FIELD_Z) {
       cudaError_t e = svk::launch_bed_slopes<T>(z, int(mesh.nx), int(mesh.ny), mesh.dx, mesh.dy, zx, zy, stream);
       if (e != cudaSuccess) return cuda_fail(e, "bed slopes");
@@ -520,6 +531,8 @@ struct Solver final : public sv_ctx {
     P.efx = (efx && efy) ? efx : nullptr;
     P.efy = (efx && efy) ? efy : nullptr;
     P.eloss_first = (prm.flags & SV_FLAG_ELOSS_FIRST) ? 1 : 0;
+    P.hc[0] = hcomp[0];
+    P.hc[1] = hcomp[1];
     P.manning = prm.manning; P.rain_mode = prm.rain_mode; P.head_first = prm.head_first;
     P.nstages = N;
     P.ctl = ctl;
@@ -800,6 +813,8 @@ struct Solver final : public sv_ctx {
 
   int set_variant(int v) override {
     if (v < 0 || v >= svk::kNumVariants) return fail(SV_E_ARG, "unknown kernel variant");
+    // with tile datums only the column sweep evaluates each face in one frame (face_frame)
+    if (datum && !svk::variant_is_sweep(v)) return fail(SV_E_ARG, "tile datums need a column-sweep variant (4-10)");
     variant = v;
     nblk = svk::variant_partials(variant, (long long)mesh.nx, (long long)mesh.ny);
     graph_dirty = true; ++pversion;
@@ -843,6 +858,7 @@ struct Solver final : public sv_ctx {
     int best = variant;
     float best_ms = 1e30f;
     for (int v = 0; v < svk::kNumVariants; ++v) {
+      if (datum && !svk::variant_is_sweep(v)) continue;
       P.nblk = svk::variant_partials(v, (long long)mesh.nx, (long long)mesh.ny);
       // the batch variant runs as the batched kernel (see launch_stage_kernel): time that one
       auto launch = [&]() -> cudaError_t {

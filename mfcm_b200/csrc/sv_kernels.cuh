@@ -79,6 +79,7 @@ template <typename T> struct StageParams {
   const T* hb0p; const T* hb1p;
   const T* irate; T* icap;   // infiltration rate (m/s) and remaining capacity (m), or nullptr
   const T* efx; const T* efy;  // energy-loss coefficients fx/m, fy/m, or nullptr
+  T* hc[2];              // FP32: per-cell compensation of the depth update (state parity), or nullptr
   int manning, rain_mode, head_first;
   int eloss_first;       // energy loss applied before roughness (configuration order)
   int stage, nstages, mode;
@@ -102,6 +103,16 @@ constexpr int kDatumTX = 32, kDatumTY = 8;
 __host__ __device__ inline long long datum_tile(int gx, int gy, int dtiles_x) {
   return (long long)(gy / kDatumTY) * dtiles_x + gx / kDatumTX;
 }
+// FP32 with tile datums: the beds of a face's two cells, (ax, ay) below or left of (bx, by),
+// in the frame of the lower cell's datum tile: b's offset moved by the exact FP64 datum
+// difference and rounded once, a's unchanged.
+template <typename T>
+__device__ __forceinline__ void face_frame(const StageParams<T>& P, CellV<T>& a, CellV<T>& b, int ax, int ay, int bx,
+                                           int by) {
+  const long long ta = datum_tile(ax, ay, P.dtiles_x), tb = datum_tile(bx, by, P.dtiles_x);
+  if (ta != tb) b.z = T(double(b.z) + (P.zdat[tb] - P.zdat[ta]));
+}
+
 // Bed of cell (gx, gy) in the frame of datum tile `ref`: the stored value itself, or, for a
 // cell of another datum tile, its offset moved by the FP64 datum difference and rounded once.
 template <typename T>
@@ -295,11 +306,16 @@ __device__ __forceinline__ void finish_cell(const StageParams<T>& P, const DevFo
     // k_j*0 (j < s) can only contribute a NaN, which happens exactly when some earlier
     // k_j is not finite, i.e. when acc is not finite while U0 is.
     const T cB = T(P.b[st] * dt_d);
+    // FP32 (hc set): the accumulator holds the increment sum_s k_s cB_s, added to U0 once at
+    // the last stage; the depth takes it with a per-cell compensation carried across
+    // timesteps. Rounding a small, nearly uniform increment (steady rain) onto the depth at
+    // every stage otherwise biases the FP32 volume by ~1e-4 over thousands of timesteps.
+    const bool incr = sizeof(T) == 4 && P.hc[0] != nullptr;
     T u0v[3], accv[3];
 #pragma unroll
     for (int f = 0; f < 3; ++f) {
       u0v[f] = first ? (f == 0 ? h : (f == 1 ? u : v)) : ld(U0[f], g);
-      accv[f] = first ? u0v[f] : ld(A[f], g);
+      accv[f] = first ? (incr ? T(0) : u0v[f]) : ld(A[f], g);
     }
     if (!last) {
       const T cA = T(P.a_next[st] * dt_d);
@@ -310,10 +326,30 @@ __device__ __forceinline__ void finish_cell(const StageParams<T>& P, const DevFo
         P.Yout[f][g] = y;
       }
     }
+    if (!incr) {
 #pragma unroll
-    for (int f = 0; f < 3; ++f) {
-      out[f] = accv[f] + k[f] * cB;
-      A[f][g] = out[f];
+      for (int f = 0; f < 3; ++f) {
+        out[f] = accv[f] + k[f] * cB;
+        A[f][g] = out[f];
+      }
+    } else {
+#pragma unroll
+      for (int f = 0; f < 3; ++f) {
+        const T d = accv[f] + k[f] * cB;  // increment sum so far
+        if (!last) {
+          A[f][g] = d;
+          out[f] = d;
+        } else if (f == 0) {  // U_N.h = U0.h + d with the carried compensation (Neumaier)
+          const T y = d + ld(P.hc[cur], g);
+          const T t = u0v[0] + y;
+          P.hc[cur ^ 1][g] = (sfabs(u0v[0]) >= sfabs(y)) ? (u0v[0] - t) + y : (y - t) + u0v[0];
+          out[0] = t;
+          A[0][g] = t;
+        } else {
+          out[f] = u0v[f] + d;
+          A[f][g] = out[f];
+        }
+      }
     }
   } else {
     // general tableau: Y_{s+1} = ((U0 + k_0 c_0) + k_1 c_1) + ... with stored k_j
@@ -640,13 +676,16 @@ __device__ __forceinline__ void sweep_strip(const StageParams<T>& P, long long g
   c.manning = P.manning; c.rain_mode = P.rain_mode; c.head_first = P.head_first;
   const DevForcing fc = *P.fc;
 
-  const long long zref = P.zdat ? datum_tile(min(tile_x * kSweepOut, nx - 1), y0, P.dtiles_x) : 0;
+  // FP32 with tile datums: the window keeps each cell's raw bed offset; a face whose two
+  // cells lie in different datum tiles is evaluated in its lower cell's frame (face_frame),
+  // the same whichever strip computes it, so the flux out of one cell is the flux into the
+  // other and the volume is conserved across strip boundaries
   auto load_row = [&](int gy) {
     const int r = min(max(gy, 0), ny - 1);
     const long long g = (long long)r * nx + gxc;
     RowV<T> v;
     v.h = ld(Yh, g); v.u = ld(Yu, g); v.v = ld(Yv, g);
-    v.z = load_bed(P.z, P.zdat, P.dtiles_x, g, gxc, r, zref);
+    v.z = ld(P.z, g);
     v.zx = ld(P.zx, g); v.zy = ld(P.zy, g);
     return v;
   };
@@ -723,7 +762,13 @@ __device__ __forceinline__ void sweep_strip(const StageParams<T>& P, long long g
       if (fy <= ny) {
         const int edge = fy == 0 ? -1 : (fy == ny ? 1 : 0);
         const CellV<T> lo = mkcell(Rm, Sm), hi = mkcell(R0, S0);
-        face_flux<T, 1>(edge == -1 ? hi : lo, edge == 1 ? lo : hi, edge, hdy, divy, FN);
+        if (P.zdat && edge == 0) {
+          CellV<T> lo2 = lo, hi2 = hi;
+          face_frame<T>(P, lo2, hi2, gx, fy - 1, gx, fy);
+          face_flux<T, 1>(lo2, hi2, edge, hdy, divy, FN);
+        } else {
+          face_flux<T, 1>(edge == -1 ? hi : lo, edge == 1 ? lo : hi, edge, hdy, divy, FN);
+        }
       }
     }
     // output row k-2
@@ -734,7 +779,13 @@ __device__ __forceinline__ void sweep_strip(const StageParams<T>& P, long long g
       FaceF<T> FW{T(0), T(0), T(0), T(0)};
       if (wface_lane && r < ny) {
         const int edge = gx == 0 ? -1 : (gx == nx ? 1 : 0);
-        face_flux<T, 0>(edge == -1 ? me : lf, edge == 1 ? lf : me, edge, hdx, divx, FW);
+        if (P.zdat && edge == 0) {
+          CellV<T> lf2 = lf, me2 = me;
+          face_frame<T>(P, lf2, me2, gx - 1, r, gx, r);
+          face_flux<T, 0>(lf2, me2, edge, hdx, divx, FW);
+        } else {
+          face_flux<T, 0>(edge == -1 ? me : lf, edge == 1 ? lf : me, edge, hdx, divx, FW);
+        }
       }
       const FaceF<T> FE{dn1(FW.h), dn1(FW.u), dn1(FW.v), dn1(FW.z)};
       if (out_lane && r < ny) {

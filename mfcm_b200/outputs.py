@@ -11,8 +11,9 @@
 - Measures (src/SaintVenant/Measure.hpp:57-177): the volume of the wetted domain and the depth
   at the cell nearest a location, one point per update, written as a time series CSV with
   columns "ID" (the time) and the measure's name.
-- Checkpoints: the state h, u, v (and the infiltration capacity when that term is active) as
-  one raw binary block in the solver's value type, followed by a JSON trailer with the
+- Checkpoints: the state h, u, v (with the infiltration capacity when that term is active,
+  and the FP32 solvers' depth-update compensation) as one raw binary block in the solver's
+  value type, followed by a JSON trailer with the
   timestep, the running counters and tallies and the mesh. Restoring one into a solver of
   the same shape and precision continues the solve bit for bit. The reference has no restart.
 
@@ -30,7 +31,7 @@ import numpy as np
 from . import FIELD
 
 _NAMES = {"h": "H", "u": "U", "v": "V", "z_bed": "Z", "IR": "INFIL_RATE", "IC": "INFIL_CAP",
-          "fdx": "ELOSS_FX", "fdy": "ELOSS_FY"}
+          "fdx": "ELOSS_FX", "fdy": "ELOSS_FY", "h_comp": "H_COMP"}
 
 
 def fmt_value(x):
@@ -170,7 +171,9 @@ def save_checkpoint(solver, path, t=None, infiltration=False):
     binary block in the solver's value type, then a JSON trailer: dt, the running counters and
     tallies, the mesh, the precision and the simulated time `t`."""
     dtype = np.float64 if getattr(solver, "precision", "f64") == "f64" else np.float32
-    names = ["h", "u", "v"] + (["IC"] if infiltration else [])
+    # FP32 solvers carry a compensation of the depth update: part of the state
+    comp = getattr(solver, "depth_compensation", False)
+    names = ["h", "u", "v"] + (["IC"] if infiltration else []) + (["h_comp"] if comp else [])
     block = raw_binary_bytes([solver_field(solver, n) for n in names], dtype)
     meta = {"fields": names, "dt": solver.get_dt(), "stats": solver.stats(), "t": t,
             "nx": solver.nx, "ny": solver.ny, "dx": solver.dx, "dy": solver.dy,
@@ -194,7 +197,7 @@ def load_checkpoint(solver, path):
     if meta["precision"] != getattr(solver, "precision", "f64"):
         raise ValueError("checkpoint precision does not match the solver")
     shape = (solver.ny, solver.nx)
-    for k, name in enumerate(meta["fields"]):
+    for k, name in enumerate(meta["fields"]):  # the depth first: setting it clears the compensation
         solver.set_field(_NAMES[name], arr[:, k].astype(np.float64).reshape(shape))
     solver.set_dt(meta["dt"])
     solver.set_stats(meta["stats"])
