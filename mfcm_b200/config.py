@@ -1,0 +1,580 @@
+"""Reads the reference's `.mf` configuration decks and drives a solve from one.
+
+The reader follows the reference's parser (src/Config/mf_parser/mf_parser_read.hpp:207-408):
+
+- a line is `key words == data`: the key is the words before `==`, joined by single
+  spaces, and the data is the rest of the line, or a quoted string with escapes and `\\`
+  continuations;
+- a line holding `{` opens the children of the last key, and `}` closes them;
+- `!` starts a comment, and `#include "file"` reads another file, relative to this one;
+- repeated keys are kept in order, as in a Boost property tree.
+
+On top of the tree sit the parts of the schema that drive this solver:
+
+- the mesh (Cartesian2DMesh.cpp:30-40);
+- the scheme and its time parameters, with the time parser's units, hours by default
+  (TimeParameters.cpp:23-38, TimeParser.cpp:20-104);
+- fields built by `set` / `add` / `multiply` of constant or sloped values within id-list
+  selections (FieldGenerator.cpp:100-178, MeshSelection.cpp:146-193);
+- time series, inline or CSV (TimeSeries.cpp:179-296);
+- the source terms: Manning roughness, infiltration, energy loss (SourceTerm.cpp:32-50);
+- the boundaries: discharge, head, stage, each a list of constant or time-series entries on
+  cell selections (DischargeBoundarySourceTerm.hpp:114-146 and siblings).
+
+Raster fields, WKT geometry selections, formatted (calendar) times, eddy viscosity, outputs
+and measures are not read: a deck that uses them raises ConfigError naming the feature.
+"""
+import math
+import os
+import re
+
+import numpy as np
+
+from . import (TimeSeries, Forcing, num_steps, RAIN_NONE, RAIN_UNIFORM, RAIN_FIELDS, HEAD_NONE, HEAD_FIELDS,
+               STAGE_FIELDS)
+
+
+class ConfigError(ValueError):
+    pass
+
+
+# ------------------------------------------------------------------------------------ tree
+class Node:
+    """A property-tree node: a value and an ordered list of (key, child) pairs."""
+
+    def __init__(self, value=""):
+        self.value = value
+        self.children = []
+
+    def add(self, key):
+        n = Node()
+        self.children.append((key, n))
+        return n
+
+    def equal_range(self, key):
+        return [n for k, n in self.children if k == key]
+
+    def child(self, key):
+        r = self.equal_range(key)
+        return r[0] if r else None
+
+    def get(self, path, default=None):
+        """Value at a dotted path (ptree.get); `default` when absent, ConfigError if required."""
+        n = self
+        for part in path.split("."):
+            n = n.child(part)
+            if n is None:
+                if default is None:
+                    raise ConfigError(f"missing configuration key {path!r}")
+                return default
+        return n.value
+
+    def __iter__(self):
+        return iter(self.children)
+
+
+_ESCAPES = {"0": "\0", "a": "\a", "b": "\b", "f": "\f", "n": "\n", "r": "\r", "t": "\t", "v": "\v",
+            '"': '"', "'": "'", "\\": "\\"}
+
+
+def _expand(s):
+    out, i = [], 0
+    while i < len(s):
+        c = s[i]
+        if c == "\\":
+            i += 1
+            if i >= len(s) or s[i] not in _ESCAPES:
+                raise ConfigError("unknown escape sequence")
+            out.append(_ESCAPES[s[i]])
+        else:
+            out.append(c)
+        i += 1
+    return "".join(out)
+
+
+def _isspace(c):
+    return ord(c) < 128 and c.isspace()
+
+
+class _Line:
+    def __init__(self, text):
+        self.t = text
+        self.i = 0
+
+    def skip(self):
+        while self.i < len(self.t) and _isspace(self.t[self.i]):
+            self.i += 1
+
+    def peek(self):
+        return self.t[self.i] if self.i < len(self.t) else "\0"
+
+    def word(self):
+        self.skip()
+        s = self.i
+        while self.i < len(self.t) and not _isspace(self.t[self.i]) and self.t[self.i] != "!":
+            self.i += 1
+        return _expand(self.t[s:self.i])
+
+    def rest(self):
+        self.skip()
+        s = self.i
+        while self.i < len(self.t) and self.t[self.i] != "!":
+            self.i += 1
+        e = self.i
+        while e > s and _isspace(self.t[e - 1]):
+            e -= 1
+        return _expand(self.t[s:e])
+
+    def string(self, may_continue=True):
+        """A quoted string; returns (text, continued on the next line?). Keys and include names
+        may not continue."""
+        self.skip()
+        if self.peek() != '"':
+            raise ConfigError('expected "')
+        self.i += 1
+        s, esc = self.i, False
+        while self.i < len(self.t) and (esc or self.t[self.i] != '"'):
+            esc = (not esc and self.t[self.i] == "\\")
+            self.i += 1
+        if self.i >= len(self.t):
+            raise ConfigError("unexpected end of line")
+        text = _expand(self.t[s:self.i])
+        self.i += 1
+        self.skip()
+        if self.peek() == "\\":
+            if not may_continue:
+                raise ConfigError("unexpected \\")
+            self.i += 1
+            self.skip()
+            if self.peek() in ("\0", "!"):
+                return text, True
+            raise ConfigError("expected end of line after \\")
+        return text, False
+
+    def key(self):
+        self.skip()
+        if self.peek() == '"':  # a quoted key is followed by the data itself, with no ==
+            return self.string(False)[0]
+        words = []
+        w = self.word()
+        while w and w != "==":
+            words.append(w)
+            w = self.word()
+        return " ".join(words)
+
+
+def read_mf(source, filename="<string>", _depth=0, _root=None):
+    """Parse `.mf` text (or a path when `source` names an existing file) into a Node tree."""
+    if _root is None and os.path.exists(str(source)) and "\n" not in str(source):
+        filename = str(source)
+        source = open(source).read()
+    root = _root if _root is not None else Node()
+    stack = [root]
+    last = None
+    state = "key"
+    for line_no, raw in enumerate(source.split("\n"), 1):
+        ln = _Line(raw)
+        try:
+            ln.skip()
+            if ln.peek() == "#":
+                ln.i += 1
+                directive = ln.word()
+                if directive != "include":
+                    raise ConfigError("unknown directive")
+                if _depth > 100:
+                    raise ConfigError("include depth too large, probably recursive include")
+                name, _ = ln.string(False)
+                path = name if os.path.isabs(name) else os.path.join(os.path.dirname(os.path.abspath(filename)), name)
+                if not os.path.exists(path):
+                    raise ConfigError(f"cannot open include file {name}")
+                read_mf(open(path).read(), path, _depth + 1, stack[-1])
+                ln.skip()
+                if ln.peek() != "\0":
+                    raise ConfigError("expected end of line")
+                continue
+            while True:
+                ln.skip()
+                if ln.peek() in ("\0", "!"):
+                    if state == "data":
+                        state = "key"
+                    break
+                c = ln.peek()
+                if state == "key":
+                    if c == "{":
+                        if last is None:
+                            raise ConfigError("unexpected {")
+                        stack.append(last)
+                        last = None
+                        ln.i += 1
+                    elif c == "}":
+                        if len(stack) <= 1:
+                            raise ConfigError("unmatched }")
+                        stack.pop()
+                        last = None
+                        ln.i += 1
+                    else:
+                        last = stack[-1].add(ln.key())
+                        state = "data"
+                elif state == "data":
+                    if c == "{":
+                        stack.append(last)
+                        last = None
+                        ln.i += 1
+                        state = "key"
+                    elif c == "}":
+                        if len(stack) <= 1:
+                            raise ConfigError("unmatched }")
+                        stack.pop()
+                        last = None
+                        ln.i += 1
+                        state = "key"
+                    elif c == '"':
+                        last.value, more = ln.string()
+                        state = "cont" if more else "key"
+                    else:
+                        last.value = ln.rest()
+                        state = "key"
+                else:  # continuation of a quoted string
+                    if c != '"':
+                        raise ConfigError('expected " after \\ in previous line')
+                    text, more = ln.string()
+                    last.value += text
+                    state = "cont" if more else "key"
+        except ConfigError as e:
+            raise ConfigError(f"{filename}:{line_no}: {e}") from None
+    if len(stack) != 1:
+        raise ConfigError(f"{filename}: unmatched {{")
+    return root
+
+
+# ------------------------------------------------------------------------------- time
+_UNITS = {"seconds": 1.0, "second": 1.0, "secs": 1.0, "sec": 1.0, "s": 1.0,
+          "minutes": 60.0, "minute": 60.0, "mins": 60.0, "min": 60.0, "m": 60.0,
+          "hours": 3600.0, "hour": 3600.0, "hrs": 3600.0, "hr": 3600.0, "h": 3600.0}
+
+
+class TimeParser:
+    """Times in user units: a number times the unit factor, hours unless `time unit` says
+    otherwise (a named unit or a factor). Calendar time formats are not read."""
+
+    def __init__(self, conf, parent=None):
+        self.factor = parent.factor if parent else 3600.0
+        if conf is not None:
+            if conf.get("time format", "") != "":
+                raise ConfigError("calendar time formats (`time format`) are not supported")
+            u = conf.get("time unit", "default")
+            if u in _UNITS:
+                self.factor = _UNITS[u]
+            elif u != "default":
+                try:
+                    self.factor = float(u)
+                except ValueError:
+                    raise ConfigError(f"unknown time unit {u!r}") from None
+
+    def parse(self, s):
+        return float(s) * self.factor
+
+
+def _floats(s, n=None):
+    vals = [float(x) for x in re.split(r"[,\s]+", s.strip()) if x]
+    if n is not None and len(vals) != n:
+        raise ConfigError(f"expected {n} numbers in {s!r}")
+    return vals
+
+
+# -------------------------------------------------------------------------- the model
+class Model:
+    """A configured solve: mesh, time parameters, scheme, fields, source terms and
+    boundaries read from a deck."""
+
+    def __init__(self, tree, base_path="."):
+        self.tree = tree
+        self.base = base_path
+        mesh = tree.child("mesh")
+        if mesh is None:
+            raise ConfigError("missing `mesh` section")
+        self.nx, self.ny = [int(v) for v in _floats(mesh.get("cell count"), 2)]
+        self.dx, self.dy = _floats(mesh.get("cell size"), 2)
+        self.origin = tuple(_floats(mesh.get("origin", "0.0, 0.0"), 2))
+        if float(mesh.get("angle", "0.0")) != 0.0:
+            raise ConfigError("rotated meshes are not supported")
+        scheme = tree.child("scheme")
+        if scheme is None:
+            raise ConfigError("missing `scheme` section")
+        if (scheme.value or "runge-kutta") != "runge-kutta":
+            raise ConfigError(f"unknown scheme type {scheme.value!r}")
+        self.parser = TimeParser(scheme)
+        self.start_time = self.parser.parse(scheme.get("start time", "0"))
+        self.end_time = self.parser.parse(scheme.get("end time"))
+        sd = self.parser.parse(scheme.get("step duration", "0"))
+        self.step_duration = sd if sd != 0.0 else float(scheme.get("step duration seconds", "60"))
+        self.initial_timestep = float(scheme.get("initial timestep seconds", "1.0"))
+        self.method = scheme.get("method", "classic")
+        self._series = {}
+        self.source_terms = [n for n in tree.equal_range("source term")]
+        self.boundaries = [n for n in tree.equal_range("boundary")]
+        kinds = [b.value for b in self.boundaries]
+        for k in kinds:
+            if k not in ("discharge", "head", "stage"):
+                raise ConfigError(f"unknown boundary type {k!r}")
+        if "head" in kinds and "stage" in kinds:
+            raise ConfigError("a head and a stage boundary together are not supported")
+        hs = [i for i, k in enumerate(kinds) if k in ("head", "stage")]
+        ds = [i for i, k in enumerate(kinds) if k == "discharge"]
+        self.head_first = bool(hs and ds and hs[0] < ds[0])
+        names = [s.value for s in self.source_terms]
+        for n in names:
+            if n not in ("manning roughness", "infiltration", "energy loss"):
+                raise ConfigError(f"source term {n!r} is not supported")
+        self.manning = "manning roughness" in names
+        self.eloss_first = ("energy loss" in names and self.manning and
+                            names.index("energy loss") < names.index("manning roughness"))
+
+    # --- selections and fields
+    def selection(self, conf):
+        """Cell indices of a MeshSelection (None = global)."""
+        kind = conf.value if conf is not None else ""
+        if kind in ("", "global"):
+            return None
+        if kind == "id list":
+            ids = [int(n.value) for n in conf.equal_range("id")]
+            for n in conf.equal_range("ids"):
+                ids += [int(x) for x in _floats(n.value)]
+            ids = sorted(set(i for i in ids if 0 <= i < self.nx * self.ny))
+            return np.asarray(ids, dtype=np.int64)
+        raise ConfigError(f"mesh selection {kind!r} is not supported (geometry selections need WKT)")
+
+    def _input_field(self, spec):
+        out = np.zeros(self.nx * self.ny)
+        sel = self.selection(spec.child("within"))
+        kind = (spec.value or "").lower()
+        if kind == "constant" or kind not in ("slope", "composite", "raster"):
+            if kind == "constant":
+                v = float(spec.get("value"))
+            else:
+                try:
+                    v = float(kind)
+                except ValueError:
+                    raise ConfigError(f"{kind!r} is not a known input field specifier") from None
+            if sel is None:
+                out[:] = out * 0.0 + v
+            else:
+                out[sel] = out[sel] * 0.0 + v
+            return out
+        if kind == "slope":
+            if sel is not None:
+                raise ConfigError("sloped input fields need a global selection")
+            ox, oy, oz = _floats(spec.get("origin"), 3)
+            sx, sy = _floats(spec.get("slope"), 2)
+            i = np.arange(self.nx * self.ny)
+            x = self.origin[0] + ((i % self.nx) + 0.5) * self.dx + ((i // self.nx) + 0.5) * 0.0
+            y = self.origin[1] + ((i % self.nx) + 0.5) * 0.0 + ((i // self.nx) + 0.5) * self.dy
+            return oz + sx * (x - ox) + sy * (y - oy)
+        raise ConfigError(f"input fields of type {kind!r} are not supported")
+
+    def field(self, name, init):
+        """FieldGenerator (FieldGenerator.cpp:137-178): the initial value, then each `set`,
+        `add` or `multiply` of the `field == name` section in order."""
+        f = np.full(self.nx * self.ny, float(init))
+        for conf in self.tree.equal_range("field"):
+            if conf.value != name:
+                continue
+            for key, spec in conf:
+                if key == "set":
+                    f = self._set(f, spec)
+                elif key == "add":
+                    f = f + self._input_field(spec)
+                elif key == "multiply":
+                    inp = np.ones(self.nx * self.ny)
+                    sel = self.selection(spec.child("within"))
+                    v = self._input_field(spec)
+                    if sel is None:
+                        inp = v
+                    else:
+                        inp[sel] = v[sel]
+                    f = f * inp
+                else:
+                    raise ConfigError(f"unknown field operation {key!r}")
+        return f.reshape(self.ny, self.nx)
+
+    def _set(self, f, spec):
+        sel = self.selection(spec.child("within"))
+        v = self._input_field(spec)
+        if sel is None:
+            return v
+        f = f.copy()
+        f[sel] = v[sel]
+        return f
+
+    # --- time series
+    def series(self, name):
+        if name in self._series:
+            return self._series[name]
+        conf = next((n for n in self.tree.equal_range("time series") if n.value == name), None)
+        if conf is None:
+            raise ConfigError(f"could not find time series {name!r}")
+        src = conf.get("source", "not specified").lower()
+        if src == "inline":
+            sconf = conf.child("source")
+            tp = TimeParser(sconf, self.parser)
+            data = sconf.child("data")
+            if data is None:
+                raise ConfigError(f"time series {name!r}: inline source without data")
+            times, values = [], []
+            for k, n in data:
+                t = tp.parse(k.lower())
+                if times and t <= times[-1]:
+                    raise ConfigError("times in time series must increase")
+                times.append(t)
+                values.append(float(n.value))
+        elif src == "csv":
+            times, values = self._csv(conf, TimeParser(conf, self.parser))
+        else:
+            raise ConfigError(f"unknown time series source {src!r}")
+        ts = TimeSeries(times, values)
+        self._series[name] = ts
+        return ts
+
+    def _csv(self, conf, tp):
+        """TimeSeries::load_csv (TimeSeries.cpp:209-259): rapidcsv's label row is `skip rows`
+        (+1 with headers, so the first row by default) and its row-name column `skip cols`
+        (-1: none); named or 1-based numbered time and value columns."""
+        fn = conf.get("filename")
+        path = fn if os.path.isabs(fn) else os.path.join(self.base, fn)
+        sep = conf.get("separator", ",")
+        comment = conf.get("comment character", "#")
+        headers = conf.get("headers", "true").lower() in ("true", "1", "yes")
+        label_row = int(conf.get("skip rows", "-1")) + (1 if headers else 0)
+        name_col = int(conf.get("skip cols", "-1"))
+        rows = []
+        for line in open(path):
+            line = line.rstrip("\r\n")
+            if not line.strip() or line.lstrip().startswith(comment):
+                continue
+            cells = [c.strip() for c in line.split(sep)]
+            if name_col >= 0:
+                del cells[name_col]
+            rows.append(cells)
+        if label_row >= 0:
+            head, body = rows[label_row], rows[label_row + 1:]
+        else:
+            head, body = None, rows
+        if headers:
+            try:
+                tcol = head.index(conf.get("time column"))
+                vcol = head.index(conf.get("value column"))
+            except ValueError as e:
+                raise ConfigError(f"{fn}: {e}") from None
+        else:
+            tcol = int(conf.get("time column", "1")) - 1
+            vcol = int(conf.get("value column", "2")) - 1
+        return [tp.parse(r[tcol]) for r in body], [float(r[vcol]) for r in body]
+
+    # --- building and running
+    def build(self, solver_cls, precision="f64", **kw):
+        """A solver with the mesh, scheme, fields and source terms of the deck."""
+        kwargs = dict(dy=self.dy, rk_method=self.method, step_duration=self.step_duration,
+                      initial_dt=self.initial_timestep, manning=self.manning, head_first=self.head_first,
+                      eloss_first=self.eloss_first)
+        if precision != "f64" or solver_cls.__name__ != "OracleSolver":
+            kwargs["precision"] = precision
+        kwargs.update(kw)
+        s = solver_cls(self.nx, self.ny, self.dx, **kwargs)
+        s.set_field("Z", self.field("z_bed", 0.0))
+        for f in ("h", "u", "v"):
+            s.set_field(f.upper(), self.field(f, 0.0))
+        for st in self.source_terms:
+            if st.value == "manning roughness":
+                # ManningRoughnessSourceTerm.cpp:90-109: defaults, then per-cell fields
+                d = (float(st.get("default shallow n", "0.03")), float(st.get("default deep n", "0.3")),
+                     float(st.get("default shallow depth", "0.1")), float(st.get("default deep depth", "0.3")))
+                s.set_manning(*d)
+                for name, fid, dv in (("n_shallow", "N_SHALLOW", d[0]), ("n_deep", "N_DEEP", d[1]),
+                                      ("d_shallow", "D_SHALLOW", d[2]), ("d_deep", "D_DEEP", d[3])):
+                    if any(c.value == name for c in self.tree.equal_range("field")):
+                        s.set_field(fid, self.field(name, dv))
+            elif st.value == "infiltration":
+                s.set_field("INFIL_RATE", self.field("IR", float(st.get("default infiltration rate", "1e-6"))))
+                s.set_field("INFIL_CAP", self.field("IC", float(st.get("default infiltration capacity", "0.1"))))
+            elif st.value == "energy loss":
+                if st.child("model") is not None:
+                    raise ConfigError("energy-loss models are not supported")
+                s.set_field("ELOSS_FX", self.field("fdx", float(st.get("default fx/m", "0.0"))))
+                s.set_field("ELOSS_FY", self.field("fdy", float(st.get("default fy/m", "0.0"))))
+        return s
+
+    def boundary_values(self, t):
+        """start_new_step of every boundary for the step [t, t + L]: per-cell (q0, q1) of the
+        discharge boundaries (added) and (h0, h1) of the head or stage boundaries (assigned,
+        NaN where unselected), or None when the deck has none."""
+        L = self.step_duration
+        n = self.nx * self.ny
+        q = None
+        hb = None
+        for b in self.boundaries:
+            for key, e in b:
+                sel = self.selection(e.child("cells"))
+                if key == "constant":
+                    v0 = v1 = float(e.get("value"))
+                elif key == "time series":
+                    ts = self.series(e.get("values"))
+                    v0, v1 = ts.at(t), ts.at(t + L)
+                else:
+                    raise ConfigError(f"unknown boundary entry {key!r}")
+                if b.value == "discharge":
+                    if q is None:
+                        q = (np.zeros(n), np.zeros(n))
+                    idx = slice(None) if sel is None else sel
+                    q[0][idx] += v0
+                    q[1][idx] += v1
+                else:
+                    if hb is None:
+                        hb = (np.full(n, np.nan), np.full(n, np.nan))
+                    idx = slice(None) if sel is None else sel
+                    hb[0][idx] = v0
+                    hb[1][idx] = v1
+        return q, hb
+
+    def forcing(self, solver, t):
+        """Upload the step's boundary values to `solver` and set its forcing: one uniform
+        rain pair when every cell gets the same discharge, per-cell fields otherwise."""
+        q, hb = self.boundary_values(t)
+        f = Forcing()
+        f.rain_kind = RAIN_NONE
+        f.head_kind = HEAD_NONE
+        if q is not None:
+            if np.all(q[0] == q[0][0]) and np.all(q[1] == q[1][0]):
+                f.rain_kind, f.rain_q0, f.rain_q1 = RAIN_UNIFORM, float(q[0][0]), float(q[1][0])
+            else:
+                f.rain_kind = RAIN_FIELDS
+        if hb is not None:  # head targets first: a forcing that names them needs them set
+            solver.set_field("HBDY0", hb[0].reshape(self.ny, self.nx))
+            solver.set_field("HBDY1", hb[1].reshape(self.ny, self.nx))
+            f.head_kind = STAGE_FIELDS if any(b.value == "stage" for b in self.boundaries) else HEAD_FIELDS
+        solver.set_forcing(f)
+        if f.rain_kind == RAIN_FIELDS:  # per-cell discharge after the forcing that clears them
+            solver.set_field("QBDY0", q[0].reshape(self.ny, self.nx))
+            solver.set_field("QBDY1", q[1].reshape(self.ny, self.nx))
+        return f
+
+    def solve(self, solver, on_step=None):
+        """TypedTemporalScheme::solve over the deck's start and end times."""
+        n = num_steps(self.start_time, self.end_time, self.step_duration)
+        per_step = []
+        for i in range(n):
+            t = self.start_time + i * self.step_duration
+            if on_step:
+                on_step(t, solver)
+            self.forcing(solver, t)
+            per_step.append(solver.advance())
+        if on_step:
+            on_step(self.start_time + n * self.step_duration, solver)
+        return per_step
+
+
+def load(path):
+    """Read a deck; relative file names inside it resolve against its directory."""
+    return Model(read_mf(path), base_path=os.path.dirname(os.path.abspath(path)))
+
+
+__all__ = ["ConfigError", "Node", "read_mf", "TimeParser", "Model", "load"]

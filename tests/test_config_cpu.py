@@ -1,0 +1,179 @@
+"""The `.mf` configuration front end (mfcm_b200/config.py): the reader's grammar and errors,
+the time units, the field generators, selections and time series, and a whole deck whose
+solve equals the same problem set up through the API, bit for bit (oracle, CPU)."""
+import os
+
+import numpy as np
+import pytest
+
+from mfcm_b200 import config, solve, TimeSeries, HEAD_FIELDS
+from mfcm_b200.config import ConfigError, read_mf
+from oracle.sv_oracle_py import OracleSolver
+from tests.scenarios import same
+
+DECKS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "decks")
+
+
+def test_reader_keys_values_nesting_and_repeats():
+    t = read_mf('mesh\n{\n  cell count == 10 20   ! trailing comment\n  "quoted key" "a \\"b\\"\\tc"\n}\n'
+                'boundary == head\n{\n}\nboundary == stage\n'
+                'long == "first part" \\\n        " second"\n')
+    mesh = t.child("mesh")
+    assert mesh.get("cell count") == "10 20"
+    assert mesh.get("quoted key") == 'a "b"\tc'
+    assert [n.value for n in t.equal_range("boundary")] == ["head", "stage"]
+    assert t.get("long") == "first part second"
+
+
+def test_reader_errors():
+    for bad in ("}\n", "{\n", "a\n{\n", "#define x\n", 'a == "open\n', 'k == "x" \\ y\n',
+                '"k" \\\n', 'k == "x" \\\nnext\n'):
+        with pytest.raises(ConfigError):
+            read_mf(bad)
+
+
+def test_include_is_relative_to_the_including_file(tmp_path):
+    (tmp_path / "sub").mkdir()
+    (tmp_path / "sub" / "inner.mf").write_text("x == 1\n")
+    (tmp_path / "main.mf").write_text('a\n{\n#include "sub/inner.mf"\n}\n')
+    t = read_mf(str(tmp_path / "main.mf"))
+    assert t.child("a").get("x") == "1"
+
+
+def test_time_units():
+    assert config.TimeParser(read_mf("")).parse("2") == 7200.0          # hours by default
+    assert config.TimeParser(read_mf("time unit == minutes\n")).parse("1.5") == 90.0
+    assert config.TimeParser(read_mf("time unit == 10\n")).parse("3") == 30.0
+    with pytest.raises(ConfigError):
+        config.TimeParser(read_mf("time unit == fortnights\n"))
+    with pytest.raises(ConfigError):
+        config.TimeParser(read_mf("time format == %Y\n"))
+
+
+def test_deck_fields_series_and_boundaries():
+    m = config.load(os.path.join(DECKS, "catchment.mf"))
+    assert (m.nx, m.ny, m.dx, m.step_duration, m.end_time) == (24, 16, 5.0, 30.0, 120.0)
+    assert m.series("storm").t == [0.0, 60.0, 90.0, 180.0, 6000.0]      # CSV times in minutes
+    z = m.field("z_bed", 0.0)
+    assert z[0, 0] == 10.0 + (-0.01) * 2.5 + 0.002 * 2.5
+    assert z.ravel()[150] == (10.0 + (-0.01) * 32.5 + 0.002 * 32.5) + 0.75   # the id-list bump
+    assert z.ravel()[151] == 10.0 + (-0.01) * 37.5 + 0.002 * 32.5
+    q, hb = m.boundary_values(30.0)
+    assert q[0][0] == m.series("storm").at(30.0) and q[1][0] == m.series("storm").at(60.0)
+    assert np.count_nonzero(~np.isnan(hb[0])) == 16 and np.all(hb[0][23::24] == 0.0)
+
+
+def test_unsupported_features_are_named():
+    base = "mesh\n{\ncell count == 4 4\ncell size == 1 1\n}\nscheme == runge-kutta\n{\nend time == 1\n}\n"
+    for extra, what in (("source term == eddy viscosity\n", "eddy viscosity"),
+                        ("boundary == weir\n", "weir")):
+        with pytest.raises(ConfigError, match=what):
+            config.Model(read_mf(base + extra))
+    m = config.Model(read_mf(base + "field == h\n{\nset == raster\n{\nname == dem\n}\n}\n"))
+    with pytest.raises(ConfigError, match="raster"):
+        m.field("h", 0.0)
+
+
+def _direct(m):
+    """The same problem as catchment.mf, set up through the API."""
+    o = OracleSolver(m.nx, m.ny, m.dx, m.dy, step_duration=m.step_duration, initial_dt=1.0)
+    o.set_field("Z", m.field("z_bed", 0.0))
+    o.set_field("H", np.full((m.ny, m.nx), 0.002))
+    o.set_field("U", np.zeros((m.ny, m.nx)))
+    o.set_field("V", np.zeros((m.ny, m.nx)))
+    o.set_manning(0.035, 0.035, 0.1, 0.3)
+    storm = TimeSeries([0.0, 60.0, 90.0, 180.0, 6000.0], [1e-5, 2e-5, 2e-5, 0.0, 0.0])
+    hb = np.full((m.ny, m.nx), np.nan)
+    hb[:, -1] = 0.0
+    o.set_field("HBDY0", hb)
+    o.set_field("HBDY1", hb)
+    for i in range(4):
+        t = 30.0 * i
+        from mfcm_b200 import Forcing, RAIN_UNIFORM
+        f = Forcing()
+        f.rain_kind, f.rain_q0, f.rain_q1 = RAIN_UNIFORM, storm.at(t), storm.at(t + 30.0)
+        f.head_kind = HEAD_FIELDS
+        o.set_forcing(f)
+        o.advance()
+    return o
+
+
+def test_deck_solve_equals_the_api_setup():
+    m = config.load(os.path.join(DECKS, "catchment.mf"))
+    a = m.build(OracleSolver)
+    m.solve(a)
+    b = _direct(m)
+    for f in ("H", "U", "V"):
+        assert same(a.get_field(f), b.get_field(f)), f
+    assert a.stats() == b.stats()
+    assert a.stats()["accepted"] > 0 and a.stats()["outflow"] > 0.0
+
+
+def test_inline_series_multiply_and_infiltration_deck():
+    deck = read_mf("""
+mesh
+{
+  cell count == 6 4
+  cell size == 2 2
+}
+scheme == runge-kutta
+{
+  time unit == minutes
+  end time == 2
+  step duration == 1
+}
+time series == pulse
+{
+  source == inline
+  {
+    time unit == seconds
+    data
+    {
+      0 == 0.0
+      30 == 3e-5
+      90 == 0
+    }
+  }
+}
+field == z_bed
+{
+  set == 1.0
+  multiply == 2.5
+  {
+    within == id list
+    {
+      ids == 0 1 2
+    }
+  }
+  add == constant
+  {
+    value == 0.25
+  }
+}
+field == IR
+{
+  set == 1e-6
+}
+field == IC
+{
+  set == 5e-4
+}
+source term == infiltration
+boundary == discharge
+{
+  time series == rain
+  {
+    values == pulse
+  }
+}
+""")
+    m = config.Model(deck)
+    assert (m.end_time, m.step_duration) == (120.0, 60.0)
+    ts = m.series("pulse")
+    assert ts.t == [0.0, 30.0, 90.0] and abs(ts.at(60.0) - 1.5e-5) < 1e-20
+    z = m.field("z_bed", 0.0).ravel()
+    assert list(z[:4]) == [2.75, 2.75, 2.75, 1.25]
+    a = m.build(OracleSolver)
+    m.solve(a)
+    ic = a.get_field("INFIL_CAP")
+    assert np.all(ic < 5e-4) and np.all(ic >= 0.0)       # capacity consumed as it infiltrates
