@@ -14,14 +14,15 @@ On top of the tree sit the parts of the schema that drive this solver:
 - the mesh (Cartesian2DMesh.cpp:30-40);
 - the scheme and its time parameters, with the time parser's units, hours by default
   (TimeParameters.cpp:23-38, TimeParser.cpp:20-104);
-- fields built by `set` / `add` / `multiply` of constant or sloped values within id-list
-  selections (FieldGenerator.cpp:100-178, MeshSelection.cpp:146-193);
+- fields built by `set` / `add` / `multiply` of constant, sloped, composite or NIMROD raster
+  inputs within id-list selections (FieldGenerator.cpp:26-178, MeshSelection.cpp:146-193,
+  Raster.cpp:35-68; the raster reader is mfcm_b200/raster.py);
 - time series, inline or CSV (TimeSeries.cpp:179-296);
 - the source terms: Manning roughness, infiltration, energy loss (SourceTerm.cpp:32-50);
 - the boundaries: discharge, head, stage, each a list of constant or time-series entries on
   cell selections (DischargeBoundarySourceTerm.hpp:114-146 and siblings).
 
-Raster fields, WKT geometry selections, formatted (calendar) times, eddy viscosity, outputs
+GDAL rasters, WKT geometry selections, formatted (calendar) times, eddy viscosity, outputs
 and measures are not read: a deck that uses them raises ConfigError naming the feature.
 """
 import math
@@ -30,6 +31,7 @@ import re
 
 import numpy as np
 
+from .raster import NimrodRaster, RasterError
 from . import (TimeSeries, Forcing, num_steps, RAIN_NONE, RAIN_UNIFORM, RAIN_FIELDS, HEAD_NONE, HEAD_FIELDS,
                STAGE_FIELDS)
 
@@ -311,6 +313,7 @@ class Model:
         self.initial_timestep = float(scheme.get("initial timestep seconds", "1.0"))
         self.method = scheme.get("method", "classic")
         self._series = {}
+        self._rasters = {}
         self.source_terms = [n for n in tree.equal_range("source term")]
         self.boundaries = [n for n in tree.equal_range("boundary")]
         kinds = [b.value for b in self.boundaries]
@@ -344,24 +347,24 @@ class Model:
             return np.asarray(ids, dtype=np.int64)
         raise ConfigError(f"mesh selection {kind!r} is not supported (geometry selections need WKT)")
 
-    def _input_field(self, spec):
-        out = np.zeros(self.nx * self.ny)
+    def _assign(self, f, sel, v):
+        """field *= 0 then += v on the selection (load_constant_input_field,
+        FieldGenerator.cpp:43-57): a NaN or infinite value stays NaN."""
+        idx = slice(None) if sel is None else sel
+        f[idx] = f[idx] * 0.0 + v
+
+    def _load_input(self, f, spec):
+        """load_input_field (FieldGenerator.cpp:104-135) into the flat field `f`, in place."""
         sel = self.selection(spec.child("within"))
         kind = (spec.value or "").lower()
-        if kind == "constant" or kind not in ("slope", "composite", "raster"):
-            if kind == "constant":
-                v = float(spec.get("value"))
-            else:
-                try:
-                    v = float(kind)
-                except ValueError:
-                    raise ConfigError(f"{kind!r} is not a known input field specifier") from None
-            if sel is None:
-                out[:] = out * 0.0 + v
-            else:
-                out[sel] = out[sel] * 0.0 + v
-            return out
-        if kind == "slope":
+        if kind == "composite":  # FieldGenerator.cpp:26-41, ConstantFieldGeneratorModel
+            if sel is not None:
+                raise ConfigError("composite input fields need a global selection")
+            for m in spec.equal_range("model"):
+                if m.value != "constant":
+                    raise ConfigError(f"unknown field model type {m.value!r}")
+                self._assign(f, self.selection(m.child("cells")), float(m.get("value")))
+        elif kind == "slope":
             if sel is not None:
                 raise ConfigError("sloped input fields need a global selection")
             ox, oy, oz = _floats(spec.get("origin"), 3)
@@ -369,42 +372,64 @@ class Model:
             i = np.arange(self.nx * self.ny)
             x = self.origin[0] + ((i % self.nx) + 0.5) * self.dx + ((i // self.nx) + 0.5) * 0.0
             y = self.origin[1] + ((i % self.nx) + 0.5) * 0.0 + ((i // self.nx) + 0.5) * self.dy
-            return oz + sx * (x - ox) + sy * (y - oy)
-        raise ConfigError(f"input fields of type {kind!r} are not supported")
+            f[:] = oz + sx * (x - ox) + sy * (y - oy)
+        elif kind == "raster":
+            r = self.raster(spec.get("name"))
+            f[:] = r.map_to_mesh(self.nx, self.ny, self.dx, self.dy, self.origin, cells=sel, field=f).reshape(-1)
+        else:
+            if kind == "constant":
+                v = float(spec.get("value"))
+            else:
+                try:
+                    v = float(kind)
+                except ValueError:
+                    raise ConfigError(f"{kind!r} is not a known input field specifier") from None
+            self._assign(f, sel, v)
+        return f
+
+    def raster(self, name):
+        """RasterDatabase::get_raster_field_ptr (Raster.cpp:35-68): the `raster field == name`
+        section's file, NIMROD only (GDAL is not available)."""
+        if name in self._rasters:
+            return self._rasters[name]
+        conf = next((n for n in self.tree.equal_range("raster field") if n.value == name), None)
+        if conf is None:
+            raise ConfigError(f"could not find raster field {name!r}")
+        src = conf.get("source").lower()
+        if src == "gdal":
+            raise ConfigError(f"raster field {name!r}: GDAL rasters are not supported (no GDAL)")
+        if src != "nimrod":
+            raise ConfigError(f"unknown source type {src!r} for raster field {name!r}")
+        boxes = conf.equal_range("bbox")
+        if len(boxes) > 1:
+            raise ConfigError("only one bounding box can be applied to a NIMROD data file")
+        fn = conf.get("filename", ".")
+        path = fn if os.path.isabs(fn) else os.path.join(self.base, fn)
+        try:
+            r = NimrodRaster(path, bbox=_floats(boxes[0].value, 4) if boxes else None)
+        except (OSError, RasterError) as e:
+            raise ConfigError(f"raster field {name!r}: {e}") from None
+        self._rasters[name] = r
+        return r
 
     def field(self, name, init):
         """FieldGenerator (FieldGenerator.cpp:137-178): the initial value, then each `set`,
-        `add` or `multiply` of the `field == name` section in order."""
+        `add` or `multiply` of the `field == name` section in order; `add` loads its input
+        into zeros and `multiply` into ones."""
         f = np.full(self.nx * self.ny, float(init))
         for conf in self.tree.equal_range("field"):
             if conf.value != name:
                 continue
             for key, spec in conf:
                 if key == "set":
-                    f = self._set(f, spec)
+                    self._load_input(f, spec)
                 elif key == "add":
-                    f = f + self._input_field(spec)
+                    f = f + self._load_input(np.zeros(self.nx * self.ny), spec)
                 elif key == "multiply":
-                    inp = np.ones(self.nx * self.ny)
-                    sel = self.selection(spec.child("within"))
-                    v = self._input_field(spec)
-                    if sel is None:
-                        inp = v
-                    else:
-                        inp[sel] = v[sel]
-                    f = f * inp
+                    f = f * self._load_input(np.ones(self.nx * self.ny), spec)
                 else:
                     raise ConfigError(f"unknown field operation {key!r}")
         return f.reshape(self.ny, self.nx)
-
-    def _set(self, f, spec):
-        sel = self.selection(spec.child("within"))
-        v = self._input_field(spec)
-        if sel is None:
-            return v
-        f = f.copy()
-        f[sel] = v[sel]
-        return f
 
     # --- time series
     def series(self, name):
