@@ -93,10 +93,17 @@ class _Backend:
         a = np.ascontiguousarray(np.asarray(values, dtype=np.float64).reshape(-1))
         self._call("set_field", fid, a.ctypes.data_as(C.POINTER(C.c_double)), a.size)
 
-    def get_field(self, field):
+    def get_field(self, field, out=None):
+        """A field as FP64. `out`, a C-contiguous float64 array of the field's size (pinned
+        host memory, for one DMA copy), receives it in place of a new array."""
         fid = _field_id(field)
         n = self.field_size(fid)
-        a = np.empty(n, dtype=np.float64)
+        if out is None:
+            a = np.empty(n, dtype=np.float64)
+        else:
+            if out.dtype != np.float64 or out.size != n or not out.flags["C_CONTIGUOUS"]:
+                raise ValueError(f"out must be a C-contiguous float64 array of {n} values")
+            a = out.reshape(-1)
         self._call("get_field", fid, a.ctypes.data_as(C.POINTER(C.c_double)), n)
         return a if fid in FACE_FIELDS else a.reshape(self.ny, self.nx)
 

@@ -18,6 +18,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/sv.h"
@@ -149,7 +150,6 @@ struct Solver final : public sv_ctx {
   bool datum = false;              // SV_F32_DATUM64
   double* zdat = nullptr;          // per datum tile FP64 datum
   int dtiles_x = 0, dtiles_y = 0;
-  std::vector<double> host_datum;
   T* man[4] = {};
   double man_s[4] = {0.03, 0.3, 0.1, 0.3};  // ManningRoughnessSourceTerm.cpp:99-102
   std::vector<double> host_n_shallow;
@@ -251,7 +251,6 @@ struct Solver final : public sv_ctx {
       dtiles_y = int((m->ny + svk::kDatumTY - 1) / svk::kDatumTY);
       SV_CUDA(alloc(&zdat, size_t(dtiles_x) * dtiles_y));
       SV_CUDA(cudaMemsetAsync(zdat, 0, sizeof(double) * size_t(dtiles_x) * dtiles_y, stream));
-      host_datum.assign(size_t(dtiles_x) * dtiles_y, 0.0);
     }
     SV_CUDA(alloc(&ctl, 1));
     SV_CUDA(alloc(&dbg_ctl, 1));
@@ -295,18 +294,45 @@ struct Solver final : public sv_ctx {
     return nullptr;
   }
 
+  // Fields cross the interface in FP64. An FP64 solver copies them straight between the host
+  // buffer and its own array; another value type stages them in a stream-ordered FP64
+  // buffer and converts on the device, so a field costs one copy at the link's speed (DMA
+  // when the caller's buffer is pinned) and no pass over it on the host.
   int upload(T* dst, const double* host, uint64_t n) {
-    std::vector<T> tmp(n);
-    for (uint64_t i = 0; i < n; ++i) tmp[i] = T(host[i]);
-    SV_CUDA(cudaMemcpyAsync(dst, tmp.data(), n * sizeof(T), cudaMemcpyHostToDevice, stream));
-    SV_CUDA(cudaStreamSynchronize(stream));
+    cudaError_t e;
+    if constexpr (std::is_same<T, double>::value) {
+      e = cudaMemcpyAsync(dst, host, n * sizeof(double), cudaMemcpyHostToDevice, stream);
+    } else {
+      double* st = nullptr;
+      SV_CUDA(cudaMallocAsync(&st, std::max<uint64_t>(n, 1) * sizeof(double), stream));
+      e = cudaMemcpyAsync(st, host, n * sizeof(double), cudaMemcpyHostToDevice, stream);
+      if (e == cudaSuccess) e = svk::launch_from_f64<T>(st, dst, (long long)n, stream);
+      cudaError_t f = cudaFreeAsync(st, stream);
+      if (e == cudaSuccess) e = f;
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return cuda_fail(e, "field upload");
     return SV_OK;
   }
-  int download(const T* src, double* host, uint64_t n) {
-    std::vector<T> tmp(n);
-    SV_CUDA(cudaMemcpyAsync(tmp.data(), src, n * sizeof(T), cudaMemcpyDeviceToHost, stream));
-    SV_CUDA(cudaStreamSynchronize(stream));
-    for (uint64_t i = 0; i < n; ++i) host[i] = double(tmp[i]);
+  int download(const T* src, double* host, uint64_t n, bool absolute_bed = false) {
+    cudaError_t e;
+    if constexpr (std::is_same<T, double>::value) {
+      (void)absolute_bed;
+      e = cudaMemcpyAsync(host, src, n * sizeof(double), cudaMemcpyDeviceToHost, stream);
+    } else {
+      double* st = nullptr;
+      SV_CUDA(cudaMallocAsync(&st, std::max<uint64_t>(n, 1) * sizeof(double), stream));
+      if (absolute_bed)  // FP32 with tile datums: bed = FP64 datum + FP32 offset
+        e = svk::launch_datum_absolute(reinterpret_cast<const float*>(src), int(mesh.nx), int(mesh.ny), dtiles_x, zdat,
+                                       st, stream);
+      else
+        e = svk::launch_to_f64<T>(src, st, (long long)n, stream);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(host, st, n * sizeof(double), cudaMemcpyDeviceToHost, stream);
+      cudaError_t f = cudaFreeAsync(st, stream);
+      if (e == cudaSuccess) e = f;
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return cuda_fail(e, "field download");
     return SV_OK;
   }
 
@@ -349,43 +375,22 @@ struct Solver final : public sv_ctx {
   // multiple of 2^-10 m (datum differences are then exact in FP64); stored bed = FP32
   // offset from it; bed slopes from the FP64 bed (Minmod3 in FP64, rounded once).
   int set_bed_with_datum(const double* host, uint64_t n) {
-    std::vector<double> dat(size_t(dtiles_x) * dtiles_y, 0.0);
-    std::vector<char> seen(dat.size(), 0);
-    for (uint64_t i = 0; i < n; ++i) {
-      double v = host[i];
-      if (v != v) continue;
-      int gx = int(i % mesh.nx), gy = int(i / mesh.nx);
-      size_t t = size_t(svk::datum_tile(gx, gy, dtiles_x));
-      if (!seen[t] || v < dat[t]) { dat[t] = v; seen[t] = 1; }
+    if constexpr (!std::is_same<T, float>::value) {
+      (void)host; (void)n;
+      return fail(SV_E_STATE, "tile datums need an FP32 solver");
+    } else {
+      double* dz = nullptr;
+      SV_CUDA(cudaMallocAsync(&dz, std::max<uint64_t>(n, 1) * sizeof(double), stream));
+      cudaError_t e = cudaMemcpyAsync(dz, host, n * sizeof(double), cudaMemcpyHostToDevice, stream);
+      if (e == cudaSuccess)
+        e = svk::launch_datum_bed(dz, int(mesh.nx), int(mesh.ny), mesh.dx, mesh.dy, dtiles_x, dtiles_y, zdat, z, zx, zy,
+                                  stream);
+      cudaError_t f = cudaFreeAsync(dz, stream);
+      if (e == cudaSuccess) e = f;
+      if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+      if (e != cudaSuccess) return cuda_fail(e, "datum bed");
+      return SV_OK;
     }
-    for (double& d : dat) d = std::floor(d * 1024.0) / 1024.0;
-    std::vector<T> off(n);
-    for (uint64_t i = 0; i < n; ++i) {
-      int gx = int(i % mesh.nx), gy = int(i / mesh.nx);
-      off[i] = T(host[i] - dat[size_t(svk::datum_tile(gx, gy, dtiles_x))]);
-    }
-    host_datum = dat;
-    SV_CUDA(cudaMemcpyAsync(z, off.data(), n * sizeof(T), cudaMemcpyHostToDevice, stream));
-    SV_CUDA(cudaMemcpyAsync(zdat, dat.data(), dat.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
-    // FP64 slopes on a temporary device copy of the FP64 bed
-    double *dz = nullptr, *dzx = nullptr, *dzy = nullptr;
-    SV_CUDA(cudaMalloc(&dz, n * sizeof(double)));
-    SV_CUDA(cudaMalloc(&dzx, n * sizeof(double)));
-    SV_CUDA(cudaMalloc(&dzy, n * sizeof(double)));
-    SV_CUDA(cudaMemcpyAsync(dz, host, n * sizeof(double), cudaMemcpyHostToDevice, stream));
-    cudaError_t e = svk::launch_bed_slopes<double>(dz, int(mesh.nx), int(mesh.ny), mesh.dx, mesh.dy, dzx, dzy, stream);
-    std::vector<double> hx(n), hy(n);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(hx.data(), dzx, n * sizeof(double), cudaMemcpyDeviceToHost, stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(hy.data(), dzy, n * sizeof(double), cudaMemcpyDeviceToHost, stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-    cudaFree(dz); cudaFree(dzx); cudaFree(dzy);
-    if (e != cudaSuccess) return cuda_fail(e, "datum bed slopes");
-    std::vector<T> fx(n), fy(n);
-    for (uint64_t i = 0; i < n; ++i) { fx[i] = T(hx[i]); fy[i] = T(hy[i]); }
-    SV_CUDA(cudaMemcpyAsync(zx, fx.data(), n * sizeof(T), cudaMemcpyHostToDevice, stream));
-    SV_CUDA(cudaMemcpyAsync(zy, fy.data(), n * sizeof(T), cudaMemcpyHostToDevice, stream));
-    SV_CUDA(cudaStreamSynchronize(stream));
-    return SV_OK;
   }
 
   int debug_ptr(int id, T*& p, long long& count) {
@@ -430,11 +435,7 @@ struct Solver final : public sv_ctx {
       src = *slot;
     }
     if ((long long)n != count) return fail(SV_E_ARG, "field size mismatch");
-    int r = download(src, host, n);
-    if (r == SV_OK && datum && id == SV_FIELD_Z)
-      for (uint64_t i = 0; i < n; ++i)
-        host[i] += host_datum[size_t(svk::datum_tile(int(i % mesh.nx), int(i / mesh.nx), dtiles_x))];
-    return r;
+    return download(src, host, n, datum && id == SV_FIELD_Z);
   }
 
   int set_manning(double a, double b, double c, double d) override {

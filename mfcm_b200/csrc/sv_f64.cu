@@ -35,6 +35,23 @@ cudaError_t launch_accept(Ctl* ctl, cudaStream_t s) {
   accept_kernel<<<1, 1, 0, s>>>(ctl);
   return cudaGetLastError();
 }
+// In this unit (no contraction) so that the FP64 slopes round like those of the FP64 solver.
+cudaError_t launch_datum_bed(const double* z, int nx, int ny, double dx, double dy, int dtiles_x, int dtiles_y,
+                             double* zdat, float* off, float* zx, float* zy, cudaStream_t s) {
+  const long long n = (long long)nx * ny, nt = (long long)dtiles_x * dtiles_y;
+  if (n <= 0) return cudaSuccess;
+  datum_tiles_kernel<<<unsigned((nt + 7) / 8), 256, 0, s>>>(z, nx, ny, dtiles_x, dtiles_y, zdat);
+  datum_offsets_kernel<<<elementwise_blocks(n), 256, 0, s>>>(z, nx, ny, dtiles_x, zdat, off);
+  bed_slopes_kernel<double, float><<<unsigned((n + 255) / 256), 256, 0, s>>>(z, nx, ny, dx, dy, zx, zy);
+  return cudaGetLastError();
+}
+cudaError_t launch_datum_absolute(const float* off, int nx, int ny, int dtiles_x, const double* zdat, double* z,
+                                  cudaStream_t s) {
+  const long long n = (long long)nx * ny;
+  if (n <= 0) return cudaSuccess;
+  datum_absolute_kernel<<<elementwise_blocks(n), 256, 0, s>>>(off, nx, ny, dtiles_x, zdat, z);
+  return cudaGetLastError();
+}
 cudaError_t launch_begin_step(Ctl* ctl, int new_step, long long budget, cudaStream_t s) {
   begin_step_kernel<<<1, 1, 0, s>>>(ctl, new_step, budget);
   return cudaGetLastError();

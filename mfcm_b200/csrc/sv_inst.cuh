@@ -81,6 +81,21 @@ template <> cudaError_t launch_bed_slopes<SV_T>(const SV_T* z, int nx, int ny, d
   return cudaGetLastError();
 }
 
+static unsigned elementwise_blocks(long long n) {
+  const long long b = (n + 255) / 256;
+  return unsigned(b < 148 * 16 ? (b > 0 ? b : 1) : 148 * 16);  // grid-stride beyond 16 blocks per SM
+}
+template <> cudaError_t launch_from_f64<SV_T>(const double* src, SV_T* dst, long long n, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  convert_kernel<double, SV_T><<<elementwise_blocks(n), 256, 0, s>>>(src, dst, n);
+  return cudaGetLastError();
+}
+template <> cudaError_t launch_to_f64<SV_T>(const SV_T* src, double* dst, long long n, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  convert_kernel<SV_T, double><<<elementwise_blocks(n), 256, 0, s>>>(src, dst, n);
+  return cudaGetLastError();
+}
+
 template <typename T, int TX, int TY, int MINB, bool P2>
 static cudaError_t launch_stage_batch_p(const StageParams<T>* Ps, const long long* tile_start, int ninst,
                                         long long total_tiles, cudaStream_t s) {

@@ -855,17 +855,70 @@ __global__ void __launch_bounds__(32 * WPB, MINB)
 }
 
 // Bed slopes once per bed upload (SaintVenantConstants, Constants.cpp:39-40).
-template <typename T>
-__global__ void bed_slopes_kernel(const T* z, int nx, int ny, double dx, double dy, T* zx, T* zy) {
+// The slopes are computed in T and stored as TO (FP32 with tile datums: FP64 slopes of the
+// FP64 bed, rounded once).
+template <typename T, typename TO = T>
+__global__ void bed_slopes_kernel(const T* z, int nx, int ny, double dx, double dy, TO* zx, TO* zy) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   long long n = (long long)nx * ny;
   if (i >= n) return;
   int gx = int(i % nx), gy = int(i / nx);
   bool hasW = gx > 0, hasE = gx < nx - 1, hasN = gy < ny - 1, hasS = gy > 0;
   T cz = z[i];
-  zx[i] = minmod3<T>(hasW ? z[i - 1] : cz, hasW, cz, hasE, hasE ? z[i + 1] : cz, mkdiv<T>(dx));
-  zy[i] = minmod3<T>(hasN ? z[i + nx] : cz, hasN, cz, hasS, hasS ? z[i - nx] : cz, mkdiv<T>(dy));
+  zx[i] = TO(minmod3<T>(hasW ? z[i - 1] : cz, hasW, cz, hasE, hasE ? z[i + 1] : cz, mkdiv<T>(dx)));
+  zy[i] = TO(minmod3<T>(hasN ? z[i + nx] : cz, hasN, cz, hasS, hasS ? z[i - nx] : cz, mkdiv<T>(dy)));
 }
+
+// Fields arrive and leave in FP64 (the interface's type); a solver of another value type
+// converts them here, one rounding per value as a host cast would do.
+template <typename TI, typename TO>
+__global__ void convert_kernel(const TI* __restrict__ src, TO* __restrict__ dst, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    dst[i] = TO(src[i]);
+}
+
+#ifdef SV_DEFINE_COMMON_KERNELS  // non-template kernels: defined in one unit only
+// Datum of each 32 x 8 tile of an FP64 bed: the tile's lowest non-NaN value (among values
+// that compare equal, such as -0.0 and 0.0, the first in row-major order), rounded down to a
+// multiple of 2^-10 m; 0 for a tile without a valid bed. One warp per tile, a lane per column.
+__global__ void datum_tiles_kernel(const double* z, int nx, int ny, int dtiles_x, int dtiles_y, double* zdat) {
+  const long long t = (long long)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  if (t >= (long long)dtiles_x * dtiles_y) return;  // whole warp
+  const int lane = threadIdx.x & 31;
+  const int gx = int(t % dtiles_x) * kDatumTX + lane, ty = int(t / dtiles_x);
+  double best = 0.0;
+  long long bi = -1;  // row-major index of `best`; -1 = none yet
+  if (gx < nx) {
+    for (int r = 0; r < kDatumTY; ++r) {
+      const int gy = ty * kDatumTY + r;
+      if (gy >= ny) break;
+      const long long i = (long long)gy * nx + gx;
+      const double v = z[i];
+      if (v != v) continue;
+      if (bi < 0 || v < best) { best = v; bi = i; }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ob = __shfl_down_sync(kFull, best, o);
+    const long long oi = __shfl_down_sync(kFull, bi, o);
+    if (oi >= 0 && (bi < 0 || ob < best || (ob == best && oi < bi))) { best = ob; bi = oi; }
+  }
+  if (lane == 0) zdat[t] = floor((bi < 0 ? 0.0 : best) * 1024.0) / 1024.0;
+}
+
+// FP32 offset of each cell's bed from its tile's datum (FP64 difference, rounded once), or the
+// absolute FP64 bed from an offset (`to_abs`).
+__global__ void datum_offsets_kernel(const double* z, int nx, int ny, int dtiles_x, const double* zdat, float* off) {
+  const long long n = (long long)nx * ny;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    off[i] = float(z[i] - zdat[datum_tile(int(i % nx), int(i / nx), dtiles_x)]);
+}
+__global__ void datum_absolute_kernel(const float* off, int nx, int ny, int dtiles_x, const double* zdat, double* z) {
+  const long long n = (long long)nx * ny;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    z[i] = double(off[i]) + zdat[datum_tile(int(i % nx), int(i / nx), dtiles_x)];
+}
+#endif
 
 // Steps queued for one batch member by one batched advance. The member runs them back to
 // back at its own pace: when a step ends, the controller records it and starts the next one

@@ -32,6 +32,15 @@ inline long long variant_partials(int v, long long nx, long long ny) {
 template <typename T> cudaError_t launch_variant(const StageParams<T>& P, int variant, cudaStream_t s);
 template <typename T> cudaError_t launch_bed_slopes(const T* z, int nx, int ny, double dx, double dy, T* zx, T* zy,
                                                     cudaStream_t s);
+// FP64 <-> T conversion of a field on the device
+template <typename T> cudaError_t launch_from_f64(const double* src, T* dst, long long n, cudaStream_t s);
+template <typename T> cudaError_t launch_to_f64(const T* src, double* dst, long long n, cudaStream_t s);
+// FP32 with tile datums, from an FP64 bed on the device: the tile datums, the FP32 offsets and
+// the bed slopes (FP64, rounded once); and the absolute FP64 bed back from the offsets
+cudaError_t launch_datum_bed(const double* z, int nx, int ny, double dx, double dy, int dtiles_x, int dtiles_y,
+                             double* zdat, float* off, float* zx, float* zy, cudaStream_t s);
+cudaError_t launch_datum_absolute(const float* off, int nx, int ny, int dtiles_x, const double* zdat, double* z,
+                                  cudaStream_t s);
 template <typename T> cudaError_t launch_volume(const T* h, int nx, int ny, double area, double* part, int tile,
                                                 cudaStream_t s);
 template <typename T> cudaError_t launch_debug(const StageParams<T>& P, const DebugParams<T>& D, T* nh, T* sf,

@@ -27,7 +27,10 @@ def test_deck_solve_equals_the_oracle():
     for k in ("H", "U", "V"):
         d = first_diff(g[k], o[k])
         assert d is None, f"{k}: first mismatch at {d[0]}: gpu {d[1]!r} oracle {d[2]!r}"
-    assert gs["accepted"] == os_["accepted"] and gs["volume"] == os_["volume"]
+    assert gs["accepted"] == os_["accepted"]
+    # the volume is a diagnostic sum: the GPU adds 32 x 8 tile partials in a tree, the oracle
+    # sums sequentially with compensation, so the two may differ in the last bit
+    assert abs(gs["volume"] - os_["volume"]) <= 1e-13 * os_["volume"]
 
 
 def test_deck_solve_in_fp32_with_fp64_datums():
