@@ -108,6 +108,7 @@ typedef struct {
 #define SV_FIELD_H_COMP 17      /* FP32 solvers: compensation carried by the depth update
                                    (part of the state for a bit-exact restart; zeroed
                                    whenever SV_FIELD_H is set)                              */
+#define SV_FIELD_EDDY_MU 18     /* eddy viscosity: per-cell constant coefficient mu, m^2/s */
 #define SV_FIELD_DHDT 20        /* dUdt_[0] of the last sv_eval_dudt(0, ...)              */
 #define SV_FIELD_DUDT 21
 #define SV_FIELD_DVDT 22
@@ -182,6 +183,24 @@ int sv_get_field(sv_ctx* ctx, int field_id, double* host, uint64_t n);
 /* ManningRoughnessSourceTerm "default shallow/deep n/depth" (ManningRoughnessSourceTerm.cpp:99-102);
  * uniform values (a later sv_set_field of that id makes it per-cell). */
 int sv_set_manning(sv_ctx* ctx, double n_shallow, double n_deep, double d_shallow, double d_deep);
+/* EddyViscositySourceTerm (EddyViscositySourceTerm.cpp:43-137): du/dt -= mu (u_xx + u_yy),
+ * dv/dt -= mu (v_xx + v_yy) on cells deeper than 1e-6 m, capped like the roughness term, the
+ * second derivatives being Minmod3 slopes of the stage's slopes. SV_EDDY_CONSTANT: mu is the
+ * field SV_FIELD_EDDY_MU when set, else `mu` ("default mu"); SV_EDDY_SMAGORINSKY: mu =
+ * mu_const + mu_smag * cell area * sqrt(u_x^2 + v_y^2 + 0.5 (|u_y| + |v_x|)^2) per cell and
+ * stage ("constant coefficient", "dynamic coefficient"). */
+#define SV_EDDY_OFF 0
+#define SV_EDDY_CONSTANT 1
+#define SV_EDDY_SMAGORINSKY 2
+int sv_set_eddy_viscosity(sv_ctx* ctx, int mode, double mu, double mu_const, double mu_smag);
+/* Configuration order of the momentum source terms (Solver.cpp:98-104): each adds to du/dt and
+ * dv/dt, so the order sets the rounding. `terms` lists SV_TERM_* at most once each; terms not
+ * listed follow in the default order (roughness, energy loss, eddy viscosity). Replaces
+ * SV_FLAG_ELOSS_FIRST. */
+#define SV_TERM_MANNING 1
+#define SV_TERM_ELOSS 2
+#define SV_TERM_EDDY 3
+int sv_set_source_order(sv_ctx* ctx, const int* terms, int n);
 /* SaintVenantSolver::start_new_step (Solver.cpp:116-129): boundary values for [t, t + L]. */
 int sv_set_forcing(sv_ctx* ctx, const sv_forcing* forcing);
 /* TypedTemporalScheme::dt_ (TemporalScheme.hpp:78) */

@@ -111,6 +111,22 @@ class _Backend:
         """ManningRoughnessSourceTerm defaults (ManningRoughnessSourceTerm.cpp:99-102)."""
         self._call("set_manning", float(n_shallow), float(n_deep), float(d_shallow), float(d_deep))
 
+    def set_eddy_viscosity(self, mode="constant", mu=1.0, mu_const=0.05, mu_smag=0.5):
+        """EddyViscositySourceTerm (EddyViscositySourceTerm.cpp:112-137): mode "off",
+        "constant" (the EDDY_MU field when set, else `mu`, "default mu") or "smagorinsky"
+        (mu_const + mu_smag * cell area * |strain|, "constant coefficient" and "dynamic
+        coefficient"); defaults are the reference's."""
+        if mode not in _abi.EDDY_MODES:
+            raise ValueError(f"unknown eddy viscosity mode {mode!r}")
+        self._call("set_eddy_viscosity", _abi.EDDY_MODES[mode], float(mu), float(mu_const), float(mu_smag))
+
+    def set_source_order(self, terms):
+        """Configuration order of the momentum source terms, names from "manning", "energy
+        loss" and "eddy viscosity" (each adds to du/dt, so the order sets the rounding)."""
+        codes = [_abi.TERMS[t] for t in terms]
+        arr = (C.c_int * max(1, len(codes)))(*codes)
+        self._call("set_source_order", arr, len(codes))
+
     def set_forcing(self, forcing):
         self._call("set_forcing", C.byref(forcing))
 

@@ -23,7 +23,7 @@ RK_STAGES = [1, 2, 2, 2, 3, 3, 3, 3, 3, 4, 4, 4]
 
 FIELD = dict(
     Z=0, H=1, U=2, V=3, N_SHALLOW=4, N_DEEP=5, D_SHALLOW=6, D_DEEP=7, QBDY0=8, QBDY1=9,
-    HBDY0=10, HBDY1=11, RAIN_PATTERN=12, INFIL_RATE=13, INFIL_CAP=14, ELOSS_FX=15, ELOSS_FY=16, H_COMP=17, DHDT=20, DUDT=21, DVDT=22, DHDX=23, DUDX=24, DVDX=25,
+    HBDY0=10, HBDY1=11, RAIN_PATTERN=12, INFIL_RATE=13, INFIL_CAP=14, ELOSS_FX=15, ELOSS_FY=16, H_COMP=17, EDDY_MU=18, DHDT=20, DUDT=21, DVDT=22, DHDX=23, DUDX=24, DVDX=25,
     DHDY=26, DUDY=27, DVDY=28, DZDX=29, DZDY=30, FLUX_H=40, FLUX_U=41, FLUX_V=42, FLUX_Z=43,
     FLUX_BRANCH=44, STATE_BASE=100, K_BASE=200,
 )
@@ -32,6 +32,8 @@ FACE_FIELDS = {40, 41, 42, 43, 44}
 RAIN_NONE, RAIN_UNIFORM, RAIN_FIELDS, RAIN_PATTERN = 0, 1, 2, 3
 HEAD_NONE, HEAD_EDGES, HEAD_FIELDS, STAGE_EDGES, STAGE_FIELDS = 0, 1, 2, 3, 4
 EDGE_XMIN, EDGE_XMAX, EDGE_YMIN, EDGE_YMAX = 1, 2, 4, 8
+EDDY_MODES = {"off": 0, "constant": 1, "smagorinsky": 2}
+TERMS = {"manning": 1, "energy loss": 2, "eddy viscosity": 3}
 
 
 class MeshDesc(C.Structure):
@@ -84,6 +86,8 @@ def declare(lib, prefix, ctx_type=C.c_void_p):
         "advance": (C.c_int, [ctx_type, P(Stats)]),
         "get_stats": (C.c_int, [ctx_type, P(Stats)]),
         "set_stats": (C.c_int, [ctx_type, P(Stats)]),
+        "set_eddy_viscosity": (C.c_int, [ctx_type, C.c_int, d, d, d]),
+        "set_source_order": (C.c_int, [ctx_type, P(C.c_int), C.c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, prefix + name)

@@ -18,11 +18,12 @@ On top of the tree sit the parts of the schema that drive this solver:
   inputs within id-list selections (FieldGenerator.cpp:26-178, MeshSelection.cpp:146-193,
   Raster.cpp:35-68; the raster reader is mfcm_b200/raster.py);
 - time series, inline or CSV (TimeSeries.cpp:179-296);
-- the source terms: Manning roughness, infiltration, energy loss (SourceTerm.cpp:32-50);
+- the source terms: Manning roughness, infiltration, energy loss, eddy viscosity
+  (SourceTerm.cpp:32-50), the momentum terms in their configured order;
 - the boundaries: discharge, head, stage, each a list of constant or time-series entries on
   cell selections (DischargeBoundarySourceTerm.hpp:114-146 and siblings).
 
-GDAL rasters, WKT geometry selections, formatted (calendar) times, eddy viscosity, outputs
+GDAL rasters, WKT geometry selections, formatted (calendar) times, outputs
 and measures are not read: a deck that uses them raises ConfigError naming the feature.
 """
 import math
@@ -327,11 +328,26 @@ class Model:
         self.head_first = bool(hs and ds and hs[0] < ds[0])
         names = [s.value for s in self.source_terms]
         for n in names:
-            if n not in ("manning roughness", "infiltration", "energy loss"):
+            if n not in ("manning roughness", "infiltration", "energy loss", "eddy viscosity"):
                 raise ConfigError(f"source term {n!r} is not supported")
         self.manning = "manning roughness" in names
         self.eloss_first = ("energy loss" in names and self.manning and
                             names.index("energy loss") < names.index("manning roughness"))
+        momentum = {"manning roughness": "manning", "energy loss": "energy loss", "eddy viscosity": "eddy viscosity"}
+        self.term_order = [momentum[n] for n in names if n in momentum]
+        # EddyViscositySourceTerm::create_source_term (EddyViscositySourceTerm.cpp:112-137)
+        self.eddy = None
+        for st in self.source_terms:
+            if st.value != "eddy viscosity":
+                continue
+            vt = st.get("viscosity type", "constant")
+            if vt == "constant":
+                self.eddy = ("constant", float(st.get("default mu", "1.0")))
+            elif vt == "smagorinsky":
+                self.eddy = ("smagorinsky", float(st.get("constant coefficient", "0.05")),
+                             float(st.get("dynamic coefficient", "0.5")))
+            else:
+                raise ConfigError(f"unknown viscosity type {vt!r}")
 
     # --- selections and fields
     def selection(self, conf):
@@ -526,6 +542,14 @@ class Model:
                     raise ConfigError("energy-loss models are not supported")
                 s.set_field("ELOSS_FX", self.field("fdx", float(st.get("default fx/m", "0.0"))))
                 s.set_field("ELOSS_FY", self.field("fdy", float(st.get("default fy/m", "0.0"))))
+            elif st.value == "eddy viscosity":
+                if self.eddy[0] == "constant":
+                    s.set_eddy_viscosity("constant", mu=self.eddy[1])
+                    if any(c.value == "mu" for c in self.tree.equal_range("field")):
+                        s.set_field("EDDY_MU", self.field("mu", self.eddy[1]))
+                else:
+                    s.set_eddy_viscosity("smagorinsky", mu_const=self.eddy[1], mu_smag=self.eddy[2])
+                s.set_source_order(self.term_order)
         return s
 
     def boundary_values(self, t):

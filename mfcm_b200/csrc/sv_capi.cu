@@ -102,6 +102,8 @@ struct sv_ctx {
   virtual int set_field(int id, const double* host, uint64_t n) = 0;
   virtual int get_field(int id, double* host, uint64_t n) = 0;
   virtual int set_manning(double, double, double, double) = 0;
+  virtual int set_eddy(int, double, double, double) = 0;
+  virtual int set_source_order(const int*, int) = 0;
   virtual int set_forcing(const sv_forcing*) = 0;
   virtual int set_dt(double) = 0;
   virtual int get_dt(double*) = 0;
@@ -157,6 +159,14 @@ struct Solver final : public sv_ctx {
   T *irate = nullptr, *icap = nullptr;  // InfiltrationSourceTerm fields (.hpp:106-109)
   T *efx = nullptr, *efy = nullptr;     // EnergyLossSourceTerm fields (.hpp:199-202)
   T* hcomp[2] = {};                     // FP32: compensation of the depth update, per state parity
+  // EddyViscositySourceTerm (EddyViscositySourceTerm.cpp:112-137): mode (SV_EDDY_*), the
+  // constant coefficient ("default mu", or the per-cell field) and the Smagorinsky
+  // coefficients ("constant coefficient", "dynamic coefficient")
+  int eddy_mode = SV_EDDY_OFF;
+  double eddy_mu = 1.0, eddy_c = 0.05, eddy_s = 0.5;
+  T* eddy_mup = nullptr;
+  int term_order_[3] = {SV_TERM_MANNING, SV_TERM_ELOSS, SV_TERM_EDDY};
+  bool order_set = false;  // else roughness / energy loss per SV_FLAG_ELOSS_FIRST, then eddy viscosity
   // FP32 with the batches' variant runs the batched column sweep as a batch of one, so a
   // solver on its own and a batch member execute the same machine code and give the same
   // bits (FP32 is contracted per kernel); that kernel reads its parameters from device memory
@@ -290,6 +300,7 @@ struct Solver final : public sv_ctx {
       case SV_FIELD_ELOSS_FX: lazy = true; return &efx;
       case SV_FIELD_ELOSS_FY: lazy = true; return &efy;
       case SV_FIELD_H_COMP: return hcomp[cur] ? &hcomp[cur] : nullptr;
+      case SV_FIELD_EDDY_MU: lazy = true; return &eddy_mup;
     }
     return nullptr;
   }
@@ -438,6 +449,36 @@ struct Solver final : public sv_ctx {
     return download(src, host, n, datum && id == SV_FIELD_Z);
   }
 
+  int term_order() const {
+    int t[3] = {term_order_[0], term_order_[1], term_order_[2]};
+    if (!order_set && (prm.flags & SV_FLAG_ELOSS_FIRST)) { t[0] = SV_TERM_ELOSS; t[1] = SV_TERM_MANNING; }
+    return t[0] | (t[1] << 2) | (t[2] << 4);
+  }
+  int set_eddy(int mode, double mu, double mc, double ms) override {
+    if (mode < SV_EDDY_OFF || mode > SV_EDDY_SMAGORINSKY) return fail(SV_E_ARG, "unknown eddy viscosity mode");
+    if (!std::isfinite(mu) || !std::isfinite(mc) || !std::isfinite(ms))
+      return fail(SV_E_ARG, "eddy viscosity coefficients must be finite");
+    eddy_mode = mode; eddy_mu = mu; eddy_c = mc; eddy_s = ms;
+    graph_dirty = true; ++pversion;
+    return SV_OK;
+  }
+  int set_source_order(const int* terms, int n) override {
+    if (n < 0 || n > 3 || (n > 0 && !terms)) return fail(SV_E_ARG, "at most three source terms");
+    int t[3], k = 0;
+    bool seen[4] = {};
+    for (int i = 0; i < n; ++i) {
+      if (terms[i] < SV_TERM_MANNING || terms[i] > SV_TERM_EDDY || seen[terms[i]])
+        return fail(SV_E_ARG, "source order lists roughness, energy loss and eddy viscosity at most once each");
+      seen[terms[i]] = true;
+      t[k++] = terms[i];
+    }
+    for (int x = SV_TERM_MANNING; x <= SV_TERM_EDDY; ++x)
+      if (!seen[x]) t[k++] = x;  // terms not listed follow in the default order
+    for (int i = 0; i < 3; ++i) term_order_[i] = t[i];
+    order_set = true;
+    graph_dirty = true; ++pversion;
+    return SV_OK;
+  }
   int set_manning(double a, double b, double c, double d) override {
     man_s[0] = a; man_s[1] = b; man_s[2] = c; man_s[3] = d;
     for (int i = 0; i < 4; ++i) man[i] = nullptr;  // uniform values replace per-cell fields
@@ -532,6 +573,10 @@ struct Solver final : public sv_ctx {
     P.efx = (efx && efy) ? efx : nullptr;
     P.efy = (efx && efy) ? efy : nullptr;
     P.eloss_first = (prm.flags & SV_FLAG_ELOSS_FIRST) ? 1 : 0;
+    P.eddy = eddy_mode;
+    P.eddy_mu = T(eddy_mu); P.eddy_c = T(eddy_c); P.eddy_s = T(eddy_s);
+    P.eddy_mup = eddy_mup;
+    P.term_order = term_order();
     P.hc[0] = hcomp[0];
     P.hc[1] = hcomp[1];
     P.manning = prm.manning; P.rain_mode = prm.rain_mode; P.head_first = prm.head_first;
@@ -609,7 +654,8 @@ struct Solver final : public sv_ctx {
     return SV_OK;
   }
   cudaError_t launch_stage_kernel(const svk::StageParams<T>& P, int st) {
-    if (batch_path(variant)) return svk::launch_sweep_batch<T>(d_sp + st, d_ws, 1, nblk, pow2_mesh(), stream);
+    if (batch_path(variant))
+      return svk::launch_sweep_batch<T>(d_sp + st, d_ws, 1, nblk, pow2_mesh(), eddy_mode != SV_EDDY_OFF, stream);
     return svk::launch_variant<T>(P, variant, stream);
   }
 
@@ -864,7 +910,7 @@ struct Solver final : public sv_ctx {
       // the batch variant runs as the batched kernel (see launch_stage_kernel): time that one
       auto launch = [&]() -> cudaError_t {
         if (!batch_path(v)) return svk::launch_variant<T>(P, v, stream);
-        return svk::launch_sweep_batch<T>(d_sp + N, d_ws + 2, 1, P.nblk, pow2_mesh(), stream);
+        return svk::launch_sweep_batch<T>(d_sp + N, d_ws + 2, 1, P.nblk, pow2_mesh(), eddy_mode != SV_EDDY_OFF, stream);
       };
       if (batch_path(v)) {
         if (!d_sp) {
@@ -973,7 +1019,7 @@ struct Batch final : public sv_batch_base {
   svk::StepQueue* d_queue = nullptr;        // [nact] steps queued by the current advance
   int nact = 0, cap = 0;
   long long total_tiles = 0;
-  bool p2 = true, dirty = true;
+  bool p2 = true, eddy = false, dirty = true;
   std::vector<int> active;                  // slot ids in launch order
   std::vector<unsigned long long> versions; // members' pversion at the last rebuild
   cudaGraphExec_t graph = nullptr;
@@ -1071,6 +1117,7 @@ struct Batch final : public sv_batch_base {
     std::vector<long long> ht(nact + 1, 0);
     std::vector<Ctl*> hc(std::max(nact, 1));
     p2 = true;
+    eddy = false;
     for (int k = 0; k < nact; ++k) {
       Solver<T>* m = members[active[k]];
       // the tile prefix and the partials follow the batch kernel's decomposition
@@ -1078,6 +1125,7 @@ struct Batch final : public sv_batch_base {
       ht[k + 1] = ht[k] + m->nblk;
       int e2;
       p2 = p2 && std::frexp(m->mesh.dx, &e2) == 0.5 && std::frexp(m->mesh.dy, &e2) == 0.5;
+      eddy = eddy || m->eddy_mode != SV_EDDY_OFF;
       for (int st = 0; st < N; ++st) hp[size_t(st) * nact + k] = m->stage_params(st);
       hf[k] = m->finalize_params(true);
       hf[k].q = d_queue + k;
@@ -1102,8 +1150,10 @@ struct Batch final : public sv_batch_base {
   int enqueue_timestep() {
     for (int st = 0; st < N; ++st) {
       cudaError_t e = svk::variant_is_sweep(svk::batch_variant<T>())
-                          ? svk::launch_sweep_batch<T>(d_params + size_t(st) * nact, d_tiles, nact, total_tiles, p2, stream)
-                          : svk::launch_stage_batch<T>(d_params + size_t(st) * nact, d_tiles, nact, total_tiles, p2, stream);
+                          ? svk::launch_sweep_batch<T>(d_params + size_t(st) * nact, d_tiles, nact, total_tiles, p2,
+                                                       eddy, stream)
+                          : svk::launch_stage_batch<T>(d_params + size_t(st) * nact, d_tiles, nact, total_tiles, p2,
+                                                       eddy, stream);
       if (e != cudaSuccess) return cuda_fail(e, "batched stage kernel");
     }
     cudaError_t e = svk::launch_finalize_batch(d_fin, nact, stream);
@@ -1313,6 +1363,11 @@ void sv_destroy(sv_ctx* ctx) { delete ctx; }
 int sv_set_field(sv_ctx* ctx, int id, const double* host, uint64_t n) { SV_CHECK_CTX(ctx); return ctx->set_field(id, host, n); }
 int sv_get_field(sv_ctx* ctx, int id, double* host, uint64_t n) { SV_CHECK_CTX(ctx); return ctx->get_field(id, host, n); }
 int sv_set_manning(sv_ctx* ctx, double a, double b, double c, double d) { SV_CHECK_CTX(ctx); return ctx->set_manning(a, b, c, d); }
+int sv_set_eddy_viscosity(sv_ctx* ctx, int mode, double mu, double mu_const, double mu_smag) {
+  SV_CHECK_CTX(ctx);
+  return ctx->set_eddy(mode, mu, mu_const, mu_smag);
+}
+int sv_set_source_order(sv_ctx* ctx, const int* terms, int n) { SV_CHECK_CTX(ctx); return ctx->set_source_order(terms, n); }
 int sv_set_forcing(sv_ctx* ctx, const sv_forcing* f) { SV_CHECK_CTX(ctx); return ctx->set_forcing(f); }
 int sv_set_dt(sv_ctx* ctx, double dt) { SV_CHECK_CTX(ctx); return ctx->set_dt(dt); }
 int sv_get_dt(sv_ctx* ctx, double* dt) { SV_CHECK_CTX(ctx); if (!dt) return SV_E_ARG; return ctx->get_dt(dt); }

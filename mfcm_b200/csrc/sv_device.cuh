@@ -391,6 +391,34 @@ __device__ __forceinline__ float pow43_(float x) { return __powf(x, 4.0f / 3.0f)
 __device__ __forceinline__ double manning_inv_h(double h) { return h / (h * h + 1e-3); }
 __device__ __forceinline__ float manning_inv_h(float h) { return __fdividef(h, h * h + 1e-3f); }
 
+// Roughness term (ManningRoughnessSourceTerm.cpp): the increments fu, fv of du/dt, dv/dt;
+// false (no increment) on cells of 1e-6 m depth or less.
+template <typename T, typename CC>
+__device__ __forceinline__ bool manning_term(T h, T u, T v, T ns, T nd, T ds, T dd, const CC& c, T& fu, T& fv,
+                                             T* n_out, T* sf_out) {
+  T n;
+  if (ns == nd) {
+    n = ns;  // mix(n, n, t) = n + 0*t = n: t = smoothstep(...) is always finite
+  } else {
+    T t = sfmin(sfmax((h - ds) / (dd - ds), T(0)), T(1));
+    T ss = t * t * (T(3) - T(2) * t);
+    n = ns + (nd - ns) * ss;
+  }
+  if (n_out) *n_out = n;
+  if (h > T(1e-6)) {
+    T inv_h = manning_inv_h(h);
+    T sf = n * n * ssqrt(u * u + v * v) * pow43_(inv_h);
+    if (sf_out) *sf_out = sf;
+    fu = -T(kG) * sf * u;
+    fv = -T(kG) * sf * v;
+    T fudt = fu * c.dt, fvdt = fv * c.dt;
+    if (sfabs(fudt) > sfabs(u) && ssign(fudt) != ssign(u)) fu = -c.divdt(u);
+    if (sfabs(fvdt) > sfabs(v) && ssign(fvdt) != ssign(v)) fv = -c.divdt(v);
+    return true;
+  }
+  if (sf_out) *sf_out = T(0);
+  return false;
+}
 template <typename T, typename CC>
 __device__ __forceinline__ void manning_apply(T h, T u, T v, T ns, T nd, T ds, T dd, const CC& c,
                                               T& du, T& dv, T* n_out, T* sf_out) {
@@ -420,7 +448,18 @@ __device__ __forceinline__ void manning_apply(T h, T u, T v, T ns, T nd, T ds, T
 }
 
 // Energy loss (EnergyLossSourceTerm.cpp:64-87): du = -0.5 u fx |U|, dv = -0.5 v fy |U| on
-// cells deeper than 1e-6 m, capped like the roughness term; adds to du, dv.
+// cells deeper than 1e-6 m, capped like the roughness term.
+template <typename T, typename CC>
+__device__ __forceinline__ bool energy_loss_term(T h, T u, T v, T fx, T fy, const CC& c, T& eu, T& ev) {
+  if (!(h > T(1e-6))) return false;
+  T hyp = ssqrt(u * u + v * v);
+  eu = T(-0.5) * u * fx * hyp;
+  ev = T(-0.5) * v * fy * hyp;
+  T eudt = eu * c.dt, evdt = ev * c.dt;
+  if (sfabs(eudt) > sfabs(u) && ssign(eudt) != ssign(u)) eu = -c.divdt(u);
+  if (sfabs(evdt) > sfabs(v) && ssign(evdt) != ssign(v)) ev = -c.divdt(v);
+  return true;
+}
 template <typename T, typename CC>
 __device__ __forceinline__ void energy_loss_apply(T h, T u, T v, T fx, T fy, const CC& c, T& du, T& dv) {
   if (!(h > T(1e-6))) return;
@@ -432,6 +471,35 @@ __device__ __forceinline__ void energy_loss_apply(T h, T u, T v, T fx, T fy, con
   if (sfabs(evdt) > sfabs(v) && ssign(evdt) != ssign(v)) ev = -c.divdt(v);
   du = du + eu;
   dv = dv + ev;
+}
+
+// Inputs of the eddy-viscosity term at one cell: the stage's first slopes of u and v and
+// their second derivatives (Minmod3 of the slopes along the same axis,
+// EddyViscositySourceTerm.hpp:222-228).
+template <typename T> struct EddyIn {
+  T ux, uy, vx, vy;      // du/dx, du/dy, dv/dx, dv/dy
+  T uxx, uyy, vxx, vyy;  // d2u/dx2, d2u/dy2, d2v/dx2, d2v/dy2
+};
+// Smagorinsky coefficient (SmagorinskyCoefficientKernel, EddyViscositySourceTerm.cpp:97-110):
+// mu_c + mu_s * area * sqrt(u_x^2 + v_y^2 + 0.5 (|u_y| + |v_x|)^2), the square taken as a
+// product (the reference's pow(x, 2))
+template <typename T>
+__device__ __forceinline__ T smagorinsky_mu(T mc, T ms, T area, const EddyIn<T>& e) {
+  const T a = sfabs(e.uy) + sfabs(e.vx);
+  return mc + ms * area * ssqrt(e.ux * e.ux + e.vy * e.vy + T(0.5) * (a * a));
+}
+// Eddy viscosity (EddyViscositySourceKernel, EddyViscositySourceTerm.cpp:46-78):
+// du = -mu (u_xx + u_yy), dv = -mu (v_xx + v_yy) on cells deeper than 1e-6 m, capped like the
+// roughness term.
+template <typename T, typename CC>
+__device__ __forceinline__ bool eddy_term(T h, T u, T v, T mu, const EddyIn<T>& e, const CC& c, T& fu, T& fv) {
+  if (!(h > T(1e-6))) return false;
+  fu = -mu * (e.uxx + e.uyy);
+  fv = -mu * (e.vxx + e.vyy);
+  T fudt = fu * c.dt, fvdt = fv * c.dt;
+  if (sfabs(fudt) > sfabs(u) && ssign(fudt) != ssign(u)) fu = -c.divdt(u);
+  if (sfabs(fvdt) > sfabs(v) && ssign(fvdt) != ssign(v)) fv = -c.divdt(v);
+  return true;
 }
 
 // Infiltration (InfiltrationSourceTerm.cpp:43-62): the depth taken this evaluation,

@@ -13,23 +13,26 @@ inline bool pow2_mesh(double dx, double dy) {
   return std::frexp(dx, &e) == 0.5 && std::frexp(dy, &e) == 0.5;
 }
 
-template <typename T, int TX, int TY, int MINB, bool P2>
+template <typename T, int TX, int TY, int MINB, bool P2, bool EDDY>
 static cudaError_t launch_stage_p(const StageParams<T>& P, cudaStream_t s) {
   using SM = StageSmem<T, TX, TY>;
   static bool attr_set = false;
   if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(stage_kernel<T, TX, TY, MINB, P2>,
+    cudaError_t e = cudaFuncSetAttribute(stage_kernel<T, TX, TY, MINB, P2, EDDY>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(SM)));
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
   dim3 grid((P.nx + TX - 1) / TX, (P.ny + TY - 1) / TY);
-  stage_kernel<T, TX, TY, MINB, P2><<<grid, TX * TY, sizeof(SM), s>>>(P);
+  stage_kernel<T, TX, TY, MINB, P2, EDDY><<<grid, TX * TY, sizeof(SM), s>>>(P);
   return cudaGetLastError();
 }
+// kernels compiled with the eddy-viscosity term run only for solvers that have it
 template <typename T, int TX, int TY, int MINB> static cudaError_t launch_stage_t(const StageParams<T>& P, cudaStream_t s) {
-  return pow2_mesh(P.dx, P.dy) ? launch_stage_p<T, TX, TY, MINB, true>(P, s)
-                               : launch_stage_p<T, TX, TY, MINB, false>(P, s);
+  const bool p2 = pow2_mesh(P.dx, P.dy);
+  if (P.eddy)
+    return p2 ? launch_stage_p<T, TX, TY, MINB, true, true>(P, s) : launch_stage_p<T, TX, TY, MINB, false, true>(P, s);
+  return p2 ? launch_stage_p<T, TX, TY, MINB, true, false>(P, s) : launch_stage_p<T, TX, TY, MINB, false, false>(P, s);
 }
 
 template <> size_t stage_smem_bytes<SV_T>(int tile) {
@@ -56,8 +59,14 @@ template <typename T, int TY, int MINB> static cudaError_t launch_sweep_t(const 
   const long long ntiles = variant_partials(variant, P.nx, P.ny);
   dim3 block(32, WPB);
   dim3 grid(unsigned((ntiles + WPB - 1) / WPB));
-  if (pow2_mesh(P.dx, P.dy)) sweep_kernel<T, TY, WPB, MINB, true><<<grid, block, 0, s>>>(P);
-  else sweep_kernel<T, TY, WPB, MINB, false><<<grid, block, 0, s>>>(P);
+  const bool p2 = pow2_mesh(P.dx, P.dy);
+  if (P.eddy) {
+    if (p2) sweep_kernel<T, TY, WPB, MINB, true, true><<<grid, block, 0, s>>>(P);
+    else sweep_kernel<T, TY, WPB, MINB, false, true><<<grid, block, 0, s>>>(P);
+  } else {
+    if (p2) sweep_kernel<T, TY, WPB, MINB, true, false><<<grid, block, 0, s>>>(P);
+    else sweep_kernel<T, TY, WPB, MINB, false, false><<<grid, block, 0, s>>>(P);
+  }
   return cudaGetLastError();
 }
 
@@ -96,36 +105,45 @@ template <> cudaError_t launch_to_f64<SV_T>(const SV_T* src, double* dst, long l
   return cudaGetLastError();
 }
 
-template <typename T, int TX, int TY, int MINB, bool P2>
+template <typename T, int TX, int TY, int MINB, bool P2, bool EDDY>
 static cudaError_t launch_stage_batch_p(const StageParams<T>* Ps, const long long* tile_start, int ninst,
                                         long long total_tiles, cudaStream_t s) {
   using SM = StageSmem<T, TX, TY>;
   static bool attr_set = false;
   if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(stage_batch_kernel<T, TX, TY, MINB, P2>,
+    cudaError_t e = cudaFuncSetAttribute(stage_batch_kernel<T, TX, TY, MINB, P2, EDDY>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(SM)));
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
   if (total_tiles <= 0) return cudaSuccess;
-  stage_batch_kernel<T, TX, TY, MINB, P2><<<unsigned(total_tiles), TX * TY, sizeof(SM), s>>>(Ps, tile_start, ninst);
+  stage_batch_kernel<T, TX, TY, MINB, P2, EDDY><<<unsigned(total_tiles), TX * TY, sizeof(SM), s>>>(Ps, tile_start,
+                                                                                                     ninst);
   return cudaGetLastError();
 }
 
 template <> cudaError_t launch_stage_batch<SV_T>(const StageParams<SV_T>* Ps, const long long* tile_start, int ninst,
-                                                 long long total_tiles, bool p2, cudaStream_t s) {
-  return p2 ? launch_stage_batch_p<SV_T, 32, 8, 3, true>(Ps, tile_start, ninst, total_tiles, s)
-            : launch_stage_batch_p<SV_T, 32, 8, 3, false>(Ps, tile_start, ninst, total_tiles, s);
+                                                 long long total_tiles, bool p2, bool eddy, cudaStream_t s) {
+  if (eddy)
+    return p2 ? launch_stage_batch_p<SV_T, 32, 8, 3, true, true>(Ps, tile_start, ninst, total_tiles, s)
+              : launch_stage_batch_p<SV_T, 32, 8, 3, false, true>(Ps, tile_start, ninst, total_tiles, s);
+  return p2 ? launch_stage_batch_p<SV_T, 32, 8, 3, true, false>(Ps, tile_start, ninst, total_tiles, s)
+            : launch_stage_batch_p<SV_T, 32, 8, 3, false, false>(Ps, tile_start, ninst, total_tiles, s);
 }
 
 template <> cudaError_t launch_sweep_batch<SV_T>(const StageParams<SV_T>* Ps, const long long* warp_start, int ninst,
-                                                 long long total_warps, bool p2, cudaStream_t s) {
+                                                 long long total_warps, bool p2, bool eddy, cudaStream_t s) {
   constexpr int WPB = 4, TY = 32, MINB = 4;  // variant 8
   if (total_warps <= 0) return cudaSuccess;
   dim3 block(32, WPB);
   dim3 grid(unsigned((total_warps + WPB - 1) / WPB));
-  if (p2) sweep_batch_kernel<SV_T, TY, WPB, MINB, true><<<grid, block, 0, s>>>(Ps, warp_start, ninst);
-  else sweep_batch_kernel<SV_T, TY, WPB, MINB, false><<<grid, block, 0, s>>>(Ps, warp_start, ninst);
+  if (eddy) {
+    if (p2) sweep_batch_kernel<SV_T, TY, WPB, MINB, true, true><<<grid, block, 0, s>>>(Ps, warp_start, ninst);
+    else sweep_batch_kernel<SV_T, TY, WPB, MINB, false, true><<<grid, block, 0, s>>>(Ps, warp_start, ninst);
+  } else {
+    if (p2) sweep_batch_kernel<SV_T, TY, WPB, MINB, true, false><<<grid, block, 0, s>>>(Ps, warp_start, ninst);
+    else sweep_batch_kernel<SV_T, TY, WPB, MINB, false, false><<<grid, block, 0, s>>>(Ps, warp_start, ninst);
+  }
   return cudaGetLastError();
 }
 

@@ -89,6 +89,15 @@ template <typename T> struct StageParams {
   Ctl* ctl;
   double* part;          // per-CTA partials (see part_* offsets)
   long long nblk;
+  // eddy viscosity (run by the kernels compiled with it): 0 off, 1 constant coefficient
+  // (eddy_mup per cell, else eddy_mu), 2 Smagorinsky (eddy_c + eddy_s * area * |strain|)
+  int eddy;
+  T eddy_mu, eddy_c, eddy_s;
+  const T* eddy_mup;
+  // the momentum source terms in configuration order, 2 bits per slot: 1 roughness,
+  // 2 energy loss, 3 eddy viscosity (each adds to du/dt and dv/dt, so the order sets the
+  // rounding); used by the kernels compiled with eddy viscosity
+  int term_order;
 };
 
 // partial layout: [0, nblk) cn max, [nblk, 2nblk) cn min, [2nblk, 3nblk) volume,
@@ -181,13 +190,14 @@ template <> struct MkDivX<DivF> { __device__ static DivF make(double d) { return
 // fluxes; returns the rain rate added, the depth rate removed by the head assignment and the
 // depth rate that entered through mesh-edge faces (the reference's walls pass flow through
 // their one-sided branches; taken before any boundary assignment).
-template <typename T, typename CC>
+template <typename T, typename CC, bool EDDY = false>
 __device__ __forceinline__ void cell_dudt(const StageParams<T>& P, const DevForcing& fc, const CC& c,
                                           long long g, int gx,
                                           int gy, T h, T u, T v, T dhdx, T dhdy, T dzdx, T dzdy,
                                           const FaceF<T>& fw, const FaceF<T>& fe, const FaceF<T>& fs,
                                           const FaceF<T>& fn, T& kh, T& ku, T& kv, double& rain,
-                                          double& removed, double& wall, T* n_out, T* sf_out) {
+                                          double& removed, double& wall, T* n_out, T* sf_out,
+                                          const EddyIn<T>* ed = nullptr) {
   T dhdt = c.divx(fw.h - fe.h) + c.divy(fs.h - fn.h);
   T dudt = c.divx(fw.u - fe.u) + c.divy(fs.u - fn.u);
   T dvdt = c.divx(fw.v - fe.v) + c.divy(fs.v - fn.v);
@@ -215,8 +225,35 @@ __device__ __forceinline__ void cell_dudt(const StageParams<T>& P, const DevForc
   auto do_eloss = [&]() {
     if (P.efx) energy_loss_apply<T>(h, u, v, ld(P.efx, g), ld(P.efy, g), c, dudt, dvdt);
   };
-  if (P.eloss_first) { do_eloss(); do_manning(); }
-  else { do_manning(); do_eloss(); }
+  if constexpr (!EDDY) {
+    if (P.eloss_first) { do_eloss(); do_manning(); }
+    else { do_manning(); do_eloss(); }
+  } else {
+    // each term's increments depend on the cell's state only; they are added in the
+    // configured order
+    T fu1 = T(0), fv1 = T(0), fu2 = T(0), fv2 = T(0), fu3 = T(0), fv3 = T(0);
+    bool on1 = false, on2 = false, on3 = false;
+    if (P.manning) {
+      T ns = P.man_p[0] ? ld(P.man_p[0], g) : P.man_s[0];
+      T nd = P.man_p[1] ? (P.man_p[1] == P.man_p[0] ? ns : ld(P.man_p[1], g)) : P.man_s[1];
+      T ds = P.man_p[2] ? ld(P.man_p[2], g) : P.man_s[2];
+      T dd = P.man_p[3] ? ld(P.man_p[3], g) : P.man_s[3];
+      on1 = manning_term<T>(h, u, v, ns, nd, ds, dd, c, fu1, fv1, n_out, sf_out);
+    }
+    if (P.efx) on2 = energy_loss_term<T>(h, u, v, ld(P.efx, g), ld(P.efy, g), c, fu2, fv2);
+    if (P.eddy) {
+      const T mu = P.eddy == 2 ? smagorinsky_mu<T>(P.eddy_c, P.eddy_s, T(P.cell_area), *ed)
+                               : (P.eddy_mup ? ld(P.eddy_mup, g) : P.eddy_mu);
+      on3 = eddy_term<T>(h, u, v, mu, *ed, c, fu3, fv3);
+    }
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+      const int t = (P.term_order >> (2 * s)) & 3;
+      if (t == 1 && on1) { dudt = dudt + fu1; dvdt = dvdt + fv1; }
+      else if (t == 2 && on2) { dudt = dudt + fu2; dvdt = dvdt + fv2; }
+      else if (t == 3 && on3) { dudt = dudt + fu3; dvdt = dvdt + fv3; }
+    }
+  }
   if (P.irate) {  // infiltration (InfiltrationSourceTerm.cpp:43-62), capacity consumed in place
     T cap = P.icap[g];
     T dh = infiltration_depth<T>(h, ld(P.irate, g), cap, c);
@@ -277,17 +314,17 @@ __device__ __forceinline__ void cell_dudt(const StageParams<T>& P, const DevForc
 
 // One cell of one stage after its four face fluxes are known: dU/dt, then the Runge-Kutta
 // combination (RungeKutta.hpp:377-388) and, on the last stage, the CFL quantity and volume.
-template <typename T, typename CC>
+template <typename T, typename CC, bool EDDY = false>
 __device__ __forceinline__ void finish_cell(const StageParams<T>& P, const DevForcing& fc, const CC& c,
                                             long long g, int gx, int gy, T h, T u, T v, T dhdx, T dhdy, T dzdx,
                                             T dzdy, const FaceF<T>& fw, const FaceF<T>& fe, const FaceF<T>& fs,
                                             const FaceF<T>& fn, bool first, bool last, int cur, double dt_d,
                                             double& rain, double& removed, double& walls, double& xcfl,
-                                            double& xcfl_min, double& vol) {
+                                            double& xcfl_min, double& vol, const EddyIn<T>* ed = nullptr) {
   T kh, ku, kv;
   double r_, o_, w_;
-  cell_dudt<T>(P, fc, c, g, gx, gy, h, u, v, dhdx, dhdy, dzdx, dzdy, fw, fe, fs, fn, kh, ku, kv, r_, o_, w_,
-               (T*)nullptr, (T*)nullptr);
+  cell_dudt<T, CC, EDDY>(P, fc, c, g, gx, gy, h, u, v, dhdx, dhdy, dzdx, dzdy, fw, fe, fs, fn, kh, ku, kv, r_, o_,
+                         w_, (T*)nullptr, (T*)nullptr, ed);
   rain += r_;
   removed += o_;
   walls += w_;
@@ -391,7 +428,7 @@ struct StageSmem {
 };
 
 // One TX x TY tile of one stage: bx, by = tile coordinates, blk = partial-sum slot.
-template <typename T, int TX, int TY, bool P2>
+template <typename T, int TX, int TY, bool P2, bool EDDY>
 __device__ __forceinline__ void stage_tile(const StageParams<T>& P, int bx, int by, long long blk,
                                            StageSmem<T, TX, TY>& s) {
   using DX = DivX<T, P2>;
@@ -505,8 +542,20 @@ __device__ __forceinline__ void stage_tile(const StageParams<T>& P, int bx, int 
     FaceF<T> fs{s.fyf[0][ty][tx], s.fyf[1][ty][tx], s.fyf[2][ty][tx], s.fyf[3][ty][tx]};
     FaceF<T> fn{s.fyf[0][ty + 1][tx], s.fyf[1][ty + 1][tx], s.fyf[2][ty + 1][tx], s.fyf[3][ty + 1][tx]};
     const DevForcing fc = *P.fc;
-    finish_cell<T>(P, fc, c, g, gx, gy, h, u, v, s.slp[0][sy][sx], s.slp[4][sy][sx], s.slp[3][sy][sx],
-                   s.slp[7][sy][sx], fw, fe, fs, fn, first, last, cur, dt_d, rain, removed, walls, xcfl, xcfl_min, vol);
+    EddyIn<T> ed{};
+    if constexpr (EDDY) {
+      if (P.eddy) {  // second derivatives from the slopes of the tile + ring
+        const bool hasW = gx > 0, hasE = gx < nx - 1, hasN = gy < ny - 1, hasS = gy > 0;
+        ed.ux = s.slp[1][sy][sx]; ed.uy = s.slp[5][sy][sx]; ed.vx = s.slp[2][sy][sx]; ed.vy = s.slp[6][sy][sx];
+        ed.uxx = minmod3<T>(s.slp[1][sy][sx - 1], hasW, ed.ux, hasE, s.slp[1][sy][sx + 1], divx);
+        ed.vxx = minmod3<T>(s.slp[2][sy][sx - 1], hasW, ed.vx, hasE, s.slp[2][sy][sx + 1], divx);
+        ed.uyy = minmod3<T>(s.slp[5][sy + 1][sx], hasN, ed.uy, hasS, s.slp[5][sy - 1][sx], divy);
+        ed.vyy = minmod3<T>(s.slp[6][sy + 1][sx], hasN, ed.vy, hasS, s.slp[6][sy - 1][sx], divy);
+      }
+    }
+    finish_cell<T, CellCtx<T, DX>, EDDY>(P, fc, c, g, gx, gy, h, u, v, s.slp[0][sy][sx], s.slp[4][sy][sx],
+                                         s.slp[3][sy][sx], s.slp[7][sy][sx], fw, fe, fs, fn, first, last, cur, dt_d,
+                                         rain, removed, walls, xcfl, xcfl_min, vol, &ed);
   }
   if (last && !(P.mode & M_DEBUGK)) {
     double mx = block_max<NT>(xcfl, s.red);
@@ -530,18 +579,18 @@ __device__ __forceinline__ void stage_tile(const StageParams<T>& P, int bx, int 
   }
 }
 
-template <typename T, int TX, int TY, int MINB, bool P2>
+template <typename T, int TX, int TY, int MINB, bool P2, bool EDDY>
 __global__ void __launch_bounds__(TX * TY, MINB) stage_kernel(const StageParams<T> P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   auto& s = *reinterpret_cast<StageSmem<T, TX, TY>*>(smem_raw);
-  stage_tile<T, TX, TY, P2>(P, blockIdx.x, blockIdx.y, (long long)blockIdx.y * gridDim.x + blockIdx.x, s);
+  stage_tile<T, TX, TY, P2, EDDY>(P, blockIdx.x, blockIdx.y, (long long)blockIdx.y * gridDim.x + blockIdx.x, s);
 }
 
 // Batched stage: one launch covers every tile of every instance of a batch. tile_start has
 // ninst + 1 entries (prefix sums of the instances' tile counts); each CTA finds its instance,
 // copies that instance's parameters to shared memory and runs the same tile body. Instances
 // whose step is finished (their controller's done flag) return at once.
-template <typename T, int TX, int TY, int MINB, bool P2>
+template <typename T, int TX, int TY, int MINB, bool P2, bool EDDY>
 __global__ void __launch_bounds__(TX * TY, MINB)
     stage_batch_kernel(const StageParams<T>* __restrict__ Ps, const long long* __restrict__ tile_start, int ninst) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -562,7 +611,7 @@ __global__ void __launch_bounds__(TX * TY, MINB)
   __syncthreads();
   const long long local = tile - tile_start[inst_sh];
   const int tiles_x = (Psh.nx + TX - 1) / TX;
-  stage_tile<T, TX, TY, P2>(Psh, int(local % tiles_x), int(local / tiles_x), local, s);
+  stage_tile<T, TX, TY, P2, EDDY>(Psh, int(local % tiles_x), int(local / tiles_x), local, s);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -644,7 +693,7 @@ __device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefe
 // One warp's strip `gw` (row-major over strips of kSweepOut columns x TY rows) of one
 // solver's stage. Called by the single-solver kernel (P in parameter space) and by the
 // batched kernel (P in shared memory).
-template <typename T, int TY, bool P2>
+template <typename T, int TY, bool P2, bool EDDY>
 __device__ __forceinline__ void sweep_strip(const StageParams<T>& P, long long gw) {
   using DX = DivX<T, P2>;
   const Ctl* ctl = P.ctl;
@@ -692,6 +741,7 @@ __device__ __forceinline__ void sweep_strip(const StageParams<T>& P, long long g
 
   RowV<T> Rm{}, R0{}, Rp{};   // rows k-2, k-1, k
   SlopeV<T> Sm{}, S0{};       // slopes of rows k-2, k-1
+  T Smm_uy = T(0), Smm_vy = T(0);  // y slopes of u, v of row k-3 (eddy viscosity)
   T fyA[3] = {}, fyB[3] = {};  // (U[k-1]-U[k-2])/dy, (U[k]-U[k-1])/dy
   FaceF<T> FS{}, FN{};
   double rain = 0.0, removed = 0.0, walls = 0.0, xcfl = 0.0, xmin = 1.0 / 0.0, vol = 0.0;
@@ -725,6 +775,7 @@ __device__ __forceinline__ void sweep_strip(const StageParams<T>& P, long long g
     prefetch_rows(k);
     Rm = R0; R0 = Rp; Rp = Rnext;
     if (k < y0 + TY + 1) Rnext = load_row(k + 1);  // prefetch the next row
+    if constexpr (EDDY) { Smm_uy = Sm.uy; Smm_vy = Sm.vy; }
     Sm = S0;
     fyA[0] = fyB[0]; fyA[1] = fyB[1]; fyA[2] = fyB[2];
     // forward y quotients between rows k-1 and k
@@ -776,6 +827,25 @@ __device__ __forceinline__ void sweep_strip(const StageParams<T>& P, long long g
       const int r = k - 2;
       const CellV<T> me = mkcell(Rm, Sm);
       const CellV<T> lf = shfl_cell_up(me);
+      EddyIn<T> ed{};
+      if constexpr (EDDY) {
+        if (P.eddy) {  // second derivatives of row r: x by shuffles, y from rows r+1, r, r-1
+          ed.ux = Sm.ux; ed.uy = Sm.uy; ed.vx = Sm.vx; ed.vy = Sm.vy;
+          {
+            T r_ = dn1(Sm.ux), l_ = up1(Sm.ux);
+            T fq = divx(r_ - Sm.ux);
+            ed.uxx = minmod3q<T>(up1(fq), hasW, fq, hasE, divx(r_ - l_));
+          }
+          {
+            T r_ = dn1(Sm.vx), l_ = up1(Sm.vx);
+            T fq = divx(r_ - Sm.vx);
+            ed.vxx = minmod3q<T>(up1(fq), hasW, fq, hasE, divx(r_ - l_));
+          }
+          const bool hasN = r < ny - 1, hasS = r > 0;  // Y axis: north is the left neighbour
+          ed.uyy = minmod3q<T>(divy(Sm.uy - S0.uy), hasN, divy(Smm_uy - Sm.uy), hasS, divy(Smm_uy - S0.uy));
+          ed.vyy = minmod3q<T>(divy(Sm.vy - S0.vy), hasN, divy(Smm_vy - Sm.vy), hasS, divy(Smm_vy - S0.vy));
+        }
+      }
       FaceF<T> FW{T(0), T(0), T(0), T(0)};
       if (wface_lane && r < ny) {
         const int edge = gx == 0 ? -1 : (gx == nx ? 1 : 0);
@@ -790,8 +860,9 @@ __device__ __forceinline__ void sweep_strip(const StageParams<T>& P, long long g
       const FaceF<T> FE{dn1(FW.h), dn1(FW.u), dn1(FW.v), dn1(FW.z)};
       if (out_lane && r < ny) {
         const long long g = (long long)r * nx + gx;
-        finish_cell<T>(P, fc, c, g, gx, r, me.h, me.u, me.v, me.dhdx, me.dhdy, me.dzdx, me.dzdy, FW, FE, FS, FN,
-                       first, last, cur, dt_d, rain, removed, walls, xcfl, xmin, vol);
+        finish_cell<T, CellCtx<T, DX>, EDDY>(P, fc, c, g, gx, r, me.h, me.u, me.v, me.dhdx, me.dhdy, me.dzdx,
+                                             me.dzdy, FW, FE, FS, FN, first, last, cur, dt_d, rain, removed, walls,
+                                             xcfl, xmin, vol, &ed);
       }
     }
     FS = FN;
@@ -814,20 +885,20 @@ __device__ __forceinline__ void sweep_strip(const StageParams<T>& P, long long g
   }
 }
 
-template <typename T, int TY, int WPB, int MINB, bool P2>
+template <typename T, int TY, int WPB, int MINB, bool P2, bool EDDY>
 __global__ void __launch_bounds__(32 * WPB, MINB) sweep_kernel(const __grid_constant__ StageParams<T> P) {
   if (P.ctl->done) return;
   const int tiles_x = (P.nx + kSweepOut - 1) / kSweepOut;
   const long long ntiles = (long long)tiles_x * ((P.ny + TY - 1) / TY);
   const long long gw = (long long)blockIdx.x * WPB + threadIdx.y;
   if (gw >= ntiles) return;  // whole warp: no block-level synchronisation below
-  sweep_strip<T, TY, P2>(P, gw);
+  sweep_strip<T, TY, P2, EDDY>(P, gw);
 }
 
 // Batched column sweep: the strips of every instance of a batch, warp_start[i] being the
 // first global warp of instance i. Each warp finds its instance, stages its parameters in
 // shared memory and sweeps its strip; instances whose step is finished return at once.
-template <typename T, int TY, int WPB, int MINB, bool P2>
+template <typename T, int TY, int WPB, int MINB, bool P2, bool EDDY>
 __global__ void __launch_bounds__(32 * WPB, MINB)
     sweep_batch_kernel(const StageParams<T>* __restrict__ Ps, const long long* __restrict__ warp_start, int ninst) {
   __shared__ __align__(16) StageParams<T> Psh[WPB];
@@ -851,7 +922,7 @@ __global__ void __launch_bounds__(32 * WPB, MINB)
   __syncwarp();
   const StageParams<T>& P = Psh[threadIdx.y];
   if (P.ctl->done) return;
-  sweep_strip<T, TY, P2>(P, gw - warp_start[inst]);
+  sweep_strip<T, TY, P2, EDDY>(P, gw - warp_start[inst]);
 }
 
 // Bed slopes once per bed upload (SaintVenantConstants, Constants.cpp:39-40).
@@ -1250,8 +1321,18 @@ __global__ void debug_cell_kernel(const StageParams<T> P, const DebugParams<T> D
   const DevForcing fc = *P.fc;
   T kh, ku, kv;
   double rain, removed, wall;
-  cell_dudt<T>(P, fc, c, g, gx, gy, D.h[g], D.u[g], D.v[g], D.dhdx[g], D.dhdy[g], D.dzdx[g], D.dzdy[g], fw, fe, fs,
-               fn, kh, ku, kv, rain, removed, wall, nh + g, sf + g);
+  EddyIn<T> ed{};
+  if (P.eddy) {  // second derivatives from the mesh-wide slope fields
+    const int nx = P.nx;
+    const bool hasW = gx > 0, hasE = gx < nx - 1, hasN = gy < P.ny - 1, hasS = gy > 0;
+    ed.ux = D.dudx[g]; ed.uy = D.dudy[g]; ed.vx = D.dvdx[g]; ed.vy = D.dvdy[g];
+    ed.uxx = minmod3<T>(hasW ? D.dudx[g - 1] : ed.ux, hasW, ed.ux, hasE, hasE ? D.dudx[g + 1] : ed.ux, c.divx);
+    ed.vxx = minmod3<T>(hasW ? D.dvdx[g - 1] : ed.vx, hasW, ed.vx, hasE, hasE ? D.dvdx[g + 1] : ed.vx, c.divx);
+    ed.uyy = minmod3<T>(hasN ? D.dudy[g + nx] : ed.uy, hasN, ed.uy, hasS, hasS ? D.dudy[g - nx] : ed.uy, c.divy);
+    ed.vyy = minmod3<T>(hasN ? D.dvdy[g + nx] : ed.vy, hasN, ed.vy, hasS, hasS ? D.dvdy[g - nx] : ed.vy, c.divy);
+  }
+  cell_dudt<T, CellCtx<T>, true>(P, fc, c, g, gx, gy, D.h[g], D.u[g], D.v[g], D.dhdx[g], D.dhdy[g], D.dzdx[g],
+                                 D.dzdy[g], fw, fe, fs, fn, kh, ku, kv, rain, removed, wall, nh + g, sf + g, &ed);
   P.Kout[0][g] = kh; P.Kout[1][g] = ku; P.Kout[2][g] = kv;
 }
 

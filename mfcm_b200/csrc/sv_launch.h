@@ -46,14 +46,14 @@ template <typename T> cudaError_t launch_volume(const T* h, int nx, int ny, doub
 template <typename T> cudaError_t launch_debug(const StageParams<T>& P, const DebugParams<T>& D, T* nh, T* sf,
                                                cudaStream_t s);
 // batched launches: every tile of every instance (tiled 32 x 8 kernel, 3 CTAs/SM); p2 when
-// every instance's dx and dy are powers of two
+// every instance's dx and dy are powers of two, eddy when any instance has eddy viscosity
 template <typename T> cudaError_t launch_stage_batch(const StageParams<T>* Ps, const long long* tile_start, int ninst,
-                                                     long long total_tiles, bool p2, cudaStream_t s);
+                                                     long long total_tiles, bool p2, bool eddy, cudaStream_t s);
 // batches of FP64 instances use the tiled variant 1; FP32 batches the column sweep of
 // variant 8 (launch_sweep_batch), the fastest single-solver kernels of each precision
 template <typename T> constexpr int batch_variant() { return sizeof(T) == 8 ? 1 : 8; }
 template <typename T> cudaError_t launch_sweep_batch(const StageParams<T>* Ps, const long long* warp_start, int ninst,
-                                                     long long total_warps, bool p2, cudaStream_t s);
+                                                     long long total_warps, bool p2, bool eddy, cudaStream_t s);
 cudaError_t launch_finalize(const FinalizeParams& F, cudaStream_t s);
 cudaError_t launch_finalize_batch(const FinalizeParams* Fs, int ninst, cudaStream_t s);
 cudaError_t launch_begin_queue(const FinalizeParams* Fs, int n, cudaStream_t s);

@@ -226,12 +226,20 @@ struct Params {
   int manning = 1;            // Manning source term present
   int head_first = 0;         // boundary order: 0 = discharge then head, 1 = head then discharge
   int eloss_first = 0;        // source order: 1 = energy loss listed before Manning roughness
+  // EddyViscositySourceTerm (EddyViscositySourceTerm.cpp:112-137): 0 off, 1 constant
+  // coefficient (the F_EDDY_MU field when set, else eddy_mu), 2 Smagorinsky
+  int eddy = 0;
+  double eddy_mu = 1.0, eddy_c = 0.05, eddy_s = 0.5;
+  // the momentum terms in configuration order (1 roughness, 2 energy loss, 3 eddy viscosity);
+  // when not set, roughness and energy loss per eloss_first, then eddy viscosity
+  int term_order[3] = {1, 2, 3};
+  int order_set = 0;
 };
 
 enum Field : int {
   F_Z = 0, F_H = 1, F_U = 2, F_V = 3, F_N_SHALLOW = 4, F_N_DEEP = 5, F_D_SHALLOW = 6, F_D_DEEP = 7,
   F_QBDY0 = 8, F_QBDY1 = 9, F_HBDY0 = 10, F_HBDY1 = 11, F_RAIN_PATTERN = 12,
-  F_INFIL_RATE = 13, F_INFIL_CAP = 14, F_ELOSS_FX = 15, F_ELOSS_FY = 16,
+  F_INFIL_RATE = 13, F_INFIL_CAP = 14, F_ELOSS_FX = 15, F_ELOSS_FY = 16, F_EDDY_MU = 18,
   F_DHDT = 20, F_DUDT = 21, F_DVDT = 22, F_DHDX = 23, F_DUDX = 24, F_DVDX = 25,
   F_DHDY = 26, F_DUDY = 27, F_DVDY = 28, F_DZDX = 29, F_DZDY = 30, F_NH = 31, F_SF = 32,
   F_FLUX_H = 40, F_FLUX_U = 41, F_FLUX_V = 42, F_FLUX_Z = 43, F_FLUX_BRANCH = 44,
@@ -276,6 +284,8 @@ class SolverBase {
   virtual void set_field(int id, const double* src, size_t n) = 0;
   virtual void get_field(int id, double* dst, size_t n) const = 0;
   virtual void set_manning(double ns, double nd, double ds, double dd) = 0;
+  virtual void set_eddy(int mode, double mu, double mc, double ms) = 0;
+  virtual void set_source_order(const int* terms, int n) = 0;
   virtual void set_forcing(const Forcing& f) = 0;
   virtual void set_dt(double dt) = 0;
   virtual double get_dt() const = 0;
@@ -308,6 +318,9 @@ class Solver final : public SolverBase {
   Vec irate, icap;                      // InfiltrationSourceTerm (InfiltrationSourceTerm.hpp:106-109)
   Vec efx, efy;                         // EnergyLossSourceTerm (EnergyLossSourceTerm.hpp:199-202)
   unsigned present = 0;                 // which of those four fields were set (bits 0-3)
+  Vec emu;                              // eddy viscosity coefficient field "mu"
+  bool emu_set = false;
+  Vec d2udx2, d2udy2, d2vdx2, d2vdy2;   // EddyViscositySourceTerm.hpp:154-157
   Forcing forcing;
   TT dt_;
   Stats st_;
@@ -331,6 +344,8 @@ class Solver final : public SolverBase {
     hb0.assign(n, std::numeric_limits<T>::quiet_NaN()); hb1.assign(n, std::numeric_limits<T>::quiet_NaN());
     pattern.assign(n, T(0));
     irate.assign(n, T(0)); icap.assign(n, T(0)); efx.assign(n, T(0)); efy.assign(n, T(0));
+    emu.assign(n, T(0));
+    for (Vec* d : {&d2udx2, &d2udy2, &d2vdx2, &d2vdy2}) d->assign(n, T(0));
     dt_ = TT(p.initial_dt);
     rain_sum_.assign(N, 0.0); out_sum_.assign(N, 0.0); wall_sum_.assign(N, 0.0);
     update_constants();
@@ -354,7 +369,7 @@ class Solver final : public SolverBase {
       case F_D_DEEP: return &dd; case F_QBDY0: return &qb0; case F_QBDY1: return &qb1;
       case F_HBDY0: return &hb0; case F_HBDY1: return &hb1; case F_RAIN_PATTERN: return &pattern;
       case F_INFIL_RATE: return &irate; case F_INFIL_CAP: return &icap;
-      case F_ELOSS_FX: return &efx; case F_ELOSS_FY: return &efy;
+      case F_ELOSS_FX: return &efx; case F_ELOSS_FY: return &efy; case F_EDDY_MU: return &emu;
       case F_DHDT: return &K[0].h; case F_DUDT: return &K[0].u; case F_DVDT: return &K[0].v;
       case F_DHDX: return &dUdx.h; case F_DUDX: return &dUdx.u; case F_DVDX: return &dUdx.v;
       case F_DHDY: return &dUdy.h; case F_DUDY: return &dUdy.u; case F_DVDY: return &dUdy.v;
@@ -382,6 +397,7 @@ class Solver final : public SolverBase {
     for (size_t i = 0; i < n; ++i) (*f)[i] = T(src[i]);
     if (id == F_Z) update_constants();
     if (id >= F_INFIL_RATE && id <= F_ELOSS_FY) present |= 1u << (id - F_INFIL_RATE);
+    if (id == F_EDDY_MU) emu_set = true;
   }
   void get_field(int id, double* dst, size_t n) const override {
     const Vec* f = field_ptr(id);
@@ -391,6 +407,23 @@ class Solver final : public SolverBase {
   void set_manning(double a, double b, double c, double d) override {
     std::fill(ns.begin(), ns.end(), T(a)); std::fill(nd.begin(), nd.end(), T(b));
     std::fill(ds.begin(), ds.end(), T(c)); std::fill(dd.begin(), dd.end(), T(d));
+  }
+  void set_eddy(int mode, double mu, double mc, double ms) override {
+    if (mode < 0 || mode > 2) throw std::runtime_error("unknown eddy viscosity mode");
+    p.eddy = mode; p.eddy_mu = mu; p.eddy_c = mc; p.eddy_s = ms;
+  }
+  void set_source_order(const int* terms, int n) override {
+    if (n < 0 || n > 3) throw std::runtime_error("at most three source terms");
+    bool seen[4] = {};
+    int k = 0;
+    for (int i = 0; i < n; ++i) {
+      if (terms[i] < 1 || terms[i] > 3 || seen[terms[i]]) throw std::runtime_error("bad source order");
+      seen[terms[i]] = true;
+      p.term_order[k++] = terms[i];
+    }
+    for (int x = 1; x <= 3; ++x)
+      if (!seen[x]) p.term_order[k++] = x;
+    p.order_set = 1;
   }
   void set_dt(double dt) override { dt_ = TT(dt); }
   double get_dt() const override { return double(dt_); }
@@ -611,6 +644,31 @@ class Solver final : public SolverBase {
     }
   }
 
+  // SmagorinskyCoefficientKernel::operator() (EddyViscositySourceTerm.cpp:97-110) when
+  // Smagorinsky, else the coefficient field (or its default); then
+  // EddyViscositySourceKernel::operator() (EddyViscositySourceTerm.cpp:46-78). The square
+  // pow(x, 2) is taken as x * x.
+  void eddy_cell(size_t c, const State& S, State& D, double timestep) {
+    T mu;
+    if (p.eddy == 2) {
+      T cell_area = T(m.cell_area());
+      T a = std::fabs(dUdy.u[c]) + std::fabs(dUdx.v[c]);
+      mu = T(p.eddy_c) + T(p.eddy_s) * cell_area *
+           std::sqrt(dUdx.u[c] * dUdx.u[c] + dUdy.v[c] * dUdy.v[c] + T(0.5) * (a * a));
+    } else {
+      mu = emu_set ? emu[c] : T(p.eddy_mu);
+    }
+    T h = S.h[c], u = S.u[c], v = S.v[c];
+    if (h > 1e-6) {
+      T dudt = -mu * (d2udx2[c] + d2udy2[c]);
+      T dvdt = -mu * (d2vdx2[c] + d2vdy2[c]);
+      if (std::fabs(dudt * timestep) > std::fabs(u) && ssign(dudt * timestep) != ssign(u)) dudt = -u / timestep;
+      if (std::fabs(dvdt * timestep) > std::fabs(v) && ssign(dvdt * timestep) != ssign(v)) dvdt = -v / timestep;
+      D.u[c] += dudt;
+      D.v[c] += dvdt;
+    }
+  }
+
   // InfiltrationSourceKernel::operator() (InfiltrationSourceTerm.cpp:43-62): the capacity
   // field is consumed at every evaluation, repeated timesteps included.
   void infiltration_cell(size_t c, const State& S, State& D, double timestep) {
@@ -705,8 +763,28 @@ class Solver final : public SolverBase {
 #pragma omp parallel for schedule(static)
       for (size_t c = 0; c < n; ++c) eloss_cell(c, S, D, double(timestep));
     };
-    if (p.eloss_first) { run_eloss(); run_manning(); }
-    else { run_manning(); run_eloss(); }
+    auto run_eddy = [&]() {
+      if (!p.eddy) return;
+      // second derivatives: Minmod3 of the slopes along the same axis
+      // (EddyViscositySourceTerm.hpp:222-228)
+#pragma omp parallel for schedule(static)
+      for (size_t i = 0; i < n; ++i) slope_x<T>(m, dUdx.u.data(), d2udx2.data(), i);
+#pragma omp parallel for schedule(static)
+      for (size_t i = 0; i < n; ++i) slope_y<T>(m, dUdy.u.data(), d2udy2.data(), i);
+#pragma omp parallel for schedule(static)
+      for (size_t i = 0; i < n; ++i) slope_x<T>(m, dUdx.v.data(), d2vdx2.data(), i);
+#pragma omp parallel for schedule(static)
+      for (size_t i = 0; i < n; ++i) slope_y<T>(m, dUdy.v.data(), d2vdy2.data(), i);
+#pragma omp parallel for schedule(static)
+      for (size_t c = 0; c < n; ++c) eddy_cell(c, S, D, double(timestep));
+    };
+    int order[3] = {p.term_order[0], p.term_order[1], p.term_order[2]};
+    if (!p.order_set && p.eloss_first) { order[0] = 2; order[1] = 1; }
+    for (int t : order) {
+      if (t == 1) run_manning();
+      else if (t == 2) run_eloss();
+      else run_eddy();
+    }
     if ((present & 3u) == 3u) {
 #pragma omp parallel for schedule(static)
       for (size_t c = 0; c < n; ++c) infiltration_cell(c, S, D, double(timestep));

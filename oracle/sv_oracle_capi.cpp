@@ -71,6 +71,14 @@ int svo_set_manning(void* h, double a, double b, double c, double d) {
   static_cast<svo::SolverBase*>(h)->set_manning(a, b, c, d);
   return 0;
 }
+int svo_set_eddy_viscosity(void* h, int mode, double mu, double mc, double ms) {
+  try { static_cast<svo::SolverBase*>(h)->set_eddy(mode, mu, mc, ms); return 0; }
+  catch (const std::exception& e) { return fail(e); }
+}
+int svo_set_source_order(void* h, const int* terms, int n) {
+  try { static_cast<svo::SolverBase*>(h)->set_source_order(terms, n); return 0; }
+  catch (const std::exception& e) { return fail(e); }
+}
 int svo_set_forcing(void* h, const sv_forcing* f) {
   svo::Forcing g;
   g.rain_kind = f->rain_kind; g.rain_q0 = f->rain_q0; g.rain_q1 = f->rain_q1;

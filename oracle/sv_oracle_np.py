@@ -228,12 +228,15 @@ def face_fluxes(h, u, v, z, sl, nx, ny, dx, dy):
 
 def update_dudt(h, u, v, z, dx, dy, *, manning=None, qbdy=None, hbdy=None, time_now=0.0, timestep=1.0,
                 step_length=60.0, rain_mode="reference", head_first=False, eloss=None, eloss_first=False,
-                infil=None, stage=False):
+                infil=None, stage=False, eddy=None, order=None):
     """dU/dt of one state (SaintVenantSolver::update_dUdt, Solver.cpp:73-114). Arrays are
     (ny, nx). manning = (n_shallow, n_deep, d_shallow, d_deep) per-cell arrays or None (no
     roughness term); eloss = (fx, fy) energy-loss coefficients or None; infil = (rate,
     capacity) or None; qbdy = (q0, q1) and hbdy = (h0, h1) per-cell boundary values or None,
-    hbdy holding water levels when `stage` (a stage boundary). Returns a dict of slopes, face
+    hbdy holding water levels when `stage` (a stage boundary). eddy = ("constant", mu) with mu
+    a scalar or per-cell array, or ("smagorinsky", mu_const, mu_smag), or None; order lists the
+    momentum terms ("manning", "energy loss", "eddy viscosity") in configuration order
+    (default: per eloss_first, then eddy viscosity). Returns a dict of slopes, face
     fields, dhdt/dudt/dvdt and, with infiltration, the capacity left ("infil_cap")."""
     ny, nx = h.shape
     sl = {"dhdx": slope_x(h, dx), "dudx": slope_x(u, dx), "dvdx": slope_x(v, dx),
@@ -291,12 +294,35 @@ def update_dudt(h, u, v, z, dx, dy, *, manning=None, qbdy=None, hbdy=None, time_
             ev = np.where(capv, -v / timestep, ev)
             return np.where(wet, dudt + eu, dudt), np.where(wet, dvdt + ev, dvdt)
 
-        if eloss_first:
-            dudt, dvdt = energy_loss(dudt, dvdt)
-            dudt, dvdt = roughness(dudt, dvdt)
-        else:
-            dudt, dvdt = roughness(dudt, dvdt)
-            dudt, dvdt = energy_loss(dudt, dvdt)
+        def eddy_viscosity(dudt, dvdt):
+            # SmagorinskyCoefficientKernel and EddyViscositySourceKernel
+            # (EddyViscositySourceTerm.cpp:46-110); second derivatives are Minmod3 slopes of
+            # the slopes along the same axis (EddyViscositySourceTerm.hpp:222-228)
+            if eddy is None:
+                return dudt, dvdt
+            uxx, uyy = slope_x(sl["dudx"], dx), slope_y(sl["dudy"], dy)
+            vxx, vyy = slope_x(sl["dvdx"], dx), slope_y(sl["dvdy"], dy)
+            if eddy[0] == "smagorinsky":
+                a = np.abs(sl["dudy"]) + np.abs(sl["dvdx"])
+                strain = np.sqrt((sl["dudx"] * sl["dudx"] + sl["dvdy"] * sl["dvdy"]) + 0.5 * (a * a))
+                mu = eddy[1] + (eddy[2] * (dx * dy)) * strain
+            else:
+                mu = np.broadcast_to(np.asarray(eddy[1], dtype=np.float64), h.shape)
+            wet = h > 1e-6
+            eu = (-mu) * (uxx + uyy)
+            ev = (-mu) * (vxx + vyy)
+            capu = (np.abs(eu * timestep) > np.abs(u)) & (sign(eu * timestep) != sign(u))
+            capv = (np.abs(ev * timestep) > np.abs(v)) & (sign(ev * timestep) != sign(v))
+            eu = np.where(capu, -u / timestep, eu)
+            ev = np.where(capv, -v / timestep, ev)
+            return np.where(wet, dudt + eu, dudt), np.where(wet, dvdt + ev, dvdt)
+
+        terms = {"manning": roughness, "energy loss": energy_loss, "eddy viscosity": eddy_viscosity}
+        if order is None:
+            order = ["energy loss", "manning"] if eloss_first else ["manning", "energy loss"]
+        order = list(order) + [t for t in ("manning", "energy loss", "eddy viscosity") if t not in order]
+        for t in order:
+            dudt, dvdt = terms[t](dudt, dvdt)
         cap_left = None
         if infil is not None:
             # InfiltrationSourceKernel::operator() (InfiltrationSourceTerm.cpp:43-62)

@@ -65,7 +65,7 @@ def test_deck_fields_series_and_boundaries():
 
 def test_unsupported_features_are_named():
     base = "mesh\n{\ncell count == 4 4\ncell size == 1 1\n}\nscheme == runge-kutta\n{\nend time == 1\n}\n"
-    for extra, what in (("source term == eddy viscosity\n", "eddy viscosity"),
+    for extra, what in (("source term == eddy viscosity\n{\nviscosity type == laminar\n}\n", "laminar"),
                         ("boundary == weir\n", "weir")):
         with pytest.raises(ConfigError, match=what):
             config.Model(read_mf(base + extra))
@@ -74,9 +74,16 @@ def test_unsupported_features_are_named():
         m.field("h", 0.0)
 
 
-def _direct(m):
-    """The same problem as catchment.mf, set up through the API."""
+def _direct(m, eddy=False):
+    """The same problem as catchment.mf, set up through the API (with `eddy`, the constant
+    eddy viscosity 0.4 m^2/s, 0.6 on cells 30-32, listed before the roughness term)."""
     o = OracleSolver(m.nx, m.ny, m.dx, m.dy, step_duration=m.step_duration, initial_dt=1.0)
+    if eddy:
+        mu = np.full(m.nx * m.ny, 0.4)
+        mu[30:33] += 0.2
+        o.set_field("EDDY_MU", mu.reshape(m.ny, m.nx))
+        o.set_eddy_viscosity("constant", mu=0.4)
+        o.set_source_order(["eddy viscosity", "manning"])
     o.set_field("Z", m.field("z_bed", 0.0))
     o.set_field("H", np.full((m.ny, m.nx), 0.002))
     o.set_field("U", np.zeros((m.ny, m.nx)))
@@ -177,3 +184,20 @@ boundary == discharge
     m.solve(a)
     ic = a.get_field("INFIL_CAP")
     assert np.all(ic < 5e-4) and np.all(ic >= 0.0)       # capacity consumed as it infiltrates
+
+
+def test_eddy_viscosity_deck_equals_the_api_setup():
+    text = open(os.path.join(DECKS, "catchment.mf")).read().replace(
+        "source term == manning roughness",
+        "source term == eddy viscosity\n{\n  viscosity type == constant\n  default mu == 0.4\n}\n"
+        "field == mu\n{\n  set == 0.4\n  add == 0.2\n  {\n    within == id list\n    {\n      ids == 30 31 32\n"
+        "    }\n  }\n}\nsource term == manning roughness")
+    m = config.Model(read_mf(text, filename=os.path.join(DECKS, "catchment.mf")), base_path=DECKS)
+    assert m.eddy == ("constant", 0.4) and m.term_order == ["eddy viscosity", "manning"]
+    a = m.build(OracleSolver)
+    m.solve(a)
+    b = _direct(m, eddy=True)
+    for f in ("H", "U", "V"):
+        assert same(a.get_field(f), b.get_field(f)), f
+    plain = _direct(m)
+    assert not same(a.get_field("U"), plain.get_field("U"))

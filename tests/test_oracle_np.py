@@ -172,3 +172,75 @@ def test_infiltration_capacity_is_consumed_by_every_stage():
     # worth is gone, and deep cells emptied their 5e-4 m capacity
     taken = cap - o.get_field("INFIL_CAP")
     assert taken.max() > 2e-4 and np.any(o.get_field("INFIL_CAP") == 0.0)
+
+
+EDDY_ORDERS = [None, ["eddy viscosity", "manning", "energy loss"], ["energy loss", "eddy viscosity", "manning"]]
+
+
+def _eddy_setup(o, mode, shape, rng):
+    if mode == "smagorinsky":
+        o.set_eddy_viscosity("smagorinsky", mu_const=0.05, mu_smag=0.5)
+        return ("smagorinsky", 0.05, 0.5)
+    if mode == "field":
+        mu = rng.uniform(0.0, 3.0, shape)
+        o.set_field("EDDY_MU", mu)
+        o.set_eddy_viscosity("constant", mu=2.0)    # the field takes precedence
+        return ("constant", mu)
+    o.set_eddy_viscosity("constant", mu=0.7)
+    return ("constant", 0.7)
+
+
+@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("mode", ["constant", "field", "smagorinsky"])
+@pytest.mark.parametrize("order", EDDY_ORDERS)
+def test_oracle_eddy_viscosity_matches_numpy(case, mode, order):
+    """Eddy viscosity (constant, per-cell and Smagorinsky coefficients) in any position among
+    the momentum terms, against the numpy restatement."""
+    nx, ny, dx, dy, nan_cells, seed = case
+    z, h, u, v = wet_dry_state(nx, ny, dx, seed=seed + 3, nan_cells=0)
+    rng = np.random.default_rng(seed + 100)
+    shape = (ny, nx)
+    fx, fy = rng.uniform(0.0, 0.5, shape), rng.uniform(0.0, 0.5, shape)
+    n = (0.03, 0.05, 0.1, 0.3)
+    o = OracleSolver(nx, ny, dx, dy, rain_mode="physical")
+    for name, a in (("Z", z), ("H", h), ("U", u), ("V", v), ("ELOSS_FX", fx), ("ELOSS_FY", fy)):
+        o.set_field(name, a)
+    o.set_manning(*n)
+    eddy = _eddy_setup(o, mode, shape, rng)
+    if order:
+        o.set_source_order(order)
+    o.eval_dudt(0, 7.5, 0.37)
+    ref = onp.update_dudt(h, u, v, z, dx, dy, manning=tuple(np.full(shape, x) for x in n), time_now=7.5,
+                          timestep=0.37, rain_mode="physical", eloss=(fx, fy), eddy=eddy, order=order)
+    _check(o, ref, KS)
+    base = onp.update_dudt(h, u, v, z, dx, dy, manning=tuple(np.full(shape, x) for x in n), time_now=7.5,
+                           timestep=0.37, rain_mode="physical", eloss=(fx, fy))
+    if nx > 2 and ny > 2:
+        assert not same(ref["dudt"], base["dudt"])      # the term acts
+
+
+def test_oracle_eddy_viscosity_steps_match_numpy():
+    nx, ny, dx = 30, 22, 2.0
+    z, h, u, v = wet_dry_state(nx, ny, dx, seed=21)
+    shape = (ny, nx)
+    o = OracleSolver(nx, ny, dx, rain_mode="physical", cn_target=0.5)
+    for name, a in (("Z", z), ("H", h), ("U", u), ("V", v)):
+        o.set_field(name, a)
+    o.set_eddy_viscosity("smagorinsky", mu_const=0.05, mu_smag=0.5)
+    o.set_source_order(["eddy viscosity", "manning"])
+    cn, rep, nd = o.do_timestep(0.0, 0.2)
+    (hN, uN, vN), cn2, rep2, nd2 = onp.do_timestep(
+        h, u, v, z, dx, dx, 0.0, 0.2, cn_target=0.5, manning=tuple(np.full(shape, x) for x in (0.03, 0.3, 0.1, 0.3)),
+        rain_mode="physical", eddy=("smagorinsky", 0.05, 0.5), order=["eddy viscosity", "manning"])
+    assert (cn, bool(rep), nd) == (cn2, rep2, nd2)
+    for k, a in zip((0, 1, 2), (hN, uN, vN)):
+        assert same(o.get_field(100 + 3 * o.nstages + k), a)
+
+
+def test_source_order_is_validated():
+    o = OracleSolver(4, 4, 1.0)
+    for bad in (["manning", "manning"],):
+        with pytest.raises(Exception):
+            o.set_source_order(bad)
+    with pytest.raises(ValueError):
+        o.set_eddy_viscosity("laminar")
