@@ -109,7 +109,9 @@ enum class FieldId : int {
   d_deep = SV_FIELD_D_DEEP, qbdy0 = SV_FIELD_QBDY0, qbdy1 = SV_FIELD_QBDY1, hbdy0 = SV_FIELD_HBDY0,
   hbdy1 = SV_FIELD_HBDY1, rain_pattern = SV_FIELD_RAIN_PATTERN, dzdx_bed = SV_FIELD_DZDX,
   dzdy_bed = SV_FIELD_DZDY, hflux = SV_FIELD_FLUX_H, uflux = SV_FIELD_FLUX_U, vflux = SV_FIELD_FLUX_V,
-  zflux = SV_FIELD_FLUX_Z, branch = SV_FIELD_FLUX_BRANCH
+  zflux = SV_FIELD_FLUX_Z, branch = SV_FIELD_FLUX_BRANCH, infil_rate = SV_FIELD_INFIL_RATE,
+  infil_cap = SV_FIELD_INFIL_CAP, eloss_fx = SV_FIELD_ELOSS_FX, eloss_fy = SV_FIELD_ELOSS_FY,
+  eddy_mu = SV_FIELD_EDDY_MU
 };
 
 // Host copy of one SaintVenantState (src/SaintVenant/State.hpp:40-42).
@@ -185,6 +187,17 @@ class SaintVenantSolver {
   // ManningRoughnessSourceTerm uniform parameters (ManningRoughnessSourceTerm.cpp:90-109)
   void set_manning(double n_shallow, double n_deep, double d_shallow, double d_deep) {
     check(sv_set_manning(ctx_.get(), n_shallow, n_deep, d_shallow, d_deep), ctx_.get());
+  }
+
+  // EddyViscositySourceTerm (EddyViscositySourceTerm.cpp:112-137): SV_EDDY_CONSTANT with
+  // "default mu" (or the eddy_mu field), SV_EDDY_SMAGORINSKY with the constant and dynamic
+  // coefficients
+  void set_eddy_viscosity(int mode, double mu = 1.0, double mu_const = 0.05, double mu_smag = 0.5) {
+    check(sv_set_eddy_viscosity(ctx_.get(), mode, mu, mu_const, mu_smag), ctx_.get());
+  }
+  // the momentum source terms (SV_TERM_*) in the order of the configuration's source terms
+  void set_source_order(const std::vector<int>& terms) {
+    check(sv_set_source_order(ctx_.get(), terms.data(), int(terms.size())), ctx_.get());
   }
 
   // SaintVenantSolver::update_dUdt (Solver.cpp:73-114)
