@@ -204,10 +204,11 @@ class Runner:
             self.run(timesteps)
 
 
-def profile_traffic(name):
-    """Per-launch DRAM bytes per cell of a stage kernel from a committed ncu capture."""
+def profile_traffic(name, key="bytes_per_cell_per_launch"):
+    """Per-launch DRAM bytes (or warp instructions) per cell of a stage kernel from a committed
+    ncu capture."""
     try:
-        return json.load(open(os.path.join(ROOT, "profiles", name)))["bytes_per_cell_per_launch"]
+        return json.load(open(os.path.join(ROOT, "profiles", name)))[key]
     except Exception:
         return None
 
@@ -263,6 +264,14 @@ def timed_run(w, precision, args, device, barrier, dist):
                                if traffic_pc else None),
             "kernel": f"{kernel} (variant {variant})", "alg_bytes_per_launch": alg_bytes_launch,
             "stage_launch_ms": stage_avg_s * 1e3, "stage_share_of_step": tm["stage_ms"] / max(1e-9, tm["total_ms"])}
+    # the bound that holds: instruction issue. Warp instructions per cell from the same ncu
+    # capture; each of the 148 SMs' 4 schedulers issues at most one per cycle at the SM clock
+    # sampled during the timed region
+    inst_pc = profile_traffic(f"{kernel}_{precision}_2048_traffic.json", "warp_inst_per_cell_per_launch")
+    if inst_pc and clocks.get("sm_mhz"):
+        issue_ms = inst_pc * ncells / (148 * 4 * clocks["sm_mhz"] * 1e6) * 1e3
+        roof["issue"] = {"warp_inst_per_cell": inst_pc, "issue_limited_ms": issue_ms,
+                         "frac": issue_ms / (stage_avg_s * 1e3), "sm_mhz": clocks["sm_mhz"]}
     res = {"value": work / (ms_max * 1e-3), "ms": ms_max, "accepted": accepted, "repeated": repeated,
            "variant": variant, "autotune_ms": tune, "roofline": roof, "clocks": clocks, "timesteps": tm["timesteps"],
            "sim_time_s": runner.t_step,

@@ -137,6 +137,8 @@ __device__ __forceinline__ T load_bed(const T* z, const double* zdat, int dtiles
 // NaN-propagating max/min for the CFL reduction
 __device__ __forceinline__ double nmax(double a, double b) { return (a != a || b != b) ? (a + b) : (a > b ? a : b); }
 __device__ __forceinline__ double nmin(double a, double b) { return (a != a || b != b) ? (a + b) : (a < b ? a : b); }
+__device__ __forceinline__ float nmax(float a, float b) { return (a != a || b != b) ? (a + b) : (a > b ? a : b); }
+__device__ __forceinline__ float nmin(float a, float b) { return (a != a || b != b) ? (a + b) : (a < b ? a : b); }
 
 template <int NT> __device__ double block_sum(double v, double* red) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -319,8 +321,8 @@ __device__ __forceinline__ void finish_cell(const StageParams<T>& P, const DevFo
                                             long long g, int gx, int gy, T h, T u, T v, T dhdx, T dhdy, T dzdx,
                                             T dzdy, const FaceF<T>& fw, const FaceF<T>& fe, const FaceF<T>& fs,
                                             const FaceF<T>& fn, bool first, bool last, int cur, double dt_d,
-                                            double& rain, double& removed, double& walls, double& xcfl,
-                                            double& xcfl_min, double& vol, const EddyIn<T>* ed = nullptr) {
+                                            double& rain, double& removed, double& walls, T& xcfl,
+                                            T& xcfl_min, double& vol, const EddyIn<T>* ed = nullptr) {
   T kh, ku, kv;
   double r_, o_, w_;
   cell_dudt<T, CC, EDDY>(P, fc, c, g, gx, gy, h, u, v, dhdx, dhdy, dzdx, dzdy, fw, fe, fs, fn, kh, ku, kv, r_, o_,
@@ -410,8 +412,8 @@ __device__ __forceinline__ void finish_cell(const StageParams<T>& P, const DevFo
     T hh = sfmax(out[0], T(0));
     T cc = ssqrt(T(kG) * hh);
     T xx = c.divx(sfabs(out[1]) + cc) + c.divy(sfabs(out[2]) + cc);
-    xcfl = nmax(xcfl, double(xx));
-    xcfl_min = nmin(xcfl_min, double(xx));
+    xcfl = nmax(xcfl, xx);  // a max or min of T values is exact in T
+    xcfl_min = nmin(xcfl_min, xx);
     vol += double(out[0]) * P.cell_area;
   }
 }
@@ -525,7 +527,8 @@ __device__ __forceinline__ void stage_tile(const StageParams<T>& P, int bx, int 
   const int tx = tid % TX, ty = tid / TX;
   const int gx = x0 + tx, gy = y0 + ty;
   const bool valid = gx < nx && gy < ny;
-  double rain = 0.0, removed = 0.0, walls = 0.0, xcfl = 0.0, xcfl_min = 1.0 / 0.0, vol = 0.0;
+  double rain = 0.0, removed = 0.0, walls = 0.0, vol = 0.0;
+  T xcfl = T(0), xcfl_min = T(1.0 / 0.0);
   const bool last = P.mode & M_LAST;
   if (valid) {
     const long long g = (long long)gy * nx + gx;
@@ -558,8 +561,8 @@ __device__ __forceinline__ void stage_tile(const StageParams<T>& P, int bx, int 
                                          rain, removed, walls, xcfl, xcfl_min, vol, &ed);
   }
   if (last && !(P.mode & M_DEBUGK)) {
-    double mx = block_max<NT>(xcfl, s.red);
-    double mn = block_min<NT>(xcfl_min, s.red);
+    double mx = block_max<NT>(double(xcfl), s.red);
+    double mn = block_min<NT>(double(xcfl_min), s.red);
     double vs = block_sum<NT>(vol, s.red);
     if (tid == 0) {
       P.part[blk] = mx;
@@ -744,7 +747,8 @@ __device__ __forceinline__ void sweep_strip(const StageParams<T>& P, long long g
   T Smm_uy = T(0), Smm_vy = T(0);  // y slopes of u, v of row k-3 (eddy viscosity)
   T fyA[3] = {}, fyB[3] = {};  // (U[k-1]-U[k-2])/dy, (U[k]-U[k-1])/dy
   FaceF<T> FS{}, FN{};
-  double rain = 0.0, removed = 0.0, walls = 0.0, xcfl = 0.0, xmin = 1.0 / 0.0, vol = 0.0;
+  double rain = 0.0, removed = 0.0, walls = 0.0, vol = 0.0;
+  T xcfl = T(0), xmin = T(1.0 / 0.0);
 
   // L1 prefetch of rows ahead (addresses clamped into the mesh, like the loads)
   auto prefetch_rows = [&](int k) {
@@ -770,11 +774,12 @@ __device__ __forceinline__ void sweep_strip(const StageParams<T>& P, long long g
     if (fc.head_kind == 2) { prefetch_l1(P.hb0p + g); prefetch_l1(P.hb1p + g); }
   };
 
-  RowV<T> Rnext = load_row(y0 - 2);
   for (int k = y0 - 2; k <= y0 + TY + 1; ++k) {
     prefetch_rows(k);
-    Rm = R0; R0 = Rp; Rp = Rnext;
-    if (k < y0 + TY + 1) Rnext = load_row(k + 1);  // prefetch the next row
+    // row k is loaded where it enters the window: the L1 prefetch issued three iterations
+    // earlier has brought it in, and not holding it a row ahead in registers leaves room
+    // for more resident warps
+    Rm = R0; R0 = Rp; Rp = load_row(k);
     if constexpr (EDDY) { Smm_uy = Sm.uy; Smm_vy = Sm.vy; }
     Sm = S0;
     fyA[0] = fyB[0]; fyA[1] = fyB[1]; fyA[2] = fyB[2];
@@ -868,7 +873,7 @@ __device__ __forceinline__ void sweep_strip(const StageParams<T>& P, long long g
     FS = FN;
   }
   if (last && !(P.mode & M_DEBUGK)) {
-    double mx = warp_max(xcfl), mn = warp_min(xmin), vs = warp_sum<T>(vol);
+    double mx = warp_max(double(xcfl)), mn = warp_min(double(xmin)), vs = warp_sum<T>(vol);
     if (lane == 0) {
       P.part[gw] = mx;
       P.part[P.nblk + gw] = mn;
