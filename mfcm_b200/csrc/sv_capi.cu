@@ -17,6 +17,8 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <map>
+#include <mutex>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -123,6 +125,32 @@ struct sv_ctx {
 
 namespace {
 
+// FP64 staging buffers of field transfers come from one stream-ordered pool per device that
+// keeps freed memory mapped. The device's default pool unmaps freed memory at every
+// synchronisation, and mapping it again costs more than the copy itself (5-20 ms against
+// 2.5 ms for a 134 MB field). Destroying a solver trims the pool back to nothing.
+cudaMemPool_t staging_pool(int device, bool create) {
+  static std::mutex mu;
+  static std::map<int, cudaMemPool_t> pools;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = pools.find(device);
+  if (it != pools.end()) return it->second;
+  if (!create) return nullptr;
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  cudaMemPool_t pool = nullptr;
+  if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;  // the caller falls back to the default pool
+  }
+  uint64_t keep = ~0ull;
+  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  pools[device] = pool;
+  return pool;
+}
+
 #define SV_CUDA(call)                                  \
   do {                                                 \
     cudaError_t e_ = (call);                           \
@@ -154,7 +182,7 @@ struct Solver final : public sv_ctx {
   int dtiles_x = 0, dtiles_y = 0;
   T* man[4] = {};
   double man_s[4] = {0.03, 0.3, 0.1, 0.3};  // ManningRoughnessSourceTerm.cpp:99-102
-  std::vector<double> host_n_shallow;
+  int* d_flag = nullptr;  // result of a field comparison on the device
   T *q0 = nullptr, *q1 = nullptr, *pat = nullptr, *hb0 = nullptr, *hb1 = nullptr;
   T *irate = nullptr, *icap = nullptr;  // InfiltrationSourceTerm fields (.hpp:106-109)
   T *efx = nullptr, *efy = nullptr;     // EnergyLossSourceTerm fields (.hpp:199-202)
@@ -198,6 +226,7 @@ struct Solver final : public sv_ctx {
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
+    if (cudaMemPool_t pool = staging_pool(device, false)) cudaMemPoolTrimTo(pool, 0);
   }
 
   size_t device_bytes = 0;
@@ -309,13 +338,19 @@ struct Solver final : public sv_ctx {
   // buffer and its own array; another value type stages them in a stream-ordered FP64
   // buffer and converts on the device, so a field costs one copy at the link's speed (DMA
   // when the caller's buffer is pinned) and no pass over it on the host.
+  cudaError_t stage_alloc(double** p, uint64_t n) {
+    const size_t bytes = std::max<uint64_t>(n, 1) * sizeof(double);
+    cudaMemPool_t pool = staging_pool(device, true);
+    return pool ? cudaMallocFromPoolAsync(reinterpret_cast<void**>(p), bytes, pool, stream)
+                : cudaMallocAsync(reinterpret_cast<void**>(p), bytes, stream);
+  }
   int upload(T* dst, const double* host, uint64_t n) {
     cudaError_t e;
     if constexpr (std::is_same<T, double>::value) {
       e = cudaMemcpyAsync(dst, host, n * sizeof(double), cudaMemcpyHostToDevice, stream);
     } else {
       double* st = nullptr;
-      SV_CUDA(cudaMallocAsync(&st, std::max<uint64_t>(n, 1) * sizeof(double), stream));
+      SV_CUDA(stage_alloc(&st, n));
       e = cudaMemcpyAsync(st, host, n * sizeof(double), cudaMemcpyHostToDevice, stream);
       if (e == cudaSuccess) e = svk::launch_from_f64<T>(st, dst, (long long)n, stream);
       cudaError_t f = cudaFreeAsync(st, stream);
@@ -332,7 +367,7 @@ struct Solver final : public sv_ctx {
       e = cudaMemcpyAsync(host, src, n * sizeof(double), cudaMemcpyDeviceToHost, stream);
     } else {
       double* st = nullptr;
-      SV_CUDA(cudaMallocAsync(&st, std::max<uint64_t>(n, 1) * sizeof(double), stream));
+      SV_CUDA(stage_alloc(&st, n));
       if (absolute_bed)  // FP32 with tile datums: bed = FP64 datum + FP32 offset
         e = svk::launch_datum_absolute(reinterpret_cast<const float*>(src), int(mesh.nx), int(mesh.ny), dtiles_x, zdat,
                                        st, stream);
@@ -353,19 +388,18 @@ struct Solver final : public sv_ctx {
     bool lazy;
     T** slot = field_slot(id, lazy);
     if (!slot) return fail(SV_E_ARG, "field id not settable");
-    if (id == SV_FIELD_N_DEEP && man[0] && host_n_shallow.size() == n &&
-        std::memcmp(host_n_shallow.data(), host, n * sizeof(double)) == 0) {
-      man[1] = man[0];  // n_deep identical to n_shallow: read one array
+    if (id == SV_FIELD_N_DEEP && man[0]) return set_n_deep(host, n);
+    if (id == SV_FIELD_N_SHALLOW && man[1] && man[1] == man[0]) {
+      // n_deep shares n_shallow's array: it keeps its values in an array of its own
+      T* own = nullptr;
+      SV_CUDA(alloc_cells(&own, false));
+      SV_CUDA(cudaMemcpyAsync(own, man[0], size_t(ncells) * sizeof(T), cudaMemcpyDeviceToDevice, stream));
+      man[1] = own;
       graph_dirty = true; ++pversion;
-      return SV_OK;
     }
-    if (lazy && (*slot == nullptr || (id == SV_FIELD_N_DEEP && man[1] == man[0]))) {
+    if (lazy && *slot == nullptr) {
       SV_CUDA(alloc_cells(slot, false));
       graph_dirty = true; ++pversion;
-    }
-    if (id == SV_FIELD_N_SHALLOW) {
-      host_n_shallow.assign(host, host + n);
-      if (man[1] == man[0] && man[1] != nullptr) { man[1] = nullptr; graph_dirty = true; ++pversion; }
     }
     if (id == SV_FIELD_Z && datum) return set_bed_with_datum(host, n);
     int r = upload(*slot, host, n);
@@ -382,6 +416,35 @@ struct Solver final : public sv_ctx {
     return r;
   }
 
+  // n_deep equal to n_shallow once both are in the solver's value type (compared bit for bit
+  // on the device): the kernels read one array. Otherwise n_deep gets an array of its own.
+  int set_n_deep(const double* host, uint64_t n) {
+    double* st = nullptr;
+    if (!d_flag) SV_CUDA(alloc(&d_flag, 1));
+    SV_CUDA(stage_alloc(&st, n));
+    int flag = 0;
+    cudaError_t e = cudaMemcpyAsync(st, host, n * sizeof(double), cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_flag, 0, sizeof(int), stream);
+    if (e == cudaSuccess) e = svk::launch_differs<T>(st, man[0], (long long)n, d_flag, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess && flag) {
+      if (!man[1] || man[1] == man[0]) {
+        e = alloc_cells(&man[1], false);
+        graph_dirty = true; ++pversion;
+      }
+      if (e == cudaSuccess) e = svk::launch_from_f64<T>(st, man[1], (long long)n, stream);
+    } else if (e == cudaSuccess && man[1] != man[0]) {
+      man[1] = man[0];
+      graph_dirty = true; ++pversion;
+    }
+    cudaError_t f = cudaFreeAsync(st, stream);
+    if (e == cudaSuccess) e = f;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return cuda_fail(e, "n_deep upload");
+    return SV_OK;
+  }
+
   // FP32-with-datum bed: per 32 x 8 tile datum = the tile's lowest bed rounded down to a
   // multiple of 2^-10 m (datum differences are then exact in FP64); stored bed = FP32
   // offset from it; bed slopes from the FP64 bed (Minmod3 in FP64, rounded once).
@@ -391,7 +454,7 @@ struct Solver final : public sv_ctx {
       return fail(SV_E_STATE, "tile datums need an FP32 solver");
     } else {
       double* dz = nullptr;
-      SV_CUDA(cudaMallocAsync(&dz, std::max<uint64_t>(n, 1) * sizeof(double), stream));
+      SV_CUDA(stage_alloc(&dz, n));
       cudaError_t e = cudaMemcpyAsync(dz, host, n * sizeof(double), cudaMemcpyHostToDevice, stream);
       if (e == cudaSuccess)
         e = svk::launch_datum_bed(dz, int(mesh.nx), int(mesh.ny), mesh.dx, mesh.dy, dtiles_x, dtiles_y, zdat, z, zx, zy,
@@ -482,7 +545,6 @@ struct Solver final : public sv_ctx {
   int set_manning(double a, double b, double c, double d) override {
     man_s[0] = a; man_s[1] = b; man_s[2] = c; man_s[3] = d;
     for (int i = 0; i < 4; ++i) man[i] = nullptr;  // uniform values replace per-cell fields
-    host_n_shallow.clear();
     graph_dirty = true; ++pversion;
     return SV_OK;
   }

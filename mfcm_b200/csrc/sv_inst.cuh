@@ -99,6 +99,12 @@ template <> cudaError_t launch_from_f64<SV_T>(const double* src, SV_T* dst, long
   convert_kernel<double, SV_T><<<elementwise_blocks(n), 256, 0, s>>>(src, dst, n);
   return cudaGetLastError();
 }
+template <> cudaError_t launch_differs<SV_T>(const double* src, const SV_T* ref, long long n, int* flag,
+                                             cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  differs_kernel<SV_T><<<elementwise_blocks(n), 256, 0, s>>>(src, ref, n, flag);
+  return cudaGetLastError();
+}
 template <> cudaError_t launch_to_f64<SV_T>(const SV_T* src, double* dst, long long n, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
   convert_kernel<SV_T, double><<<elementwise_blocks(n), 256, 0, s>>>(src, dst, n);

@@ -953,6 +953,17 @@ __global__ void convert_kernel(const TI* __restrict__ src, TO* __restrict__ dst,
     dst[i] = TO(src[i]);
 }
 
+// Whether an FP64 field, once converted to T, differs bit for bit from a stored one: sets *flag.
+__device__ __forceinline__ bool same_bits(double a, double b) { return __double_as_longlong(a) == __double_as_longlong(b); }
+__device__ __forceinline__ bool same_bits(float a, float b) { return __float_as_uint(a) == __float_as_uint(b); }
+template <typename T>
+__global__ void differs_kernel(const double* __restrict__ src, const T* __restrict__ ref, long long n, int* flag) {
+  bool diff = false;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    diff = diff || !same_bits(T(src[i]), ref[i]);
+  if (diff) *flag = 1;
+}
+
 #ifdef SV_DEFINE_COMMON_KERNELS  // non-template kernels: defined in one unit only
 // Datum of each 32 x 8 tile of an FP64 bed: the tile's lowest non-NaN value (among values
 // that compare equal, such as -0.0 and 0.0, the first in row-major order), rounded down to a

@@ -35,6 +35,8 @@ template <typename T> cudaError_t launch_bed_slopes(const T* z, int nx, int ny, 
 // FP64 <-> T conversion of a field on the device
 template <typename T> cudaError_t launch_from_f64(const double* src, T* dst, long long n, cudaStream_t s);
 template <typename T> cudaError_t launch_to_f64(const T* src, double* dst, long long n, cudaStream_t s);
+// *flag = 1 when T(src[i]) differs bit for bit from ref[i] for some i (flag left as it was otherwise)
+template <typename T> cudaError_t launch_differs(const double* src, const T* ref, long long n, int* flag, cudaStream_t s);
 // FP32 with tile datums, from an FP64 bed on the device: the tile datums, the FP32 offsets and
 // the bed slopes (FP64, rounded once); and the absolute FP64 bed back from the offsets
 cudaError_t launch_datum_bed(const double* z, int nx, int ny, double dx, double dy, int dtiles_x, int dtiles_y,

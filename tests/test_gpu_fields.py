@@ -73,3 +73,22 @@ def test_datum_bed_on_a_ragged_mesh():
     assert _bits_equal(got, expect)
     assert np.max(np.abs(got[~np.isnan(z)] - z[~np.isnan(z)])) < 2.0 ** -16 * 400   # FP32 offsets
     s.close()
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_n_deep_shares_n_shallow_only_while_equal(precision):
+    """A deep-water roughness field equal to the shallow one is read from one array; setting
+    either field later leaves the other with its own values."""
+    nx, ny = 40, 30
+    rng = np.random.default_rng(8)
+    a, b = rng.uniform(0.02, 0.06, (ny, nx)), rng.uniform(0.02, 0.06, (ny, nx))
+    cast = (lambda x: x) if precision == "f64" else (lambda x: x.astype(np.float32).astype(np.float64))
+    s = SaintVenantSolver(nx, ny, 1.0, precision=precision)
+    s.set_field("N_SHALLOW", a)
+    s.set_field("N_DEEP", a)                  # shared
+    s.set_field("N_SHALLOW", b)               # n_deep keeps a
+    assert _bits_equal(s.get_field("N_DEEP"), cast(a)) and _bits_equal(s.get_field("N_SHALLOW"), cast(b))
+    s.set_field("N_DEEP", b)                  # shared again
+    s.set_field("N_DEEP", a)                  # an array of its own
+    assert _bits_equal(s.get_field("N_DEEP"), cast(a)) and _bits_equal(s.get_field("N_SHALLOW"), cast(b))
+    s.close()
