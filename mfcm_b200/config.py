@@ -23,8 +23,11 @@ On top of the tree sit the parts of the schema that drive this solver:
 - the boundaries: discharge, head, stage, each a list of constant or time-series entries on
   cell selections (DischargeBoundarySourceTerm.hpp:114-146 and siblings).
 
-GDAL rasters, WKT geometry selections, formatted (calendar) times, outputs
-and measures are not read: a deck that uses them raises ConfigError naming the feature.
+- outputs (`output == name`, cell fields as timed CSV files) and depth-point measures
+  (`measures { h-point == name }`), written by `Model.solve`.
+
+GDAL rasters, WKT geometry selections and formatted (calendar) times are not read: a deck that
+uses them raises ConfigError naming the feature.
 """
 import math
 import os
@@ -33,6 +36,7 @@ import re
 import numpy as np
 
 from .raster import NimrodRaster, RasterError
+from .outputs import MultiFieldOutput, DepthPointMeasure, _NAMES as _OUTPUT_FIELDS
 from . import (TimeSeries, Forcing, num_steps, RAIN_NONE, RAIN_UNIFORM, RAIN_FIELDS, HEAD_NONE, HEAD_FIELDS,
                STAGE_FIELDS)
 
@@ -606,18 +610,86 @@ class Model:
             solver.set_field("QBDY1", q[1].reshape(self.ny, self.nx))
         return f
 
-    def solve(self, solver, on_step=None):
-        """TypedTemporalScheme::solve over the deck's start and end times."""
+    # --- outputs and measures
+    def _path(self, fn):
+        return fn if os.path.isabs(fn) else os.path.join(self.base, fn)
+
+    def outputs(self):
+        """make_field_output_file (OutputFile.hpp:229-258) for each enabled `output == name`
+        section: the fields named by its `field` keys (the section's name when there are
+        none), written from `start time` every `every` (or `every seconds`) to
+        `<filename>_<t>.csv`, `filename` defaulting to output/<name> beside the deck. Field
+        names the solver does not have are skipped, as in the reference. Only cell outputs
+        are written."""
+        outs = []
+        for conf in self.tree.equal_range("output"):
+            name = conf.value
+            if conf.get("enabled", "true").strip().lower() in ("false", "0"):
+                continue
+            at = conf.get("at", "cells")
+            if at != "cells":
+                raise ConfigError(f"output {name!r}: only cell outputs are supported (at == {at})")
+            fields = [f.value for f in conf.equal_range("field")] or [name]
+            fields = [f for f in fields if f in _OUTPUT_FIELDS or f == "stage"]
+            start = self.parser.parse(conf.get("start time")) if conf.child("start time") is not None else self.start_time
+            if conf.child("every") is not None:
+                every = self.parser.parse(conf.get("every"))
+            elif conf.child("every seconds") is not None:
+                every = float(conf.get("every seconds"))
+            else:
+                raise ConfigError(f"output {name!r}: needs `every` or `every seconds`")
+            out = MultiFieldOutput(self._path(conf.get("filename", os.path.join("output", name))), fields, every,
+                                   start, origin=self.origin, delimiter=conf.get("delimiter", ", "))
+            outs.append(out)
+        return outs
+
+    def measures(self):
+        """SaintVenantHPointMeasure::create_measures (SaintVenant/Measure.hpp:214-224): one depth
+        measure per `h-point == name` of the `measures` section, at the cell nearest its
+        `location`, written to `filename` (default output/measures/<name>.csv beside the deck).
+        The reference builds no other measure from a deck."""
+        res = []
+        mconf = self.tree.child("measures")
+        if mconf is None:
+            return res
+        for conf in mconf.equal_range("h-point"):
+            try:
+                m = DepthPointMeasure(_floats(conf.get("location"), 2), self.nx, self.ny, self.dx, self.dy,
+                                      self.origin, name=conf.value)
+            except ValueError as e:
+                raise ConfigError(f"measure {conf.value!r}: {e}") from None
+            m.filename = self._path(conf.get("filename", os.path.join("output", "measures", conf.value + ".csv")))
+            res.append(m)
+        return res
+
+    def solve(self, solver, on_step=None, write_outputs=True):
+        """TypedTemporalScheme::solve (TemporalScheme.hpp:244-276) over the deck's start and end
+        times. Each step begins with the measures (end_of_step, SaintVenant/Solver.hpp:90-98),
+        then the outputs (do_outputs, RungeKutta.hpp:444-449), then `on_step`; the outputs run
+        once more at the end time. The reference never writes its measures
+        (Output/Measure.hpp:87-98 has no caller); here each is written to its file at the end.
+        With `write_outputs` false, no file is written."""
+        outs = self.outputs() if write_outputs else []
+        meas = self.measures() if write_outputs else []
         n = num_steps(self.start_time, self.end_time, self.step_duration)
         per_step = []
         for i in range(n):
             t = self.start_time + i * self.step_duration
+            for m in meas:
+                m.update(t, solver)
+            for o in outs:
+                o.timed_output(t, solver)
             if on_step:
                 on_step(t, solver)
             self.forcing(solver, t)
             per_step.append(solver.advance())
+        t_end = self.start_time + n * self.step_duration
+        for o in outs:
+            o.timed_output(t_end, solver)
         if on_step:
-            on_step(self.start_time + n * self.step_duration, solver)
+            on_step(t_end, solver)
+        for m in meas:
+            m.write(m.filename)
         return per_step
 
 

@@ -108,8 +108,9 @@ class MultiFieldOutput:
     """TimedOutputFile + MultiFieldOutputFile (OutputFile.hpp:121-224): named cell fields to
     `<base>_<std::to_string(t)>.csv` every `every` seconds from `start`."""
 
-    def __init__(self, base, fields, every, start=0.0, origin=(0.0, 0.0)):
+    def __init__(self, base, fields, every, start=0.0, origin=(0.0, 0.0), delimiter=", "):
         self.base = base
+        self.delimiter = delimiter
         self.fields = list(fields)
         self.every = float(every)
         self.start = float(start)
@@ -122,7 +123,7 @@ class MultiFieldOutput:
             return None
         path = f"{self.base}_{fmt_value(t)}.csv"
         loc = cell_locations(solver.nx, solver.ny, solver.dx, solver.dy, *self.origin)
-        write_csv(path, self.fields, [solver_field(solver, f) for f in self.fields], loc)
+        write_csv(path, self.fields, [solver_field(solver, f) for f in self.fields], loc, self.delimiter)
         self.output_no += 1
         self.written.append(path)
         return path

@@ -201,3 +201,49 @@ def test_eddy_viscosity_deck_equals_the_api_setup():
         assert same(a.get_field(f), b.get_field(f)), f
     plain = _direct(m)
     assert not same(a.get_field("U"), plain.get_field("U"))
+
+
+def test_deck_outputs_and_measures(tmp_path):
+    """Output sections write timed CSV files of the named cell fields; an h-point measure records
+    the depth of the cell nearest its location at the start of every step."""
+    text = open(os.path.join(DECKS, "catchment.mf")).read() + """
+output == state
+{
+  field == h
+  field == stage
+  field == no such field
+  every seconds == 60
+  delimiter == ;
+  filename == out/state
+}
+output == quiet
+{
+  enabled == false
+  every seconds == 30
+}
+measures
+{
+  h-point == gauge
+  {
+    location == 62.5 42.5
+  }
+}
+"""
+    (tmp_path / "deck.mf").write_text(text)
+    for extra in ("boundaries.mf", "storm.csv"):
+        (tmp_path / extra).write_text(open(os.path.join(DECKS, extra)).read())
+    m = config.load(str(tmp_path / "deck.mf"))
+    seen = []
+    s = m.build(OracleSolver)
+    m.solve(s, on_step=lambda t, x: seen.append((t, x.get_field("H").ravel()[8 * 24 + 12])))
+    files = sorted(p.name for p in (tmp_path / "out").iterdir())
+    assert files == ["state_0.000000.csv", "state_120.000000.csv", "state_60.000000.csv"]
+    lines = (tmp_path / "out" / "state_120.000000.csv").read_text().splitlines()
+    assert lines[0] == 'X;Y;"h";"stage";'
+    h = s.get_field("H").ravel()
+    z = s.get_field("Z").ravel()
+    assert lines[1] == f"2.5;2.5;{h[0]:f};{z[0] + h[0]:f};"
+    assert not (tmp_path / "output" / "quiet_0.000000.csv").exists()
+    gauge = (tmp_path / "output" / "measures" / "gauge.csv").read_text().splitlines()
+    assert gauge[0] == '"ID", "gauge", ' and len(gauge) == 1 + 4      # steps at 0, 30, 60, 90 s
+    assert [float(r.split(",")[1]) for r in gauge[1:]] == [round(v, 6) for t, v in seen[:4]]
