@@ -26,7 +26,8 @@ On top of the tree sit the parts of the schema that drive this solver:
 - outputs (`output == name`, cell fields as timed CSV files) and depth-point measures
   (`measures { h-point == name }`), written by `Model.solve`.
 
-GDAL rasters, WKT geometry selections and formatted (calendar) times are not read: a deck that
+Point selections (`at` with a `wkt` of points) are read. GDAL rasters and vector files and
+formatted (calendar) times are not read: a deck that
 uses them raises ConfigError naming the feature.
 """
 import math
@@ -289,6 +290,102 @@ def _floats(s, n=None):
     return vals
 
 
+# ------------------------------------------------------------------------------- WKT
+_WKT_TOKEN = re.compile(r"\s*(?:([A-Za-z]+)|([-+]?(?:\d+\.?\d*|\.\d+)(?:[eE][-+]?\d+)?)|([(),]))")
+_WKT_KINDS = ("multilinestring", "multipolygon", "multipoint", "linestring", "polygon", "point")
+
+
+def read_wkt(text):
+    """Geometries of a WKT string, as the reference's grammar reads them
+    (Geometry/GeometryParser.hpp:92-222): a comma-separated list of POINT, MULTIPOINT,
+    LINESTRING, MULTILINESTRING, POLYGON and MULTIPOLYGON, tags in any case with optional Z and
+    M, coordinates separated by spaces and points by commas. Returns (kind, has_z, has_m,
+    coordinates) tuples: a point is a list of numbers, a line string a list of points, a polygon
+    or multi line string a list of line strings, a multi polygon a list of polygons."""
+    toks, pos = [], 0
+    while pos < len(text):
+        if not text[pos:].strip():
+            break
+        m = _WKT_TOKEN.match(text, pos)
+        if not m:
+            raise ConfigError(f"failed to parse WKT at {text[pos:]!r}")
+        toks.append(("w", m.group(1).lower()) if m.group(1) else (("n", float(m.group(2))) if m.group(2)
+                                                                    else ("p", m.group(3))))
+        pos = m.end()
+    i = 0
+
+    def peek():
+        return toks[i] if i < len(toks) else ("end", None)
+
+    def expect(v):
+        nonlocal i
+        if peek() != ("p", v):
+            raise ConfigError(f"failed to parse WKT: expected {v!r}")
+        i += 1
+
+    def seq(item):  # '(' item (',' item)* ')'
+        nonlocal i
+        expect("(")
+        out = [item()]
+        while peek() == ("p", ","):
+            i += 1
+            out.append(item())
+        expect(")")
+        return out
+
+    def coords():  # numbers separated by spaces
+        nonlocal i
+        out = []
+        while peek()[0] == "n":
+            out.append(peek()[1])
+            i += 1
+        if not out:
+            raise ConfigError("failed to parse WKT: expected a coordinate")
+        return out
+
+    def point_text():
+        expect("(")
+        c = coords()
+        expect(")")
+        return c
+
+    def line_text():
+        return seq(coords)
+
+    def multiline_text():
+        return seq(line_text)
+
+    body = {"point": point_text, "multipoint": lambda: seq(point_text), "linestring": line_text,
+            "multilinestring": multiline_text, "polygon": multiline_text,
+            "multipolygon": lambda: seq(multiline_text)}
+
+    def geometry():
+        nonlocal i
+        t = peek()
+        if t[0] != "w":
+            raise ConfigError("failed to parse WKT: expected a geometry tag")
+        word = t[1]
+        kind = next((k for k in _WKT_KINDS if word.startswith(k)), None)
+        if kind is None:
+            raise ConfigError(f"failed to parse WKT: unknown geometry {word!r}")
+        i += 1
+        flags = word[len(kind):]
+        while peek()[0] == "w":  # Z and M may stand apart from the tag
+            flags += peek()[1]
+            i += 1
+        if flags not in ("", "z", "m", "zm"):
+            raise ConfigError(f"failed to parse WKT: bad dimension {flags!r}")
+        return kind, "z" in flags, "m" in flags, body[kind]()
+
+    geoms = [geometry()]
+    while peek() == ("p", ","):
+        i += 1
+        geoms.append(geometry())
+    if i != len(toks):
+        raise ConfigError("failed to parse WKT: trailing text")
+    return geoms
+
+
 # -------------------------------------------------------------------------- the model
 class Model:
     """A configured solve: mesh, time parameters, scheme, fields, source terms and
@@ -365,7 +462,30 @@ class Model:
                 ids += [int(x) for x in _floats(n.value)]
             ids = sorted(set(i for i in ids if 0 <= i < self.nx * self.ny))
             return np.asarray(ids, dtype=np.int64)
-        raise ConfigError(f"mesh selection {kind!r} is not supported (geometry selections need WKT)")
+        if kind == "at":
+            return self._at_selection(conf)
+        raise ConfigError(f"unknown mesh selection method {kind!r}")
+
+    def _at_selection(self, conf):
+        """MeshSelection "at" (Mesh/MeshSelection.cpp:172-178): the cells containing the points
+        of the `wkt` geometry collection (Cartesian2DMesh::get_nearest_object_index); points
+        outside the mesh select nothing. Other geometry types cannot select cells, as in the
+        reference (MeshSelection.cpp:115-128)."""
+        if conf.child("wkt") is None:
+            if conf.child("source") is not None:
+                raise ConfigError("geometry from a vector file needs GDAL, which is not available")
+            return np.zeros(0, dtype=np.int64)
+        cells = set()
+        for kind, _, _, c in read_wkt(conf.get("wkt")):
+            if kind != "point":
+                raise ConfigError(f"cannot select cells with a {kind} geometry")
+            if len(c) < 2:
+                raise ConfigError("a point needs x and y")
+            cx = (c[0] - self.origin[0]) * (1.0 / self.dx)
+            cy = (c[1] - self.origin[1]) * (1.0 / self.dy)
+            if 0.0 <= cx < self.nx and 0.0 <= cy < self.ny:
+                cells.add(int(cy) * self.nx + int(cx))
+        return np.asarray(sorted(cells), dtype=np.int64)
 
     def _assign(self, f, sel, v):
         """field *= 0 then += v on the selection (load_constant_input_field,
@@ -698,4 +818,4 @@ def load(path):
     return Model(read_mf(path), base_path=os.path.dirname(os.path.abspath(path)))
 
 
-__all__ = ["ConfigError", "Node", "read_mf", "TimeParser", "Model", "load"]
+__all__ = ["ConfigError", "Node", "read_mf", "read_wkt", "TimeParser", "Model", "load"]

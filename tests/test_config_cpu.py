@@ -247,3 +247,26 @@ measures
     gauge = (tmp_path / "output" / "measures" / "gauge.csv").read_text().splitlines()
     assert gauge[0] == '"ID", "gauge", ' and len(gauge) == 1 + 4      # steps at 0, 30, 60, 90 s
     assert [float(r.split(",")[1]) for r in gauge[1:]] == [round(v, 6) for t, v in seen[:4]]
+
+
+def test_wkt_reader():
+    g = config.read_wkt("POINT (1 2), point z(1 2 3), MULTIPOINT ((1 2), (3 4)), LINESTRING (0 0, 1 1),"
+                        " POLYGON ((0 0, 4 0, 4 4, 0 0)), MULTIPOLYGON (((0 0, 1 0, 0 1, 0 0))), Point ZM (1 2 3 4)")
+    assert [x[0] for x in g] == ["point", "point", "multipoint", "linestring", "polygon", "multipolygon", "point"]
+    assert g[1][1:] == (True, False, [1.0, 2.0, 3.0]) and g[6][1:3] == (True, True)
+    assert g[4][3] == [[[0.0, 0.0], [4.0, 0.0], [4.0, 4.0], [0.0, 0.0]]]
+    for bad in ("POINT (1 2", "CIRCLE (1 2)", "POINT Q (1 2)", "POINT (1 2) junk", "POINT ()", "MULTIPOINT (1 2)"):
+        with pytest.raises(ConfigError):
+            config.read_wkt(bad)
+
+
+def test_point_selections():
+    base = ("mesh\n{\ncell count == 24 16\ncell size == 5 5\n}\nscheme == runge-kutta\n{\nend time == 1\n}\n"
+            "field == z_bed\n{\n  set == 1.0\n  add == constant\n  {\n    value == 0.5\n    within == at\n    {\n"
+            "      wkt == %s\n    }\n  }\n}\n")
+    m = config.Model(read_mf(base % "POINT (12.5 7.5), POINT (1000 1000), POINT Z (2.5 2.5 9)"))
+    z = m.field("z_bed", 0.0).ravel()
+    assert list(np.flatnonzero(z != 1.0)) == [0, 26] and z[26] == 1.5      # (1000, 1000) is outside
+    m = config.Model(read_mf(base % "LINESTRING (0 0, 10 10)"))
+    with pytest.raises(ConfigError, match="linestring"):
+        m.field("z_bed", 0.0)
