@@ -197,7 +197,7 @@ def test_oracle_eddy_viscosity_matches_numpy(case, mode, order):
     """Eddy viscosity (constant, per-cell and Smagorinsky coefficients) in any position among
     the momentum terms, against the numpy restatement."""
     nx, ny, dx, dy, nan_cells, seed = case
-    z, h, u, v = wet_dry_state(nx, ny, dx, seed=seed + 3, nan_cells=0)
+    z, h, u, v = wet_dry_state(nx, ny, dx, seed=seed + 3, nan_cells=nan_cells)   # coded-out cells too
     rng = np.random.default_rng(seed + 100)
     shape = (ny, nx)
     fx, fy = rng.uniform(0.0, 0.5, shape), rng.uniform(0.0, 0.5, shape)
