@@ -170,7 +170,9 @@ typedef struct sv_ctx sv_ctx;
 
 /* SaintVenantSolver constructor (src/SaintVenant/Solver.cpp:32-71) + RungeKuttaSolver
  * (src/TemporalScheme/RungeKutta.hpp:319-331): allocates U_[0..N], the k stages and the
- * bed constants on device `device`. */
+ * bed constants on device `device`. Later calls on the solver launch work on that device's
+ * streams: make `device` the current CUDA device before each call (one process per GPU,
+ * as the replicas run, satisfies this once and for all). */
 int sv_create(const sv_mesh_desc* mesh, const sv_params* params, int device, sv_ctx** out);
 /* ~SaintVenantSolver */
 void sv_destroy(sv_ctx* ctx);
