@@ -102,7 +102,9 @@ class FloodServer:
 
     def estimate_bytes(self, req):
         """Device memory of one member: 15 cell fields (two states, two stage buffers, bed and
-        its slopes), the per-cell Manning field, and the per-tile partial sums."""
+        its slopes), the per-cell Manning field, and the per-tile partial sums. Field uploads
+        stage through one FP64 buffer (8 bytes per cell of the largest mesh) that the library's
+        pool holds outside this estimate."""
         cells = req.nx * req.ny
         tiles = math.ceil(req.nx / 32) * math.ceil(req.ny / 8)
         return cells * self.value_bytes * 16 + tiles * 11 * 8 + 4096
