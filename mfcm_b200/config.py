@@ -12,24 +12,23 @@ The reader follows the reference's parser (src/Config/mf_parser/mf_parser_read.h
 On top of the tree sit the parts of the schema that drive this solver:
 
 - the mesh (Cartesian2DMesh.cpp:30-40);
-- the scheme and its time parameters, with the time parser's units, hours by default
-  (TimeParameters.cpp:23-38, TimeParser.cpp:20-104);
+- the scheme and its time parameters, with the time parser's units (hours by default) or
+  calendar times in a `time format` (TimeParameters.cpp:23-38, TimeParser.cpp:20-134);
 - fields built by `set` / `add` / `multiply` of constant, sloped, composite or NIMROD raster
-  inputs within id-list selections (FieldGenerator.cpp:26-178, MeshSelection.cpp:146-193,
-  Raster.cpp:35-68; the raster reader is mfcm_b200/raster.py);
+  inputs within global, id-list or point (WKT) selections (FieldGenerator.cpp:26-178,
+  MeshSelection.cpp:146-193, Raster.cpp:35-68; the raster reader is mfcm_b200/raster.py);
 - time series, inline or CSV (TimeSeries.cpp:179-296);
 - the source terms: Manning roughness, infiltration, energy loss, eddy viscosity
   (SourceTerm.cpp:32-50), the momentum terms in their configured order;
 - the boundaries: discharge, head, stage, each a list of constant or time-series entries on
-  cell selections (DischargeBoundarySourceTerm.hpp:114-146 and siblings).
-
+  cell selections (DischargeBoundarySourceTerm.hpp:114-146 and siblings);
 - outputs (`output == name`, cell fields as timed CSV files) and depth-point measures
   (`measures { h-point == name }`), written by `Model.solve`.
 
-Point selections (`at` with a `wkt` of points) are read. GDAL rasters and vector files and
-formatted (calendar) times are not read: a deck that
-uses them raises ConfigError naming the feature.
+GDAL rasters and vector files, geometries other than points in selections, and face or vertex
+outputs are not read: a deck that uses them raises ConfigError naming the feature.
 """
+import datetime
 import math
 import os
 import re
@@ -261,15 +260,47 @@ _UNITS = {"seconds": 1.0, "second": 1.0, "secs": 1.0, "sec": 1.0, "s": 1.0,
           "hours": 3600.0, "hour": 3600.0, "hrs": 3600.0, "hr": 3600.0, "h": 3600.0}
 
 
+def _calendar(fmt, text):
+    """std::get_time with `fmt`: a naive calendar time, or None when `text` does not start with
+    a time in that format (characters after the time are ignored, as get_time leaves them)."""
+    text = text.strip()
+    try:
+        return datetime.datetime.strptime(text, fmt)
+    except ValueError as e:
+        msg = str(e)
+        if msg.startswith("unconverted data remains: "):
+            rest = msg[len("unconverted data remains: "):]
+            try:
+                return datetime.datetime.strptime(text[:len(text) - len(rest)], fmt)
+            except ValueError:
+                return None
+        return None
+
+
 class TimeParser:
-    """Times in user units: a number times the unit factor, hours unless `time unit` says
-    otherwise (a named unit or a factor). Calendar time formats are not read."""
+    """Times in user units (TimeParser.cpp:44-134): a number times the unit factor, hours
+    unless `time unit` says otherwise (a named unit or a factor). With a `time format`, a time
+    written in that format counts in seconds from `time zero`. The difference is calendar
+    arithmetic, which is what mktime gives for times without daylight saving. Anything else
+    falls back to a number. A parser for a nested section inherits the format and time zero.
+    The reference requires `time zero` again in every such section, or its read throws."""
 
     def __init__(self, conf, parent=None):
         self.factor = parent.factor if parent else 3600.0
+        self.fmt = parent.fmt if parent else ""
+        self.zero = parent.zero if parent else None
         if conf is not None:
-            if conf.get("time format", "") != "":
-                raise ConfigError("calendar time formats (`time format`) are not supported")
+            fmt = conf.get("time format", self.fmt)
+            if fmt:
+                zero_text = conf.get("time zero", "")
+                if zero_text or self.zero is None or fmt != self.fmt:
+                    if not zero_text:
+                        raise ConfigError("a `time format` needs a `time zero`")
+                    zero = _calendar(fmt, zero_text)
+                    if zero is None:
+                        raise ConfigError(f"time zero {zero_text!r} does not match the format {fmt!r}")
+                    self.zero = zero
+                self.fmt = fmt
             u = conf.get("time unit", "default")
             if u in _UNITS:
                 self.factor = _UNITS[u]
@@ -280,7 +311,14 @@ class TimeParser:
                     raise ConfigError(f"unknown time unit {u!r}") from None
 
     def parse(self, s):
-        return float(s) * self.factor
+        if self.fmt:
+            t = _calendar(self.fmt, s)
+            if t is not None:
+                return (t - self.zero).total_seconds()
+        try:
+            return float(s) * self.factor
+        except ValueError:
+            raise ConfigError(f"cannot read {s!r} as a time") from None
 
 
 def _floats(s, n=None):

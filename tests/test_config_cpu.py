@@ -270,3 +270,40 @@ def test_point_selections():
     m = config.Model(read_mf(base % "LINESTRING (0 0, 10 10)"))
     with pytest.raises(ConfigError, match="linestring"):
         m.field("z_bed", 0.0)
+
+
+def test_calendar_times(tmp_path):
+    """A `time format` makes times calendar times counted from `time zero`; nested sections
+    (a CSV time series here) inherit the format and the time zero; plain numbers still count
+    in the unit."""
+    (tmp_path / "rain.csv").write_text("when,rate\n2023-03-01 00:00,1e-5\n2023-03-01 00:30,3e-5\n"
+                                       "2023-03-01 02:00,0\n")
+    deck = tmp_path / "deck.mf"
+    deck.write_text("""
+mesh
+{
+  cell count == 4 4
+  cell size == 1 1
+}
+scheme == runge-kutta
+{
+  time format == %Y-%m-%d %H:%M
+  time zero == 2023-03-01 00:00
+  start time == 2023-03-01 00:10
+  end time == 2023-03-01 01:10
+  step duration == 0.5
+}
+time series == rain
+{
+  source == csv
+  filename == rain.csv
+  time column == when
+  value column == rate
+}
+""")
+    m = config.load(str(deck))
+    assert (m.start_time, m.end_time, m.step_duration) == (600.0, 4200.0, 1800.0)
+    ts = m.series("rain")
+    assert ts.t == [0.0, 1800.0, 7200.0] and ts.v == [1e-5, 3e-5, 0.0]
+    with pytest.raises(ConfigError, match="time zero"):
+        config.TimeParser(read_mf("time format == %Y-%m-%d\n"))
