@@ -43,7 +43,12 @@ def test_facade_header_compiles_for_float_and_datum_options(tmp_path):
                    "  auto tp = std::make_shared<TimeParameters>();\n"
                    "  Options o; o.datum64 = true;\n"
                    "  using S = SaintVenantSolver<double, float>;\n"
-                   "  try { RungeKuttaSolver<S> rk(tp, \"ralston4\", mesh, o); } catch (const std::runtime_error&) {}\n"
+                   "  try {\n"
+                   "    RungeKuttaSolver<S> rk(tp, \"ralston4\", mesh, o);\n"
+                   "    rk.solver().set_eddy_viscosity(SV_EDDY_SMAGORINSKY);\n"
+                   "    rk.solver().set_source_order({SV_TERM_EDDY, SV_TERM_MANNING});\n"
+                   "    rk.solver().set_field(FieldId::eddy_mu, std::vector<double>(64, 0.5));\n"
+                   "  } catch (const std::runtime_error&) {}\n"
                    "  return TimeSeries({0.0, 10.0}, {0.0, 1.0}).at(5.0) == 0.5 ? 0 : 1;\n"
                    "}\n")
     r = subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src), "-L",
