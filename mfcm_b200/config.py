@@ -788,6 +788,9 @@ class Model:
             if at != "cells":
                 raise ConfigError(f"output {name!r}: only cell outputs are supported (at == {at})")
             fields = [f.value for f in conf.equal_range("field")] or [name]
+            for f in fields:
+                if f in ("mannings_n", "friction_slope"):  # ManningRoughnessSourceTerm.hpp:151-158
+                    raise ConfigError(f"output {name!r}: {f!r} is formed inside the stage kernels and not kept")
             fields = [f for f in fields if f in _OUTPUT_FIELDS or f == "stage"]
             start = self.parser.parse(conf.get("start time")) if conf.child("start time") is not None else self.start_time
             if conf.child("every") is not None:

@@ -19,7 +19,8 @@
 
 Field names follow the reference: "h", "u", "v" (State.hpp:139-149), "stage" (z_bed + h,
 Solver.hpp:90-98; formed here in FP64 from the host copies), "z_bed" (Constants.hpp:39),
-"IR" and "IC" (infiltration rate and capacity), "fdx" and "fdy" (energy-loss coefficients).
+"fx" and "fy" (energy-loss coefficients, EnergyLossSourceTerm.hpp:236-243; also under their
+input-field names "fdx" and "fdy"), and "IR" and "IC" (infiltration rate and capacity).
 """
 import json
 import math
@@ -31,7 +32,7 @@ import numpy as np
 from . import FIELD
 
 _NAMES = {"h": "H", "u": "U", "v": "V", "z_bed": "Z", "IR": "INFIL_RATE", "IC": "INFIL_CAP",
-          "fdx": "ELOSS_FX", "fdy": "ELOSS_FY", "h_comp": "H_COMP"}
+          "fx": "ELOSS_FX", "fy": "ELOSS_FY", "fdx": "ELOSS_FX", "fdy": "ELOSS_FY", "h_comp": "H_COMP"}
 
 
 def fmt_value(x):

@@ -307,3 +307,12 @@ time series == rain
     assert ts.t == [0.0, 1800.0, 7200.0] and ts.v == [1e-5, 3e-5, 0.0]
     with pytest.raises(ConfigError, match="time zero"):
         config.TimeParser(read_mf("time format == %Y-%m-%d\n"))
+
+
+def test_output_field_names():
+    base = ("mesh\n{\ncell count == 4 4\ncell size == 1 1\n}\nscheme == runge-kutta\n{\nend time == 1\n}\n"
+            "output == o\n{\nfield == %s\nevery seconds == 10\n}\n")
+    assert [o.fields for o in config.Model(read_mf(base % "fx")).outputs()] == [["fx"]]
+    assert [o.fields for o in config.Model(read_mf(base % "nothing")).outputs()] == [[]]   # skipped, as there
+    with pytest.raises(ConfigError, match="friction_slope"):
+        config.Model(read_mf(base % "friction_slope")).outputs()
