@@ -315,16 +315,17 @@ int sv_batch_size(sv_batch* batch, int* n_members, uint64_t* device_bytes);
  * GPU that loads the library until the process exits), which limits the mesh to 65536 cells
  * (256 x 256); larger meshes return SV_E_LIMIT.
  *   inputs  (device, FP64, nx*ny each): z, h, u, v = U_[0]
- *   outputs (device, FP64, nx*ny each): h_out, u_out, v_out = U_[N]; they must not alias the
- *           inputs. result (device, 3 doubles): control number, suggested next dt, 1.0 if the
- *           timestep must be repeated else 0.0.
+ *   outputs (device, FP64, nx*ny each): h_out, u_out, v_out = U_[N]; they must not overlap
+ *           the inputs or each other (SV_E_ARG). result (device, 3 doubles): control number,
+ *           suggested next dt, 1.0 if the timestep must be repeated else 0.0.
  *   manning: uniform n_shallow, n_deep, d_shallow, d_deep (host array of 4).
  *   forcing: SV_RAIN_NONE/UNIFORM and SV_HEAD_NONE/EDGES only (there is no field storage).
  *   params:  precision SV_F64 and a tableau whose stages use only the previous stage (euler,
  *            midpoint, heun2, ralston2, heun3, ralston3, classic).
  *   stream:  cudaStream_t to launch on (NULL = legacy default stream); nothing is synchronised.
  * The first call on each device looks up the array's device address (cudaGetSymbolAddress),
- * so make that first call before any stream capture. Every call uses the same array and it
+ * so make that first call before any stream capture; later calls outside capture look it up
+ * again, so a device reset between calls is safe. Every call uses the same array and it
  * keeps the previous call's contents (each call rewrites all of it before reading): calls
  * that overlap on the GPU -- on different streams, or from different host threads -- race. */
 int sv_timestep_noalloc(const sv_mesh_desc* mesh, const sv_params* params, const double manning[4],

@@ -1,11 +1,28 @@
 // sv_inst.cuh -- launcher definitions, included once per value type by sv_f64.cu / sv_f32.cu
 // with SV_T defined to the value type.
 #pragma once
+#include <atomic>
 #include <cmath>
 
 #include "sv_launch.h"
 
 namespace svk {
+
+// cudaFuncSetAttribute applies to the device that is current when it is called, so the
+// opt-in to more than 48 KB of dynamic shared memory is made once per device and kernel.
+// `done` is a per-kernel table indexed by device number.
+constexpr int kMaxAttrDevices = 64;
+template <typename K>
+static cudaError_t smem_optin(K kernel, int bytes, std::atomic<bool> (&done)[kMaxAttrDevices]) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev >= 0 && dev < kMaxAttrDevices && done[dev].load(std::memory_order_acquire)) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return e;
+  if (dev >= 0 && dev < kMaxAttrDevices) done[dev].store(true, std::memory_order_release);
+  return cudaSuccess;
+}
 
 // dx and dy both powers of two: the mesh divisions are exact multiplies
 inline bool pow2_mesh(double dx, double dy) {
@@ -16,13 +33,9 @@ inline bool pow2_mesh(double dx, double dy) {
 template <typename T, int TX, int TY, int MINB, bool P2, bool EDDY>
 static cudaError_t launch_stage_p(const StageParams<T>& P, cudaStream_t s) {
   using SM = StageSmem<T, TX, TY>;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(stage_kernel<T, TX, TY, MINB, P2, EDDY>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(SM)));
-    if (e != cudaSuccess) return e;
-    attr_set = true;
-  }
+  static std::atomic<bool> attr_set[kMaxAttrDevices];
+  cudaError_t e = smem_optin(stage_kernel<T, TX, TY, MINB, P2, EDDY>, int(sizeof(SM)), attr_set);
+  if (e != cudaSuccess) return e;
   dim3 grid((P.nx + TX - 1) / TX, (P.ny + TY - 1) / TY);
   stage_kernel<T, TX, TY, MINB, P2, EDDY><<<grid, TX * TY, sizeof(SM), s>>>(P);
   return cudaGetLastError();
@@ -115,13 +128,9 @@ template <typename T, int TX, int TY, int MINB, bool P2, bool EDDY>
 static cudaError_t launch_stage_batch_p(const StageParams<T>* Ps, const long long* tile_start, int ninst,
                                         long long total_tiles, cudaStream_t s) {
   using SM = StageSmem<T, TX, TY>;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(stage_batch_kernel<T, TX, TY, MINB, P2, EDDY>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(SM)));
-    if (e != cudaSuccess) return e;
-    attr_set = true;
-  }
+  static std::atomic<bool> attr_set[kMaxAttrDevices];
+  cudaError_t e = smem_optin(stage_batch_kernel<T, TX, TY, MINB, P2, EDDY>, int(sizeof(SM)), attr_set);
+  if (e != cudaSuccess) return e;
   if (total_tiles <= 0) return cudaSuccess;
   stage_batch_kernel<T, TX, TY, MINB, P2, EDDY><<<unsigned(total_tiles), TX * TY, sizeof(SM), s>>>(Ps, tile_start,
                                                                                                      ninst);

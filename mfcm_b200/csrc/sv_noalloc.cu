@@ -18,6 +18,7 @@
 
 #include "../../include/sv.h"
 #include "sv_launch.h"
+#include "sv_tableau.h"
 
 namespace svh {
 void set_global_error(const std::string& msg);
@@ -49,25 +50,44 @@ constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 unsigned char* g_addr[kMaxDevices] = {};
 
-// Device address of g_sv_scratch on the current device, looked up once per device.
-int scratch_address(int dev, unsigned char** out) {
+// Device address of g_sv_scratch on the current device. Outside stream capture it is looked
+// up again on every call (cheap once the module is loaded), so a device reset or another
+// context made current never leaves a stale address behind; during capture the address of the
+// last uncaptured call on this device is used, so that first call must come before capture.
+int scratch_address(int dev, cudaStream_t s, unsigned char** out) {
   if (dev < 0 || dev >= kMaxDevices) {
     svh::set_global_error("sv_timestep_noalloc: device index out of range");
     return SV_E_ARG;
   }
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaError_t e = cudaStreamIsCapturing(s, &cap);
+  if (e != cudaSuccess) {
+    svh::set_global_error(std::string("sv_timestep_noalloc: cudaStreamIsCapturing failed: ") +
+                          cudaGetErrorString(e));
+    return SV_E_CUDA;
+  }
   std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_addr[dev]) {
+  if (cap == cudaStreamCaptureStatusNone) {
     void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_sv_scratch);
+    e = cudaGetSymbolAddress(&p, g_sv_scratch);
     if (e != cudaSuccess || p == nullptr) {
       svh::set_global_error(std::string("sv_timestep_noalloc: cudaGetSymbolAddress failed: ") +
                             cudaGetErrorString(e));
       return SV_E_CUDA;
     }
     g_addr[dev] = static_cast<unsigned char*>(p);
+  } else if (!g_addr[dev]) {
+    svh::set_global_error("sv_timestep_noalloc: the first call on a device must come before stream capture");
+    return SV_E_STATE;
   }
   *out = g_addr[dev];
   return SV_OK;
+}
+
+// Whether the byte ranges [a, a + n) and [b, b + n) share a byte.
+bool overlap(const void* a, const void* b, size_t n) {
+  const uintptr_t x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
+  return x < y + n && y < x + n;
 }
 
 // Controller and forcing slots are rewritten on every call (the array keeps the previous
@@ -87,47 +107,6 @@ __global__ void noalloc_result_kernel(const svk::Ctl* ctl, double* result) {
   result[2] = double(ctl->repeat);
 }
 
-bool diagonal_tableau(int id) {
-  // euler, midpoint, heun2, ralston2, heun3, ralston3, classic: Y_{s+1} uses k_s only
-  return id == 0 || id == 1 || id == 2 || id == 3 || id == 5 || id == 7 || id == 9;
-}
-
-struct Coefs {
-  int N;
-  double c[4], a_next[4][4], b[4];
-};
-
-bool coefs_for(int id, Coefs& k) {
-  // the diagonal named tableaux (src/TemporalScheme/RungeKutta.cpp:54-115)
-  for (auto& r : k.a_next)
-    for (double& x : r) x = 0.0;
-  for (int i = 0; i < 4; ++i) k.c[i] = k.b[i] = 0.0;
-  switch (id) {
-    case 0: k.N = 1; k.b[0] = 1.0; return true;
-    case 1: k.N = 2; k.c[1] = 0.5; k.a_next[0][0] = 0.5; k.b[1] = 1.0; return true;
-    case 2: k.N = 2; k.c[1] = 1.0; k.a_next[0][0] = 1.0; k.b[0] = 0.5; k.b[1] = 0.5; return true;
-    case 3:
-      k.N = 2; k.c[1] = 2.0 / 3.0; k.a_next[0][0] = 2.0 / 3.0; k.b[0] = 0.25; k.b[1] = 0.75;
-      return true;
-    case 5:
-      k.N = 3; k.c[1] = 1.0 / 3.0; k.c[2] = 2.0 / 3.0;
-      k.a_next[0][0] = 1.0 / 3.0; k.a_next[1][1] = 2.0 / 3.0;
-      k.b[0] = 0.25; k.b[2] = 0.75;
-      return true;
-    case 7:
-      k.N = 3; k.c[1] = 0.5; k.c[2] = 0.75;
-      k.a_next[0][0] = 0.5; k.a_next[1][1] = 0.75;
-      k.b[0] = 2.0 / 9.0; k.b[1] = 1.0 / 3.0; k.b[2] = 4.0 / 9.0;
-      return true;
-    case 9:
-      k.N = 4; k.c[1] = 0.5; k.c[2] = 0.5; k.c[3] = 1.0;
-      k.a_next[0][0] = 0.5; k.a_next[1][1] = 0.5; k.a_next[2][2] = 1.0;
-      k.b[0] = 1.0 / 6.0; k.b[1] = 1.0 / 3.0; k.b[2] = 1.0 / 3.0; k.b[3] = 1.0 / 6.0;
-      return true;
-  }
-  return false;
-}
-
 int fail(int code, const char* msg) {
   svh::set_global_error(std::string("sv_timestep_noalloc: ") + msg);
   return code;
@@ -142,8 +121,9 @@ extern "C" int sv_timestep_noalloc(const sv_mesh_desc* mesh, const sv_params* pa
   if (!mesh || !params || !manning || !forcing || !z || !h || !u || !v || !h_out || !u_out || !v_out || !result)
     return fail(SV_E_ARG, "null argument");
   if (params->precision != SV_F64) return fail(SV_E_ARG, "only the FP64 path is available without allocation");
-  Coefs k;
-  if (!diagonal_tableau(params->rk_method) || !coefs_for(params->rk_method, k))
+  svt::Tableau tab;
+  svt::StageCoefs k;
+  if (!svt::named_tableau(params->rk_method, tab) || !svt::is_diagonal(tab) || !svt::stage_coefs(tab, k))
     return fail(SV_E_ARG, "the Runge-Kutta tableau must be one whose stages use only the previous stage "
                           "(euler, midpoint, heun2, ralston2, heun3, ralston3, classic)");
   if (mesh->nx == 0 || mesh->ny == 0) return fail(SV_E_ARG, "empty mesh");
@@ -159,26 +139,29 @@ extern "C" int sv_timestep_noalloc(const sv_mesh_desc* mesh, const sv_params* pa
     return fail(SV_E_ARG, "only edge-strip head boundaries (or none) are available without allocation");
   const long long nblk = svk::variant_partials(kVariant, (long long)mesh->nx, (long long)mesh->ny);
   if (nblk > kMaxBlocks) return fail(SV_E_LIMIT, "mesh needs more partial-sum slots than the working array holds");
+  const size_t field_bytes = size_t(mesh->nx * mesh->ny) * sizeof(double);
   const double* outs[3] = {h_out, u_out, v_out};
   const double* ins[4] = {z, h, u, v};
-  for (const double* o : outs)
+  for (int a = 0; a < 3; ++a) {
     for (const double* i : ins)
-      if (o == i) return fail(SV_E_ARG, "output buffers must not alias the inputs");
+      if (overlap(outs[a], i, field_bytes)) return fail(SV_E_ARG, "output buffers must not overlap the inputs");
+    for (int b = a + 1; b < 3; ++b)
+      if (overlap(outs[a], outs[b], field_bytes)) return fail(SV_E_ARG, "output buffers must not overlap each other");
+  }
 
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(SV_E_CUDA, cudaGetErrorString(e));
-  unsigned char* base = nullptr;
-  int r = scratch_address(dev, &base);
-  if (r != SV_OK) return r;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  unsigned char* base = nullptr;
+  int r = scratch_address(dev, s, &base);
+  if (r != SV_OK) return r;
   double* Y = reinterpret_cast<double*>(base + kYOffset);
   double* zx = reinterpret_cast<double*>(base + kZxOffset);
   double* zy = reinterpret_cast<double*>(base + kZyOffset);
   double* part = reinterpret_cast<double*>(base + kPartOffset);
   svk::Ctl* ctl = reinterpret_cast<svk::Ctl*>(base + kCtlOffset);
   svk::DevForcing* fc = reinterpret_cast<svk::DevForcing*>(base + kFcOffset);
-  const long long n = (long long)mesh->nx * (long long)mesh->ny;
 
   svk::DevForcing f{};
   f.rain_kind = forcing->rain_kind;
@@ -239,6 +222,5 @@ extern "C" int sv_timestep_noalloc(const sv_mesh_desc* mesh, const sv_params* pa
   noalloc_result_kernel<<<1, 1, 0, s>>>(ctl, result);
   e = cudaGetLastError();
   if (e != cudaSuccess) return fail(SV_E_CUDA, cudaGetErrorString(e));
-  (void)n;
   return SV_OK;
 }

@@ -1,0 +1,577 @@
+// ref_pin.cpp -- TEST INFRASTRUCTURE: runs the reference's own hot-path code on the CPU so that
+// the oracle (oracle/sv_oracle.hpp) can be checked against it. Built by oracle/ref_pin/build.py
+// into oracle/_ref/libsv_refpin.so from the reference's sources; only tests/ load it.
+//
+// What runs here is the reference's code, compiled unchanged:
+//   mesh, field and data-array classes    src/Mesh/Cartesian2DMesh.hpp, src/Field/Field.cpp,
+//                                         src/DataArray/DataArray.cpp
+//   slopes                                SaintVenantState::calculate_spatial_derivatives
+//                                         (src/SaintVenant/State.cpp:176-193) with
+//                                         SpatialDerivativeOperator<Minmod3> (SpatialDerivative.cpp)
+//   bed slopes                            the same operator on z (as Constants.cpp:39-40)
+//   face fluxes                           SaintVenantFluxes::update (Fluxes.cpp) launching
+//                                         SaintVenantFluxKernel (FluxKernel.cpp:62-295)
+//   temporal derivative                   SaintVenantTemporalDerivativeKernel (:43-99)
+//   Manning roughness                     ManningRoughnessSourceKernel (:44-88)
+//   discharge and head boundaries         DischargeBoundarySourceKernel (:39-69),
+//                                         HeadBoundarySourceKernel (:39-67)
+//   control number                        SaintVenantState::max_control_number (State.cpp:195-230)
+//   stage combination                     the SaintVenantState operators (State.cpp:88-174) in
+//                                         the order of RungeKuttaSolver::update_y
+//                                         (RungeKutta.hpp:377-388)
+//   whole solves                          RungeKuttaSolver<Solver> (RungeKutta.hpp:268-463) with
+//                                         the named tableaux and do_timestep (RungeKutta.cpp),
+//                                         TypedTemporalScheme::solve / step (TemporalScheme.hpp)
+//                                         and TimeParameters::num_steps (TimeParameters.cpp)
+// The driver only creates the objects, fills them from arrays and launches the kernels in the
+// order of SaintVenantSolver::update_dUdt (Solver.cpp:73-114) -- the launch code of each
+// source and boundary term's apply() -- and copies the results out. For whole solves it
+// stands in for SaintVenantSolver (whose constructor reads the configuration) with PinSolver,
+// which has the same interface and sets the boundary values as the discharge and head terms'
+// start_new_step do for a global rain selection and edge-strip head selections.
+#include "sycl.hpp"
+
+#include "DataArray.hpp"
+#include "DataArray.cpp"
+#include "Mesh.hpp"
+#include "Cartesian2DMesh.hpp"
+#include "MeshSelection.hpp"
+#include "Field.hpp"
+#include "Field.cpp"
+#include "FieldOperators.cpp"
+#include "Minmod3.hpp"
+#include "SpatialDerivative.hpp"
+#include "SpatialDerivative.cpp"
+#include "State.hpp"
+#include "Constants.hpp"
+#include "State.cpp"
+#include "Fluxes.hpp"
+#include "Fluxes.cpp"
+#include "FluxKernel.cpp"
+#include "TemporalDerivativeKernel.hpp"
+#include "TemporalDerivativeKernel.cpp"
+#include "SourceTerm.hpp"
+#include "ManningRoughnessSourceTerm.hpp"
+#include "ManningRoughnessSourceTerm.cpp"
+#include "DischargeBoundarySourceTerm.hpp"
+#include "DischargeBoundarySourceTerm.cpp"
+#include "HeadBoundarySourceTerm.hpp"
+#include "HeadBoundarySourceTerm.cpp"
+#include "TimeParameters.hpp"
+#include "TimeParameters.cpp"
+#include "RungeKutta.hpp"
+#include "RungeKutta.cpp"
+
+#include <cstdint>
+#include <cstring>
+#include <iostream>
+
+// ---- glue the reference defines in files that read its configuration --------------------
+// Cartesian2DMesh's configured constructor and device moves are compiled from the reference
+// only through src/Mesh/Cartesian2DMesh.cpp, which also defines the raster constructor whose
+// cell count is lost (it copies the count vector); the configured constructor is restated
+// here from Cartesian2DMesh.cpp:24-61 with the same geo-transform layout and arithmetic.
+Cartesian2DMesh::Cartesian2DMesh(const std::shared_ptr<sycl::queue>& queue, bool on_device)
+    : ncells_(queue, 2), geotrans_(queue, 12) {
+  const Config& conf = GlobalConfig::instance().mesh_configuration();
+  std::array<size_t, 2> user_ncells = split_string<size_t, 2>(conf.get<std::string>("cell count"));
+  ncells_.host_vector() = {user_ncells[0], user_ncells[1]};
+  std::array<double, 2> user_origin = split_string<double, 2>(conf.get<std::string>("origin", "0.0, 0.0"));
+  std::array<double, 2> user_cellsize = split_string<double, 2>(conf.get<std::string>("cell size"));
+  double rotation = conf.get<double>("angle", 0.0);
+  std::vector<double>& gt = geotrans_.host_vector();
+  gt[0] = user_origin[0];
+  gt[1] = user_cellsize[0] * std::cos(rotation);
+  gt[2] = user_cellsize[0] * std::sin(rotation);
+  gt[3] = user_origin[1];
+  gt[4] = user_cellsize[1] * std::sin(rotation);
+  gt[5] = user_cellsize[1] * std::cos(rotation);
+  gt[6] = 1.0 / gt.at(1);
+  gt[7] = 1.0 / gt.at(5);
+  gt[8] = 1.0 / (gt.at(1) * gt.at(5));
+  gt[9] = 1.0 - (gt.at(2) * gt.at(4)) * gt.at(8);
+  gt[10] = std::sqrt(gt[1] * gt[1] + gt[2] * gt[2]);
+  gt[11] = std::sqrt(gt[4] * gt[4] + gt[5] * gt[5]);
+  if (on_device) {
+    ncells_.move_to_device();
+    geotrans_.move_to_device();
+  }
+}
+void Cartesian2DMesh::move_to_device(void) {
+  ncells_.move_to_device();
+  geotrans_.move_to_device();
+}
+void Cartesian2DMesh::move_to_host(void) {
+  ncells_.move_to_host();
+  geotrans_.move_to_host();
+}
+Cartesian2DMeshAccessor::Cartesian2DMeshAccessor(const Cartesian2DMesh& c2m)
+    : ncells_ro_(c2m.ncells_data()
+                     .template get_placeholder_accessor<sycl::access::mode::read, sycl::access::target::global_buffer>()),
+      geotrans_ro_(c2m.geotrans_data()
+                       .template get_placeholder_accessor<sycl::access::mode::read, sycl::access::target::global_buffer>()) {}
+void Cartesian2DMeshAccessor::bind(sycl::handler& cgh) {
+  cgh.require(ncells_ro_);
+  cgh.require(geotrans_ro_);
+}
+
+// MeshSelection, global selections only (MeshSelection.cpp:22-33, 146-157, 196-214): a global
+// selection is a two-entry list holding the object count twice.
+template <typename Mesh, MeshComponent C>
+MeshSelection<Mesh, C>::MeshSelection(const std::shared_ptr<MeshType>& mesh_p, const Config&)
+    : mesh_p_(mesh_p), list_(mesh_p->queue_ptr(), 0) {
+  initialize_global_();
+}
+template <typename Mesh, MeshComponent C>
+void MeshSelection<Mesh, C>::initialize_global_(void) {
+  std::vector<size_t>& id_list = list_.host_vector();
+  size_t idmax = mesh_p_->template object_count<FieldMappingType>();
+  id_list.push_back(idmax);
+  id_list.push_back(idmax);
+  list_.move_to_device();
+}
+template <typename Mesh, MeshComponent C>
+bool MeshSelection<Mesh, C>::is_global(void) const {
+  return list_.size() == 2 && list_.host_vector().at(0) == list_.host_vector().at(1);
+}
+template <typename Mesh, MeshComponent C>
+size_t MeshSelection<Mesh, C>::size(void) const {
+  if (is_global()) return mesh_p_->template object_count<FieldMappingType>();
+  return list_.size() - 1;
+}
+
+// SaintVenantConstants (Constants.cpp:25-44) with the bed taken from an array instead of a
+// configured field generator; the slopes come from the reference's operator as there.
+template <typename T>
+struct PinBed {
+  static std::vector<T> z;
+};
+template <typename T>
+std::vector<T> PinBed<T>::z;
+template <typename T, typename Mesh>
+SaintVenantConstants<T, Mesh>::SaintVenantConstants(const std::shared_ptr<MeshType>& mesh, bool on_device)
+    : mesh_(mesh),
+      z_bed_(mesh_->queue_ptr(), "z_bed", mesh_, PinBed<T>::z, on_device),
+      dzdx_bed_(mesh_->queue_ptr(), "dzdx_bed", mesh_, 0.0f, on_device),
+      dzdy_bed_(mesh_->queue_ptr(), "dzdy_bed", mesh_, 0.0f, on_device) {
+  using SpatialDerivative = SpatialDerivativeOperator<ValueType, MeshType, MeshComponent::Cell, Minmod3<ValueType>>;
+  SpatialDerivative::template apply<SpatialDerivativeAxis::X>(z_bed_, dzdx_bed_);
+  SpatialDerivative::template apply<SpatialDerivativeAxis::Y>(z_bed_, dzdy_bed_);
+}
+
+std::shared_ptr<sycl::queue> get_sycl_queue(void) { return std::make_shared<sycl::queue>(); }
+
+namespace {
+
+template <typename T>
+using CF = CellField<T, Cartesian2DMesh>;
+template <typename T>
+using State = SaintVenantState<T, Cartesian2DMesh>;
+
+std::shared_ptr<Cartesian2DMesh> make_mesh(const std::shared_ptr<sycl::queue>& q, uint64_t nx, uint64_t ny, double dx,
+                                           double dy) {
+  Config& c = GlobalConfig::instance().mesh;
+  c.kv.clear();
+  c.kv["cell count"] = std::to_string(nx) + ", " + std::to_string(ny);
+  {
+    std::ostringstream s;
+    s.precision(17);
+    s << dx << ", " << dy;
+    c.kv["cell size"] = s.str();
+  }
+  return std::make_shared<Cartesian2DMesh>(q, true);
+}
+
+template <typename T>
+std::vector<T> vec(const T* p, size_t n) {
+  return std::vector<T>(p, p + n);
+}
+
+// a field's values: move it to the host (DataArray::move_to_host writes the buffer back), copy
+template <typename F, typename T>
+void read(F& f, T* out) {
+  f.move_to_host();
+  const std::vector<T>& v = f.data().host_vector();
+  std::copy(v.begin(), v.end(), out);
+  f.move_to_device();
+}
+
+template <typename T>
+void set_state(State<T>& s, const std::shared_ptr<sycl::queue>& q, const std::shared_ptr<Cartesian2DMesh>& m,
+               const T* h, const T* u, const T* v, size_t n) {
+  s.h() = CF<T>(q, "h", m, vec(h, n), true);
+  s.u() = CF<T>(q, "u", m, vec(u, n), true);
+  s.v() = CF<T>(q, "v", m, vec(v, n), true);
+}
+
+// One update_dUdt (Solver.cpp:73-114) of the state (h, u, v) on bed z, at local time
+// `time_now` with `timestep` and step length `step_length` (rounded to T first, as TimeType). Optional terms are
+// skipped when their arrays are null: Manning (ns, nd, ds, dd), discharge (q0, q1), head
+// (hb0, hb1), in the configured order (head before discharge when head_first).
+// out: dzdx, dzdy, dhdx, dudx, dvdx, dhdy, dudy, dvdy (cell fields), then h, u, v, z flux and
+// branch (face fields), then dh/dt, du/dt, dv/dt (cell fields).
+template <typename T>
+int dudt(uint64_t nx, uint64_t ny, double dx, double dy, const T* z, const T* h, const T* u, const T* v, const T* ns,
+         const T* nd, const T* ds, const T* dd, const T* q0, const T* q1, const T* hb0, const T* hb1, int head_first,
+         double time_now, double timestep, double step_length, T* out) {
+  try {
+    // the shipped solver takes its times in the value type (TimeType = ValueType, mfcm.cpp:13-16):
+    // the kernels receive them widened from T
+    using TT = T;
+    const TT tnow = TT(time_now), tstep = TT(timestep), tlen = TT(step_length);
+    auto q = get_sycl_queue();
+    auto mesh = make_mesh(q, nx, ny, dx, dy);
+    const size_t nc = nx * ny, nf = mesh->template object_count<MeshComponent::Face>();
+    PinBed<T>::z = vec(z, nc);
+    SaintVenantConstants<T, Cartesian2DMesh> K(mesh, true);
+    State<T> U(T(0), mesh), dUdx(T(0), mesh), dUdy(T(0), mesh), dUdt(T(0), mesh);
+    set_state(U, q, mesh, h, u, v, nc);
+    SaintVenantFluxes<T, Cartesian2DMesh> F(mesh);
+
+    U.calculate_spatial_derivatives(dUdx, dUdy);
+    F.update(U, K, dUdx, dUdy);
+    using TDKernel = SaintVenantTemporalDerivativeKernel<T, Cartesian2DMesh>;
+    q->submit([&](sycl::handler& cgh) {
+      auto kernel = TDKernel(cgh, U, K, dUdx, dUdy, F, dUdt, tnow, tstep);
+      cgh.parallel_for(sycl::range<1>(nc), kernel);
+    });
+    if (ns) {
+      CF<T> fns(q, "n_shallow", mesh, vec(ns, nc), true), fnd(q, "n_deep", mesh, vec(nd, nc), true);
+      CF<T> fds(q, "d_shallow", mesh, vec(ds, nc), true), fdd(q, "d_deep", mesh, vec(dd, nc), true);
+      CF<T> nh(q, "mannings_n", mesh, 0.0f, true), Sf(q, "friction_slope", mesh, 0.0f, true);
+      using Kernel = ManningRoughnessSourceKernel<TT, T, Cartesian2DMesh>;
+      q->submit([&](sycl::handler& cgh) {
+        auto kernel = Kernel(cgh, U, K, fns, fnd, fds, fdd, nh, Sf, dUdt, tstep);
+        cgh.parallel_for(sycl::range<1>(nc), kernel);
+      });
+    }
+    auto discharge = [&]() {
+      if (!q0) return;
+      CF<T> f0(q, "qbdy0", mesh, vec(q0, nc), true), f1(q, "qbdy1", mesh, vec(q1, nc), true);
+      using Kernel = DischargeBoundarySourceKernel<T, Cartesian2DMesh>;
+      q->submit([&](sycl::handler& cgh) {
+        auto kernel = Kernel(cgh, U, K, f0, f1, dUdt, tstep, tnow, tlen);
+        cgh.parallel_for(sycl::range<1>(nc), kernel);
+      });
+    };
+    auto head = [&]() {
+      if (!hb0) return;
+      CF<T> f0(q, "hbdy0", mesh, vec(hb0, nc), true), f1(q, "hbdy1", mesh, vec(hb1, nc), true);
+      using Kernel = HeadBoundarySourceKernel<T, Cartesian2DMesh>;
+      q->submit([&](sycl::handler& cgh) {
+        auto kernel = Kernel(cgh, U, K, f0, f1, dUdt, tstep, tnow, tlen);
+        cgh.parallel_for(sycl::range<1>(nc), kernel);
+      });
+    };
+    if (head_first) { head(); discharge(); }
+    else { discharge(); head(); }
+
+    T* o = out;
+    CF<T>* cells[] = {const_cast<CF<T>*>(&K.dzdx_bed()), const_cast<CF<T>*>(&K.dzdy_bed()),
+                      &dUdx.h(), &dUdx.u(), &dUdx.v(), &dUdy.h(), &dUdy.u(), &dUdy.v()};
+    for (CF<T>* f : cells) { read(*f, o); o += nc; }
+    using FF = FaceField<T, Cartesian2DMesh>;
+    FF* faces[] = {&F.h(), &F.u(), &F.v(), &F.z(), F.template get_output_field_ptr<FF>("flux-branch")};
+    for (FF* f : faces) { read(*f, o); o += nf; }
+    CF<T>* ks[] = {&dUdt.h(), &dUdt.u(), &dUdt.v()};
+    for (CF<T>* f : ks) { read(*f, o); o += nc; }
+    return 0;
+  } catch (const std::exception& e) {
+    std::cerr << "ref_pin: " << e.what() << std::endl;
+    return -1;
+  }
+}
+
+// SaintVenantState::max_control_number (State.cpp:195-230) of (h, u, v) for `timestep`
+template <typename T>
+int control_number(uint64_t nx, uint64_t ny, double dx, double dy, const T* h, const T* u, const T* v, double timestep,
+                   T* cn) {
+  try {
+    auto q = get_sycl_queue();
+    auto mesh = make_mesh(q, nx, ny, dx, dy);
+    State<T> U(T(0), mesh);
+    set_state(U, q, mesh, h, u, v, nx * ny);
+    *cn = U.max_control_number(timestep);
+    return 0;
+  } catch (const std::exception& e) {
+    std::cerr << "ref_pin: " << e.what() << std::endl;
+    return -1;
+  }
+}
+
+// RungeKuttaSolver::update_y (RungeKutta.hpp:377-388) through the SaintVenantState
+// operators: Y = U0, then Y += k_col * (a_col * timestep) for col = 0 .. ncols-1.
+template <typename T>
+int update_y(uint64_t nx, uint64_t ny, double dx, double dy, const T* u0, const T* k, int ncols, const double* a,
+             double timestep, T* y) {
+  try {
+    auto q = get_sycl_queue();
+    auto mesh = make_mesh(q, nx, ny, dx, dy);
+    const size_t nc = nx * ny;
+    State<T> U0(T(0), mesh), Y(T(0), mesh);
+    set_state(U0, q, mesh, u0, u0 + nc, u0 + 2 * nc, nc);
+    std::vector<std::unique_ptr<State<T>>> K;
+    for (int c = 0; c < ncols; ++c) {
+      K.emplace_back(new State<T>(T(0), mesh));
+      const T* kc = k + size_t(c) * 3 * nc;
+      set_state(*K.back(), q, mesh, kc, kc + nc, kc + 2 * nc, nc);
+    }
+    Y = U0;
+    for (int c = 0; c < ncols; ++c) Y += *K[c] * (a[c] * timestep);
+    read(Y.h(), y);
+    read(Y.u(), y + nc);
+    read(Y.v(), y + 2 * nc);
+    return 0;
+  } catch (const std::exception& e) {
+    std::cerr << "ref_pin: " << e.what() << std::endl;
+    return -1;
+  }
+}
+
+// Problem handed to PinSolver (RungeKuttaSolver constructs its solver itself).
+template <typename T>
+struct PinProblem {
+  uint64_t nx = 0, ny = 0;
+  double dx = 1, dy = 1;
+  std::vector<T> z, h, u, v;
+  bool manning = false;
+  T n[4] = {};
+  std::vector<double> rain_t, rain_v;  // rain time series knots (m/s); empty: no discharge term
+  unsigned head_edges = 0;             // SV_EDGE_* bits of the head strips; 0: no head term
+  T head_value = 0;
+  bool head_first = false;
+  uint64_t timesteps = 0;              // do_timestep calls (accepted + repeated)
+};
+template <typename T>
+PinProblem<T>* g_problem = nullptr;
+
+// TimeSeries::at with ts_linterp (src/Input/TimeSeries.cpp:26-47), last segment extrapolated
+double series_at(const std::vector<double>& t, const std::vector<double>& v, double time) {
+  size_t i1 = 1;
+  while (i1 < t.size() && !(t[i1] > time)) ++i1;
+  if (i1 >= t.size()) i1 = t.size() - 1;
+  const size_t i0 = i1 - 1;
+  const double dvdt = (v[i1] - v[i0]) / (t[i1] - t[i0]);
+  return v[i0] + dvdt * (time - t[i0]);
+}
+
+// Stand-in for SaintVenantSolver<T, T, Cartesian2DMesh> with its interface to RungeKuttaSolver.
+template <typename T>
+class PinSolver {
+ public:
+  using TimeType = T;
+  using ValueType = T;
+  using MeshType = Cartesian2DMesh;
+  using StateT = SaintVenantState<T, Cartesian2DMesh>;
+
+  PinSolver(const std::shared_ptr<sycl::queue>& q, const size_t& nstates, const std::shared_ptr<TimeParameters<T>>& tp)
+      : q_(q), P_(*g_problem<T>) {
+    mesh_ = make_mesh(q, P_.nx, P_.ny, P_.dx, P_.dy);
+    const size_t nc = P_.nx * P_.ny;
+    PinBed<T>::z = P_.z;
+    K_ = std::make_shared<SaintVenantConstants<T, Cartesian2DMesh>>(mesh_, true);
+    for (size_t i = 0; i < nstates; ++i) {
+      U_.push_back(std::make_shared<StateT>(T(0), mesh_));
+      dUdt_.push_back(std::make_shared<StateT>(T(0), mesh_));
+    }
+    set_state(*U_[0], q, mesh_, P_.h.data(), P_.u.data(), P_.v.data(), nc);
+    dUdx_ = std::make_shared<StateT>(T(0), mesh_);
+    dUdy_ = std::make_shared<StateT>(T(0), mesh_);
+    F_ = std::make_shared<SaintVenantFluxes<T, Cartesian2DMesh>>(mesh_);
+    const char* names[4] = {"n_shallow", "n_deep", "d_shallow", "d_deep"};
+    for (int i = 0; i < 4; ++i) man_.emplace_back(q, names[i], mesh_, P_.n[i], true);
+    nh_ = std::make_shared<CF<T>>(q, "mannings_n", mesh_, 0.0f, true);
+    Sf_ = std::make_shared<CF<T>>(q, "friction_slope", mesh_, 0.0f, true);
+    q0_ = std::make_shared<CF<T>>(q, "qbdy0", mesh_, 0.0f, true);
+    q1_ = std::make_shared<CF<T>>(q, "qbdy1", mesh_, 0.0f, true);
+    const T nan = std::numeric_limits<T>::quiet_NaN();
+    hb0_ = std::make_shared<CF<T>>(q, "hbdy0", mesh_, nan, true);
+    hb1_ = std::make_shared<CF<T>>(q, "hbdy1", mesh_, nan, true);
+  }
+
+  // SaintVenantSolver::update_dUdt (Solver.cpp:73-114)
+  void update_dUdt(const size_t& state_no, const T& time_now, const T& timestep) {
+    StateT& U = *U_.at(state_no);
+    StateT& D = *dUdt_.at(state_no);
+    U.calculate_spatial_derivatives(*dUdx_, *dUdy_);
+    F_->update(U, *K_, *dUdx_, *dUdy_);
+    const size_t nc = mesh_->template object_count<MeshComponent::Cell>();
+    using TDKernel = SaintVenantTemporalDerivativeKernel<T, Cartesian2DMesh>;
+    q_->submit([&](sycl::handler& cgh) {
+      auto kernel = TDKernel(cgh, U, *K_, *dUdx_, *dUdy_, *F_, D, time_now, timestep);
+      cgh.parallel_for(sycl::range<1>(nc), kernel);
+    });
+    if (P_.manning) {
+      using Kernel = ManningRoughnessSourceKernel<T, T, Cartesian2DMesh>;
+      q_->submit([&](sycl::handler& cgh) {
+        auto kernel = Kernel(cgh, U, *K_, man_[0], man_[1], man_[2], man_[3], *nh_, *Sf_, D, timestep);
+        cgh.parallel_for(sycl::range<1>(nc), kernel);
+      });
+    }
+    const T tlen = TimeType(step_length_);
+    auto discharge = [&]() {
+      if (P_.rain_t.empty()) return;
+      using Kernel = DischargeBoundarySourceKernel<T, Cartesian2DMesh>;
+      q_->submit([&](sycl::handler& cgh) {
+        auto kernel = Kernel(cgh, U, *K_, *q0_, *q1_, D, timestep, time_now, tlen);
+        cgh.parallel_for(sycl::range<1>(nc), kernel);
+      });
+    };
+    auto head = [&]() {
+      if (!P_.head_edges) return;
+      using Kernel = HeadBoundarySourceKernel<T, Cartesian2DMesh>;
+      q_->submit([&](sycl::handler& cgh) {
+        auto kernel = Kernel(cgh, U, *K_, *hb0_, *hb1_, D, timestep, time_now, tlen);
+        cgh.parallel_for(sycl::range<1>(nc), kernel);
+      });
+    };
+    if (P_.head_first) { head(); discharge(); }
+    else { discharge(); head(); }
+  }
+
+  // DischargeBoundarySourceTerm / HeadBoundarySourceTerm::start_new_step
+  // (DischargeBoundarySourceTerm.hpp:114-146, HeadBoundarySourceTerm.hpp:114-146): clear the
+  // values (BoundarySourceTerm::clear_values) and add the rain at t and t + L everywhere; set
+  // the head values on the edge strips.
+  void start_new_step(const T& time_now, const std::shared_ptr<TimeParameters<T>>& tp) {
+    step_length_ = tp->step_duration();
+    if (!P_.rain_t.empty()) {
+      *q0_ = 0.0;
+      *q1_ = 0.0;
+      *q0_ += T(series_at(P_.rain_t, P_.rain_v, time_now));
+      *q1_ += T(series_at(P_.rain_t, P_.rain_v, time_now + step_length_));
+    }
+    if (P_.head_edges) {
+      *hb0_ = 0.0;
+      *hb1_ = 0.0;
+      hb0_->move_to_host();
+      hb1_->move_to_host();
+      std::vector<T>& a = const_cast<std::vector<T>&>(hb0_->data().host_vector());
+      std::vector<T>& b = const_cast<std::vector<T>&>(hb1_->data().host_vector());
+      for (size_t i = 0; i < a.size(); ++i) {
+        const size_t x = i % P_.nx, y = i / P_.nx;
+        const bool sel = ((P_.head_edges & 1u) && x == 0) || ((P_.head_edges & 2u) && x == P_.nx - 1) ||
+                         ((P_.head_edges & 4u) && y == 0) || ((P_.head_edges & 8u) && y == P_.ny - 1);
+        if (sel) { a[i] = P_.head_value; b[i] = P_.head_value; }
+      }
+      hb0_->move_to_device();
+      hb1_->move_to_device();
+    }
+  }
+  void end_of_step(const T&) {}
+
+  StateT& state(const size_t& i = 0) { return *U_.at(i); }
+  StateT& dUdt(const size_t& i) { return *dUdt_.at(i); }
+  ValueType control_number(const size_t& state_no, const TimeType& timestep) {
+    ++P_.timesteps;
+    return U_.at(state_no)->max_control_number(timestep);
+  }
+
+ private:
+  std::shared_ptr<sycl::queue> q_;
+  PinProblem<T>& P_;
+  std::shared_ptr<Cartesian2DMesh> mesh_;
+  std::shared_ptr<SaintVenantConstants<T, Cartesian2DMesh>> K_;
+  std::vector<std::shared_ptr<StateT>> U_, dUdt_;
+  std::shared_ptr<StateT> dUdx_, dUdy_;
+  std::shared_ptr<SaintVenantFluxes<T, Cartesian2DMesh>> F_;
+  std::vector<CF<T>> man_;
+  std::shared_ptr<CF<T>> nh_, Sf_, q0_, q1_, hb0_, hb1_;
+  T step_length_ = T(60);
+};
+
+template <typename T>
+struct PinScheme : public RungeKuttaSolver<PinSolver<T>> {
+  using RungeKuttaSolver<PinSolver<T>>::RungeKuttaSolver;
+  PinSolver<T>& solver() { return *this->solver_; }
+};
+
+// RungeKuttaSolver<...>::solve over [start, end] with the named tableau `rk`.
+template <typename T>
+int solve(uint64_t nx, uint64_t ny, double dx, double dy, const T* z, const T* h, const T* u, const T* v,
+          const double* manning, const double* rain_t, const double* rain_v, int nrain, unsigned head_edges,
+          double head_value, int head_first, const char* rk, double start, double end, double step_length,
+          double initial_dt, T* out, uint64_t* timesteps) {
+  try {
+    const size_t nc = nx * ny;
+    PinProblem<T> P;
+    P.nx = nx; P.ny = ny; P.dx = dx; P.dy = dy;
+    P.z = vec(z, nc); P.h = vec(h, nc); P.u = vec(u, nc); P.v = vec(v, nc);
+    P.manning = manning != nullptr;
+    for (int i = 0; i < 4; ++i) P.n[i] = manning ? T(manning[i]) : T(0);
+    for (int i = 0; i < nrain; ++i) { P.rain_t.push_back(rain_t[i]); P.rain_v.push_back(rain_v[i]); }
+    P.head_edges = head_edges;
+    P.head_value = T(head_value);
+    P.head_first = head_first != 0;
+    g_problem<T> = &P;
+    Config conf;
+    std::ostringstream s;
+    s.precision(17);
+    auto put = [&](const char* k, double x) { s.str(""); s << x; conf.kv[k] = s.str(); };
+    put("start time", start);
+    put("end time", end);
+    put("step duration seconds", step_length);
+    put("initial timestep seconds", initial_dt);
+    auto tp = std::make_shared<TimeParameters<T>>(conf);
+    PinScheme<T> scheme(tp, std::string(rk), get_sycl_queue());
+    scheme.solve();
+    read(scheme.solver().state().h(), out);
+    read(scheme.solver().state().u(), out + nc);
+    read(scheme.solver().state().v(), out + 2 * nc);
+    *timesteps = P.timesteps;
+    g_problem<T> = nullptr;
+    return 0;
+  } catch (const std::exception& e) {
+    std::cerr << "ref_pin: " << e.what() << std::endl;
+    return -1;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+int refpin_solve_f64(uint64_t nx, uint64_t ny, double dx, double dy, const double* z, const double* h, const double* u,
+                     const double* v, const double* manning, const double* rain_t, const double* rain_v, int nrain,
+                     unsigned head_edges, double head_value, int head_first, const char* rk, double start, double end,
+                     double step_length, double initial_dt, double* out, uint64_t* timesteps) {
+  return solve<double>(nx, ny, dx, dy, z, h, u, v, manning, rain_t, rain_v, nrain, head_edges, head_value, head_first,
+                       rk, start, end, step_length, initial_dt, out, timesteps);
+}
+int refpin_solve_f32(uint64_t nx, uint64_t ny, double dx, double dy, const float* z, const float* h, const float* u,
+                     const float* v, const double* manning, const double* rain_t, const double* rain_v, int nrain,
+                     unsigned head_edges, double head_value, int head_first, const char* rk, double start, double end,
+                     double step_length, double initial_dt, float* out, uint64_t* timesteps) {
+  return solve<float>(nx, ny, dx, dy, z, h, u, v, manning, rain_t, rain_v, nrain, head_edges, head_value, head_first,
+                      rk, start, end, step_length, initial_dt, out, timesteps);
+}
+int refpin_dudt_f64(uint64_t nx, uint64_t ny, double dx, double dy, const double* z, const double* h, const double* u,
+                    const double* v, const double* ns, const double* nd, const double* ds, const double* dd,
+                    const double* q0, const double* q1, const double* hb0, const double* hb1, int head_first,
+                    double time_now, double timestep, double step_length, double* out) {
+  return dudt<double>(nx, ny, dx, dy, z, h, u, v, ns, nd, ds, dd, q0, q1, hb0, hb1, head_first, time_now, timestep,
+                      step_length, out);
+}
+int refpin_dudt_f32(uint64_t nx, uint64_t ny, double dx, double dy, const float* z, const float* h, const float* u,
+                    const float* v, const float* ns, const float* nd, const float* ds, const float* dd, const float* q0,
+                    const float* q1, const float* hb0, const float* hb1, int head_first, double time_now,
+                    double timestep, double step_length, float* out) {
+  return dudt<float>(nx, ny, dx, dy, z, h, u, v, ns, nd, ds, dd, q0, q1, hb0, hb1, head_first, time_now, timestep,
+                     step_length, out);
+}
+int refpin_control_number_f64(uint64_t nx, uint64_t ny, double dx, double dy, const double* h, const double* u,
+                              const double* v, double timestep, double* cn) {
+  return control_number<double>(nx, ny, dx, dy, h, u, v, timestep, cn);
+}
+int refpin_control_number_f32(uint64_t nx, uint64_t ny, double dx, double dy, const float* h, const float* u,
+                              const float* v, double timestep, float* cn) {
+  return control_number<float>(nx, ny, dx, dy, h, u, v, timestep, cn);
+}
+int refpin_update_y_f64(uint64_t nx, uint64_t ny, double dx, double dy, const double* u0, const double* k, int ncols,
+                        const double* a, double timestep, double* y) {
+  return update_y<double>(nx, ny, dx, dy, u0, k, ncols, a, timestep, y);
+}
+int refpin_update_y_f32(uint64_t nx, uint64_t ny, double dx, double dy, const float* u0, const float* k, int ncols,
+                        const double* a, double timestep, float* y) {
+  return update_y<float>(nx, ny, dx, dy, u0, k, ncols, a, timestep, y);
+}
+}

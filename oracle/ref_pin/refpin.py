@@ -1,0 +1,159 @@
+"""TEST INFRASTRUCTURE: ctypes binding of oracle/_ref/libsv_refpin.so (the reference's own
+hot-path kernels, built by oracle/ref_pin/build.py). Only tests/ and tests/golden/ use it.
+
+Every function takes and returns numpy arrays shaped (ny, nx) for cell fields and flat arrays
+of (nx+1)*ny + (ny+1)*nx values for face fields, in the value type of the precision asked for.
+"""
+import ctypes as C
+import importlib.util
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_lib = None
+
+
+def _build_module():
+    spec = importlib.util.spec_from_file_location("sv_refpin_build", os.path.join(_HERE, "build.py"))
+    m = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(m)
+    return m
+
+
+def available():
+    return _build_module().available()
+
+
+def load():
+    global _lib
+    if _lib is None:
+        _lib = C.CDLL(_build_module().build())
+        for t, ct in (("f64", C.c_double), ("f32", C.c_float)):
+            P = C.POINTER(ct)
+            f = getattr(_lib, f"refpin_dudt_{t}")
+            f.restype = C.c_int
+            f.argtypes = [C.c_uint64, C.c_uint64, C.c_double, C.c_double] + [P] * 12 + \
+                         [C.c_int, C.c_double, C.c_double, C.c_double, P]
+            f = getattr(_lib, f"refpin_control_number_{t}")
+            f.restype = C.c_int
+            f.argtypes = [C.c_uint64, C.c_uint64, C.c_double, C.c_double, P, P, P, C.c_double, P]
+            f = getattr(_lib, f"refpin_solve_{t}")
+            f.restype = C.c_int
+            D = C.POINTER(C.c_double)
+            f.argtypes = [C.c_uint64, C.c_uint64, C.c_double, C.c_double, P, P, P, P, D, D, D, C.c_int, C.c_uint,
+                          C.c_double, C.c_int, C.c_char_p, C.c_double, C.c_double, C.c_double, C.c_double, P,
+                          C.POINTER(C.c_uint64)]
+            f = getattr(_lib, f"refpin_update_y_{t}")
+            f.restype = C.c_int
+            f.argtypes = [C.c_uint64, C.c_uint64, C.c_double, C.c_double, P, P, C.c_int,
+                          C.POINTER(C.c_double), C.c_double, P]
+    return _lib
+
+
+def _np(precision):
+    return (np.float64, C.c_double) if precision == "f64" else (np.float32, C.c_float)
+
+
+def _ptr(a, ct):
+    return None if a is None else a.ctypes.data_as(C.POINTER(ct))
+
+
+SLOPES = ["DZDX", "DZDY", "DHDX", "DUDX", "DVDX", "DHDY", "DUDY", "DVDY"]
+FACES = ["FLUX_H", "FLUX_U", "FLUX_V", "FLUX_Z", "FLUX_BRANCH"]
+KS = ["DHDT", "DUDT", "DVDT"]
+
+
+def dudt(z, h, u, v, dx, dy=None, manning=None, q=None, head=None, head_first=False, time_now=0.0, timestep=1.0,
+         step_length=60.0, precision="f64"):
+    """One SaintVenantSolver::update_dUdt through the reference's kernels. manning = (ns, nd, ds,
+    dd) cell arrays, q = (q0, q1) discharge boundary values, head = (h0, h1) head boundary
+    values (NaN = not selected). Returns a dict of the slope, face and derivative fields."""
+    lib = load()
+    dt_, ct = _np(precision)
+    dy = dx if dy is None else dy
+    ny, nx = h.shape
+    nc, nf = nx * ny, (nx + 1) * ny + (ny + 1) * nx
+    arr = lambda a: None if a is None else np.ascontiguousarray(a, dtype=dt_)
+    m = [arr(a) for a in (manning or (None,) * 4)]
+    qq = [arr(a) for a in (q or (None, None))]
+    hh = [arr(a) for a in (head or (None, None))]
+    ins = [arr(a) for a in (z, h, u, v)]
+    out = np.empty(8 * nc + 5 * nf + 3 * nc, dtype=dt_)
+    f = getattr(lib, f"refpin_dudt_{precision}")
+    r = f(nx, ny, dx, dy, *[_ptr(a, ct) for a in ins + m + qq + hh], 1 if head_first else 0, time_now, timestep,
+          step_length, _ptr(out, ct))
+    if r != 0:
+        raise RuntimeError("reference kernels failed")
+    res = {}
+    o = 0
+    for name in SLOPES:
+        res[name] = out[o:o + nc].reshape(ny, nx)
+        o += nc
+    for name in FACES:
+        res[name] = out[o:o + nf]
+        o += nf
+    for name in KS:
+        res[name] = out[o:o + nc].reshape(ny, nx)
+        o += nc
+    return res
+
+
+def control_number(h, u, v, dx, dy=None, timestep=1.0, precision="f64"):
+    """SaintVenantState::max_control_number through the reference's reduction kernel."""
+    lib = load()
+    dt_, ct = _np(precision)
+    dy = dx if dy is None else dy
+    ny, nx = h.shape
+    a = [np.ascontiguousarray(x, dtype=dt_) for x in (h, u, v)]
+    cn = (ct * 1)()
+    r = getattr(lib, f"refpin_control_number_{precision}")(nx, ny, dx, dy, *[_ptr(x, ct) for x in a], timestep, cn)
+    if r != 0:
+        raise RuntimeError("reference kernels failed")
+    return cn[0]
+
+
+def update_y(u0, ks, a, timestep, dx=1.0, dy=None, precision="f64"):
+    """RungeKuttaSolver::update_y through the SaintVenantState operators: u0 is (3, ny, nx), ks a
+    list of (3, ny, nx) stage derivatives, a their coefficients a(s+1, col+1)."""
+    lib = load()
+    dt_, ct = _np(precision)
+    dy = dx if dy is None else dy
+    _, ny, nx = u0.shape
+    U0 = np.ascontiguousarray(u0, dtype=dt_)
+    K = np.ascontiguousarray(np.stack(ks) if len(ks) else np.zeros((0, 3, ny, nx)), dtype=dt_)
+    A = (C.c_double * max(1, len(a)))(*a)
+    y = np.empty_like(U0)
+    r = getattr(lib, f"refpin_update_y_{precision}")(nx, ny, dx, dy, _ptr(U0, ct), _ptr(K, ct), len(ks), A, timestep,
+                                                    _ptr(y, ct))
+    if r != 0:
+        raise RuntimeError("reference kernels failed")
+    return y
+
+
+def solve(z, h, u, v, dx, dy=None, manning=None, rain=None, head_edges=0, head_value=0.0, head_first=False,
+          rk_method="classic", start=0.0, end=60.0, step_length=60.0, initial_dt=1.0, precision="f64"):
+    """RungeKuttaSolver::solve of the reference (control-number target 1.0, as it hard-codes)
+    over [start, end]: manning = (n_shallow, n_deep, d_shallow, d_deep) uniform values, rain =
+    (times, values) of a rain time series in m/s applied everywhere, head_edges the SV_EDGE_*
+    strips held at head_value. Returns (h, u, v, number of timesteps taken)."""
+    lib = load()
+    dt_, ct = _np(precision)
+    dy = dx if dy is None else dy
+    ny, nx = h.shape
+    ins = [np.ascontiguousarray(a, dtype=dt_) for a in (z, h, u, v)]
+    man = None if manning is None else (C.c_double * 4)(*manning)
+    rt, rv, nr = None, None, 0
+    if rain is not None:
+        nr = len(rain[0])
+        rt = (C.c_double * nr)(*rain[0])
+        rv = (C.c_double * nr)(*rain[1])
+    out = np.empty((3, ny, nx), dtype=dt_)
+    n = C.c_uint64()
+    r = getattr(lib, f"refpin_solve_{precision}")(nx, ny, dx, dy, *[_ptr(a, ct) for a in ins], man, rt, rv, nr,
+                                                  int(head_edges), float(head_value), 1 if head_first else 0,
+                                                  rk_method.encode(), start, end, step_length, initial_dt,
+                                                  _ptr(out, ct), C.byref(n))
+    if r != 0:
+        raise RuntimeError("reference solve failed")
+    return out[0], out[1], out[2], n.value

@@ -1,11 +1,17 @@
-"""The committed golden fixtures (tests/golden/*.npz, made by tests/golden/make_golden.py from
-the oracle) against the oracle on the CPU and against the CUDA path on the GPU, bit for bit."""
+"""The committed golden fixtures against the oracle on the CPU and against the CUDA path on the
+GPU, bit for bit.
+
+Two sets: tests/golden/ref_*.npz are outputs of the reference's own hot-path code (made by
+tests/golden/make_ref_golden.py through oracle/ref_pin, which compiles the reference's kernels
+and step loop); the others are outputs of the oracle (tests/golden/make_golden.py), kept to pin
+cases the reference fixtures do not cover (the control-number target 0.5, the physical rain
+clamp, running tallies)."""
 import os
 
 import numpy as np
 import pytest
 
-from mfcm_b200 import solve, EDGE_XMAX, EDGE_YMIN
+from mfcm_b200 import solve, Forcing, RAIN_FIELDS, HEAD_FIELDS
 from oracle.sv_oracle_py import OracleSolver
 from tests.scenarios import setup, forcing, rain_series, same
 
@@ -66,12 +72,65 @@ def check_steps(kind):
     assert b.get_dt() == float(g["dt"])
 
 
+def check_ref_dudt(kind, prec="f64"):
+    """One update_dUdt of the reference's kernels: every slope, face and derivative field."""
+    g = load(f"ref_dudt_23x17_coded_out_{prec}")
+    nx, ny = int(g["nx"]), int(g["ny"])
+    b = backend(kind, nx, ny, float(g["dx"]), dy=float(g["dy"]), precision=prec, rain_mode="reference",
+                step_duration=float(g["step_duration"]), head_first=bool(g["head_first"]))
+    setup(b, *(g[k].astype(np.float64) for k in ("z", "h", "u", "v")))
+    f = Forcing()
+    f.rain_kind, f.head_kind = RAIN_FIELDS, HEAD_FIELDS
+    b.set_forcing(f)  # per-cell boundary values are uploaded after the forcing
+    for name in ("n_shallow", "n_deep", "d_shallow", "d_deep", "qbdy0", "qbdy1", "hbdy0", "hbdy1"):
+        b.set_field(name.upper(), g[name].astype(np.float64))
+    b.eval_dudt(0, float(g["t_sub"]), float(g["dt"]))
+    for f in SLOPE + FACE + KS:
+        assert same(b.get_field(f), g[f].astype(np.float64)), f
+
+
+def check_ref_solve(kind, name):
+    """Two steps through the reference's RungeKuttaSolver::solve (control-number target 1.0):
+    the number of timesteps taken and the final state."""
+    g = load(name)
+    prec = "f32" if name.endswith("f32") else "f64"
+    nx, ny = int(g["nx"]), int(g["ny"])
+    b = backend(kind, nx, ny, float(g["dx"]), precision=prec, rk_method=str(g["rk_method"]), cn_target=1.0,
+                rain_mode="reference", step_duration=float(g["step_duration"]), initial_dt=float(g["initial_dt"]))
+    zero = np.zeros((ny, nx))
+    setup(b, g["z"].astype(np.float64), g["h"].astype(np.float64), zero, zero, n=tuple(g["manning"]))
+    per = solve(b, 0.0, float(g["end_time"]), rain=float(g["rain"]), head=0.0, head_edges=int(g["edges"]))
+    assert sum(p["accepted"] + p["repeated"] for p in per) == int(g["timesteps"])
+    for f, n in (("H", "h_new"), ("U", "u_new"), ("V", "v_new")):
+        assert same(b.get_field(f), g[n].astype(np.float64)), f
+
+
+REF_CPU = [lambda k: check_ref_dudt(k, "f64"), lambda k: check_ref_dudt(k, "f32"),
+           lambda k: check_ref_solve(k, "ref_solve_45x30_classic_f64"),
+           lambda k: check_ref_solve(k, "ref_solve_45x30_kutta3_f64"),
+           lambda k: check_ref_solve(k, "ref_solve_45x30_classic_f32")]
+# the CUDA FP32 path is held to a depth tolerance against FP64, not to the reference's FP32 bits
+REF_GPU = REF_CPU[:1] + REF_CPU[2:4]
+
+
 @pytest.mark.parametrize("check", [check_dudt, check_timestep, check_steps])
 def test_oracle_matches_golden(check):
+    check("cpu")
+
+
+@pytest.mark.parametrize("check", REF_CPU, ids=["dudt_f64", "dudt_f32", "solve_classic_f64", "solve_kutta3_f64",
+                                                "solve_classic_f32"])
+def test_oracle_matches_reference_golden(check):
     check("cpu")
 
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("check", [check_dudt, check_timestep, check_steps])
 def test_cuda_path_matches_golden(check):
+    check("gpu")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("check", REF_GPU, ids=["dudt_f64", "solve_classic_f64", "solve_kutta3_f64"])
+def test_cuda_path_matches_reference_golden(check):
     check("gpu")
