@@ -64,6 +64,8 @@ def parse():
     p.add_argument("--size", type=int, default=4096)
     p.add_argument("--spinup", type=int, default=600, help="timesteps run from dry before timing")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
+    p.add_argument("--window-steps", type=int, default=10,
+                   help="60 s steps from dry of the 1024^2 window both CPU baselines are timed on")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-extras", action="store_true", help="skip the fp64, precision, serving, batched parts")
@@ -203,6 +205,61 @@ class Runner:
         if timesteps > 0:
             self.run(timesteps)
 
+    def finish_step(self):
+        """Run to the end of the current step (the next step boundary)."""
+        while not self.need_begin:
+            _, done, _ = self.s.run_timesteps(1 << 40, begin=False)
+            if done:
+                self.need_begin = True
+                self.t_step += self.L
+
+
+def common_state(w, args, device):
+    """The state both precisions are timed from: the plain FP64 path (bit for bit the
+    reference arithmetic) spun up from dry for --spinup timesteps and then to the end of that
+    step, so that a solver of either precision can start the next step from it."""
+    s = make_solver(w, "f64", device)
+    r = Runner(s)
+    r.spinup(args.spinup)
+    r.finish_step()
+    st = s.stats()
+    state = {"h": s.get_field("H"), "u": s.get_field("U"), "v": s.get_field("V"), "dt": s.get_dt(),
+             "t_step": r.t_step, "spinup_accepted": st["accepted"], "spinup_repeated": st["repeated"]}
+    s.close()
+    return state
+
+
+def solver_at(w, precision, state, device):
+    """A solver of `precision` holding the common state (FP64 values rounded once to FP32 for
+    the FP32 paths) and its next timestep."""
+    s = make_solver(w, precision, device)
+    for f in ("H", "U", "V"):
+        s.set_field(f, state[f.lower()])
+    s.set_dt(state["dt"])
+    return s
+
+
+def headline_error(w, state, precision, device):
+    """Error of the FP32 headline against FP64 on the headline workload itself: from the common
+    state both advance one whole 60 s step (device-controlled timesteps), then the depth fields
+    and FP64 volumes are compared."""
+    out = {}
+    for prec in ("f64", precision):
+        s = solver_at(w, prec, state, device)
+        s.set_forcing(forcing_at(state["t_step"], s.step_duration))
+        st = s.advance()
+        out[prec] = (s.get_field("H"), s.stats()["volume"], st["accepted"], st["repeated"])
+        s.close()
+    d = np.abs(out[precision][0] - out["f64"][0])
+    wet = out["f64"][0] > 1e-3
+    return {"case": f"one 60 s step from the common state at t = {state['t_step']:.0f} s",
+            "max_depth_err_m": float(d.max()), "p99_depth_err_m": float(np.percentile(d, 99)),
+            "mean_depth_err_m": float(d.mean()), "cells_over_1mm_fraction": float((d > 1e-3).mean()),
+            "max_depth_err_wet_m": float(d[wet].max()) if wet.any() else None,
+            "rel_volume_err": abs(out[precision][1] - out["f64"][1]) / out["f64"][1],
+            "accepted": {precision: out[precision][2], "f64": out["f64"][2]},
+            "repeated": {precision: out[precision][3], "f64": out["f64"][3]}}
+
 
 def profile_traffic(name, key="bytes_per_cell_per_launch"):
     """Per-launch DRAM bytes (or warp instructions) per cell of a stage kernel from a committed
@@ -221,21 +278,18 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def timed_run(w, precision, args, device, barrier, dist):
-    """Spin up, pick the kernel, then time args.steps timesteps with per-kernel events."""
-    solver = make_solver(w, precision, device)
-    runner = Runner(solver)
+def timed_run(w, precision, args, device, barrier, dist, state):
+    """From the common state: pick the kernel, then time args.steps timesteps with per-kernel
+    events."""
+    solver = solver_at(w, precision, state, device)
+    runner = Runner(solver, t0=state["t_step"])
     if args.variant == "auto":
-        first = min(50, args.spinup)
-        runner.spinup(first)
         variant = solver.autotune()
         tune = solver.autotune_ms()
-        runner.spinup(args.spinup - first)
     else:
         variant = int(args.variant)
         tune = None
         solver.set_kernel_variant(variant)
-        runner.spinup(args.spinup)
     runner.run(max(3, args.warmup))
     st0 = solver.stats()
     barrier()
@@ -274,19 +328,22 @@ def timed_run(w, precision, args, device, barrier, dist):
                          "frac": issue_ms / (stage_avg_s * 1e3), "sm_mhz": clocks["sm_mhz"]}
     res = {"value": work / (ms_max * 1e-3), "ms": ms_max, "accepted": accepted, "repeated": repeated,
            "variant": variant, "autotune_ms": tune, "roofline": roof, "clocks": clocks, "timesteps": tm["timesteps"],
-           "sim_time_s": runner.t_step,
+           "sim_time_s": runner.t_step, "ms_per_timestep": tm["total_ms"] / max(1, tm["timesteps"]),
+           "stage_ms": stage_avg_s * 1e3,
            "launches": int(tm["stage_launches"] + tm["finalize_launches"] + tm["begin_launches"])}
     return solver, res
 
 
-def precision_study(device, nx=8192, ny=1024, dx=0.5, seconds=60.0):
-    """Dam break on a flat bed at 350 m (8192 x 1024 cells, dx = 0.5 m, h = 1 m for x below the
+def precision_study(device, nx=8192, ny=1024, dx=0.5, seconds=60.0, h0=1.0):
+    """Dam break on a flat bed at 350 m (8192 x 1024 cells, dx = 0.5 m, h = h0 for x below the
     centre, dry beyond, frictionless, no rain, 60 s): max depth error and relative volume
     error of the FP32 paths against FP64, the front position of each against Ritter's
     2 sqrt(g h0) t, and the depth and velocity at the dam against Ritter's 4/9 h0 and
-    2/3 sqrt(g h0)."""
+    2/3 sqrt(g h0). The depth error is given over the whole grid and away from the moving
+    bore (cells more than 20 m from FP64's front), because a bore that arrives one timestep
+    earlier or later differs there by up to its own height whatever the precision."""
     from mfcm_b200 import SaintVenantSolver, synth
-    z, h = synth.dam_break(nx, ny, 350.0, 1.0)
+    z, h = synth.dam_break(nx, ny, 350.0, h0)
     out = {}
     mid = nx // 2
     for prec in ("f64", "f32", "f32_datum64"):
@@ -304,14 +361,19 @@ def precision_study(device, nx=8192, ny=1024, dx=0.5, seconds=60.0):
                      "repeated": st["repeated"], "seconds": el}
         s.close()
     h64, v64 = out["f64"]["h"], out["f64"]["volume"]
-    c0 = math.sqrt(9.81 * 1.0)
-    res = {"case": f"dam break {nx}x{ny}, dx={dx} m, bed 350 m, {seconds:.0f} s, no friction",
-           "ritter_front_m": 2.0 * c0 * seconds, "ritter_h_dam": 4.0 / 9.0, "ritter_u_dam": 2.0 / 3.0 * c0}
+    c0 = math.sqrt(9.81 * h0)
+    res = {"case": f"dam break {nx}x{ny}, dx={dx} m, bed 350 m, h0 = {h0} m, {seconds:.0f} s, no friction",
+           "ritter_front_m": 2.0 * c0 * seconds, "ritter_h_dam": 4.0 / 9.0 * h0, "ritter_u_dam": 2.0 / 3.0 * c0}
+    x = (np.arange(nx) + 0.5) * dx - mid * dx
+    away = np.abs(x - out["f64"]["front_m"]) > 20.0
     for prec in ("f64", "f32", "f32_datum64"):
         o = out[prec]
         r = {k: o[k] for k in ("front_m", "h_dam", "u_dam", "accepted", "repeated", "seconds")}
         if prec != "f64":
-            r["max_depth_err_m"] = float(np.max(np.abs(o["h"] - h64)))
+            d = np.abs(o["h"] - h64)
+            r["max_depth_err_m"] = float(d.max())
+            r["max_depth_err_away_from_bore_m"] = float(d[:, away].max())
+            r["mean_depth_err_m"] = float(d.mean())
             r["rel_volume_err"] = abs(o["volume"] - v64) / v64
             r["within_1mm"] = r["max_depth_err_m"] <= 1e-3
         res[prec] = r
@@ -431,10 +493,47 @@ def batched_ensemble(device, precision="f32_datum64"):
     return r32
 
 
+def window_workload(w, n=1024):
+    """The top-left n x n window of the catchment's bed, Manning and rain fields, as a
+    catchment of its own (outflow on its edges)."""
+    n = min(n, w["nx"], w["ny"])
+    sl = (slice(0, n), slice(0, n))
+    return {"nx": n, "ny": n, "dx": w["dx"], "z": w["z"][sl], "n": w["n"][sl], "rain": w["rain"][sl]}
+
+
+def window_state(w, steps, device=None):
+    """The state both CPU baselines (this arm's and the reference arm's) are timed on: the
+    1024 x 1024 window spun up from dry for `steps` whole 60 s steps in plain FP64 -- on the
+    GPU here, on the oracle in the reference arm (which has no GPU). The two FP64 paths are
+    bit for bit the same, so both arms time the CPU on the same state."""
+    ww = window_workload(w)
+    if device is not None:
+        s = make_solver(ww, "f64", device)
+    else:
+        from oracle.sv_oracle_py import OracleSolver
+        s = OracleSolver(ww["nx"], ww["ny"], ww["dx"], cn_target=0.5, rain_mode="physical", step_duration=60.0,
+                         initial_dt=1.0, openmp=True, threads=os.cpu_count() or 1)
+        zeros = np.zeros((ww["ny"], ww["nx"]))
+        s.set_field("Z", ww["z"])
+        for f in ("H", "U", "V"):
+            s.set_field(f, zeros)
+        s.set_field("N_SHALLOW", ww["n"])
+        s.set_field("N_DEEP", ww["n"])
+        s.set_field("RAIN_PATTERN", ww["rain"])
+    acc = 0
+    for k in range(steps):
+        s.set_forcing(forcing_at(60.0 * k, 60.0))
+        acc = s.advance()["accepted"]
+    state = {"h": s.get_field("H"), "u": s.get_field("U"), "v": s.get_field("V"), "dt": s.get_dt(),
+             "t_step": 60.0 * steps, "spinup_accepted": acc}
+    s.close()
+    return state
+
+
 def cpu_baseline(w, state, cpu_seconds, precision):
-    """The oracle (the reference's arithmetic restated in C++, OpenMP, all host threads) on a
-    1024 x 1024 window of the catchment, at the given state; timed over whole accepted
-    timesteps."""
+    """The oracle (the reference's arithmetic restated in C++, OpenMP, all host threads) on the
+    1024 x 1024 window of the catchment (window_workload), at the window state of
+    window_state; timed over whole accepted timesteps."""
     from oracle.sv_oracle_py import OracleSolver, threads_available
     threads = os.cpu_count() or 1
     n = min(1024, w["nx"])
@@ -448,7 +547,7 @@ def cpu_baseline(w, state, cpu_seconds, precision):
     o.set_field("N_SHALLOW", w["n"][sl])
     o.set_field("N_DEEP", w["n"][sl])
     o.set_field("RAIN_PATTERN", w["rain"][sl])
-    o.set_forcing(forcing_at(600.0, 60.0))
+    o.set_forcing(forcing_at(state["t_step"], 60.0))
     dt = state["dt"]
     cn, rep, nd = o.do_timestep(0.0, dt)  # one untimed warm-up timestep
     if not rep:
@@ -465,7 +564,8 @@ def cpu_baseline(w, state, cpu_seconds, precision):
     el = time.perf_counter() - t0
     used = threads_available(True)
     return {"value": acc * n * n / el, "unit": UNIT, "cores": used, "kind": "port",
-            "sample": f"{acc} accepted RK4 timesteps of a {n}x{n} window of the {w['nx']}x{w['ny']} catchment "
+            "sample": f"{acc} accepted RK4 timesteps of the {n}x{n} window of the {w['nx']}x{w['ny']} catchment, "
+                      f"from its FP64 state after {state['t_step']:.0f} s from dry "
                       f"(oracle {precision}, {el:.1f} s, OpenMP {used} threads)"}
 
 
@@ -484,7 +584,7 @@ def source_terms_cost(w, state, precision, variant, device, timesteps=20):
         if on:
             for name, val in (("ELOSS_FX", 0.05), ("ELOSS_FY", 0.05), ("INFIL_RATE", 2e-6), ("INFIL_CAP", 0.05)):
                 s.set_field(name, np.full((w["ny"], w["nx"]), val))
-        r = Runner(s, t0=600.0)
+        r = Runner(s, t0=state["t_step"])
         r.run(3)
         _, tm = r.run(timesteps, timing=True)
         out["with" if on else "without"] = tm["stage_ms"] / max(1, tm["stage_launches"])
@@ -506,9 +606,8 @@ def run_reference(args):
     if rank != 0:
         return 0
     w = workload(args.size)
-    zeros = np.zeros((w["ny"], w["nx"]))
-    # state: a 2 cm film stands in for the spun-up state (this arm has no GPU spin-up)
-    state = {"h": zeros + 0.02, "u": zeros, "v": zeros, "dt": 0.5}
+    # the window state the GPU arm's CPU baseline is timed on, spun up here on the oracle
+    state = window_state(w, args.window_steps)
     prec = oracle_precision(args.precision)
     # each step is a bounded sample (about 1 s of CPU work; at least one whole timestep)
     per_step = max(0.6, min(2.0, 120.0 / max(1, args.steps)))
@@ -525,9 +624,11 @@ def run_reference(args):
             "ms_per_step": 1e3 * el / max(1, args.steps), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": prec, "data": "synthetic", "impl": "reference", "cpu_baseline": cb,
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "config": {"workload": f"1024x1024 window of the {w['nx']}x{w['ny']} dx=2 m catchment, oracle port of "
-                                   "the reference arithmetic (the reference itself does not build here)",
-                       "scheme": "classic RK4", "cn_target": 0.5}}
+            "config": {"workload": f"1024x1024 window of the {w['nx']}x{w['ny']} dx=2 m catchment from its FP64 "
+                                   f"state after {state['t_step']:.0f} s from dry, oracle port of the reference "
+                                   "arithmetic (the reference's SYCL build cannot be built here; the oracle is pinned "
+                                   "bit for bit to the reference's kernels compiled on the CPU)",
+                       "scheme": "classic RK4", "cn_target": 0.5, "same_state_as": "the b200 arm's cpu_baseline"}}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -555,7 +656,7 @@ def measure_e2e(w, args, device, state, variant, precision):
     s.set_field("N_SHALLOW", pinned["n"])
     s.set_field("N_DEEP", pinned["n"])
     s.set_field("RAIN_PATTERN", pinned["rain"])
-    r = Runner(s, t0=600.0)
+    r = Runner(s, t0=state["t_step"])
     r.run(args.steps)
     st = s.stats()
     out = [s.get_field(f, out=results[f]) for f in ("H", "U", "V")]
@@ -593,30 +694,35 @@ def main():
         torch.cuda.synchronize(device)
 
     w = workload(args.size)
-    solver, main_res = timed_run(w, args.precision, args, device, barrier, dist)
-    state = None
-    if rank == 0 and (not args.no_cpu or not args.no_e2e):
-        state = {"h": solver.get_field("H"), "u": solver.get_field("U"), "v": solver.get_field("V"),
-                 "dt": solver.get_dt()}
+    state = common_state(w, args, device)
+    solver, main_res = timed_run(w, args.precision, args, device, barrier, dist, state)
     solver.close()
     extras = {}
     if not args.no_extras and args.precision != "f64":
-        s64, r64 = timed_run(w, "f64", args, device, barrier, dist)
-        s64_state = None
-        if rank == 0 and world == 1 and not args.no_cpu:
-            s64_state = {"h": s64.get_field("H"), "u": s64.get_field("U"), "v": s64.get_field("V"),
-                         "dt": s64.get_dt()}
+        s64, r64 = timed_run(w, "f64", args, device, barrier, dist, state)
         s64.close()
         extras["fp64"] = {"value": r64["value"], "ms_per_step": r64["ms"] / max(1, args.steps),
+                          "ms_per_timestep": r64["ms_per_timestep"], "stage_ms": r64["stage_ms"],
                           "accepted": r64["accepted"], "repeated": r64["repeated"], "kernel_variant": r64["variant"],
                           "autotune_stage_ms": r64["autotune_ms"],
                           "roofline": r64["roofline"], "clocks": r64["clocks"]}
+        # both arms start from the same state; the throughput ratio counts accepted timesteps,
+        # so it also carries the two arms' accept/repeat decisions, which the per-timestep and
+        # per-stage ratios do not
         extras["fp32_over_fp64"] = main_res["value"] / r64["value"]
-        if rank == 0 and world == 1 and not args.no_cpu:
-            st64 = {"h": s64_state["h"], "u": s64_state["u"], "v": s64_state["v"], "dt": s64_state["dt"]}
-            extras["fp64"]["cpu_baseline"] = cpu_baseline(w, st64, args.cpu_seconds, "f64")
+        extras["fp32_over_fp64_per_timestep"] = r64["ms_per_timestep"] / main_res["ms_per_timestep"]
+        extras["fp32_over_fp64_per_stage"] = r64["stage_ms"] / main_res["stage_ms"]
+        if rank == 0:
+            extras["headline_error_vs_fp64"] = headline_error(w, state, args.precision, device)
+    wstate = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        wstate = window_state(w, args.window_steps, device=device)
+        if "fp64" in extras:
+            extras["fp64"]["cpu_baseline"] = cpu_baseline(w, wstate, args.cpu_seconds, "f64")
     if rank == 0 and not args.no_extras:
         extras["precision"] = precision_study(device)
+        # the same on a 2 cm dam: levels near 350 m then carry the depth in their last bits
+        extras["precision_thin"] = precision_study(device, h0=0.02)
         extras["serving"] = serving_run(device)
         extras["batched"] = batched_ensemble(device, args.precision)
     e2e = None
@@ -626,7 +732,7 @@ def main():
         extras["source_terms"] = source_terms_cost(w, state, args.precision, main_res["variant"], device)
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cb = cpu_baseline(w, state, args.cpu_seconds, oracle_precision(args.precision))
+        cb = cpu_baseline(w, wstate, args.cpu_seconds, oracle_precision(args.precision))
 
     if rank == 0:
         line = {"metric": METRIC, "value": main_res["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -637,6 +743,7 @@ def main():
                                        "0.005 slope, lognormal rain field 30 mm/h, Voronoi n, outflow all edges)",
                            "scheme": "classic RK4", "cn_target": 0.5, "precision": args.precision,
                            "spinup_timesteps": args.spinup, "sim_time_s": main_res["sim_time_s"],
+                           "start": f"common FP64 state at t = {state['t_step']:.0f} s for every precision",
                            "l2": "inputs larger than L2 (each FP64 state field 134 MB; FP32 67 MB x 13 fields)",
                            "parallelism": f"replicas x{world}", "kernel_variant": main_res["variant"],
                            "autotune_stage_ms": main_res["autotune_ms"],

@@ -244,14 +244,18 @@ typedef struct {
  * With `timing` != NULL every kernel is bracketed by CUDA events on the ctx stream. */
 int sv_run_timesteps(sv_ctx* ctx, uint64_t max_timesteps, int begin, sv_stats* out, int* step_done,
                      sv_timing* timing);
-/* Stage-kernel variant (no reference counterpart: a launch-shape choice of this library):
- * 0-3 tiled shared-memory kernel (32x8, 32x8 at 3 CTAs/SM, 32x4 at 4 CTAs/SM, 64x4 at 3
- * CTAs/SM), 4-10 column-sweep kernel (16/32/64 rows per warp, then 32 rows capped for 3, 4,
- * 5 and 6 CTAs/SM). Every variant computes bit-identical FP64 results; FP32 results are
- * reproducible per variant. SV_F32_DATUM64 solvers take the column-sweep variants only. */
+/* Stage-kernel variant (no reference counterpart: a launch-shape and schedule choice of this
+ * library). Fused schedule, one pass per RK stage: 0-3 tiled shared-memory kernel (32x8, 32x8
+ * at 3 CTAs/SM, 32x4 at 4 CTAs/SM, 64x4 at 3 CTAs/SM), 4-10 column-sweep kernel (16/32/64 rows
+ * per warp, then 32 rows capped for 3, 4, 5 and 6 CTAs/SM; strips away from the mesh edge and
+ * from coded-out cells run an interior form of it). Split schedule, two passes per RK stage:
+ * 11 a slopes pass, then the tiled 32x8 kernel reading those slopes. Every variant computes
+ * bit-identical FP64 results; FP32 results are reproducible per variant. SV_F32_DATUM64 solvers
+ * take the column-sweep variants only. */
 int sv_set_kernel_variant(sv_ctx* ctx, int variant);
 int sv_get_kernel_variant(sv_ctx* ctx, int* variant);
-/* Autotune: times every variant's stage kernel on the current state and keeps the fastest;
+/* Autotune: times every variant's stage kernel (both schedules) on the current state and keeps
+ * the fastest;
  * `best_out` (may be NULL) receives the chosen variant. The state U_[0] is not modified. */
 int sv_autotune(sv_ctx* ctx, int* best_out);
 /* per-variant stage-kernel times (ms) measured by the last sv_autotune; ms[v] for v < n */
@@ -300,6 +304,17 @@ int sv_batch_set_step_limit(sv_batch* batch, long long max_timesteps);
  * SV_E_NONFINITE (its state is no longer usable) or SV_E_LIMIT (left part-way through the
  * step); SV_OK for empty slots */
 int sv_batch_status(sv_batch* batch, int* status, int n);
+/* Persistent mode (no reference counterpart; the reference advances one catchment per
+ * process, TemporalScheme.hpp:112-149): each sv_batch_advance / sv_batch_advance_steps runs as
+ * ONE cooperative launch that fills the device. Every member advances through its queued
+ * steps at its own dt; a member's timestep is its stage phases (column-sweep strips, 32 rows)
+ * and a finalize phase (reductions, dt controller, step queue), and idle warps take work from
+ * whichever member has some. on = 0 returns to one launch per stage. spin_limit bounds how many
+ * times a warp that finds no work polls before the launch gives up with SV_E_TIMEOUT (0: the
+ * default, 2^22 polls, about a second); after a timeout every member keeps the state of its
+ * last completed timestep. FP64 results are bit for bit those of the other modes; FP32
+ * results are reproducible for this mode. */
+int sv_batch_set_persistent(sv_batch* batch, int on, uint64_t spin_limit);
 /* the stage-kernel variant every member of the batch runs (FP32 results are reproducible
  * per variant: a solo run with this variant gives a member's bits) */
 int sv_batch_kernel_variant(sv_batch* batch, int* variant);

@@ -35,6 +35,8 @@ def _declare(lib):
     lib.sv_batch_kernel_variant.argtypes = [C.c_void_p, P(C.c_int)]
     lib.sv_batch_status.restype = C.c_int
     lib.sv_batch_status.argtypes = [C.c_void_p, P(C.c_int), C.c_int]
+    lib.sv_batch_set_persistent.restype = C.c_int
+    lib.sv_batch_set_persistent.argtypes = [C.c_void_p, C.c_int, C.c_uint64]
     lib.sv_batch_size.restype = C.c_int
     lib.sv_batch_size.argtypes = [C.c_void_p, P(C.c_int), P(C.c_uint64)]
     lib._batch_declared = True
@@ -101,6 +103,14 @@ class SaintVenantBatch:
         """Cap the timesteps one member may take within one step (0: no cap). A member that
         reaches it leaves the step part-way with status SV_E_LIMIT; the others go on."""
         r = self._lib.sv_batch_set_step_limit(self._b, int(max_timesteps))
+        if r != 0:
+            raise SvError(r, self._lib.sv_last_error(None).decode())
+
+    def set_persistent(self, on=True, spin_limit=0):
+        """Run each advance as one persistent cooperative launch (every member at its own dt;
+        idle warps take work from any member). spin_limit bounds a waiting warp's polls before
+        the launch gives up with SV_E_TIMEOUT (0: the library's default)."""
+        r = self._lib.sv_batch_set_persistent(self._b, 1 if on else 0, int(spin_limit))
         if r != 0:
             raise SvError(r, self._lib.sv_last_error(None).decode())
 

@@ -178,6 +178,69 @@ struct Solver final : public sv_ctx {
   int unroll = 8;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<void*> owned;
+  T* n_deep_own = nullptr;  // n_deep's own array once it differs from n_shallow
+  T* pslp[6] = {};          // split schedule: slopes of the stage input (allocated on first use)
+  int ensure_split() {
+    if (pslp[0]) return SV_OK;
+    for (int f = 0; f < 6; ++f) SV_CUDA(alloc_cells(&pslp[f], false));
+    graph_dirty = true; ++pversion;
+    return SV_OK;
+  }
+  // interior / general strip lists of the column sweep, per strip height (16, 32, 64 rows):
+  // interior strips (whole window inside the mesh, no coded-out bed) run the interior kernel
+  struct Strips {
+    int* d_i = nullptr;
+    int* d_b = nullptr;
+    int ni = 0, nb = 0;
+    bool valid = false;
+  };
+  Strips strips_[3];
+  unsigned char* d_sflags = nullptr;
+  static int strips_slot(int rows) { return rows == 16 ? 0 : (rows == 32 ? 1 : 2); }
+  void invalidate_strips() {
+    for (Strips& x : strips_) x.valid = false;
+    graph_dirty = true; ++pversion;
+  }
+  // the lists for variant v (a column-sweep variant), built from the bed on the device
+  int ensure_strips(int v) {
+    const int rows = svk::variant_sweep_rows(v);
+    if (rows == 0) return SV_OK;
+    Strips& L = strips_[strips_slot(rows)];
+    if (L.valid) return SV_OK;
+    const long long n = svk::variant_partials(v, (long long)mesh.nx, (long long)mesh.ny);
+    if (!L.d_i) {
+      SV_CUDA(alloc(&L.d_i, size_t(n)));
+      SV_CUDA(alloc(&L.d_b, size_t(n)));
+    }
+    if (!d_sflags)  // sized for the shortest strips, which are the most numerous
+      SV_CUDA(alloc(&d_sflags, size_t(svk::variant_partials(4, (long long)mesh.nx, (long long)mesh.ny))));
+    cudaError_t e = svk::launch_strip_flags<T>(z, int(mesh.nx), int(mesh.ny), rows, n, d_sflags, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "strip flags");
+    std::vector<unsigned char> flags(static_cast<size_t>(n));
+    SV_CUDA(cudaMemcpyAsync(flags.data(), d_sflags, size_t(n), cudaMemcpyDeviceToHost, stream));
+    SV_CUDA(cudaStreamSynchronize(stream));
+    std::vector<int> in, bd;
+    for (long long i = 0; i < n; ++i) (flags[size_t(i)] ? in : bd).push_back(int(i));
+    if (!in.empty()) SV_CUDA(cudaMemcpyAsync(L.d_i, in.data(), in.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+    if (!bd.empty()) SV_CUDA(cudaMemcpyAsync(L.d_b, bd.data(), bd.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+    SV_CUDA(cudaStreamSynchronize(stream));
+    L.ni = int(in.size());
+    L.nb = int(bd.size());
+    L.valid = true;
+    graph_dirty = true; ++pversion;
+    return SV_OK;
+  }
+  // the strip lists of variant v into P (none for other variants or lists not built yet)
+  void set_strips(svk::StageParams<T>& P, int v) const {
+    const int rows = svk::variant_sweep_rows(v);
+    P.istrips = P.bstrips = nullptr;
+    P.n_istrips = P.n_bstrips = 0;
+    if (rows == 0) return;
+    const Strips& L = strips_[strips_slot(rows)];
+    if (!L.valid) return;
+    P.istrips = L.d_i; P.n_istrips = L.ni;
+    P.bstrips = L.d_b; P.n_bstrips = L.nb;
+  }
 
   ~Solver() override {
     cudaSetDevice(device);
@@ -350,11 +413,11 @@ struct Solver final : public sv_ctx {
     if (!slot) return fail(SV_E_ARG, "field id not settable");
     if (id == SV_FIELD_N_DEEP && man[0]) return set_n_deep(host, n);
     if (id == SV_FIELD_N_SHALLOW && man[1] && man[1] == man[0]) {
-      // n_deep shares n_shallow's array: it keeps its values in an array of its own
-      T* own = nullptr;
-      SV_CUDA(alloc_cells(&own, false));
-      SV_CUDA(cudaMemcpyAsync(own, man[0], size_t(ncells) * sizeof(T), cudaMemcpyDeviceToDevice, stream));
-      man[1] = own;
+      // n_deep shares n_shallow's array: it keeps its values in an array of its own (one per
+      // solver, reused whenever the two part again)
+      if (!n_deep_own) SV_CUDA(alloc_cells(&n_deep_own, false));
+      SV_CUDA(cudaMemcpyAsync(n_deep_own, man[0], size_t(ncells) * sizeof(T), cudaMemcpyDeviceToDevice, stream));
+      man[1] = n_deep_own;
       graph_dirty = true; ++pversion;
     }
     if (lazy && *slot == nullptr) {
@@ -372,6 +435,7 @@ struct Solver final : public sv_ctx {
       cudaError_t e = svk::launch_bed_slopes<T>(z, int(mesh.nx), int(mesh.ny), mesh.dx, mesh.dy, zx, zy, stream);
       if (e != cudaSuccess) return cuda_fail(e, "bed slopes");
       SV_CUDA(cudaStreamSynchronize(stream));
+      invalidate_strips();
     }
     return r;
   }
@@ -390,7 +454,8 @@ struct Solver final : public sv_ctx {
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     if (e == cudaSuccess && flag) {
       if (!man[1] || man[1] == man[0]) {
-        e = alloc_cells(&man[1], false);
+        if (!n_deep_own) e = alloc_cells(&n_deep_own, false);
+        man[1] = n_deep_own;
         graph_dirty = true; ++pversion;
       }
       if (e == cudaSuccess) e = svk::launch_from_f64<T>(st, man[1], (long long)n, stream);
@@ -413,6 +478,7 @@ struct Solver final : public sv_ctx {
       (void)host; (void)n;
       return fail(SV_E_STATE, "tile datums need an FP32 solver");
     } else {
+      invalidate_strips();
       double* dz = nullptr;
       SV_CUDA(stage_alloc(&dz, n));
       cudaError_t e = cudaMemcpyAsync(dz, host, n * sizeof(double), cudaMemcpyHostToDevice, stream);
@@ -585,6 +651,7 @@ struct Solver final : public sv_ctx {
     P.zy = zy;
     P.zdat = datum ? zdat : nullptr;
     P.dtiles_x = dtiles_x;
+    for (int f = 0; f < 6; ++f) P.pslp[f] = pslp[f];
     for (int i = 0; i < 4; ++i) { P.man_p[i] = man[i]; P.man_s[i] = T(man_s[i]); }
     P.fc = fc;
     P.q0p = q0; P.q1p = q1; P.pat = pat; P.hb0p = hb0; P.hb1p = hb1;
@@ -613,6 +680,7 @@ struct Solver final : public sv_ctx {
   // Stage s of a timestep (RungeKutta.cpp:147-153): mode, RK coefficients and buffers.
   svk::StageParams<T> stage_params(int st) const {
     svk::StageParams<T> P = base_params();
+    set_strips(P, variant);
     const bool tally = !(prm.flags & SV_FLAG_NO_TALLIES);
     P.stage = st;
     P.c_s = tab.c(st + 1);
@@ -661,7 +729,8 @@ struct Solver final : public sv_ctx {
   }
   // Device copy of the stage parameters for the batch-of-one path (outside stream capture).
   int ensure_dev_params() {
-    if (!batch_path(variant) || sp_version == pversion) return SV_OK;
+    if (!batch_path(variant)) return ensure_strips(variant);
+    if (sp_version == pversion) return SV_OK;
     if (!d_sp) {
       SV_CUDA(alloc(&d_sp, size_t(N + 1)));
       SV_CUDA(alloc(&d_ws, size_t(4)));
@@ -884,6 +953,10 @@ struct Solver final : public sv_ctx {
     if (v < 0 || v >= svk::kNumVariants) return fail(SV_E_ARG, "unknown kernel variant");
     // with tile datums only the column sweep evaluates each face in one frame (face_frame)
     if (datum && !svk::variant_is_sweep(v)) return fail(SV_E_ARG, "tile datums need a column-sweep variant (4-10)");
+    if (svk::variant_is_split(v)) {
+      int r = ensure_split();
+      if (r) return r;
+    }
     variant = v;
     nblk = svk::variant_partials(variant, (long long)mesh.nx, (long long)mesh.ny);
     graph_dirty = true; ++pversion;
@@ -929,6 +1002,16 @@ struct Solver final : public sv_ctx {
     for (int v = 0; v < svk::kNumVariants; ++v) {
       if (datum && !svk::variant_is_sweep(v)) continue;
       P.nblk = svk::variant_partials(v, (long long)mesh.nx, (long long)mesh.ny);
+      if (!batch_path(v)) {
+        int rs = ensure_strips(v);
+        if (rs) return rs;
+      }
+      if (svk::variant_is_split(v)) {
+        int rs = ensure_split();
+        if (rs) return rs;
+        for (int f = 0; f < 6; ++f) P.pslp[f] = pslp[f];
+      }
+      set_strips(P, v);
       // the batch variant runs as the batched kernel (see launch_stage_kernel): time that one
       auto launch = [&]() -> cudaError_t {
         if (!batch_path(v)) return svk::launch_variant<T>(P, v, stream);
@@ -1025,6 +1108,7 @@ struct sv_batch_base {
   virtual int status(int*, int) = 0;
   virtual int advance_steps(int, const int*, const sv_forcing*, sv_stats*, int) = 0;
   virtual int kernel_variant() const = 0;
+  virtual int set_persistent(int, unsigned long long) = 0;
 };
 
 template <typename T>
@@ -1048,6 +1132,14 @@ struct Batch final : public sv_batch_base {
   int unroll = 8;
   long long step_limit = 0;                 // timesteps per member per step (0: no limit)
   std::vector<int> last_status;             // slot id -> outcome of the last advance
+  // persistent mode: one cooperative launch per advance (svk::persist_batch_kernel)
+  bool persistent = false;
+  unsigned long long spin_limit = 1ull << 22;  // idle polls of a waiting warp before SV_E_TIMEOUT
+  svk::PersistMember* d_pmem = nullptr;        // [nact]
+  int* d_pstatus = nullptr;
+  // the members' kernel variant: the column sweep of 32 rows (variant 8) in persistent mode,
+  // whose strips are the persistent kernel's work items; else the batches' variant
+  int member_variant() const { return persistent ? 8 : svk::batch_variant<T>(); }
 
   ~Batch() override {
     cudaSetDevice(device);
@@ -1058,7 +1150,9 @@ struct Batch final : public sv_batch_base {
   }
   void free_arrays() {
     cudaFree(d_params); cudaFree(d_fin); cudaFree(d_tiles); cudaFree(d_ctls); cudaFree(d_done); cudaFree(d_queue);
+    cudaFree(d_pmem); cudaFree(d_pstatus);
     d_params = nullptr; d_fin = nullptr; d_tiles = nullptr; d_ctls = nullptr; d_done = nullptr; d_queue = nullptr;
+    d_pmem = nullptr; d_pstatus = nullptr;
     cap = 0;
   }
   int cuda_fail(cudaError_t e, const char* where) {
@@ -1085,7 +1179,7 @@ struct Batch final : public sv_batch_base {
       delete s;
       return r;
     }
-    s->set_variant(svk::batch_variant<T>());
+    s->set_variant(member_variant());
     int slot = -1;
     for (size_t i = 0; i < members.size(); ++i)
       if (!members[i]) { slot = int(i); break; }
@@ -1132,6 +1226,8 @@ struct Batch final : public sv_batch_base {
       SV_CUDA(cudaMalloc(&d_ctls, sizeof(Ctl*) * c));
       SV_CUDA(cudaMalloc(&d_done, sizeof(int) * c));
       SV_CUDA(cudaMalloc(&d_queue, sizeof(svk::StepQueue) * c));
+      SV_CUDA(cudaMalloc(&d_pmem, sizeof(svk::PersistMember) * c));
+      SV_CUDA(cudaMalloc(&d_pstatus, sizeof(int)));
       cap = c;
     }
     std::vector<svk::StageParams<T>> hp(size_t(N) * std::max(nact, 1));
@@ -1143,7 +1239,7 @@ struct Batch final : public sv_batch_base {
     for (int k = 0; k < nact; ++k) {
       Solver<T>* m = members[active[k]];
       // the tile prefix and the partials follow the batch kernel's decomposition
-      if (m->variant != svk::batch_variant<T>()) m->set_variant(svk::batch_variant<T>());
+      if (m->variant != member_variant()) m->set_variant(member_variant());
       ht[k + 1] = ht[k] + m->nblk;
       int e2;
       p2 = p2 && std::frexp(m->mesh.dx, &e2) == 0.5 && std::frexp(m->mesh.dy, &e2) == 0.5;
@@ -1214,7 +1310,7 @@ struct Batch final : public sv_batch_base {
     // members' own streams may hold pending uploads (set_field/set_forcing synchronise, but
     // be safe): order them before the batch's work
     for (int k : active) SV_CUDA(cudaStreamSynchronize(members[k]->stream));
-    if (!graph) {
+    if (!graph && !persistent) {
       int r = build_graph();
       if (r) return r;
     }
@@ -1230,7 +1326,37 @@ struct Batch final : public sv_batch_base {
     cudaError_t e = svk::launch_begin_queue(d_fin, nact, stream);
     if (e != cudaSuccess) return cuda_fail(e, "begin queued steps");
     std::vector<int> done(nact);
-    for (long long it = 0;; ++it) {
+    if (persistent) {
+      // every member's queued steps in one cooperative launch
+      e = svk::launch_persist_init(d_fin, d_pmem, d_tiles, nact, stream);
+      if (e == cudaSuccess) e = cudaMemsetAsync(d_pstatus, 0, sizeof(int), stream);
+      svk::PersistParams<T> PP{};
+      PP.Ps = d_params;
+      PP.Fs = d_fin;
+      PP.mem = d_pmem;
+      PP.nact = nact;
+      PP.nstages = N;
+      PP.status = d_pstatus;
+      PP.spin_limit = spin_limit;
+      if (e == cudaSuccess) e = svk::launch_persist<T>(PP, p2, eddy, stream);
+      if (e != cudaSuccess) return cuda_fail(e, "persistent batch kernel");
+      int st = 0;
+      SV_CUDA(cudaMemcpyAsync(&st, d_pstatus, sizeof(int), cudaMemcpyDeviceToHost, stream));
+      SV_CUDA(cudaStreamSynchronize(stream));
+      if (st != 0) {
+        // the members keep the state of their last completed timestep (a timestep's result
+        // replaces U_[0] only in its finalize)
+        for (int k = 0; k < nact; ++k) {  // the host mirrors of the state parity
+          Ctl c;
+          int r = members[active[k]]->read_ctl(c);
+          if (r) return fail(r, members[active[k]]->err);
+        }
+        last_status.assign(members.size(), SV_E_TIMEOUT);
+        return fail(SV_E_TIMEOUT, "persistent batch kernel: a warp waited " + std::to_string(spin_limit) +
+                                      " polls for work and gave up");
+      }
+    }
+    for (long long it = 0; !persistent; ++it) {
       SV_CUDA(cudaGraphLaunch(graph, stream));
       e = svk::launch_gather_done(d_ctls, nact, d_done, stream);
       if (e != cudaSuccess) return cuda_fail(e, "gather done");
@@ -1326,7 +1452,14 @@ struct Batch final : public sv_batch_base {
     return rc;
   }
 
-  int kernel_variant() const override { return svk::batch_variant<T>(); }
+  int kernel_variant() const override { return member_variant(); }
+
+  int set_persistent(int on, unsigned long long limit) override {
+    persistent = on != 0;
+    spin_limit = limit ? limit : (1ull << 22);
+    dirty = true;
+    return SV_OK;
+  }
 
   int set_step_limit(long long n) override {
     if (n < 0) return fail(SV_E_ARG, "step limit must be >= 0");
@@ -1462,6 +1595,10 @@ int sv_batch_advance_steps(sv_batch* b, int max_steps, const int* nsteps, const 
   int r = b->impl->advance_steps(max_steps, nsteps, forcing, out, n);
   if (r) g_create_err = b->impl->err;
   return r;
+}
+int sv_batch_set_persistent(sv_batch* b, int on, uint64_t spin_limit) {
+  if (!b) return SV_E_ARG;
+  return b->impl->set_persistent(on, spin_limit);
 }
 int sv_batch_kernel_variant(sv_batch* b, int* variant) {
   if (!b || !variant) return SV_E_ARG;

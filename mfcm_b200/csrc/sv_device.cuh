@@ -211,72 +211,54 @@ template <typename T> struct CellV {
 };
 template <typename T> struct FaceF { T h, u, v, z; };
 
-// ---------------------------------------------------------------------------------------
-// SaintVenantFluxKernel::operator() (src/SaintVenant/FluxKernel.cpp:62-295) for one face
-// of direction DIR (0: vertical face, flow along x; 1: horizontal face, flow along y).
-// L / R are the cells from get_adjacent_cells (equal on the mesh edge), edge is -1/0/+1.
-// d = dx or dy; hd = 0.5*d. Returns the branch code (1, 2.25, 2.75, 3, 4, or 0 when the
-// face borders coded-out cells).
-// ---------------------------------------------------------------------------------------
-template <typename T, int DIR, typename DV>
-__device__ __forceinline__ T face_flux(CellV<T> L, CellV<T> R, int edge, T hd, const DV& divd, FaceF<T>& F) {
-  const T g = T(kG);
-  const T zb_L0 = L.z, zb_R0 = R.z;
-  T zb_L = zb_L0, zb_R = zb_R0;
-  // coded-out cells (NaN bed), FluxKernel.cpp:83-107
-  if (zb_L0 != zb_L0) {
-    L = R;
-    if (edge == 1) { F.h = F.u = F.v = F.z = T(0); return T(0); }
-    edge = -1;
-  }
-  if (zb_R0 != zb_R0) {
-    if (edge == -1) { F.h = F.u = F.v = F.z = T(0); return T(0); }
-    R = L;
-    edge = 1;
-  }
-  const bool mL = edge < 0, mR = edge > 0;
-  // edge/coded-out masks, FluxKernel.cpp:111-148 (x*0 only where the mask applies)
-  T h_L = mL ? L.h * T(0) : L.h;
-  T h_R = mR ? R.h * T(0) : R.h;
-  // normal velocity is masked, tangential is not
-  T un_L = DIR == 0 ? L.u : L.v, un_R = DIR == 0 ? R.u : R.v;
-  T ut_L = DIR == 0 ? L.v : L.u, ut_R = DIR == 0 ? R.v : R.u;
-  if (mL) un_L = un_L * T(0);
-  if (mR) un_R = un_R * T(0);
-  // slopes: normal (along DIR) and tangential
-  T dhn_L = DIR == 0 ? L.dhdx : L.dhdy, dht_L = DIR == 0 ? L.dhdy : L.dhdx;
-  T dhn_R = DIR == 0 ? R.dhdx : R.dhdy, dht_R = DIR == 0 ? R.dhdy : R.dhdx;
-  T dzn_L = DIR == 0 ? L.dzdx : L.dzdy, dzt_L = DIR == 0 ? L.dzdy : L.dzdx;
-  T dzn_R = DIR == 0 ? R.dzdx : R.dzdy, dzt_R = DIR == 0 ? R.dzdy : R.dzdx;
-  // slopes of the normal velocity component (masked with it)
-  T dunn_L = DIR == 0 ? L.dudx : L.dvdy, dunt_L = DIR == 0 ? L.dudy : L.dvdx;
-  T dunn_R = DIR == 0 ? R.dudx : R.dvdy, dunt_R = DIR == 0 ? R.dudy : R.dvdx;
-  // slopes of the tangential velocity component (not masked)
-  T dutn_L = DIR == 0 ? L.dvdx : L.dudy, dutt_L = DIR == 0 ? L.dvdy : L.dudx;
-  T dutn_R = DIR == 0 ? R.dvdx : R.dudy, dutt_R = DIR == 0 ? R.dvdy : R.dudx;
-  if (mL) {
-    dhn_L = dhn_L * T(0); dht_L = dht_L * T(0); dzn_L = dzn_L * T(0); dzt_L = dzt_L * T(0);
-    dunn_L = dunn_L * T(0); dunt_L = dunt_L * T(0);
-  }
-  if (mR) {
-    dhn_R = dhn_R * T(0); dht_R = dht_R * T(0); dzn_R = dzn_R * T(0); dzt_R = dzt_R * T(0);
-    dunn_R = dunn_R * T(0); dunt_R = dunt_R * T(0);
-  }
-  // walls for coded-out / edge cells, FluxKernel.cpp:152-157
-  if (mL) zb_L = zb_R + h_R * T(2);
-  if (mR) zb_R = zb_L + h_L * T(2);
-  // MUSCL reconstruction, FluxKernel.cpp:161-187. For DIR 0 the reference adds the
-  // normal term then the tangential (*0) term; for DIR 1 the tangential term first. Both
-  // orders give b + n (a finite exact zero never changes a non-zero sum).
-  T zb_m = add_tangential_s(zb_L + hd * dzn_L, hd, dzt_L);
-  T h_m = add_tangential_s(h_L + hd * dhn_L, hd, dht_L);
-  T un_m = add_tangential_s(un_L + hd * dunn_L, hd, dunt_L);
-  T ut_m = add_tangential_s(ut_L + hd * dutn_L, hd, dutt_L);
-  T zb_p = add_tangential_s(zb_R - hd * dzn_R, hd, dzt_R);
-  T h_p = add_tangential_s(h_R - hd * dhn_R, hd, dht_R);
-  T un_p = add_tangential_s(un_R - hd * dunn_R, hd, dunt_R);
-  T ut_p = add_tangential_s(ut_R - hd * dutn_R, hd, dutt_R);
+// One side of a face after the MUSCL reconstruction (FluxKernel.cpp:161-187): bed, depth and
+// the normal and tangential velocity components at the face.
+template <typename T> struct Side { T zb, h, un, ut; };
 
+// b + hd * n on the face side of the left cell (recon_m) or b - hd * n on that of the right
+// cell (recon_p), plus the tangential term hd * t * 0 as a finiteness test (TCHK; without it
+// the term is dropped, which only changes results whose slopes are not finite).
+template <typename T, bool TCHK> __device__ __forceinline__ T recon_m(T b, T hd, T n, T t) {
+  const T r = b + hd * n;
+  if constexpr (TCHK) return add_tangential_s(r, hd, t);
+  return r;
+}
+template <typename T, bool TCHK> __device__ __forceinline__ T recon_p(T b, T hd, T n, T t) {
+  const T r = b - hd * n;
+  if constexpr (TCHK) return add_tangential_s(r, hd, t);
+  return r;
+}
+
+// The face sides of a cell with both neighbours along DIR in the mesh and a valid bed (no edge
+// or coded-out masks apply): as the left cell of its face in +DIR (side_m) and as the right
+// cell of its face in -DIR (side_p).
+template <typename T, int DIR, bool TCHK>
+__device__ __forceinline__ Side<T> side_m(const CellV<T>& c, T hd) {
+  if constexpr (DIR == 0)
+    return {recon_m<T, TCHK>(c.z, hd, c.dzdx, c.dzdy), recon_m<T, TCHK>(c.h, hd, c.dhdx, c.dhdy),
+            recon_m<T, TCHK>(c.u, hd, c.dudx, c.dudy), recon_m<T, TCHK>(c.v, hd, c.dvdx, c.dvdy)};
+  else
+    return {recon_m<T, TCHK>(c.z, hd, c.dzdy, c.dzdx), recon_m<T, TCHK>(c.h, hd, c.dhdy, c.dhdx),
+            recon_m<T, TCHK>(c.v, hd, c.dvdy, c.dvdx), recon_m<T, TCHK>(c.u, hd, c.dudy, c.dudx)};
+}
+template <typename T, int DIR, bool TCHK>
+__device__ __forceinline__ Side<T> side_p(const CellV<T>& c, T hd) {
+  if constexpr (DIR == 0)
+    return {recon_p<T, TCHK>(c.z, hd, c.dzdx, c.dzdy), recon_p<T, TCHK>(c.h, hd, c.dhdx, c.dhdy),
+            recon_p<T, TCHK>(c.u, hd, c.dudx, c.dudy), recon_p<T, TCHK>(c.v, hd, c.dvdx, c.dvdy)};
+  else
+    return {recon_p<T, TCHK>(c.z, hd, c.dzdy, c.dzdx), recon_p<T, TCHK>(c.h, hd, c.dhdy, c.dhdx),
+            recon_p<T, TCHK>(c.v, hd, c.dvdy, c.dvdx), recon_p<T, TCHK>(c.u, hd, c.dudy, c.dudx)};
+}
+
+// The flux of a face from its two reconstructed sides (FluxKernel.cpp:189-291): the face bed,
+// the wet/dry branch and the Rusanov-type fluxes of h, the normal and the tangential momentum,
+// and the bed-step (z) term. Returns the branch code (1, 2.25, 2.75, 3 or 4).
+template <typename T, int DIR, typename DV>
+__device__ __forceinline__ T face_combine(Side<T> m, Side<T> p, const DV& divd, FaceF<T>& F) {
+  const T g = T(kG);
+  const T zb_m = m.zb, zb_p = p.zb, un_m = m.un, un_p = p.un, ut_m = m.ut, ut_p = p.ut;
+  T h_m = m.h, h_p = p.h;
   T zb_f = sfmax(zb_m, zb_p);
   T y_m = zb_m + h_m;
   T y_p = zb_p + h_p;
@@ -340,6 +322,70 @@ __device__ __forceinline__ T face_flux(CellV<T> L, CellV<T> R, int edge, T hd, c
   if (DIR == 0) { F.u = Fn; F.v = Ft; }
   else { F.u = Ft; F.v = Fn; }
   return branch;
+}
+
+// ---------------------------------------------------------------------------------------
+// SaintVenantFluxKernel::operator() (src/SaintVenant/FluxKernel.cpp:62-295) for one face
+// of direction DIR (0: vertical face, flow along x; 1: horizontal face, flow along y).
+// L / R are the cells from get_adjacent_cells (equal on the mesh edge), edge is -1/0/+1.
+// d = dx or dy; hd = 0.5*d. Returns the branch code (1, 2.25, 2.75, 3, 4, or 0 when the
+// face borders coded-out cells).
+// ---------------------------------------------------------------------------------------
+template <typename T, int DIR, typename DV>
+__device__ __forceinline__ T face_flux(CellV<T> L, CellV<T> R, int edge, T hd, const DV& divd, FaceF<T>& F) {
+  const T g = T(kG);
+  const T zb_L0 = L.z, zb_R0 = R.z;
+  T zb_L = zb_L0, zb_R = zb_R0;
+  // coded-out cells (NaN bed), FluxKernel.cpp:83-107
+  if (zb_L0 != zb_L0) {
+    L = R;
+    if (edge == 1) { F.h = F.u = F.v = F.z = T(0); return T(0); }
+    edge = -1;
+  }
+  if (zb_R0 != zb_R0) {
+    if (edge == -1) { F.h = F.u = F.v = F.z = T(0); return T(0); }
+    R = L;
+    edge = 1;
+  }
+  const bool mL = edge < 0, mR = edge > 0;
+  // edge/coded-out masks, FluxKernel.cpp:111-148 (x*0 only where the mask applies)
+  T h_L = mL ? L.h * T(0) : L.h;
+  T h_R = mR ? R.h * T(0) : R.h;
+  // normal velocity is masked, tangential is not
+  T un_L = DIR == 0 ? L.u : L.v, un_R = DIR == 0 ? R.u : R.v;
+  T ut_L = DIR == 0 ? L.v : L.u, ut_R = DIR == 0 ? R.v : R.u;
+  if (mL) un_L = un_L * T(0);
+  if (mR) un_R = un_R * T(0);
+  // slopes: normal (along DIR) and tangential
+  T dhn_L = DIR == 0 ? L.dhdx : L.dhdy, dht_L = DIR == 0 ? L.dhdy : L.dhdx;
+  T dhn_R = DIR == 0 ? R.dhdx : R.dhdy, dht_R = DIR == 0 ? R.dhdy : R.dhdx;
+  T dzn_L = DIR == 0 ? L.dzdx : L.dzdy, dzt_L = DIR == 0 ? L.dzdy : L.dzdx;
+  T dzn_R = DIR == 0 ? R.dzdx : R.dzdy, dzt_R = DIR == 0 ? R.dzdy : R.dzdx;
+  // slopes of the normal velocity component (masked with it)
+  T dunn_L = DIR == 0 ? L.dudx : L.dvdy, dunt_L = DIR == 0 ? L.dudy : L.dvdx;
+  T dunn_R = DIR == 0 ? R.dudx : R.dvdy, dunt_R = DIR == 0 ? R.dudy : R.dvdx;
+  // slopes of the tangential velocity component (not masked)
+  T dutn_L = DIR == 0 ? L.dvdx : L.dudy, dutt_L = DIR == 0 ? L.dvdy : L.dudx;
+  T dutn_R = DIR == 0 ? R.dvdx : R.dudy, dutt_R = DIR == 0 ? R.dvdy : R.dudx;
+  if (mL) {
+    dhn_L = dhn_L * T(0); dht_L = dht_L * T(0); dzn_L = dzn_L * T(0); dzt_L = dzt_L * T(0);
+    dunn_L = dunn_L * T(0); dunt_L = dunt_L * T(0);
+  }
+  if (mR) {
+    dhn_R = dhn_R * T(0); dht_R = dht_R * T(0); dzn_R = dzn_R * T(0); dzt_R = dzt_R * T(0);
+    dunn_R = dunn_R * T(0); dunt_R = dunt_R * T(0);
+  }
+  // walls for coded-out / edge cells, FluxKernel.cpp:152-157
+  if (mL) zb_L = zb_R + h_R * T(2);
+  if (mR) zb_R = zb_L + h_L * T(2);
+  // MUSCL reconstruction, FluxKernel.cpp:161-187. For DIR 0 the reference adds the
+  // normal term then the tangential (*0) term; for DIR 1 the tangential term first. Both
+  // orders give b + n (a finite exact zero never changes a non-zero sum).
+  const Side<T> m{recon_m<T, true>(zb_L, hd, dzn_L, dzt_L), recon_m<T, true>(h_L, hd, dhn_L, dht_L),
+                  recon_m<T, true>(un_L, hd, dunn_L, dunt_L), recon_m<T, true>(ut_L, hd, dutn_L, dutt_L)};
+  const Side<T> p{recon_p<T, true>(zb_R, hd, dzn_R, dzt_R), recon_p<T, true>(h_R, hd, dhn_R, dht_R),
+                  recon_p<T, true>(un_R, hd, dunn_R, dunt_R), recon_p<T, true>(ut_R, hd, dutn_R, dutt_R)};
+  return face_combine<T, DIR>(m, p, divd, F);
 }
 
 // Per-launch scalars of one stage evaluation (update_dUdt arguments and forcing).

@@ -52,6 +52,12 @@ cudaError_t launch_datum_absolute(const float* off, int nx, int ny, int dtiles_x
   datum_absolute_kernel<<<elementwise_blocks(n), 256, 0, s>>>(off, nx, ny, dtiles_x, zdat, z);
   return cudaGetLastError();
 }
+cudaError_t launch_persist_init(const FinalizeParams* Fs, PersistMember* mem, const long long* warp_start, int nact,
+                                cudaStream_t s) {
+  if (nact <= 0) return cudaSuccess;
+  persist_init_kernel<<<(nact + 127) / 128, 128, 0, s>>>(Fs, mem, warp_start, nact);
+  return cudaGetLastError();
+}
 cudaError_t launch_begin_step(Ctl* ctl, int new_step, long long budget, cudaStream_t s) {
   begin_step_kernel<<<1, 1, 0, s>>>(ctl, new_step, budget);
   return cudaGetLastError();

@@ -30,15 +30,29 @@ inline bool pow2_mesh(double dx, double dy) {
   return std::frexp(dx, &e) == 0.5 && std::frexp(dy, &e) == 0.5;
 }
 
-template <typename T, int TX, int TY, int MINB, bool P2, bool EDDY>
+template <typename T, int TX, int TY, int MINB, bool P2, bool EDDY, bool PRE = false>
 static cudaError_t launch_stage_p(const StageParams<T>& P, cudaStream_t s) {
   using SM = StageSmem<T, TX, TY>;
   static std::atomic<bool> attr_set[kMaxAttrDevices];
-  cudaError_t e = smem_optin(stage_kernel<T, TX, TY, MINB, P2, EDDY>, int(sizeof(SM)), attr_set);
+  cudaError_t e = smem_optin(stage_kernel<T, TX, TY, MINB, P2, EDDY, PRE>, int(sizeof(SM)), attr_set);
   if (e != cudaSuccess) return e;
   dim3 grid((P.nx + TX - 1) / TX, (P.ny + TY - 1) / TY);
-  stage_kernel<T, TX, TY, MINB, P2, EDDY><<<grid, TX * TY, sizeof(SM), s>>>(P);
+  stage_kernel<T, TX, TY, MINB, P2, EDDY, PRE><<<grid, TX * TY, sizeof(SM), s>>>(P);
   return cudaGetLastError();
+}
+
+// split schedule: the slopes pass, then the tiled 32 x 8 stage kernel reading its slopes
+template <typename T> static cudaError_t launch_split_t(const StageParams<T>& P, cudaStream_t s) {
+  const bool p2 = pow2_mesh(P.dx, P.dy);
+  const long long n = (long long)P.nx * P.ny;
+  const unsigned blocks = unsigned((n + 255) / 256);
+  if (p2) slopes_kernel<T, true><<<blocks, 256, 0, s>>>(P);
+  else slopes_kernel<T, false><<<blocks, 256, 0, s>>>(P);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if (P.eddy)
+    return p2 ? launch_stage_p<T, 32, 8, 3, true, true, true>(P, s) : launch_stage_p<T, 32, 8, 3, false, true, true>(P, s);
+  return p2 ? launch_stage_p<T, 32, 8, 3, true, false, true>(P, s) : launch_stage_p<T, 32, 8, 3, false, false, true>(P, s);
 }
 // kernels compiled with the eddy-viscosity term run only for solvers that have it
 template <typename T, int TX, int TY, int MINB> static cudaError_t launch_stage_t(const StageParams<T>& P, cudaStream_t s) {
@@ -71,8 +85,21 @@ template <typename T, int TY, int MINB> static cudaError_t launch_sweep_t(const 
   constexpr int WPB = 4;
   const long long ntiles = variant_partials(variant, P.nx, P.ny);
   dim3 block(32, WPB);
-  dim3 grid(unsigned((ntiles + WPB - 1) / WPB));
   const bool p2 = pow2_mesh(P.dx, P.dy);
+  // interior strips (if listed) in the interior kernel, the rest in the general one
+  if (P.istrips && P.n_istrips > 0) {
+    dim3 grid(unsigned((P.n_istrips + WPB - 1) / WPB));
+    if (P.eddy) {
+      if (p2) sweep_interior_kernel<T, TY, WPB, MINB, true, true><<<grid, block, 0, s>>>(P);
+      else sweep_interior_kernel<T, TY, WPB, MINB, false, true><<<grid, block, 0, s>>>(P);
+    } else {
+      if (p2) sweep_interior_kernel<T, TY, WPB, MINB, true, false><<<grid, block, 0, s>>>(P);
+      else sweep_interior_kernel<T, TY, WPB, MINB, false, false><<<grid, block, 0, s>>>(P);
+    }
+  }
+  const long long ngen = P.bstrips ? P.n_bstrips : ntiles;
+  if (ngen <= 0) return cudaGetLastError();
+  dim3 grid(unsigned((ngen + WPB - 1) / WPB));
   if (P.eddy) {
     if (p2) sweep_kernel<T, TY, WPB, MINB, true, true><<<grid, block, 0, s>>>(P);
     else sweep_kernel<T, TY, WPB, MINB, false, true><<<grid, block, 0, s>>>(P);
@@ -92,8 +119,16 @@ template <> cudaError_t launch_variant<SV_T>(const StageParams<SV_T>& P, int var
     case 8: return launch_sweep_t<SV_T, 32, 4>(P, variant, s);
     case 9: return launch_sweep_t<SV_T, 32, 5>(P, variant, s);
     case 10: return launch_sweep_t<SV_T, 32, 6>(P, variant, s);
+    case kSplitVariant: return launch_split_t<SV_T>(P, s);
     default: return launch_stage<SV_T>(P, variant, s);
   }
+}
+
+template <> cudaError_t launch_strip_flags<SV_T>(const SV_T* z, int nx, int ny, int ty, long long nstrips,
+                                                 unsigned char* flags, cudaStream_t s) {
+  if (nstrips <= 0) return cudaSuccess;
+  strip_flags_kernel<SV_T><<<unsigned((nstrips + 7) / 8), 256, 0, s>>>(z, nx, ny, ty, nstrips, flags);
+  return cudaGetLastError();
 }
 
 template <> cudaError_t launch_bed_slopes<SV_T>(const SV_T* z, int nx, int ny, double dx, double dy, SV_T* zx,
@@ -160,6 +195,25 @@ template <> cudaError_t launch_sweep_batch<SV_T>(const StageParams<SV_T>* Ps, co
     else sweep_batch_kernel<SV_T, TY, WPB, MINB, false, false><<<grid, block, 0, s>>>(Ps, warp_start, ninst);
   }
   return cudaGetLastError();
+}
+
+// Persistent batch kernel: one cooperative launch with as many 4-warp blocks as fit on the
+// device at once (every block resident, so warps that wait for another warp's work always
+// see it done).
+template <> cudaError_t launch_persist<SV_T>(const PersistParams<SV_T>& PP, bool p2, bool eddy, cudaStream_t s) {
+  void (*kern)(const PersistParams<SV_T>) =
+      eddy ? (p2 ? persist_batch_kernel<SV_T, true, true> : persist_batch_kernel<SV_T, false, true>)
+           : (p2 ? persist_batch_kernel<SV_T, true, false> : persist_batch_kernel<SV_T, false, false>);
+  int dev = 0, nsm = 0, per_sm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * kPersistWarps, 0);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
+  PersistParams<SV_T> arg = PP;
+  void* args[] = {&arg};
+  return cudaLaunchCooperativeKernel((const void*)kern, dim3(unsigned(per_sm * nsm)), dim3(32, kPersistWarps), args,
+                                     0, s);
 }
 
 template <typename T, int TX, int TY>

@@ -98,6 +98,14 @@ template <typename T> struct StageParams {
   // 2 energy loss, 3 eddy viscosity (each adds to du/dt and dv/dt, so the order sets the
   // rounding); used by the kernels compiled with eddy viscosity
   int term_order;
+  // column-sweep strips split by kind (see strip_flags_kernel): the interior strips run the
+  // interior kernel, the others the general one; null lists: every strip runs the general one
+  const int* istrips;
+  const int* bstrips;
+  int n_istrips, n_bstrips;
+  // split schedule: the stage input's slopes dh/dx, du/dx, dv/dx, dh/dy, du/dy, dv/dy as
+  // written by slopes_kernel (read by the stage kernel instead of computing them), or null
+  T* pslp[6];
 };
 
 // partial layout: [0, nblk) cn max, [nblk, 2nblk) cn min, [2nblk, 3nblk) volume,
@@ -105,6 +113,13 @@ template <typename T> struct StageParams {
 __host__ __device__ inline long long part_count(long long nblk, int nstages) { return (3 + 3LL * nstages) * nblk; }
 
 template <typename T> __device__ __forceinline__ T ld(const T* p, long long i) { return __ldg(p + i); }
+// Loads of the state, stage and accumulator buffers. A launch that writes and later reads them
+// itself (the persistent batch kernel, COH) must use coherent loads, ordered by its phase
+// fences; every other launch only reads what earlier launches wrote, through the read-only path.
+template <bool COH, typename T> __device__ __forceinline__ T ldst(const T* p, long long i) {
+  if constexpr (COH) return p[i];
+  return __ldg(p + i);
+}
 
 // Datum tiles of the FP32-with-datum mode: 32 x 8 cells, each with an FP64 datum; the stored
 // bed is the FP32 offset from its tile's datum.
@@ -192,7 +207,7 @@ template <> struct MkDivX<DivF> { __device__ static DivF make(double d) { return
 // fluxes; returns the rain rate added, the depth rate removed by the head assignment and the
 // depth rate that entered through mesh-edge faces (the reference's walls pass flow through
 // their one-sided branches; taken before any boundary assignment).
-template <typename T, typename CC, bool EDDY = false>
+template <typename T, typename CC, bool EDDY = false, bool EDGE = true>
 __device__ __forceinline__ void cell_dudt(const StageParams<T>& P, const DevForcing& fc, const CC& c,
                                           long long g, int gx,
                                           int gy, T h, T u, T v, T dhdx, T dhdy, T dzdx, T dzdy,
@@ -265,19 +280,23 @@ __device__ __forceinline__ void cell_dudt(const StageParams<T>& P, const DevForc
   rain = 0.0;
   removed = 0.0;
   wall = 0.0;
-  if (gx == 0) wall += double(c.divx(fw.h));
-  if (gx == P.nx - 1) wall -= double(c.divx(fe.h));
-  if (gy == 0) wall += double(c.divy(fs.h));
-  if (gy == P.ny - 1) wall -= double(c.divy(fn.h));
+  if constexpr (EDGE) {  // cells away from the mesh edge have no wall faces
+    if (gx == 0) wall += double(c.divx(fw.h));
+    if (gx == P.nx - 1) wall -= double(c.divx(fe.h));
+    if (gy == 0) wall += double(c.divy(fs.h));
+    if (gy == P.ny - 1) wall -= double(c.divy(fn.h));
+  }
   // head boundary target values for this cell (NaN = not selected); a stage boundary
   // (StageBoundarySourceTerm.cpp:48-52) gives water levels, from which the bed is subtracted
   bool head_sel = false;
   T h0 = T(0), h1 = T(0);
   const int hk = fc.head_kind;
   if (hk == 1 || hk == 3) {
-    head_sel = ((fc.head_edges & 1u) && gx == 0) || ((fc.head_edges & 2u) && gx == P.nx - 1) ||
-               ((fc.head_edges & 4u) && gy == 0) || ((fc.head_edges & 8u) && gy == P.ny - 1);
-    h0 = T(fc.hh0); h1 = T(fc.hh1);
+    if constexpr (EDGE) {  // edge strips: never a cell away from the mesh edge
+      head_sel = ((fc.head_edges & 1u) && gx == 0) || ((fc.head_edges & 2u) && gx == P.nx - 1) ||
+                 ((fc.head_edges & 4u) && gy == 0) || ((fc.head_edges & 8u) && gy == P.ny - 1);
+      h0 = T(fc.hh0); h1 = T(fc.hh1);
+    }
   } else if (hk == 2 || hk == 4) {
     h0 = ld(P.hb0p, g); h1 = ld(P.hb1p, g);
     head_sel = true;
@@ -316,7 +335,7 @@ __device__ __forceinline__ void cell_dudt(const StageParams<T>& P, const DevForc
 
 // One cell of one stage after its four face fluxes are known: dU/dt, then the Runge-Kutta
 // combination (RungeKutta.hpp:377-388) and, on the last stage, the CFL quantity and volume.
-template <typename T, typename CC, bool EDDY = false>
+template <typename T, typename CC, bool EDDY = false, bool EDGE = true, bool COH = false>
 __device__ __forceinline__ void finish_cell(const StageParams<T>& P, const DevForcing& fc, const CC& c,
                                             long long g, int gx, int gy, T h, T u, T v, T dhdx, T dhdy, T dzdx,
                                             T dzdy, const FaceF<T>& fw, const FaceF<T>& fe, const FaceF<T>& fs,
@@ -325,8 +344,8 @@ __device__ __forceinline__ void finish_cell(const StageParams<T>& P, const DevFo
                                             T& xcfl_min, double& vol, const EddyIn<T>* ed = nullptr) {
   T kh, ku, kv;
   double r_, o_, w_;
-  cell_dudt<T, CC, EDDY>(P, fc, c, g, gx, gy, h, u, v, dhdx, dhdy, dzdx, dzdy, fw, fe, fs, fn, kh, ku, kv, r_, o_,
-                         w_, (T*)nullptr, (T*)nullptr, ed);
+  cell_dudt<T, CC, EDDY, EDGE>(P, fc, c, g, gx, gy, h, u, v, dhdx, dhdy, dzdx, dzdy, fw, fe, fs, fn, kh, ku, kv, r_,
+                               o_, w_, (T*)nullptr, (T*)nullptr, ed);
   rain += r_;
   removed += o_;
   walls += w_;
@@ -353,8 +372,8 @@ __device__ __forceinline__ void finish_cell(const StageParams<T>& P, const DevFo
     T u0v[3], accv[3];
 #pragma unroll
     for (int f = 0; f < 3; ++f) {
-      u0v[f] = first ? (f == 0 ? h : (f == 1 ? u : v)) : ld(U0[f], g);
-      accv[f] = first ? (incr ? T(0) : u0v[f]) : ld(A[f], g);
+      u0v[f] = first ? (f == 0 ? h : (f == 1 ? u : v)) : ldst<COH>(U0[f], g);
+      accv[f] = first ? (incr ? T(0) : u0v[f]) : ldst<COH>(A[f], g);
     }
     if (!last) {
       const T cA = T(P.a_next[st] * dt_d);
@@ -379,7 +398,7 @@ __device__ __forceinline__ void finish_cell(const StageParams<T>& P, const DevFo
           A[f][g] = d;
           out[f] = d;
         } else if (f == 0) {  // U_N.h = U0.h + d with the carried compensation (Neumaier)
-          const T y = d + ld(P.hc[cur], g);
+          const T y = d + ldst<COH>(P.hc[cur], g);
           const T t = u0v[0] + y;
           P.hc[cur ^ 1][g] = (sfabs(u0v[0]) >= sfabs(y)) ? (u0v[0] - t) + y : (y - t) + u0v[0];
           out[0] = t;
@@ -394,12 +413,12 @@ __device__ __forceinline__ void finish_cell(const StageParams<T>& P, const DevFo
     // general tableau: Y_{s+1} = ((U0 + k_0 c_0) + k_1 c_1) + ... with stored k_j
     T u0v[3];
 #pragma unroll
-    for (int f = 0; f < 3; ++f) u0v[f] = first ? (f == 0 ? h : (f == 1 ? u : v)) : ld(U0[f], g);
+    for (int f = 0; f < 3; ++f) u0v[f] = first ? (f == 0 ? h : (f == 1 ? u : v)) : ldst<COH>(U0[f], g);
     const double* coef = last ? P.b : P.a_next;
 #pragma unroll
     for (int f = 0; f < 3; ++f) {
       T y = u0v[f];
-      for (int j = 0; j < st; ++j) y = y + ld(P.Kin[j][f], g) * T(coef[j] * dt_d);
+      for (int j = 0; j < st; ++j) y = y + ldst<COH>(P.Kin[j][f], g) * T(coef[j] * dt_d);
       y = y + k[f] * T(coef[st] * dt_d);
       out[f] = y;
       if (last) A[f][g] = y;
@@ -430,7 +449,7 @@ struct StageSmem {
 };
 
 // One TX x TY tile of one stage: bx, by = tile coordinates, blk = partial-sum slot.
-template <typename T, int TX, int TY, bool P2, bool EDDY>
+template <typename T, int TX, int TY, bool P2, bool EDDY, bool PRE = false>
 __device__ __forceinline__ void stage_tile(const StageParams<T>& P, int bx, int by, long long blk,
                                            StageSmem<T, TX, TY>& s) {
   using DX = DivX<T, P2>;
@@ -479,11 +498,20 @@ __device__ __forceinline__ void stage_tile(const StageParams<T>& P, int bx, int 
     long long g = (long long)gy * nx + gx;
     s.slp[3][sy][sx] = ld(P.zx, g);
     s.slp[7][sy][sx] = ld(P.zy, g);
+    if constexpr (PRE) {  // split schedule: slopes from the slopes pass
 #pragma unroll
-    for (int f = 0; f < 3; ++f) {
-      s.slp[f][sy][sx] = minmod3<T>(s.val[f][ly][lx - 1], hasW, s.val[f][ly][lx], hasE, s.val[f][ly][lx + 1], divx);
-      // Y axis: north (row + 1) is the left neighbour, south the right
-      s.slp[4 + f][sy][sx] = minmod3<T>(s.val[f][ly + 1][lx], hasN, s.val[f][ly][lx], hasS, s.val[f][ly - 1][lx], divy);
+      for (int f = 0; f < 3; ++f) {
+        s.slp[f][sy][sx] = ld(P.pslp[f], g);
+        s.slp[4 + f][sy][sx] = ld(P.pslp[3 + f], g);
+      }
+    } else {
+#pragma unroll
+      for (int f = 0; f < 3; ++f) {
+        s.slp[f][sy][sx] = minmod3<T>(s.val[f][ly][lx - 1], hasW, s.val[f][ly][lx], hasE, s.val[f][ly][lx + 1], divx);
+        // Y axis: north (row + 1) is the left neighbour, south the right
+        s.slp[4 + f][sy][sx] =
+            minmod3<T>(s.val[f][ly + 1][lx], hasN, s.val[f][ly][lx], hasS, s.val[f][ly - 1][lx], divy);
+      }
     }
   }
   __syncthreads();
@@ -582,11 +610,39 @@ __device__ __forceinline__ void stage_tile(const StageParams<T>& P, int bx, int 
   }
 }
 
-template <typename T, int TX, int TY, int MINB, bool P2, bool EDDY>
+template <typename T, int TX, int TY, int MINB, bool P2, bool EDDY, bool PRE = false>
 __global__ void __launch_bounds__(TX * TY, MINB) stage_kernel(const StageParams<T> P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   auto& s = *reinterpret_cast<StageSmem<T, TX, TY>*>(smem_raw);
-  stage_tile<T, TX, TY, P2, EDDY>(P, blockIdx.x, blockIdx.y, (long long)blockIdx.y * gridDim.x + blockIdx.x, s);
+  stage_tile<T, TX, TY, P2, EDDY, PRE>(P, blockIdx.x, blockIdx.y, (long long)blockIdx.y * gridDim.x + blockIdx.x, s);
+}
+
+// Split schedule, first pass: the Minmod3 slopes of the stage input (State.cpp:176-193), one
+// thread per cell, into P.pslp; the stage kernel that follows reads them instead of forming
+// them from its tile.
+template <typename T, bool P2>
+__global__ void __launch_bounds__(256) slopes_kernel(const StageParams<T> P) {
+  using DX = DivX<T, P2>;
+  const Ctl* ctl = P.ctl;
+  if (ctl->done) return;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int nx = P.nx, ny = P.ny;
+  if (i >= (long long)nx * ny) return;
+  const int cur = ctl->cur;
+  const bool first = P.mode & M_FIRST;
+  const int gx = int(i % nx), gy = int(i / nx);
+  const bool hasW = gx > 0, hasE = gx < nx - 1, hasN = gy < ny - 1, hasS = gy > 0;
+  const DX divx = MkDivX<DX>::make(P.dx), divy = MkDivX<DX>::make(P.dy);
+#pragma unroll
+  for (int f = 0; f < 3; ++f) {
+    const T* a = first ? P.S[cur][f] : P.Yin[f];
+    const T c = ld(a, i);
+    const T l = hasW ? ld(a, i - 1) : c, r = hasE ? ld(a, i + 1) : c;
+    P.pslp[f][i] = minmod3<T>(l, hasW, c, hasE, r, divx);
+    // Y axis: north (row + 1) is the left neighbour, south the right
+    const T n = hasN ? ld(a, i + nx) : c, so = hasS ? ld(a, i - nx) : c;
+    P.pslp[3 + f][i] = minmod3<T>(n, hasN, c, hasS, so, divy);
+  }
 }
 
 // Batched stage: one launch covers every tile of every instance of a batch. tile_start has
@@ -696,7 +752,7 @@ __device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefe
 // One warp's strip `gw` (row-major over strips of kSweepOut columns x TY rows) of one
 // solver's stage. Called by the single-solver kernel (P in parameter space) and by the
 // batched kernel (P in shared memory).
-template <typename T, int TY, bool P2, bool EDDY>
+template <typename T, int TY, bool P2, bool EDDY, bool COH = false>
 __device__ __forceinline__ void sweep_strip(const StageParams<T>& P, long long gw) {
   using DX = DivX<T, P2>;
   const Ctl* ctl = P.ctl;
@@ -736,7 +792,7 @@ __device__ __forceinline__ void sweep_strip(const StageParams<T>& P, long long g
     const int r = min(max(gy, 0), ny - 1);
     const long long g = (long long)r * nx + gxc;
     RowV<T> v;
-    v.h = ld(Yh, g); v.u = ld(Yu, g); v.v = ld(Yv, g);
+    v.h = ldst<COH>(Yh, g); v.u = ldst<COH>(Yu, g); v.v = ldst<COH>(Yv, g);
     v.z = ld(P.z, g);
     v.zx = ld(P.zx, g); v.zy = ld(P.zy, g);
     return v;
@@ -865,9 +921,9 @@ __device__ __forceinline__ void sweep_strip(const StageParams<T>& P, long long g
       const FaceF<T> FE{dn1(FW.h), dn1(FW.u), dn1(FW.v), dn1(FW.z)};
       if (out_lane && r < ny) {
         const long long g = (long long)r * nx + gx;
-        finish_cell<T, CellCtx<T, DX>, EDDY>(P, fc, c, g, gx, r, me.h, me.u, me.v, me.dhdx, me.dhdy, me.dzdx,
-                                             me.dzdy, FW, FE, FS, FN, first, last, cur, dt_d, rain, removed, walls,
-                                             xcfl, xmin, vol, &ed);
+        finish_cell<T, CellCtx<T, DX>, EDDY, true, COH>(P, fc, c, g, gx, r, me.h, me.u, me.v, me.dhdx, me.dhdy,
+                                                        me.dzdx, me.dzdy, FW, FE, FS, FN, first, last, cur, dt_d, rain,
+                                                        removed, walls, xcfl, xmin, vol, &ed);
       }
     }
     FS = FN;
@@ -890,14 +946,243 @@ __device__ __forceinline__ void sweep_strip(const StageParams<T>& P, long long g
   }
 }
 
+// Whether strip `gw` of the column sweep with TY output rows is interior: its window (the
+// 32 columns x TY + 4 rows of cells it loads) lies inside the mesh with a cell to spare on
+// every side. Every slope it computes is then two-sided, none of its faces is a mesh-edge face
+// and none of its output cells lies on an edge strip.
+__host__ __device__ inline bool strip_inside(long long gw, int nx, int ny, int ty) {
+  const int tiles_x = (nx + kSweepOut - 1) / kSweepOut;
+  const int x0 = int(gw % tiles_x) * kSweepOut, y0 = int(gw / tiles_x) * ty;
+  return x0 >= 2 && x0 + 30 <= nx && y0 >= 2 && y0 + ty + 2 <= ny;
+}
+
+// Per strip: 1 for an interior strip whose window holds no coded-out (NaN) bed, so that no
+// edge or coded-out mask applies to any of its faces; else 0. One warp per strip.
+template <typename T>
+__global__ void strip_flags_kernel(const T* __restrict__ z, int nx, int ny, int ty, long long nstrips,
+                                   unsigned char* __restrict__ flag) {
+  const long long gw = (long long)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  if (gw >= nstrips) return;  // whole warp
+  const int lane = threadIdx.x & 31;
+  bool ok = strip_inside(gw, nx, ny, ty);
+  if (ok) {
+    const int tiles_x = (nx + kSweepOut - 1) / kSweepOut;
+    const int gx = int(gw % tiles_x) * kSweepOut - 2 + lane, y0 = int(gw / tiles_x) * ty;
+    for (int r = y0 - 2; r <= y0 + ty + 1; ++r) {
+      const T v = z[(long long)r * nx + gx];
+      if (v != v) ok = false;
+    }
+  }
+  ok = __all_sync(kFull, ok);
+  if (lane == 0) flag[gw] = ok ? 1 : 0;
+}
+
+// One interior strip (strip_flags_kernel) of one solver's stage: the column sweep of
+// sweep_strip with every neighbour present and no mask to apply. The face fluxes are formed
+// from reconstructed face sides (side_m / side_p, then face_combine): each lane reconstructs
+// its east side once and its east neighbour takes those four values by shuffles. In FP64 the
+// arithmetic is the general path's, operation for operation; in FP32 the tangential
+// finiteness tests are dropped (they only matter for slopes that are not finite, which an
+// interior window without coded-out beds produces only from a non-finite state).
+template <typename T, int TY, bool P2, bool EDDY>
+__device__ __forceinline__ void sweep_strip_interior(const StageParams<T>& P, long long gw) {
+  using DX = DivX<T, P2>;
+  constexpr bool TCHK = sizeof(T) == 8;
+  const Ctl* ctl = P.ctl;
+  const int nx = P.nx, ny = P.ny;
+  const int tiles_x = (nx + kSweepOut - 1) / kSweepOut;
+  const int lane = threadIdx.x;
+  const int tile_x = int(gw % tiles_x), tile_y = int(gw / tiles_x);
+  const int gx = tile_x * kSweepOut - 2 + lane;  // inside the mesh for every lane
+  const bool out_lane = lane >= 2 && lane < 2 + kSweepOut;
+  const int y0 = tile_y * TY;
+
+  const int cur = ctl->cur;
+  const double dt_d = ctl->dt;
+  const double tsub = ctl->t_local + P.c_s * dt_d;
+  const bool first = P.mode & M_FIRST, last = P.mode & M_LAST;
+  const T* Yh = first ? P.S[cur][0] : P.Yin[0];
+  const T* Yu = first ? P.S[cur][1] : P.Yin[1];
+  const T* Yv = first ? P.S[cur][2] : P.Yin[2];
+  const DX divx = MkDivX<DX>::make(P.dx), divy = MkDivX<DX>::make(P.dy);
+  const T hdx = T(0.5) * T(P.dx), hdy = T(0.5) * T(P.dy);
+  CellCtx<T, DX> c;
+  c.divx = divx; c.divy = divy;
+  c.divdt = mkdiv<T>(dt_d);
+  c.divL = mkdiv<T>(P.L);
+  c.dt = T(dt_d); c.dt_d = dt_d; c.tsub_d = tsub;
+  c.manning = P.manning; c.rain_mode = P.rain_mode; c.head_first = P.head_first;
+  const DevForcing fc = *P.fc;
+  // FP32 with tile datums: a vertical face crosses datum tiles where its right cell starts a
+  // tile column, a horizontal face where its upper row starts a tile row; there the upper /
+  // right cell's bed moves into the other cell's frame (face_frame)
+  const bool xcross = P.zdat != nullptr && (gx % kDatumTX) == 0;
+
+  auto load_row = [&](int r) {
+    const long long g = (long long)r * nx + gx;
+    RowV<T> v;
+    v.h = ld(Yh, g); v.u = ld(Yu, g); v.v = ld(Yv, g);
+    v.z = ld(P.z, g);
+    v.zx = ld(P.zx, g); v.zy = ld(P.zy, g);
+    return v;
+  };
+  auto prefetch_rows = [&](int k) {
+    {
+      const int r = min(k + 1 + kSweepPfWindow, ny - 1);
+      const long long g = (long long)r * nx + gx;
+      prefetch_l1(Yh + g); prefetch_l1(Yu + g); prefetch_l1(Yv + g);
+      prefetch_l1(P.z + g); prefetch_l1(P.zx + g); prefetch_l1(P.zy + g);
+    }
+    const int r = min(k - 2 + kSweepPfCell, ny - 1);
+    const long long g = (long long)r * nx + gx;
+    if (!first) {
+      for (int f = 0; f < 3; ++f) { prefetch_l1(P.S[cur][f] + g); prefetch_l1(P.S[cur ^ 1][f] + g); }
+    }
+    if (P.manning) {
+      for (int f = 0; f < 4; ++f)
+        if (P.man_p[f]) prefetch_l1(P.man_p[f] + g);
+    }
+    if (P.irate) { prefetch_l1(P.irate + g); prefetch_l1(P.icap + g); }
+    if (P.efx) { prefetch_l1(P.efx + g); prefetch_l1(P.efy + g); }
+    if (fc.rain_kind == 3) prefetch_l1(P.pat + g);
+    if (fc.rain_kind == 2) { prefetch_l1(P.q0p + g); prefetch_l1(P.q1p + g); }
+    if (fc.head_kind == 2) { prefetch_l1(P.hb0p + g); prefetch_l1(P.hb1p + g); }
+  };
+
+  RowV<T> Rm{}, R0{}, Rp{};
+  SlopeV<T> Sm{}, S0{};
+  T Smm_uy = T(0), Smm_vy = T(0);
+  T fyA[3] = {}, fyB[3] = {};
+  FaceF<T> FS{}, FN{};
+  double rain = 0.0, removed = 0.0, walls = 0.0, vol = 0.0;
+  T xcfl = T(0), xmin = T(1.0 / 0.0);
+
+  for (int k = y0 - 2; k <= y0 + TY + 1; ++k) {
+    prefetch_rows(k);
+    Rm = R0; R0 = Rp; Rp = load_row(k);
+    if constexpr (EDDY) { Smm_uy = Sm.uy; Smm_vy = Sm.vy; }
+    Sm = S0;
+    fyA[0] = fyB[0]; fyA[1] = fyB[1]; fyA[2] = fyB[2];
+    if (k >= y0 - 1) {
+      fyB[0] = divy(Rp.h - R0.h);
+      fyB[1] = divy(Rp.u - R0.u);
+      fyB[2] = divy(Rp.v - R0.v);
+    }
+    // slopes of row k-1 (State.cpp:187-192), two-sided; the Y axis uses north as the left side
+    if (k >= y0) {
+      S0.hy = minmod3q<T>(-fyB[0], true, -fyA[0], true, divy(Rm.h - Rp.h));
+      S0.uy = minmod3q<T>(-fyB[1], true, -fyA[1], true, divy(Rm.u - Rp.u));
+      S0.vy = minmod3q<T>(-fyB[2], true, -fyA[2], true, divy(Rm.v - Rp.v));
+      {
+        T r_ = dn1(R0.h), l_ = up1(R0.h);
+        T fq = divx(r_ - R0.h);
+        S0.hx = minmod3q<T>(up1(fq), true, fq, true, divx(r_ - l_));
+      }
+      {
+        T r_ = dn1(R0.u), l_ = up1(R0.u);
+        T fq = divx(r_ - R0.u);
+        S0.ux = minmod3q<T>(up1(fq), true, fq, true, divx(r_ - l_));
+      }
+      {
+        T r_ = dn1(R0.v), l_ = up1(R0.v);
+        T fq = divx(r_ - R0.v);
+        S0.vx = minmod3q<T>(up1(fq), true, fq, true, divx(r_ - l_));
+      }
+    }
+    // horizontal face between rows k-2 and k-1 (face row fy = k-1), Fluxes.cpp:55-64
+    if (k >= y0 + 1 && out_lane) {
+      const int fy = k - 1;
+      const CellV<T> lo = mkcell(Rm, Sm);
+      CellV<T> hi = mkcell(R0, S0);
+      if (P.zdat != nullptr && (fy % kDatumTY) == 0) {
+        const long long tb = datum_tile(gx, fy, P.dtiles_x);
+        hi.z = T(double(hi.z) + (P.zdat[tb] - P.zdat[tb - P.dtiles_x]));
+      }
+      face_combine<T, 1>(side_m<T, 1, TCHK>(lo, hdy), side_p<T, 1, TCHK>(hi, hdy), divy, FN);
+    }
+    // output row k-2
+    if (k >= y0 + 2) {
+      const int r = k - 2;
+      const CellV<T> me = mkcell(Rm, Sm);
+      EddyIn<T> ed{};
+      if constexpr (EDDY) {
+        if (P.eddy) {  // second derivatives of row r: x by shuffles, y from rows r+1, r, r-1
+          ed.ux = Sm.ux; ed.uy = Sm.uy; ed.vx = Sm.vx; ed.vy = Sm.vy;
+          {
+            T r_ = dn1(Sm.ux), l_ = up1(Sm.ux);
+            T fq = divx(r_ - Sm.ux);
+            ed.uxx = minmod3q<T>(up1(fq), true, fq, true, divx(r_ - l_));
+          }
+          {
+            T r_ = dn1(Sm.vx), l_ = up1(Sm.vx);
+            T fq = divx(r_ - Sm.vx);
+            ed.vxx = minmod3q<T>(up1(fq), true, fq, true, divx(r_ - l_));
+          }
+          ed.uyy = minmod3q<T>(divy(Sm.uy - S0.uy), true, divy(Smm_uy - Sm.uy), true, divy(Smm_uy - S0.uy));
+          ed.vyy = minmod3q<T>(divy(Sm.vy - S0.vy), true, divy(Smm_vy - Sm.vy), true, divy(Smm_vy - S0.vy));
+        }
+      }
+      // west face: the left lane's east side against this lane's west side
+      const Side<T> mE = side_m<T, 0, TCHK>(me, hdx);
+      const Side<T> mW{up1(mE.zb), up1(mE.h), up1(mE.un), up1(mE.ut)};
+      CellV<T> meW = me;
+      if (xcross) {
+        const long long tb = datum_tile(gx, r, P.dtiles_x);
+        meW.z = T(double(me.z) + (P.zdat[tb] - P.zdat[tb - 1]));
+      }
+      FaceF<T> FW;
+      face_combine<T, 0>(mW, side_p<T, 0, TCHK>(meW, hdx), divx, FW);
+      const FaceF<T> FE{dn1(FW.h), dn1(FW.u), dn1(FW.v), dn1(FW.z)};
+      if (out_lane) {
+        const long long g = (long long)r * nx + gx;
+        finish_cell<T, CellCtx<T, DX>, EDDY, false>(P, fc, c, g, gx, r, me.h, me.u, me.v, me.dhdx, me.dhdy,
+                                                    me.dzdx, me.dzdy, FW, FE, FS, FN, first, last, cur, dt_d, rain,
+                                                    removed, walls, xcfl, xmin, vol, &ed);
+      }
+    }
+    FS = FN;
+  }
+  if (last && !(P.mode & M_DEBUGK)) {
+    double mx = warp_max(double(xcfl)), mn = warp_min(double(xmin)), vs = warp_sum<T>(vol);
+    if (lane == 0) {
+      P.part[gw] = mx;
+      P.part[P.nblk + gw] = mn;
+      P.part[2 * P.nblk + gw] = vs;
+    }
+  }
+  if (P.mode & M_TALLY) {
+    double rs = warp_sum<T>(rain), os = warp_sum<T>(removed), ws = warp_sum<T>(walls);
+    if (lane == 0) {
+      P.part[(3 + 3LL * P.stage) * P.nblk + gw] = rs;
+      P.part[(4 + 3LL * P.stage) * P.nblk + gw] = os;
+      P.part[(5 + 3LL * P.stage) * P.nblk + gw] = ws;
+    }
+  }
+}
+
+// The general column sweep over the strips in P.bstrips (every strip when the list is null).
 template <typename T, int TY, int WPB, int MINB, bool P2, bool EDDY>
 __global__ void __launch_bounds__(32 * WPB, MINB) sweep_kernel(const __grid_constant__ StageParams<T> P) {
   if (P.ctl->done) return;
-  const int tiles_x = (P.nx + kSweepOut - 1) / kSweepOut;
-  const long long ntiles = (long long)tiles_x * ((P.ny + TY - 1) / TY);
-  const long long gw = (long long)blockIdx.x * WPB + threadIdx.y;
-  if (gw >= ntiles) return;  // whole warp: no block-level synchronisation below
+  const long long i = (long long)blockIdx.x * WPB + threadIdx.y;
+  long long gw = i;
+  if (P.bstrips) {
+    if (i >= P.n_bstrips) return;  // whole warp: no block-level synchronisation below
+    gw = P.bstrips[i];
+  } else {
+    const int tiles_x = (P.nx + kSweepOut - 1) / kSweepOut;
+    if (i >= (long long)tiles_x * ((P.ny + TY - 1) / TY)) return;
+  }
   sweep_strip<T, TY, P2, EDDY>(P, gw);
+}
+
+// The interior column sweep over the strips in P.istrips.
+template <typename T, int TY, int WPB, int MINB, bool P2, bool EDDY>
+__global__ void __launch_bounds__(32 * WPB, MINB) sweep_interior_kernel(const __grid_constant__ StageParams<T> P) {
+  if (P.ctl->done) return;
+  const long long i = (long long)blockIdx.x * WPB + threadIdx.y;
+  if (i >= P.n_istrips) return;  // whole warp
+  sweep_strip_interior<T, TY, P2, EDDY>(P, P.istrips[i]);
 }
 
 // Batched column sweep: the strips of every instance of a batch, warp_start[i] being the
@@ -1056,6 +1341,9 @@ template <int NT> __device__ double fixed_sum(const double* p, long long n, doub
   return r;
 }
 
+__device__ __forceinline__ void finalize_control(const FinalizeParams& F, double mx, double mn, double vol,
+                                                 double rain, double outf, double wall);
+
 template <int NT> __device__ __forceinline__ void finalize_body(const FinalizeParams& F, double* red) {
   Ctl* ctl = F.ctl;
   if (ctl->done) return;
@@ -1095,6 +1383,16 @@ template <int NT> __device__ __forceinline__ void finalize_body(const FinalizePa
     }
   }
   if (threadIdx.x != 0) return;
+  finalize_control(F, mx, mn, vol, rain, outf, wall);
+}
+
+// The rest of a timestep's finalize, one thread, from its reductions (CFL max and min over
+// cells of (|u|+c)/dx + (|v|+c)/dy, volume, tallies): the control number, accept / repeat and
+// the new dt (RungeKutta.cpp:154-167), the step clock and the end-of-step trimming
+// (TemporalScheme.hpp:119-146) and, for a batch member, its step queue.
+__device__ __forceinline__ void finalize_control(const FinalizeParams& F, double mx, double mn, double vol,
+                                                 double rain, double outf, double wall) {
+  Ctl* ctl = F.ctl;
   const double dt = ctl->dt;
   // control number: max over cells of dt * x
   double cn;
@@ -1182,6 +1480,189 @@ template <int NT> __global__ void __launch_bounds__(NT) finalize_batch_kernel(co
   if (threadIdx.x == 0) Fsh = Fs[blockIdx.x];
   __syncthreads();
   finalize_body<NT>(Fsh, red);
+}
+
+// ---------------------------------------------------------------------------------------
+// Persistent batch kernel. One cooperative launch advances every member of a batch through
+// its queued steps (TypedTemporalScheme::solve / step for each member, TemporalScheme.hpp:
+// 112-149, 244-276), each member at its own dt. A member's timestep is N stage phases of
+// column-sweep strips followed by one finalize phase (reductions and the dt controller).
+// Warps claim work items from any member whose current phase has unclaimed items; the warp
+// that completes the last item of a phase opens the member's next phase. Phases are ordered by
+// release fences before each completion count and acquire fences after each claim, and the
+// state buffers are read with coherent loads (ldst<true>). A warp that finds no work waits
+// with a bounded number of polls; when the bound runs out it records SV_E_TIMEOUT in the
+// launch status and every warp returns at its next poll.
+// ---------------------------------------------------------------------------------------
+struct PersistMember {
+  unsigned long long phase;   // phases opened so far: stage = phase % (N + 1), N = the finalize
+  unsigned long long ticket;  // work items claimed so far, over all phases
+  unsigned int done;          // items of the current phase completed
+  int finished;               // 1: no more work for this member in this launch
+  long long nstrips;          // column-sweep strips of one stage
+};
+
+template <typename T> struct PersistParams {
+  const StageParams<T>* Ps;   // stage s of member k at Ps[s * nact + k]
+  const FinalizeParams* Fs;   // [nact]
+  PersistMember* mem;         // [nact]
+  int nact, nstages;
+  int* status;                // 0, or SV_E_TIMEOUT (-6) once a wait gave up
+  unsigned long long spin_limit;  // polls without work before giving up
+};
+
+constexpr int kPersistWarps = 4;   // warps per block
+constexpr int kPersistRows = 32;   // column-sweep strip height (the batches' variant 8)
+
+#ifdef SV_DEFINE_COMMON_KERNELS
+// mark the members whose step queue starts with nothing to do (their controller is done)
+__global__ void persist_init_kernel(const FinalizeParams* Fs, PersistMember* mem, const long long* warp_start,
+                                    int nact) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nact) return;
+  PersistMember m{};
+  m.nstrips = warp_start[k + 1] - warp_start[k];
+  m.finished = Fs[k].ctl->done != 0 ? 1 : 0;
+  mem[k] = m;
+}
+#endif
+
+// Fixed-order sum of p[0..n) by one warp, in exactly the order of fixed_sum<NT> (thread t of
+// NT adds p[t], p[t+NT], ..., then a binary tree): red holds NT doubles.
+template <int NT> __device__ double warp_fixed_sum(const double* p, long long n, double* red) {
+  const int lane = threadIdx.x & 31;
+  for (int t = lane; t < NT; t += 32) {
+    double a = 0.0;
+    for (long long i = t; i < n; i += NT) a += p[i];
+    red[t] = a;
+  }
+  __syncwarp();
+  for (int st = NT / 2; st > 0; st >>= 1) {
+    for (int t = lane; t < st; t += 32) red[t] += red[t + st];
+    __syncwarp();
+  }
+  const double r = red[0];
+  __syncwarp();
+  return r;
+}
+template <int NT, bool MAX> __device__ double warp_fixed_ext(const double* p, long long n, double* red) {
+  const int lane = threadIdx.x & 31;
+  for (int t = lane; t < NT; t += 32) {
+    double a = MAX ? 0.0 : 1.0 / 0.0;
+    for (long long i = t; i < n; i += NT) a = MAX ? nmax(a, p[i]) : nmin(a, p[i]);
+    red[t] = a;
+  }
+  __syncwarp();
+  for (int st = NT / 2; st > 0; st >>= 1) {
+    for (int t = lane; t < st; t += 32) red[t] = MAX ? nmax(red[t], red[t + st]) : nmin(red[t], red[t + st]);
+    __syncwarp();
+  }
+  const double r = red[0];
+  __syncwarp();
+  return r;
+}
+
+// finalize_body<1024> by one warp: the same reductions in the same order, then the controller
+__device__ __forceinline__ void finalize_warp(const FinalizeParams& F, double* red) {
+  constexpr int NT = 1024;
+  Ctl* ctl = F.ctl;
+  const double mx = warp_fixed_ext<NT, true>(F.part, F.nblk, red);
+  const double mn = warp_fixed_ext<NT, false>(F.part + F.nblk, F.nblk, red);
+  const double vol = warp_fixed_sum<NT>(F.part + 2 * F.nblk, F.nblk, red);
+  double rain = 0.0, outf = 0.0, wall = 0.0;
+  if (F.tally) {
+    for (int s = 0; s < F.nstages; ++s) {
+      double rs = warp_fixed_sum<NT>(F.part + (3 + 3LL * s) * F.nblk, F.nblk, red);
+      double os = warp_fixed_sum<NT>(F.part + (4 + 3LL * s) * F.nblk, F.nblk, red);
+      double ws = warp_fixed_sum<NT>(F.part + (5 + 3LL * s) * F.nblk, F.nblk, red);
+      double w = F.is_float ? double(float(F.b[s] * ctl->dt)) : F.b[s] * ctl->dt;
+      rain += w * rs * F.cell_area;
+      outf += w * os * F.cell_area;
+      wall += w * ws * F.cell_area;
+    }
+  }
+  if ((threadIdx.x & 31) == 0) finalize_control(F, mx, mn, vol, rain, outf, wall);
+  __syncwarp();
+}
+
+template <typename T, bool P2, bool EDDY>
+__global__ void __launch_bounds__(32 * kPersistWarps, 4) persist_batch_kernel(const PersistParams<T> PP) {
+  __shared__ __align__(16) StageParams<T> Psh[kPersistWarps];
+  __shared__ double red[kPersistWarps][1024];
+  const int lane = threadIdx.x, wib = threadIdx.y;
+  const int N = PP.nstages, nact = PP.nact;
+  const long long gwarp = (long long)blockIdx.x * kPersistWarps + wib;
+  const int k0 = nact > 0 ? int(gwarp % nact) : 0;
+  volatile int* status = PP.status;
+  unsigned long long idle = 0;
+  while (true) {
+    if (*status != 0) return;  // whole warp: another warp gave up
+    bool worked = false, active = false;
+    for (int j = 0; j < nact && !worked; ++j) {
+      const int k = (k0 + j) % nact;
+      PersistMember* m = PP.mem + k;
+      if (*(volatile int*)&m->finished) continue;
+      active = true;
+      const unsigned long long p = *(volatile unsigned long long*)&m->phase;
+      const int s = int(p % (N + 1));
+      const long long ns = m->nstrips;
+      const unsigned long long base = (p / (N + 1)) * (unsigned long long)(N * ns + 1) + (unsigned long long)s * ns;
+      const unsigned long long nwork = s < N ? (unsigned long long)ns : 1ull;
+      // claim one item of phase p (a claim can only succeed while phase p is open)
+      unsigned long long t = 0;
+      int ok = 0;
+      if (lane == 0) {
+        unsigned long long cur = *(volatile unsigned long long*)&m->ticket;
+        while (cur >= base && cur < base + nwork) {
+          const unsigned long long prev = atomicCAS(&m->ticket, cur, cur + 1);
+          if (prev == cur) { ok = 1; t = cur; break; }
+          cur = prev;
+        }
+      }
+      ok = __shfl_sync(kFull, ok, 0);
+      if (!ok) continue;
+      t = __shfl_sync(kFull, t, 0);
+      __threadfence();  // acquire: the previous phases' writes of every warp
+      if (s < N) {
+        // stage s, strip t - base: the member's parameters to shared memory, then the sweep
+        static_assert(sizeof(StageParams<T>) % 4 == 0, "parameter block copied as 32-bit words");
+        const unsigned* src = reinterpret_cast<const unsigned*>(PP.Ps + size_t(s) * nact + k);
+        unsigned* dst = reinterpret_cast<unsigned*>(&Psh[wib]);
+        for (int i = lane; i < int(sizeof(StageParams<T>) / 4); i += 32) dst[i] = src[i];
+        __syncwarp();
+        sweep_strip<T, kPersistRows, P2, EDDY, true>(Psh[wib], (long long)(t - base));
+        __syncwarp();
+      } else {
+        finalize_warp(PP.Fs[k], red[wib]);
+      }
+      __threadfence();  // release this item's writes before counting it
+      int last = 0;
+      if (lane == 0) last = atomicAdd(&m->done, 1u) + 1u == (unsigned)nwork;
+      last = __shfl_sync(kFull, last, 0);
+      if (last) {
+        __threadfence();  // acquire the other items of the phase
+        if (lane == 0) {
+          m->done = 0;
+          // after a finalize the member goes on while its controller has a step running
+          const bool more = s < N || (*(volatile int*)&PP.Fs[k].ctl->done == 0);
+          __threadfence();
+          if (more) atomicExch(&m->phase, p + 1);
+          else atomicExch(&m->finished, 1);
+        }
+        __syncwarp();
+      }
+      worked = true;
+    }
+    if (!active) return;  // every member has finished
+    if (worked) {
+      idle = 0;
+    } else if (++idle > PP.spin_limit) {
+      if (lane == 0) atomicExch((int*)PP.status, -6);
+      return;
+    } else {
+      __nanosleep(256);
+    }
+  }
 }
 
 #ifdef SV_DEFINE_COMMON_KERNELS

@@ -17,19 +17,30 @@ constexpr int kNumTiles = 4;
 template <typename T> size_t stage_smem_bytes(int tile);
 template <typename T> cudaError_t launch_stage(const StageParams<T>& P, int tile, cudaStream_t s);
 
-// Stage-kernel variants: 0..3 the tiled shared-memory kernel with kTiles[v]; 4..10 the
-// column-sweep kernel with 16 / 32 / 64 / 32 / 32 / 32 / 32 output rows per warp, the last
-// four with register caps for 3, 4, 5 and 6 resident 4-warp blocks per SM.
-constexpr int kNumVariants = 11;
+// Stage-kernel variants, in two schedules:
+//  fused (one pass per RK stage): 0..3 the tiled shared-memory kernel with kTiles[v]; 4..10
+//   the column-sweep kernel with 16 / 32 / 64 / 32 / 32 / 32 / 32 output rows per warp, the
+//   last four with register caps for 3, 4, 5 and 6 resident 4-warp blocks per SM;
+//  split (two passes per RK stage): 11 the slopes pass (slopes_kernel) then the tiled 32 x 8
+//   kernel at 3 CTAs/SM reading those slopes.
+constexpr int kNumVariants = 12;
+constexpr int kSplitVariant = 11;
 constexpr int kSweepRows[7] = {16, 32, 64, 32, 32, 32, 32};
-inline bool variant_is_sweep(int v) { return v >= 4; }
+inline bool variant_is_sweep(int v) { return v >= 4 && v <= 10; }
+inline bool variant_is_split(int v) { return v == kSplitVariant; }
 // per-CTA (tiled) or per-warp (sweep) partial count
 inline long long variant_partials(int v, long long nx, long long ny) {
+  if (v == kSplitVariant) v = 1;  // the split schedule's stage pass is the tiled 32 x 8 kernel
   if (v < 4) return ((nx + kTiles[v].tx - 1) / kTiles[v].tx) * ((ny + kTiles[v].ty - 1) / kTiles[v].ty);
   const long long ty = kSweepRows[v - 4];
   return ((nx + kSweepOut - 1) / kSweepOut) * ((ny + ty - 1) / ty);
 }
 template <typename T> cudaError_t launch_variant(const StageParams<T>& P, int variant, cudaStream_t s);
+// column-sweep variants: output rows per strip (0 for the other variants)
+inline int variant_sweep_rows(int v) { return variant_is_sweep(v) ? kSweepRows[v - 4] : 0; }
+// per-strip interior flags of the column sweep with `ty` output rows (strip_flags_kernel)
+template <typename T> cudaError_t launch_strip_flags(const T* z, int nx, int ny, int ty, long long nstrips,
+                                                     unsigned char* flags, cudaStream_t s);
 template <typename T> cudaError_t launch_bed_slopes(const T* z, int nx, int ny, double dx, double dy, T* zx, T* zy,
                                                     cudaStream_t s);
 // FP64 <-> T conversion of a field on the device
@@ -56,6 +67,10 @@ template <typename T> cudaError_t launch_stage_batch(const StageParams<T>* Ps, c
 template <typename T> constexpr int batch_variant() { return sizeof(T) == 8 ? 1 : 8; }
 template <typename T> cudaError_t launch_sweep_batch(const StageParams<T>* Ps, const long long* warp_start, int ninst,
                                                      long long total_warps, bool p2, bool eddy, cudaStream_t s);
+// persistent batch kernel (persist_batch_kernel), cooperative launch filling the device
+template <typename T> cudaError_t launch_persist(const PersistParams<T>& PP, bool p2, bool eddy, cudaStream_t s);
+cudaError_t launch_persist_init(const FinalizeParams* Fs, PersistMember* mem, const long long* warp_start, int nact,
+                                cudaStream_t s);
 cudaError_t launch_finalize(const FinalizeParams& F, cudaStream_t s);
 cudaError_t launch_finalize_batch(const FinalizeParams* Fs, int ninst, cudaStream_t s);
 cudaError_t launch_begin_queue(const FinalizeParams* Fs, int n, cudaStream_t s);

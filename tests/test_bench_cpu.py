@@ -12,7 +12,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def test_reference_arm_line():
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
-                        "--warmup", "3"], capture_output=True, text=True, timeout=600, cwd=ROOT)
+                        "--warmup", "3", "--size", "1024", "--window-steps", "1"], capture_output=True, text=True,
+                       timeout=600, cwd=ROOT)
     assert r.returncode == 0, r.stderr[-2000:]
     line = json.loads(r.stdout.strip().splitlines()[-1])
     for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
@@ -22,6 +23,9 @@ def test_reference_arm_line():
     assert line["cpu_baseline"]["value"] == line["value"] and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
+    # the reference arm times the window state the GPU arm's CPU baseline uses
+    assert line["config"]["same_state_as"] == "the b200 arm's cpu_baseline"
+    assert "from its FP64 state after 60 s from dry" in line["cpu_baseline"]["sample"]
 
 
 @pytest.mark.parametrize("name", ["sweep_kernel_f32_datum64", "sweep_batch_kernel_f32_datum64", "stage_kernel_f64"])

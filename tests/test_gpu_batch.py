@@ -213,3 +213,85 @@ def test_queued_steps_isolate_a_failing_member():
     solo, _ = _run_alone(SaintVenantSolver, CASES[0], 3, L)
     assert same(mem[0].get_field("H"), solo[0])
     batch.close()
+
+
+def _persistent_batch(precision, cases, L, spin_limit=0):
+    batch = SaintVenantBatch(precision)
+    batch.set_persistent(True, spin_limit)
+    mem = []
+    for c in cases:
+        m = batch.add(c[0], c[1], c[2], cn_target=0.5, step_duration=L, rain_mode="physical")
+        _init(m, c[0], c[1], c[2], c[5])
+        mem.append(m)
+    return batch, mem
+
+
+def test_persistent_batch_matches_solo_runs():
+    """One cooperative launch per advance: every member advances through its queued steps at
+    its own dt, and FP64 members keep the bits of their solo runs."""
+    L, steps = 20.0, 3
+    batch, mem = _persistent_batch("f64", CASES, L)
+    res = batch.advance_steps({m: [_forcing(i * L, L, c[3], c[4]) for i in range(steps)] for m, c in zip(mem, CASES)})
+    for m, c in zip(mem, CASES):
+        assert res[m.slot]["status"] == 0 and len(res[m.slot]["steps"]) == steps
+        solo, so = _run_alone(SaintVenantSolver, c, steps, L)
+        for k, f in enumerate(("H", "U", "V")):
+            assert same(m.get_field(f), solo[k]), f"{c}: {f} differs from the solo run"
+        st = res[m.slot]["steps"][-1]
+        assert abs(st["volume"] - so["volume"]) <= 1e-12 * so["volume"]
+        assert (m.stats()["accepted"], m.stats()["repeated"]) == (so["accepted"], so["repeated"])
+    # the next advance carries on from there, one step at a time
+    for m, c in zip(mem, CASES):
+        m.set_forcing(_forcing(steps * L, L, c[3], c[4]))
+    batch.advance()
+    for m, c in zip(mem, CASES):
+        solo, _ = _run_alone(SaintVenantSolver, c, steps + 1, L)
+        assert same(m.get_field("H"), solo[0])
+    batch.close()
+
+
+def test_persistent_fp32_batch_close_to_fp64():
+    L, steps = 20.0, 2
+    batch, mem = _persistent_batch("f32_datum64", CASES, L)
+    batch.advance_steps({m: [_forcing(i * L, L, c[3], c[4]) for i in range(steps)] for m, c in zip(mem, CASES)})
+    for m, c in zip(mem, CASES):
+        ref, so = _run_alone(OracleSolver, c, steps, L)
+        assert np.max(np.abs(m.get_field("H") - ref[0])) <= 1e-3
+        assert abs(m.stats()["volume"] - so["volume"]) <= 1e-6 * so["volume"]
+    batch.close()
+
+
+def test_persistent_batch_isolates_a_failing_member():
+    L = 20.0
+    batch, mem = _persistent_batch("f64", CASES, L)
+    mem[1].set_dt(float("nan"))
+    res = batch.advance_steps({m: [_forcing(i * L, L, c[3], c[4]) for i in range(2)] for m, c in zip(mem, CASES)},
+                              raise_on_error=False)
+    assert [res[m.slot]["status"] for m in mem] == [0, SV_E_NONFINITE, 0]
+    solo, _ = _run_alone(SaintVenantSolver, CASES[2], 2, L)
+    assert same(mem[2].get_field("H"), solo[0])
+    batch.close()
+
+
+def test_persistent_wait_bound_gives_up_with_a_status():
+    """A waiting warp polls at most spin_limit times; with a limit of one poll the launch gives
+    up (some warp always waits for a phase to complete) and the call returns SV_E_TIMEOUT. The
+    device stays usable, and each member keeps the state of its last completed timestep."""
+    from mfcm_b200._abi import SV_E_TIMEOUT
+    L = 20.0
+    batch, mem = _persistent_batch("f64", CASES, L, spin_limit=1)
+    for m, c in zip(mem, CASES):
+        m.set_forcing(_forcing(0.0, L, c[3], c[4]))
+    with pytest.raises(SvError) as e:
+        batch.advance()
+    assert e.value.code == SV_E_TIMEOUT
+    for m in mem:  # the state is still finite
+        assert np.isfinite(m.get_field("H")).all()
+    batch.close()
+    # the device keeps working: a fresh persistent batch with the default bound completes
+    batch, mem = _persistent_batch("f64", CASES[:1], L)
+    mem[0].set_forcing(_forcing(0.0, L, CASES[0][3], CASES[0][4]))
+    batch.advance()
+    solo, _ = _run_alone(SaintVenantSolver, CASES[0], 1, L)
+    assert same(mem[0].get_field("H"), solo[0])
+    batch.close()

@@ -1,0 +1,76 @@
+"""FP64 parity of the CUDA path with the oracle on the benchmark configurations themselves.
+
+The other parity tests use small grids. These run the plain FP64 GPU path on the full-size
+inputs of the catchment configurations (tests/config_scenarios.py): the 256 x 256 catchment for
+an hour in three rain modes, a 1024 x 1024 window of the 4096 x 4096 fractal catchment for its
+first minute, and the 8192 x 1024 dam break for 2 s. The oracle's runs of the same scenarios
+are committed as one record per output time (tests/golden/configs.json, made by
+tests/golden/make_config_golden.py): timestep counts, the FP64 volume, the maximum depth and a
+digest of the h, u, v fields.
+
+The bar is the one stated for FP64: max |dh| <= 1e-9 m and relative volume difference <= 1e-12
+at every output. The arithmetic is in fact identical, so the test asks for the same digest at
+every output (bit for bit); when a digest differs it runs the oracle live to report the largest
+depth difference.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from mfcm_b200 import SaintVenantSolver
+from tests.config_scenarios import SCENARIOS, run
+
+pytestmark = pytest.mark.gpu
+
+DEPTH_TOL = 1e-9     # m
+VOLUME_TOL = 1e-12   # relative
+GOLD_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "configs.json")
+GOLD = json.load(open(GOLD_PATH)) if os.path.exists(GOLD_PATH) else {}
+
+
+def _live_depth_difference(name):
+    """Largest |dh| at the end of the run, GPU against the oracle run now (failure diagnostics)."""
+    from oracle.sv_oracle_py import OracleSolver
+    finals = {}
+    for key, make in (("gpu", SaintVenantSolver), ("oracle", lambda *a, **k: OracleSolver(*a, openmp=True, **k))):
+        def keep(*a, _make=make, _key=key, **k):
+            b = _make(*a, **k)
+            close = b.close
+
+            def close_and_keep():
+                finals[_key] = b.get_field("H")
+                close()
+            b.close = close_and_keep
+            return b
+        run(name, keep)
+    return float(np.nanmax(np.abs(finals["gpu"] - finals["oracle"])))
+
+
+@pytest.mark.parametrize("name", list(SCENARIOS))
+def test_config_scale_run_matches_oracle(name):
+    if name not in GOLD:
+        pytest.fail(f"no committed oracle record for {name} in tests/golden/configs.json")
+    ref = GOLD[name]
+    got = run(name, SaintVenantSolver)
+    assert len(got["outputs"]) == len(ref["outputs"])
+    worst_v = 0.0
+    for g, o in zip(got["outputs"], ref["outputs"]):
+        assert g["t"] == o["t"]
+        assert (g["accepted"], g["repeated"]) == (o["accepted"], o["repeated"]), (name, g["t"], g, o)
+        dv = abs(g["volume"] - o["volume"]) / max(abs(o["volume"]), 1e-300)
+        worst_v = max(worst_v, dv)
+        assert dv <= VOLUME_TOL, (name, g["t"], g["volume"], o["volume"])
+        if g["digest"] != o["digest"]:
+            dh = _live_depth_difference(name)
+            assert dh <= DEPTH_TOL, f"{name} t={g['t']}: fields differ, final max |dh| = {dh}"
+            pytest.fail(f"{name} t={g['t']}: fields differ below the depth tolerance (final max |dh| = {dh})")
+    assert got["dt"] == ref["dt"]
+    last = got["outputs"][-1]
+    print(f"\n{name}: {len(got['outputs'])} outputs bit for bit, {last['accepted']} accepted timesteps, "
+          f"max |dh| = 0, max relative volume difference = {worst_v:.3g}")
+    if name == "plane256_reference_dry":
+        assert last["volume"] == 0.0 and last["max_h"] == 0.0, "dry cells take no rain under the reference clamp"
+    else:
+        assert last["volume"] > 0.0 and last["accepted"] > 10
