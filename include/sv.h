@@ -309,12 +309,13 @@ int sv_batch_status(sv_batch* batch, int* status, int n);
  * ONE cooperative launch that fills the device. Every member advances through its queued
  * steps at its own dt; a member's timestep is its stage phases (column-sweep strips, 32 rows)
  * and a finalize phase (reductions, dt controller, step queue), and idle warps take work from
- * whichever member has some. on = 0 returns to one launch per stage. spin_limit bounds how many
- * times a warp that finds no work polls before the launch gives up with SV_E_TIMEOUT (0: the
- * default, 2^22 polls, about a second); after a timeout every member keeps the state of its
- * last completed timestep. FP64 results are bit for bit those of the other modes; FP32
- * results are reproducible for this mode. */
-int sv_batch_set_persistent(sv_batch* batch, int on, uint64_t spin_limit);
+ * whichever member has some. on = 0 returns to one launch per stage. Two bounds end a launch
+ * with SV_E_TIMEOUT: spin_limit polls of a waiting warp during which no warp completes a work
+ * item (0: the default, 2^22 polls, about a second), and max_seconds of wall clock for the
+ * whole launch (<= 0: the default, 120 s; queue fewer steps per call for longer runs). After a
+ * timeout every member keeps the state of its last completed timestep. FP64 results are bit
+ * for bit those of the other modes; FP32 results are reproducible for this mode. */
+int sv_batch_set_persistent(sv_batch* batch, int on, uint64_t spin_limit, double max_seconds);
 /* the stage-kernel variant every member of the batch runs (FP32 results are reproducible
  * per variant: a solo run with this variant gives a member's bits) */
 int sv_batch_kernel_variant(sv_batch* batch, int* variant);

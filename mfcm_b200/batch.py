@@ -36,7 +36,7 @@ def _declare(lib):
     lib.sv_batch_status.restype = C.c_int
     lib.sv_batch_status.argtypes = [C.c_void_p, P(C.c_int), C.c_int]
     lib.sv_batch_set_persistent.restype = C.c_int
-    lib.sv_batch_set_persistent.argtypes = [C.c_void_p, C.c_int, C.c_uint64]
+    lib.sv_batch_set_persistent.argtypes = [C.c_void_p, C.c_int, C.c_uint64, C.c_double]
     lib.sv_batch_size.restype = C.c_int
     lib.sv_batch_size.argtypes = [C.c_void_p, P(C.c_int), P(C.c_uint64)]
     lib._batch_declared = True
@@ -106,11 +106,12 @@ class SaintVenantBatch:
         if r != 0:
             raise SvError(r, self._lib.sv_last_error(None).decode())
 
-    def set_persistent(self, on=True, spin_limit=0):
+    def set_persistent(self, on=True, spin_limit=0, max_seconds=0.0):
         """Run each advance as one persistent cooperative launch (every member at its own dt;
-        idle warps take work from any member). spin_limit bounds a waiting warp's polls before
-        the launch gives up with SV_E_TIMEOUT (0: the library's default)."""
-        r = self._lib.sv_batch_set_persistent(self._b, 1 if on else 0, int(spin_limit))
+        idle warps take work from any member). The launch gives up with SV_E_TIMEOUT after
+        spin_limit polls of a waiting warp with no work item completed anywhere, or after
+        max_seconds of wall clock (0: the library's defaults)."""
+        r = self._lib.sv_batch_set_persistent(self._b, 1 if on else 0, int(spin_limit), float(max_seconds))
         if r != 0:
             raise SvError(r, self._lib.sv_last_error(None).decode())
 

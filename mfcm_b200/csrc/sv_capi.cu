@@ -1108,7 +1108,7 @@ struct sv_batch_base {
   virtual int status(int*, int) = 0;
   virtual int advance_steps(int, const int*, const sv_forcing*, sv_stats*, int) = 0;
   virtual int kernel_variant() const = 0;
-  virtual int set_persistent(int, unsigned long long) = 0;
+  virtual int set_persistent(int, unsigned long long, double) = 0;
 };
 
 template <typename T>
@@ -1134,9 +1134,11 @@ struct Batch final : public sv_batch_base {
   std::vector<int> last_status;             // slot id -> outcome of the last advance
   // persistent mode: one cooperative launch per advance (svk::persist_batch_kernel)
   bool persistent = false;
-  unsigned long long spin_limit = 1ull << 22;  // idle polls of a waiting warp before SV_E_TIMEOUT
+  unsigned long long spin_limit = 1ull << 22;  // polls without global progress before SV_E_TIMEOUT
+  double max_seconds = 120.0;                  // wall-clock bound of one persistent launch
   svk::PersistMember* d_pmem = nullptr;        // [nact]
-  int* d_pstatus = nullptr;
+  int* d_pstatus = nullptr;                    // [0] status, then (8-byte aligned) the progress count
+  unsigned long long* d_pprogress = nullptr;
   // the members' kernel variant: the column sweep of 32 rows (variant 8) in persistent mode,
   // whose strips are the persistent kernel's work items; else the batches' variant
   int member_variant() const { return persistent ? 8 : svk::batch_variant<T>(); }
@@ -1150,9 +1152,9 @@ struct Batch final : public sv_batch_base {
   }
   void free_arrays() {
     cudaFree(d_params); cudaFree(d_fin); cudaFree(d_tiles); cudaFree(d_ctls); cudaFree(d_done); cudaFree(d_queue);
-    cudaFree(d_pmem); cudaFree(d_pstatus);
+    cudaFree(d_pmem); cudaFree(d_pstatus); cudaFree(d_pprogress);
     d_params = nullptr; d_fin = nullptr; d_tiles = nullptr; d_ctls = nullptr; d_done = nullptr; d_queue = nullptr;
-    d_pmem = nullptr; d_pstatus = nullptr;
+    d_pmem = nullptr; d_pstatus = nullptr; d_pprogress = nullptr;
     cap = 0;
   }
   int cuda_fail(cudaError_t e, const char* where) {
@@ -1228,6 +1230,7 @@ struct Batch final : public sv_batch_base {
       SV_CUDA(cudaMalloc(&d_queue, sizeof(svk::StepQueue) * c));
       SV_CUDA(cudaMalloc(&d_pmem, sizeof(svk::PersistMember) * c));
       SV_CUDA(cudaMalloc(&d_pstatus, sizeof(int)));
+      SV_CUDA(cudaMalloc(&d_pprogress, sizeof(unsigned long long)));
       cap = c;
     }
     std::vector<svk::StageParams<T>> hp(size_t(N) * std::max(nact, 1));
@@ -1330,6 +1333,7 @@ struct Batch final : public sv_batch_base {
       // every member's queued steps in one cooperative launch
       e = svk::launch_persist_init(d_fin, d_pmem, d_tiles, nact, stream);
       if (e == cudaSuccess) e = cudaMemsetAsync(d_pstatus, 0, sizeof(int), stream);
+      if (e == cudaSuccess) e = cudaMemsetAsync(d_pprogress, 0, sizeof(unsigned long long), stream);
       svk::PersistParams<T> PP{};
       PP.Ps = d_params;
       PP.Fs = d_fin;
@@ -1337,7 +1341,9 @@ struct Batch final : public sv_batch_base {
       PP.nact = nact;
       PP.nstages = N;
       PP.status = d_pstatus;
+      PP.progress = d_pprogress;
       PP.spin_limit = spin_limit;
+      PP.max_ns = (unsigned long long)(max_seconds * 1e9);
       if (e == cudaSuccess) e = svk::launch_persist<T>(PP, p2, eddy, stream);
       if (e != cudaSuccess) return cuda_fail(e, "persistent batch kernel");
       int st = 0;
@@ -1352,8 +1358,9 @@ struct Batch final : public sv_batch_base {
           if (r) return fail(r, members[active[k]]->err);
         }
         last_status.assign(members.size(), SV_E_TIMEOUT);
-        return fail(SV_E_TIMEOUT, "persistent batch kernel: a warp waited " + std::to_string(spin_limit) +
-                                      " polls for work and gave up");
+        return fail(SV_E_TIMEOUT, "persistent batch kernel gave up: no work item completed during " +
+                                      std::to_string(spin_limit) + " polls, or the launch ran past " +
+                                      std::to_string(max_seconds) + " s");
       }
     }
     for (long long it = 0; !persistent; ++it) {
@@ -1454,9 +1461,10 @@ struct Batch final : public sv_batch_base {
 
   int kernel_variant() const override { return member_variant(); }
 
-  int set_persistent(int on, unsigned long long limit) override {
+  int set_persistent(int on, unsigned long long limit, double seconds) override {
     persistent = on != 0;
     spin_limit = limit ? limit : (1ull << 22);
+    max_seconds = seconds > 0.0 ? seconds : 120.0;
     dirty = true;
     return SV_OK;
   }
@@ -1596,9 +1604,9 @@ int sv_batch_advance_steps(sv_batch* b, int max_steps, const int* nsteps, const 
   if (r) g_create_err = b->impl->err;
   return r;
 }
-int sv_batch_set_persistent(sv_batch* b, int on, uint64_t spin_limit) {
+int sv_batch_set_persistent(sv_batch* b, int on, uint64_t spin_limit, double max_seconds) {
   if (!b) return SV_E_ARG;
-  return b->impl->set_persistent(on, spin_limit);
+  return b->impl->set_persistent(on, spin_limit, max_seconds);
 }
 int sv_batch_kernel_variant(sv_batch* b, int* variant) {
   if (!b || !variant) return SV_E_ARG;

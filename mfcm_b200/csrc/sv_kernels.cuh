@@ -1490,9 +1490,10 @@ template <int NT> __global__ void __launch_bounds__(NT) finalize_batch_kernel(co
 // Warps claim work items from any member whose current phase has unclaimed items; the warp
 // that completes the last item of a phase opens the member's next phase. Phases are ordered by
 // release fences before each completion count and acquire fences after each claim, and the
-// state buffers are read with coherent loads (ldst<true>). A warp that finds no work waits
-// with a bounded number of polls; when the bound runs out it records SV_E_TIMEOUT in the
-// launch status and every warp returns at its next poll.
+// state buffers are read with coherent loads (ldst<true>). Every wait is bounded twice: a warp
+// that finds no work gives up after spin_limit polls during which no warp completed an item
+// (a global progress count), and every warp gives up once the launch has run max_ns; either
+// records SV_E_TIMEOUT in the launch status, and every warp returns at its next poll.
 // ---------------------------------------------------------------------------------------
 struct PersistMember {
   unsigned long long phase;   // phases opened so far: stage = phase % (N + 1), N = the finalize
@@ -1508,8 +1509,16 @@ template <typename T> struct PersistParams {
   PersistMember* mem;         // [nact]
   int nact, nstages;
   int* status;                // 0, or SV_E_TIMEOUT (-6) once a wait gave up
-  unsigned long long spin_limit;  // polls without work before giving up
+  unsigned long long* progress;   // items completed by all warps (zeroed before the launch)
+  unsigned long long spin_limit;  // polls without any completed item before giving up
+  unsigned long long max_ns;      // wall-clock bound of the launch, ns
 };
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 constexpr int kPersistWarps = 4;   // warps per block
 constexpr int kPersistRows = 32;   // column-sweep strip height (the batches' variant 8)
@@ -1594,9 +1603,15 @@ __global__ void __launch_bounds__(32 * kPersistWarps, 4) persist_batch_kernel(co
   const long long gwarp = (long long)blockIdx.x * kPersistWarps + wib;
   const int k0 = nact > 0 ? int(gwarp % nact) : 0;
   volatile int* status = PP.status;
-  unsigned long long idle = 0;
+  volatile unsigned long long* progress = PP.progress;
+  const unsigned long long t_start = global_ns();
+  unsigned long long idle = 0, seen = *progress;
   while (true) {
     if (*status != 0) return;  // whole warp: another warp gave up
+    if (global_ns() - t_start > PP.max_ns) {
+      if (lane == 0) atomicExch((int*)PP.status, -6);
+      return;
+    }
     bool worked = false, active = false;
     for (int j = 0; j < nact && !worked; ++j) {
       const int k = (k0 + j) % nact;
@@ -1637,7 +1652,10 @@ __global__ void __launch_bounds__(32 * kPersistWarps, 4) persist_batch_kernel(co
       }
       __threadfence();  // release this item's writes before counting it
       int last = 0;
-      if (lane == 0) last = atomicAdd(&m->done, 1u) + 1u == (unsigned)nwork;
+      if (lane == 0) {
+        last = atomicAdd(&m->done, 1u) + 1u == (unsigned)nwork;
+        atomicAdd(PP.progress, 1ull);
+      }
       last = __shfl_sync(kFull, last, 0);
       if (last) {
         __threadfence();  // acquire the other items of the phase
@@ -1654,8 +1672,10 @@ __global__ void __launch_bounds__(32 * kPersistWarps, 4) persist_batch_kernel(co
       worked = true;
     }
     if (!active) return;  // every member has finished
-    if (worked) {
+    const unsigned long long now = *progress;
+    if (worked || now != seen) {  // this warp or another completed an item
       idle = 0;
+      seen = now;
     } else if (++idle > PP.spin_limit) {
       if (lane == 0) atomicExch((int*)PP.status, -6);
       return;

@@ -215,9 +215,9 @@ def test_queued_steps_isolate_a_failing_member():
     batch.close()
 
 
-def _persistent_batch(precision, cases, L, spin_limit=0):
+def _persistent_batch(precision, cases, L, spin_limit=0, max_seconds=0.0):
     batch = SaintVenantBatch(precision)
-    batch.set_persistent(True, spin_limit)
+    batch.set_persistent(True, spin_limit, max_seconds)
     mem = []
     for c in cases:
         m = batch.add(c[0], c[1], c[2], cn_target=0.5, step_duration=L, rain_mode="physical")
@@ -273,14 +273,18 @@ def test_persistent_batch_isolates_a_failing_member():
     batch.close()
 
 
-def test_persistent_wait_bound_gives_up_with_a_status():
-    """A waiting warp polls at most spin_limit times; with a limit of one poll the launch gives
-    up (some warp always waits for a phase to complete) and the call returns SV_E_TIMEOUT. The
-    device stays usable, and each member keeps the state of its last completed timestep."""
+@pytest.mark.parametrize("bound", ["polls", "wall_clock"])
+def test_persistent_wait_bound_gives_up_with_a_status(bound):
+    """Every wait of the persistent kernel is bounded. With a bound of one poll without progress,
+    or of one microsecond of wall clock, the launch gives up and the call returns SV_E_TIMEOUT.
+    The device stays usable, and each member keeps the state of its last completed timestep."""
     from mfcm_b200._abi import SV_E_TIMEOUT
     L = 20.0
-    batch, mem = _persistent_batch("f64", CASES, L, spin_limit=1)
-    for m, c in zip(mem, CASES):
+    # one member: while its single warp runs a finalize no other item completes anywhere
+    cases = CASES[:1] if bound == "polls" else CASES
+    kw = dict(spin_limit=1) if bound == "polls" else dict(max_seconds=1e-6)
+    batch, mem = _persistent_batch("f64", cases, L, **kw)
+    for m, c in zip(mem, cases):
         m.set_forcing(_forcing(0.0, L, c[3], c[4]))
     with pytest.raises(SvError) as e:
         batch.advance()
