@@ -68,29 +68,60 @@ def catchment_bed(nx, ny, dx, slope, relief_frac, seed, hurst=0.8, smooth_m=10.0
     return z + synth.regional_slope(nx, ny, dx, slope)
 
 
+def fractal_bed(nx, ny, relief_m, seed, hurst=0.8):
+    """A seeded diamond-square bed of `relief_m` metres (max - min) and Hurst exponent `hurst`,
+    unsmoothed."""
+    return synth.diamond_square(nx, ny, hurst, relief_m, seed=seed)
+
+
 def make_requests(rate, count, seed=0, side=(64, 512), dxs=(1.0, 2.0, 5.0), horizon=(120.0, 600.0),
                   slope=(0.005, 0.03), relief=(0.01, 0.03), peak=(20.0, 120.0), duration=(900.0, 7200.0),
-                  hurst=0.8):
-    """Poisson arrivals at `rate` requests/s; mesh side log-uniform on `side`; beds from
-    `catchment_bed` with regional slope U(`slope`) and relief U(`relief`) x length."""
+                  hurst=0.8, relief_m=None, multiple=1):
+    """Poisson arrivals at `rate` requests/s; mesh side log-uniform on `side` (rounded to a
+    multiple of `multiple`); beds from `catchment_bed` with regional slope U(`slope`) and relief
+    U(`relief`) x length, or, with `relief_m` = (lo, hi), raw fractal beds (`fractal_bed`) of
+    relief U(relief_m) metres."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
     for i in range(count):
         t += rng.exponential(1.0 / rate)
-        s = int(round(math.exp(rng.uniform(math.log(side[0]), math.log(side[1])))))
+        s = int(round(math.exp(rng.uniform(math.log(side[0]), math.log(side[1]))) / multiple)) * multiple
+        s = max(s, multiple)
         dx = float(rng.choice(dxs))
-        z = catchment_bed(s, s, dx, float(rng.uniform(*slope)), float(rng.uniform(*relief)), seed * 100003 + i, hurst)
+        if relief_m is None:
+            z = catchment_bed(s, s, dx, float(rng.uniform(*slope)), float(rng.uniform(*relief)), seed * 100003 + i,
+                              hurst)
+        else:
+            z = fractal_bed(s, s, float(rng.uniform(*relief_m)), seed * 100003 + i, hurst)
         rain = triangular_hyetograph(float(rng.uniform(*peak)), float(rng.uniform(*duration)))
         out.append(Request(i, t, s, s, dx, z, rain, float(rng.uniform(*horizon))))
     return out
 
 
+def at_rate(requests, rate, seed=0):
+    """The same requests (same catchments, rain and horizons) arriving as a Poisson stream of
+    `rate` requests/s: fresh copies whose arrival times are redrawn, timings cleared."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for r in requests:
+        t += rng.exponential(1.0 / rate)
+        out.append(Request(r.rid, t, r.nx, r.ny, r.dx, r.z, r.rain, r.horizon, r.n, r.head_edges))
+    return out
+
+
 class FloodServer:
+    """persistent: each batch advance is one persistent cooperative launch (every running
+    request at its own dt, idle warps taking work from any request); else one launch per RK
+    stage and one per timestep's reductions, replayed as a graph."""
+
     def __init__(self, budget_bytes=150e9, max_slots=512, precision="f32", step_duration=60.0, cn_target=0.5,
-                 device=0, step_limit=20000, steps_per_advance=4):
+                 device=0, step_limit=20000, steps_per_advance=4, persistent=False):
         self.batch = SaintVenantBatch(precision, "classic", device)
         self.batch.set_step_limit(step_limit)
+        if persistent:
+            self.batch.set_persistent(True)
         # steps each running request advances per batched launch sequence: members run them
         # back to back at their own pace; new arrivals are admitted between sequences
         self.steps_per_advance = int(steps_per_advance)
@@ -180,6 +211,10 @@ class FloodServer:
                 used -= self.estimate_bytes(req)
         wall = time.perf_counter() - t0
         lat = np.array([r.latency for r in requests if not math.isnan(r.finished) and r.error is None])
+        failures = {}
+        for r in requests:
+            if r.error is not None:
+                failures[r.error] = failures.get(r.error, 0) + 1
         return {
             "requests": len(requests), "completed": int(lat.size),
             "failed": sum(1 for r in requests if r.error is not None), "wall_s": wall,
@@ -187,7 +222,7 @@ class FloodServer:
             "p95_s": float(np.percentile(lat, 95)) if lat.size else None,
             "p99_s": float(np.percentile(lat, 99)) if lat.size else None,
             "cell_updates_per_s": total_updates / wall if wall > 0 else 0.0,
-            "max_concurrent": max_active,
+            "max_concurrent": max_active, "failures": failures,
         }
 
     def close(self):

@@ -56,3 +56,16 @@ def test_memory_budget_queues_requests():
     assert summary["max_concurrent"] <= 2
     # later arrivals had to wait for memory: admission after arrival
     assert any(r.admitted - r.arrival > 1e-3 for r in reqs[2:])
+
+
+def test_persistent_serving_matches_solo_runs():
+    """The server on the persistent batch kernel: requests still overlap, and FP64 results are
+    the bits of each request solved alone."""
+    reqs = make_requests(rate=50.0, count=8, seed=9, side=(32, 80), horizon=(120.0, 240.0))
+    server = FloodServer(budget_bytes=2e9, precision="f64", persistent=True, steps_per_advance=1)
+    summary = server.run(reqs, time_limit=300)
+    server.close()
+    assert summary["completed"] == len(reqs)
+    assert summary["max_concurrent"] >= 2
+    for r in reqs[:4]:
+        assert same(r.result_h, _alone(r, 1, precision="f64")), f"request {r.rid} differs from its solo run"
