@@ -7,7 +7,8 @@ digests) and tests/test_gpu_parity_configs.py (which runs them on the CUDA path 
                  rain 50 mm/h for 600 s (ramped to zero over the next 60 s step), Manning
                  n = 0.03, walls plus an outflow strip on the lowest edge, control-number target
                  0.5, 3600 s, outputs every 600 s, in three modes: the reference rain clamp from
-                 dry (max dt 10 s: from a dry, still state the reference's next dt is infinite),
+                 dry (max dt 10 s: from a dry, still state the reference's next dt is infinite;
+                 no cell ever holds water, and the ramp-down step drains some below zero),
                  the reference clamp on a 1 mm film, and the physical clamp from dry
   fractal1024    1024 x 1024 window of the 4096 x 4096, dx = 2 m catchment (diamond-square bed,
                  Hurst 0.8, 100 m relief, plus a 0.005 slope; lognormal rain field, mean
