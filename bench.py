@@ -73,6 +73,14 @@ def parse():
     return p.parse_args()
 
 
+_T0 = time.perf_counter()
+
+
+def log(msg):
+    """Progress on stderr (the JSON line alone goes to stdout)."""
+    print(f"[bench {time.perf_counter() - _T0:7.1f} s] {msg}", file=sys.stderr, flush=True)
+
+
 def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
 
@@ -384,7 +392,7 @@ SERVING_RATES = (5.0, 10.0, 20.0, 50.0, 100.0, 200.0)
 
 
 def serving_sweep(device, count=24, horizon_scale=1.0 / 60.0, precision="f32_datum64", persistent=True,
-                  time_limit=300.0):
+                  time_limit=60.0):
     """The serving stream at every arrival rate of SERVING_RATES: `count` requests with mesh sides
     log-uniform on [128, 4096] (multiples of 32), dx in {1, 2, 5} m, raw fractal beds (Hurst 0.8,
     relief U(10, 150) m), triangular hyetographs (peak U(20, 120) mm/h, duration U(900, 7200) s),
@@ -398,12 +406,15 @@ def serving_sweep(device, count=24, horizon_scale=1.0 / 60.0, precision="f32_dat
                          horizon=(3600.0 * horizon_scale, 21600.0 * horizon_scale), relief_m=(10.0, 150.0),
                          peak=(20.0, 120.0), duration=(900.0, 7200.0), multiple=32)
     per_rate = []
+    log("serving requests generated")
     for rate in SERVING_RATES:
         reqs = at_rate(base, rate, seed=int(rate))
         srv = FloodServer(budget_bytes=150e9, precision=precision, device=device, persistent=persistent,
-                          steps_per_advance=1, step_limit=5000)
+                          steps_per_advance=1, step_limit=2000)
         summary = srv.run(reqs, time_limit=time_limit)
         srv.close()
+        log(f"serving at {rate:g}/s: {summary['completed']} completed, {summary['failed']} failed, "
+            f"p50 {summary['p50_s']}")
         summary["arrival_rate_per_s"] = rate
         summary["unfinished"] = summary["requests"] - summary["completed"] - summary["failed"]
         per_rate.append(summary)
@@ -411,6 +422,7 @@ def serving_sweep(device, count=24, horizon_scale=1.0 / 60.0, precision="f32_dat
     return {"requests_per_rate": count, "mesh_side": [128, 4096], "dx_m": [1, 2, 5], "relief_m": [10, 150],
             "horizon_s": [3600.0 * horizon_scale, 21600.0 * horizon_scale], "horizon_scale": horizon_scale,
             "horizon_note": "U(1, 6) h scaled down by the stated factor at every rate",
+            "time_limit_s": time_limit, "step_limit": 2000,
             "cells_per_request": [min(cells), max(cells)], "kernel": "persistent batch kernel" if persistent
             else "batched launches per stage", "per_rate": per_rate}
 
@@ -435,7 +447,7 @@ def ensemble_members(count=64, seed=13):
     return out
 
 
-def batched_run(device, members, precision, steps=10, per_call=5, step_s=10.0, persistent=True, perturb=0.0):
+def batched_run(device, members, precision, steps=6, per_call=3, step_s=10.0, persistent=True, perturb=0.0):
     """The ensemble advanced together, `per_call` queued steps per call (each member at its own
     pace): in one persistent launch per call, or in one launch per RK stage and timestep.
     Members that fail leave; only members that complete a step count toward the throughput.
@@ -512,9 +524,13 @@ def batched_ensemble(device, precision="f32_datum64"):
     one launch per stage is timed too, for comparison."""
     members = ensemble_members()
     r32, f32 = batched_run(device, members, precision)
+    log(f"ensemble {precision}: {r32['cell_updates_per_s']:.3e}")
     r64, f64 = batched_run(device, members, "f64")
+    log(f"ensemble f64: {r64['cell_updates_per_s']:.3e}")
     _, p64 = batched_run(device, members, "f64", perturb=1e-7)
+    log("ensemble noise floor done")
     g32, _ = batched_run(device, members, precision, persistent=False)
+    log(f"ensemble {precision} per-stage launches: {g32['cell_updates_per_s']:.3e}")
     both = sorted(set(f32) & set(f64))
     per_member = []
     for i in both:
@@ -745,13 +761,17 @@ def main():
         torch.cuda.synchronize(device)
 
     w = workload(args.size)
+    log("workload ready")
     state = common_state(w, args, device)
+    log(f"common FP64 state at t = {state['t_step']:.0f} s")
     solver, main_res = timed_run(w, args.precision, args, device, barrier, dist, state)
     solver.close()
+    log(f"{args.precision} timed: {main_res['value']:.3e} cell-updates/s, variant {main_res['variant']}")
     extras = {}
     if not args.no_extras and args.precision != "f64":
         s64, r64 = timed_run(w, "f64", args, device, barrier, dist, state)
         s64.close()
+        log(f"f64 timed: {r64['value']:.3e} cell-updates/s, variant {r64['variant']}")
         extras["fp64"] = {"value": r64["value"], "ms_per_step": r64["ms"] / max(1, args.steps),
                           "ms_per_timestep": r64["ms_per_timestep"], "stage_ms": r64["stage_ms"],
                           "accepted": r64["accepted"], "repeated": r64["repeated"], "kernel_variant": r64["variant"],
@@ -765,20 +785,26 @@ def main():
         extras["fp32_over_fp64_per_stage"] = r64["stage_ms"] / main_res["stage_ms"]
         if rank == 0:
             extras["headline_error_vs_fp64"] = headline_error(w, state, args.precision, device)
+            log("headline error done")
     wstate = None
     if rank == 0 and world == 1 and not args.no_cpu:
         wstate = window_state(w, args.window_steps, device=device)
+        log("window state done")
         if "fp64" in extras:
             extras["fp64"]["cpu_baseline"] = cpu_baseline(w, wstate, args.cpu_seconds, "f64")
     if rank == 0 and not args.no_extras:
         extras["precision"] = precision_study(device)
         # the same on a 2 cm dam: levels near 350 m then carry the depth in their last bits
         extras["precision_thin"] = precision_study(device, h0=0.02)
+        log("precision studies done")
         extras["serving"] = serving_sweep(device)
+        log("serving sweep done")
         extras["batched"] = batched_ensemble(device, args.precision)
+        log("ensemble done")
     e2e = None
     if rank == 0 and not args.no_e2e:
         e2e = measure_e2e(w, args, device, state, main_res["variant"], args.precision)
+        log("e2e done")
     if rank == 0 and not args.no_extras:
         extras["source_terms"] = source_terms_cost(w, state, args.precision, main_res["variant"], device)
     cb = None

@@ -81,8 +81,12 @@ def check_ref_dudt(kind, prec="f64"):
     setup(b, *(g[k].astype(np.float64) for k in ("z", "h", "u", "v")))
     f = Forcing()
     f.rain_kind, f.head_kind = RAIN_FIELDS, HEAD_FIELDS
-    b.set_forcing(f)  # per-cell boundary values are uploaded after the forcing
+    # the CUDA solver takes per-cell forcing only once its fields exist; the oracle clears the
+    # discharge fields when the forcing is set: upload, set the forcing, upload again
     for name in ("n_shallow", "n_deep", "d_shallow", "d_deep", "qbdy0", "qbdy1", "hbdy0", "hbdy1"):
+        b.set_field(name.upper(), g[name].astype(np.float64))
+    b.set_forcing(f)
+    for name in ("qbdy0", "qbdy1", "hbdy0", "hbdy1"):
         b.set_field(name.upper(), g[name].astype(np.float64))
     b.eval_dudt(0, float(g["t_sub"]), float(g["dt"]))
     for f in SLOPE + FACE + KS:

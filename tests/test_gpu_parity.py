@@ -154,8 +154,14 @@ def test_fp32_interior_strips_close_to_fp64(precision, variant):
     solve(g, 0.0, 120.0, rain=rain, head=0.0, head_edges=synth.lowest_edge(z))
     solve(o, 0.0, 120.0, rain=rain, head=0.0, head_edges=synth.lowest_edge(z))
     assert np.max(np.abs(g.get_field("H") - o.get_field("H"))) <= 1e-3
-    vg, vo = g.stats()["volume"], o.stats()["volume"]
-    assert abs(vg - vo) <= 1e-6 * vo, (vg, vo)
+    sg, so = g.stats(), o.stats()
+    # the FP32 run's own mass balance (initial + rain - outflow + wall flow) closes to 1e-6; its
+    # volume differs from FP64's by what the slightly different flow let out through the outflow
+    # strip, a few parts in a million after 120 s here
+    v0 = float(h.sum()) * dx * dx
+    closure = sg["volume"] - (v0 + sg["rain_in"] - sg["outflow"] + sg["wall_in"])
+    assert abs(closure) <= 1e-6 * sg["volume"], (closure, sg)
+    assert abs(sg["volume"] - so["volume"]) <= 1e-5 * so["volume"], (sg["volume"], so["volume"])
 
 
 @pytest.mark.parametrize("variant", range(12))
