@@ -20,8 +20,15 @@ latency.
   launches.
 
 One "step" is one accepted RK4 timestep of the whole grid. Inputs are seeded synthetic fields
-with the workload's shapes and statistics. Before timing, each precision is spun up from dry
-for --spinup timesteps. Every FP64 state field (134 MB) is larger than the 126 MB L2.
+with the workload's shapes and statistics. Before timing, the plain FP64 path runs the first
+60 s step from dry (at most --spinup-cap timesteps); every precision starts from that state.
+Every FP64 state field (134 MB) is larger than the 126 MB L2.
+
+Every phase is bounded by a count of timesteps rather than by simulated seconds. On this bed
+the reference's velocity formulation blows up in finite time: a cell holding a 2 mm film beside
+a nearly dry cell reaches |u| ~ 1e3 m/s, du/dt grows faster than the control number lets dt
+shrink, and simulated time converges on a limit it never passes (t ~ 91 s in the 1024 x 1024
+window). A loop run to a later step boundary would never end, in the reference as here.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -62,9 +69,12 @@ def parse():
     p.add_argument("--precision", default="f32_datum64", choices=["f32_datum64", "f32", "f64"],
                    help="precision of the headline value")
     p.add_argument("--size", type=int, default=4096)
-    p.add_argument("--spinup", type=int, default=600, help="timesteps run from dry before timing")
+    p.add_argument("--spinup-cap", type=int, default=4000,
+                   help="most timesteps of the FP64 run through the first 60 s step before timing")
+    p.add_argument("--error-span", type=float, default=10.0,
+                   help="simulated seconds both precisions advance from the common state for the headline error")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
-    p.add_argument("--window-steps", type=int, default=10,
+    p.add_argument("--window-steps", type=int, default=1,
                    help="60 s steps from dry of the 1024^2 window both CPU baselines are timed on")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
@@ -152,10 +162,10 @@ def rain_series():
     return TimeSeries([0.0, 1800.0, 1800.001, 1e7], [1.0, 1.0, 0.0, 0.0])
 
 
-def make_solver(w, precision, device, **kw):
+def make_solver(w, precision, device, step_duration=60.0, **kw):
     from mfcm_b200 import SaintVenantSolver
     s = SaintVenantSolver(w["nx"], w["ny"], w["dx"], precision=precision, cn_target=0.5,
-                          rain_mode="physical", step_duration=60.0, initial_dt=1.0, device=device, **kw)
+                          rain_mode="physical", step_duration=step_duration, initial_dt=1.0, device=device, **kw)
     zeros = np.zeros((w["ny"], w["nx"]))
     s.set_field("Z", w["z"])
     for f in ("H", "U", "V"):
@@ -181,8 +191,9 @@ class Runner:
         self.L = solver.step_duration
         self.need_begin = True
 
-    def run(self, n, timing=False):
-        """Run n timesteps (accepted or repeated), crossing step boundaries as needed."""
+    def run(self, n, timing=False, stop_at_boundary=False):
+        """Run n timesteps (accepted or repeated), crossing step boundaries as needed (or
+        stopping at the first one)."""
         tot = {"total_ms": 0.0, "stage_ms": 0.0, "finalize_ms": 0.0, "stage_launches": 0, "finalize_launches": 0,
                "begin_launches": 0, "timesteps": 0}
         last = self.s.stats()
@@ -201,66 +212,70 @@ class Runner:
             ran = (st["accepted"] + st["repeated"]) - (last["accepted"] + last["repeated"])
             last = st
             done_so_far += ran
-            if ran == 0:
+            if ran == 0 or (done and stop_at_boundary):
                 break
         tot["timesteps"] = done_so_far
         return last, tot
 
-    def spinup(self, timesteps):
-        """Spin up by a count of timesteps, not simulated seconds: the reference's velocity
-        formulation can blow up in thin films on steep cells, where dt shrinks without bound
-        and a fixed simulated span would never end."""
-        if timesteps > 0:
-            self.run(timesteps)
-
-    def finish_step(self):
-        """Run to the end of the current step (the next step boundary)."""
-        while not self.need_begin:
-            _, done, _ = self.s.run_timesteps(1 << 40, begin=False)
-            if done:
-                self.need_begin = True
-                self.t_step += self.L
+    def run_step(self, cap, chunk=200):
+        """Run the current step to its end, at most `cap` timesteps (accepted or repeated):
+        the reference's velocity formulation can blow up in thin films on steep cells, where dt
+        shrinks without bound and the step would never end. Returns True when the step ended."""
+        ran = 0
+        start = self.t_step
+        while ran < cap and self.t_step == start:
+            _, tot = self.run(min(chunk, cap - ran), stop_at_boundary=True)
+            if tot["timesteps"] == 0:
+                break
+            ran += tot["timesteps"]
+            log(f"  t_step {start:.0f} s: {ran} timesteps, dt {self.s.get_dt():.3g} s")
+        return self.t_step != start
 
 
 def common_state(w, args, device):
-    """The state both precisions are timed from: the plain FP64 path (bit for bit the
-    reference arithmetic) spun up from dry for --spinup timesteps and then to the end of that
-    step, so that a solver of either precision can start the next step from it."""
+    """The state every precision is timed from: the plain FP64 path (bit for bit the
+    reference arithmetic) run from dry through the first 60 s step, a step boundary from which
+    a solver of either precision starts the next step. If the step does not end within
+    --spinup-cap timesteps the state at the cap is used and the line says so."""
     s = make_solver(w, "f64", device)
     r = Runner(s)
-    r.spinup(args.spinup)
-    r.finish_step()
+    ended = r.run_step(args.spinup_cap)
     st = s.stats()
     state = {"h": s.get_field("H"), "u": s.get_field("U"), "v": s.get_field("V"), "dt": s.get_dt(),
-             "t_step": r.t_step, "spinup_accepted": st["accepted"], "spinup_repeated": st["repeated"]}
+             "t_step": r.t_step if ended else 0.0, "step_ended": ended,
+             "spinup_accepted": st["accepted"], "spinup_repeated": st["repeated"]}
     s.close()
     return state
 
 
-def solver_at(w, precision, state, device):
+def solver_at(w, precision, state, device, step_duration=60.0):
     """A solver of `precision` holding the common state (FP64 values rounded once to FP32 for
     the FP32 paths) and its next timestep."""
-    s = make_solver(w, precision, device)
+    s = make_solver(w, precision, device, step_duration=step_duration)
     for f in ("H", "U", "V"):
         s.set_field(f, state[f.lower()])
     s.set_dt(state["dt"])
     return s
 
 
-def headline_error(w, state, precision, device):
+def headline_error(w, state, precision, device, span, cap=3000):
     """Error of the FP32 headline against FP64 on the headline workload itself: from the common
-    state both advance one whole 60 s step (device-controlled timesteps), then the depth fields
-    and FP64 volumes are compared."""
+    state both advance one step of `span` simulated seconds (device-controlled timesteps, at
+    most `cap` each), then the depth fields and FP64 volumes are compared."""
     out = {}
     for prec in ("f64", precision):
-        s = solver_at(w, prec, state, device)
-        s.set_forcing(forcing_at(state["t_step"], s.step_duration))
-        st = s.advance()
-        out[prec] = (s.get_field("H"), s.stats()["volume"], st["accepted"], st["repeated"])
+        s = solver_at(w, prec, state, device, step_duration=span)
+        r = Runner(s, t0=state["t_step"])
+        ended = r.run_step(cap)
+        st = s.stats()
+        out[prec] = (s.get_field("H"), st["volume"], st["accepted"], st["repeated"], ended)
         s.close()
+    if not (out["f64"][4] and out[precision][4]):
+        return {"case": f"{span:g} s from the common state at t = {state['t_step']:.0f} s",
+                "reached": {p: out[p][4] for p in out}, "cap_timesteps": cap}
     d = np.abs(out[precision][0] - out["f64"][0])
     wet = out["f64"][0] > 1e-3
-    return {"case": f"one 60 s step from the common state at t = {state['t_step']:.0f} s",
+    return {"case": f"{span:g} s from the common state at t = {state['t_step']:.0f} s",
             "max_depth_err_m": float(d.max()), "p99_depth_err_m": float(np.percentile(d, 99)),
             "mean_depth_err_m": float(d.mean()), "cells_over_1mm_fraction": float((d > 1e-3).mean()),
             "max_depth_err_wet_m": float(d[wet].max()) if wet.any() else None,
@@ -342,14 +357,15 @@ def timed_run(w, precision, args, device, barrier, dist, state):
     return solver, res
 
 
-def precision_study(device, nx=8192, ny=1024, dx=0.5, seconds=60.0, h0=1.0):
+def precision_study(device, nx=8192, ny=1024, dx=0.5, seconds=60.0, h0=1.0, cap=20000):
     """Dam break on a flat bed at 350 m (8192 x 1024 cells, dx = 0.5 m, h = h0 for x below the
     centre, dry beyond, frictionless, no rain, 60 s): max depth error and relative volume
     error of the FP32 paths against FP64, the front position of each against Ritter's
     2 sqrt(g h0) t, and the depth and velocity at the dam against Ritter's 4/9 h0 and
     2/3 sqrt(g h0). The depth error is given over the whole grid and away from the moving
     bore (cells more than 20 m from FP64's front), because a bore that arrives one timestep
-    earlier or later differs there by up to its own height whatever the precision."""
+    earlier or later differs there by up to its own height whatever the precision. Each run
+    stops after `cap` timesteps if it has not reached the end by then (reached_end)."""
     from mfcm_b200 import SaintVenantSolver, synth
     z, h = synth.dam_break(nx, ny, 350.0, h0)
     out = {}
@@ -360,13 +376,13 @@ def precision_study(device, nx=8192, ny=1024, dx=0.5, seconds=60.0, h0=1.0):
         s.set_field("Z", z)
         s.set_field("H", h)
         t0 = time.perf_counter()
-        st = s.advance()
+        st, reached, _ = s.run_timesteps(cap, begin=True)  # the whole span unless dt collapses
         el = time.perf_counter() - t0
         hf, uf = s.get_field("H"), s.get_field("U")
         wet = np.where(hf[ny // 2, mid:] > 1e-3)[0]
         out[prec] = {"h": hf, "volume": s.stats()["volume"], "front_m": (wet.max() + 1) * dx if wet.size else 0.0,
                      "h_dam": float(hf[ny // 2, mid]), "u_dam": float(uf[ny // 2, mid]), "accepted": st["accepted"],
-                     "repeated": st["repeated"], "seconds": el}
+                     "repeated": st["repeated"], "seconds": el, "reached_end": reached}
         s.close()
     h64, v64 = out["f64"]["h"], out["f64"]["volume"]
     c0 = math.sqrt(9.81 * h0)
@@ -376,7 +392,7 @@ def precision_study(device, nx=8192, ny=1024, dx=0.5, seconds=60.0, h0=1.0):
     away = np.abs(x - out["f64"]["front_m"]) > 20.0
     for prec in ("f64", "f32", "f32_datum64"):
         o = out[prec]
-        r = {k: o[k] for k in ("front_m", "h_dam", "u_dam", "accepted", "repeated", "seconds")}
+        r = {k: o[k] for k in ("front_m", "h_dam", "u_dam", "accepted", "repeated", "seconds", "reached_end")}
         if prec != "f64":
             d = np.abs(o["h"] - h64)
             r["max_depth_err_m"] = float(d.max())
@@ -570,9 +586,10 @@ def window_workload(w, n=1024):
 
 def window_state(w, steps, device=None):
     """The state both CPU baselines (this arm's and the reference arm's) are timed on: the
-    1024 x 1024 window spun up from dry for `steps` whole 60 s steps in plain FP64 -- on the
-    GPU here, on the oracle in the reference arm (which has no GPU). The two FP64 paths are
-    bit for bit the same, so both arms time the CPU on the same state."""
+    1024 x 1024 window run from dry for `steps` whole 60 s steps in plain FP64 -- on the GPU
+    here, on the oracle in the reference arm (which has no GPU). The two FP64 paths are bit for
+    bit the same, so both arms time the CPU on the same state. The first step takes 37
+    timesteps; the second never ends (the thin-film blow-up near 91 s), so `steps` is 1 or 0."""
     ww = window_workload(w)
     if device is not None:
         s = make_solver(ww, "f64", device)
@@ -587,6 +604,8 @@ def window_state(w, steps, device=None):
         s.set_field("N_SHALLOW", ww["n"])
         s.set_field("N_DEEP", ww["n"])
         s.set_field("RAIN_PATTERN", ww["rain"])
+    if steps > 1:
+        raise ValueError("the window's second 60 s step never ends under the reference scheme")
     acc = 0
     for k in range(steps):
         s.set_forcing(forcing_at(60.0 * k, 60.0))
@@ -763,7 +782,8 @@ def main():
     w = workload(args.size)
     log("workload ready")
     state = common_state(w, args, device)
-    log(f"common FP64 state at t = {state['t_step']:.0f} s")
+    log(f"common FP64 state at t = {state['t_step']:.0f} s ({state['spinup_accepted']} accepted, "
+        f"{state['spinup_repeated']} repeated timesteps; step ended: {state['step_ended']})")
     solver, main_res = timed_run(w, args.precision, args, device, barrier, dist, state)
     solver.close()
     log(f"{args.precision} timed: {main_res['value']:.3e} cell-updates/s, variant {main_res['variant']}")
@@ -784,7 +804,7 @@ def main():
         extras["fp32_over_fp64_per_timestep"] = r64["ms_per_timestep"] / main_res["ms_per_timestep"]
         extras["fp32_over_fp64_per_stage"] = r64["stage_ms"] / main_res["stage_ms"]
         if rank == 0:
-            extras["headline_error_vs_fp64"] = headline_error(w, state, args.precision, device)
+            extras["headline_error_vs_fp64"] = headline_error(w, state, args.precision, device, args.error_span)
             log("headline error done")
     wstate = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -819,7 +839,8 @@ def main():
                 "config": {"workload": f"single catchment {w['nx']}x{w['ny']}, dx=2 m (diamond-square H0.8 100 m + "
                                        "0.005 slope, lognormal rain field 30 mm/h, Voronoi n, outflow all edges)",
                            "scheme": "classic RK4", "cn_target": 0.5, "precision": args.precision,
-                           "spinup_timesteps": args.spinup, "sim_time_s": main_res["sim_time_s"],
+                           "spinup_timesteps": state["spinup_accepted"] + state["spinup_repeated"],
+                           "spinup_step_ended": state["step_ended"], "sim_time_s": main_res["sim_time_s"],
                            "start": f"common FP64 state at t = {state['t_step']:.0f} s for every precision",
                            "l2": "inputs larger than L2 (each FP64 state field 134 MB; FP32 67 MB x 13 fields)",
                            "parallelism": f"replicas x{world}", "kernel_variant": main_res["variant"],

@@ -23,12 +23,21 @@
 #include <type_traits>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/sv.h"
 #include "sv_launch.h"
 #include "sv_tableau.h"
 
 using svk::Ctl;
 using svk::DevForcing;
+
+// NVTX range over one host call (a profiler shows the library's steps, advances and tuning on
+// its timeline; without a tool attached a range costs a few nanoseconds)
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
 
 namespace {
 
@@ -864,6 +873,7 @@ struct Solver final : public sv_ctx {
 
   // TypedTemporalScheme::step: timesteps until t_local reaches L, all on the device.
   int advance(sv_stats* out) override {
+    NvtxRange nv("sv_advance");
     if (graph_dirty || !graph) {
       int r = build_graph();
       if (r) return r;
@@ -901,6 +911,7 @@ struct Solver final : public sv_ctx {
   // Direct launches (no graph) of up to n device-controlled timesteps; with timing, every
   // kernel is bracketed by events and the per-kernel durations are summed after one sync.
   int run_timesteps(uint64_t n, int begin, sv_stats* out, int* step_done, sv_timing* timing) override {
+    NvtxRange nv("sv_run_timesteps");
     if (n == 0) return fail(SV_E_ARG, "max_timesteps must be positive");
     cudaError_t e = svk::launch_begin_step(ctl, begin ? 1 : 0, (long long)n, stream);
     if (e != cudaSuccess) return cuda_fail(e, "begin step");
@@ -967,6 +978,7 @@ struct Solver final : public sv_ctx {
   // Time the first-stage kernel of every variant (it reads U_[0] and writes only the stage
   // and accumulator buffers, so the state is untouched) and keep the fastest.
   int autotune(int* best_out) override {
+    NvtxRange nv("sv_autotune");
     // time against a copy of the controller with `done` cleared (the live one may hold a
     // finished or paused step, which makes every stage kernel return at once)
     Ctl c;
@@ -1325,6 +1337,7 @@ struct Batch final : public sv_batch_base {
   // one read-back. Each member runs its steps back to back at its own pace; a failing
   // member stops alone. hq receives the per-step results; last_status each slot's outcome.
   int run_queue(std::vector<svk::StepQueue>& hq) {
+    NvtxRange nv(persistent ? "sv_batch_advance (persistent)" : "sv_batch_advance");
     SV_CUDA(cudaMemcpyAsync(d_queue, hq.data(), sizeof(svk::StepQueue) * nact, cudaMemcpyHostToDevice, stream));
     cudaError_t e = svk::launch_begin_queue(d_fin, nact, stream);
     if (e != cudaSuccess) return cuda_fail(e, "begin queued steps");
