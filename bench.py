@@ -407,16 +407,19 @@ def precision_study(device, nx=8192, ny=1024, dx=0.5, seconds=60.0, h0=1.0, cap=
 SERVING_RATES = (5.0, 10.0, 20.0, 50.0, 100.0, 200.0)
 
 
-def serving_sweep(device, count=24, horizon_scale=1.0 / 60.0, precision="f32_datum64", persistent=True,
-                  time_limit=60.0):
+def serving_sweep(device, count=24, horizon_scale=1.0 / 60.0, precision="f32_datum64", persistent=False,
+                  time_limit=30.0, step_s=10.0, step_limit=400):
     """The serving stream at every arrival rate of SERVING_RATES: `count` requests with mesh sides
     log-uniform on [128, 4096] (multiples of 32), dx in {1, 2, 5} m, raw fractal beds (Hurst 0.8,
     relief U(10, 150) m), triangular hyetographs (peak U(20, 120) mm/h, duration U(900, 7200) s),
     Manning n = 0.035, outflow on every edge, FP32 state with FP64 reductions, admitted against
-    a 150 GB device-memory budget. Horizons are U(1, 6) h scaled by `horizon_scale` (so that one
-    rate's stream runs in about a minute); the same requests arrive at every rate, as a fresh
-    Poisson stream. Requests whose dt collapses (the reference scheme's thin-film blow-up on
-    steep cells) are failed by the step limit and counted as failed."""
+    a 150 GB device-memory budget, in steps of `step_s` simulated seconds (admission happens at
+    step boundaries). Horizons are U(1, 6) h scaled by `horizon_scale` (so that one rate's
+    stream runs in about `time_limit` seconds); the same requests arrive at every rate, as a
+    fresh Poisson stream. A request whose dt collapses (the reference scheme's thin-film blow-up
+    on steep cells: more than `step_limit` timesteps in one step, a mean dt below
+    step_s / step_limit) is failed and counted as failed; requests still running at the time
+    limit are counted as unfinished."""
     from mfcm_b200.serving import FloodServer, make_requests, at_rate
     base = make_requests(1.0, count, seed=11, side=(128, 4096), dxs=(1.0, 2.0, 5.0),
                          horizon=(3600.0 * horizon_scale, 21600.0 * horizon_scale), relief_m=(10.0, 150.0),
@@ -426,7 +429,7 @@ def serving_sweep(device, count=24, horizon_scale=1.0 / 60.0, precision="f32_dat
     for rate in SERVING_RATES:
         reqs = at_rate(base, rate, seed=int(rate))
         srv = FloodServer(budget_bytes=150e9, precision=precision, device=device, persistent=persistent,
-                          steps_per_advance=1, step_limit=2000)
+                          steps_per_advance=1, step_limit=step_limit, step_duration=step_s)
         summary = srv.run(reqs, time_limit=time_limit)
         srv.close()
         log(f"serving at {rate:g}/s: {summary['completed']} completed, {summary['failed']} failed, "
@@ -438,7 +441,7 @@ def serving_sweep(device, count=24, horizon_scale=1.0 / 60.0, precision="f32_dat
     return {"requests_per_rate": count, "mesh_side": [128, 4096], "dx_m": [1, 2, 5], "relief_m": [10, 150],
             "horizon_s": [3600.0 * horizon_scale, 21600.0 * horizon_scale], "horizon_scale": horizon_scale,
             "horizon_note": "U(1, 6) h scaled down by the stated factor at every rate",
-            "time_limit_s": time_limit, "step_limit": 2000,
+            "step_s": step_s, "time_limit_s": time_limit, "step_limit": step_limit,
             "cells_per_request": [min(cells), max(cells)], "kernel": "persistent batch kernel" if persistent
             else "batched launches per stage", "per_rate": per_rate}
 
