@@ -79,7 +79,7 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-extras", action="store_true", help="skip the fp64, precision, serving, batched parts")
-    p.add_argument("--variant", default="auto", help="stage-kernel variant 0-10, or auto (autotune)")
+    p.add_argument("--variant", default="auto", help="stage-kernel variant 0-13, or auto (autotune)")
     return p.parse_args()
 
 
@@ -217,7 +217,7 @@ class Runner:
         tot["timesteps"] = done_so_far
         return last, tot
 
-    def run_step(self, cap, chunk=200):
+    def run_step(self, cap, chunk=50):
         """Run the current step to its end, at most `cap` timesteps (accepted or repeated):
         the reference's velocity formulation can blow up in thin films on steep cells, where dt
         shrinks without bound and the step would never end. Returns True when the step ended."""
@@ -301,6 +301,18 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
+def dominant_kernel(variant, precision):
+    """The stage kernel that does most of a variant's work on the benchmark mesh, whose
+    interior strips (all but the edge strips) run the interior form of the column sweep."""
+    if variant < 4 or variant == 11:
+        return "stage_kernel"
+    if precision != "f64" and variant == 8:
+        return "sweep_batch_kernel"  # FP32 with the batches' variant runs the batched sweep as a batch of one
+    if variant in (12, 13):
+        return "sweep_pair_kernel"
+    return "sweep_interior_kernel"
+
+
 def timed_run(w, precision, args, device, barrier, dist, state):
     """From the common state: pick the kernel, then time args.steps timesteps with per-kernel
     events."""
@@ -331,9 +343,7 @@ def timed_run(w, precision, args, device, barrier, dist, state):
     stage_avg_s = tm["stage_ms"] * 1e-3 / max(1, solver.nstages * tm["timesteps"])
     achieved = alg_bytes_launch / stage_avg_s / 1e9
     peak, peak_kind = measured_peaks()
-    # FP32 with the batches' variant runs the batched column sweep as a batch of one
-    kernel = "stage_kernel" if variant < 4 else ("sweep_batch_kernel" if precision != "f64" and variant == 8
-                                                  else "sweep_kernel")
+    kernel = dominant_kernel(variant, precision)
     traffic_pc = profile_traffic(f"{kernel}_{precision}_2048_traffic.json")
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": (traffic_pc * ncells if traffic_pc else None), "peak_kind": peak_kind,

@@ -170,9 +170,10 @@ typedef struct sv_ctx sv_ctx;
 
 /* SaintVenantSolver constructor (src/SaintVenant/Solver.cpp:32-71) + RungeKuttaSolver
  * (src/TemporalScheme/RungeKutta.hpp:319-331): allocates U_[0..N], the k stages and the
- * bed constants on device `device`. Later calls on the solver launch work on that device's
- * streams: make `device` the current CUDA device before each call (one process per GPU,
- * as the replicas run, satisfies this once and for all). */
+ * bed constants on device `device`. The state U_[0] (h, u, v) and the bed start at zero.
+ * Later calls on the solver launch work on that device's streams: make `device` the current
+ * CUDA device before each call (one process per GPU, as the replicas run, satisfies this once
+ * and for all). */
 int sv_create(const sv_mesh_desc* mesh, const sv_params* params, int device, sv_ctx** out);
 /* ~SaintVenantSolver */
 void sv_destroy(sv_ctx* ctx);
@@ -248,10 +249,12 @@ int sv_run_timesteps(sv_ctx* ctx, uint64_t max_timesteps, int begin, sv_stats* o
  * library). Fused schedule, one pass per RK stage: 0-3 tiled shared-memory kernel (32x8, 32x8
  * at 3 CTAs/SM, 32x4 at 4 CTAs/SM, 64x4 at 3 CTAs/SM), 4-10 column-sweep kernel (16/32/64 rows
  * per warp, then 32 rows capped for 3, 4, 5 and 6 CTAs/SM; strips away from the mesh edge and
- * from coded-out cells run an interior form of it). Split schedule, two passes per RK stage:
- * 11 a slopes pass, then the tiled 32x8 kernel reading those slopes. Every variant computes
- * bit-identical FP64 results; FP32 results are reproducible per variant. SV_F32_DATUM64 solvers
- * take the column-sweep variants only. */
+ * from coded-out cells run an interior form of it), 12-13 (FP32 solvers only) the 32-row
+ * column sweep whose pairs of adjacent interior strips run two cells per lane with 8-byte
+ * loads (capped for 3 and 4 CTAs/SM; meshes with an odd row length have no pairs). Split
+ * schedule, two passes per RK stage: 11 a slopes pass, then the tiled 32x8 kernel reading
+ * those slopes. Every variant computes bit-identical FP64 results; FP32 results are
+ * reproducible per variant. SV_F32_DATUM64 solvers take the column-sweep variants only. */
 int sv_set_kernel_variant(sv_ctx* ctx, int variant);
 int sv_get_kernel_variant(sv_ctx* ctx, int* variant);
 /* Autotune: times every variant's stage kernel (both schedules) on the current state and keeps
@@ -272,6 +275,13 @@ int sv_batch_create(int precision, int rk_method, int device, sv_batch** out);
 void sv_batch_destroy(sv_batch* batch);
 /* add a catchment (allocates its device memory); *id is its slot, reused after removal */
 int sv_batch_add(sv_batch* batch, const sv_mesh_desc* mesh, const sv_params* params, int* id);
+/* a solver made by sv_create and filled on its own (bed, state, roughness; its uploads run on
+ * its own stream, so a server can prepare an arriving request while the batch advances)
+ * joins the batch as a member: *id is its slot. Its precision, tableau and device must be the
+ * batch's. The batch takes ownership: from now on the context is the member's
+ * (sv_batch_member) and is freed by sv_batch_remove or sv_batch_destroy, not sv_destroy. Not to
+ * be called while an advance of the same batch runs on another thread. */
+int sv_batch_adopt(sv_batch* batch, sv_ctx* solver, int* id);
 /* remove a catchment and free its device memory */
 int sv_batch_remove(sv_batch* batch, int id);
 /* the member's context, for sv_set_field / sv_get_field / sv_set_forcing / sv_get_stats

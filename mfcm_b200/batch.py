@@ -21,6 +21,8 @@ def _declare(lib):
     lib.sv_batch_destroy.argtypes = [C.c_void_p]
     lib.sv_batch_add.restype = C.c_int
     lib.sv_batch_add.argtypes = [C.c_void_p, P(MeshDesc), P(Params), P(C.c_int)]
+    lib.sv_batch_adopt.restype = C.c_int
+    lib.sv_batch_adopt.argtypes = [C.c_void_p, C.c_void_p, P(C.c_int)]
     lib.sv_batch_remove.restype = C.c_int
     lib.sv_batch_remove.argtypes = [C.c_void_p, C.c_int]
     lib.sv_batch_member.restype = C.c_void_p
@@ -89,6 +91,24 @@ class SaintVenantBatch:
             raise SvError(r, self._lib.sv_last_error(None).decode())
         mem = BatchMember(self, slot.value, int(nx), int(ny), float(dx), dy, float(step_duration),
                           RK_STAGES[RK_METHODS.index(self.rk_method)])
+        self.members[slot.value] = mem
+        return mem
+
+    def adopt(self, solver):
+        """A SaintVenantSolver of this batch's precision, tableau and device, created and
+        filled on its own (its uploads run on its own stream, so this can happen while the
+        batch advances on another thread), joins the batch. The batch takes the solver's
+        context over: `solver` is closed (its handle cleared) and the returned member is the
+        catchment from now on. Not to be called while an advance of this batch runs."""
+        if solver.precision != self.precision:
+            raise ValueError(f"solver precision {solver.precision} differs from the batch's {self.precision}")
+        slot = C.c_int()
+        r = self._lib.sv_batch_adopt(self._b, solver._h, C.byref(slot))
+        if r != 0:
+            raise SvError(r, self._lib.sv_last_error(None).decode())
+        solver._h = None  # owned by the batch now
+        mem = BatchMember(self, slot.value, solver.nx, solver.ny, solver.dx, solver.dy, solver.step_duration,
+                          solver.nstages)
         self.members[slot.value] = mem
         return mem
 

@@ -201,6 +201,11 @@ struct Solver final : public sv_ctx {
     int* d_i = nullptr;
     int* d_b = nullptr;
     int ni = 0, nb = 0;
+    // two-cells-per-lane variants (FP32): pairs of adjacent interior strips (first strip of
+    // each, nx even) and the interior strips left out of a pair
+    int* d_p = nullptr;
+    int* d_pi = nullptr;
+    int np = 0, npi = 0;
     bool valid = false;
   };
   Strips strips_[3];
@@ -220,6 +225,8 @@ struct Solver final : public sv_ctx {
     if (!L.d_i) {
       SV_CUDA(alloc(&L.d_i, size_t(n)));
       SV_CUDA(alloc(&L.d_b, size_t(n)));
+      SV_CUDA(alloc(&L.d_p, size_t(n)));
+      SV_CUDA(alloc(&L.d_pi, size_t(n)));
     }
     if (!d_sflags)  // sized for the shortest strips, which are the most numerous
       SV_CUDA(alloc(&d_sflags, size_t(svk::variant_partials(4, (long long)mesh.nx, (long long)mesh.ny))));
@@ -228,13 +235,34 @@ struct Solver final : public sv_ctx {
     std::vector<unsigned char> flags(static_cast<size_t>(n));
     SV_CUDA(cudaMemcpyAsync(flags.data(), d_sflags, size_t(n), cudaMemcpyDeviceToHost, stream));
     SV_CUDA(cudaStreamSynchronize(stream));
-    std::vector<int> in, bd;
+    std::vector<int> in, bd, pr, pin;
     for (long long i = 0; i < n; ++i) (flags[size_t(i)] ? in : bd).push_back(int(i));
-    if (!in.empty()) SV_CUDA(cudaMemcpyAsync(L.d_i, in.data(), in.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
-    if (!bd.empty()) SV_CUDA(cudaMemcpyAsync(L.d_b, bd.data(), bd.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+    // pairs: strips (2t, 2t+1) of one row band, both interior; their vector loads need an even
+    // row length (every row then starts 8-byte aligned)
+    const long long tiles_x = (static_cast<long long>(mesh.nx) + svk::kSweepOut - 1) / svk::kSweepOut;
+    for (long long i = 0; i < n; ++i) {
+      if (!flags[size_t(i)]) continue;
+      const long long tx = i % tiles_x;
+      if (mesh.nx % 2 == 0 && tx % 2 == 0 && tx + 1 < tiles_x && flags[size_t(i + 1)]) {
+        pr.push_back(int(i));
+        ++i;  // the pair's second strip
+      } else {
+        pin.push_back(int(i));
+      }
+    }
+    auto up = [&](int* d, const std::vector<int>& h) -> cudaError_t {
+      if (h.empty()) return cudaSuccess;
+      return cudaMemcpyAsync(d, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice, stream);
+    };
+    SV_CUDA(up(L.d_i, in));
+    SV_CUDA(up(L.d_b, bd));
+    SV_CUDA(up(L.d_p, pr));
+    SV_CUDA(up(L.d_pi, pin));
     SV_CUDA(cudaStreamSynchronize(stream));
     L.ni = int(in.size());
     L.nb = int(bd.size());
+    L.np = int(pr.size());
+    L.npi = int(pin.size());
     L.valid = true;
     graph_dirty = true; ++pversion;
     return SV_OK;
@@ -243,12 +271,18 @@ struct Solver final : public sv_ctx {
   void set_strips(svk::StageParams<T>& P, int v) const {
     const int rows = svk::variant_sweep_rows(v);
     P.istrips = P.bstrips = nullptr;
-    P.n_istrips = P.n_bstrips = 0;
+    P.ipairs = nullptr;
+    P.n_istrips = P.n_bstrips = P.n_ipairs = 0;
     if (rows == 0) return;
     const Strips& L = strips_[strips_slot(rows)];
     if (!L.valid) return;
-    P.istrips = L.d_i; P.n_istrips = L.ni;
     P.bstrips = L.d_b; P.n_bstrips = L.nb;
+    if (svk::variant_is_pair(v)) {
+      P.ipairs = L.d_p; P.n_ipairs = L.np;
+      P.istrips = L.d_pi; P.n_istrips = L.npi;
+    } else {
+      P.istrips = L.d_i; P.n_istrips = L.ni;
+    }
   }
 
   ~Solver() override {
@@ -963,7 +997,9 @@ struct Solver final : public sv_ctx {
   int set_variant(int v) override {
     if (v < 0 || v >= svk::kNumVariants) return fail(SV_E_ARG, "unknown kernel variant");
     // with tile datums only the column sweep evaluates each face in one frame (face_frame)
-    if (datum && !svk::variant_is_sweep(v)) return fail(SV_E_ARG, "tile datums need a column-sweep variant (4-10)");
+    if (datum && !svk::variant_is_sweep(v))
+      return fail(SV_E_ARG, "tile datums need a column-sweep variant (4-10, 12-13)");
+    if (svk::variant_is_pair(v) && sizeof(T) != 4) return fail(SV_E_ARG, "variants 12-13 are FP32 only");
     if (svk::variant_is_split(v)) {
       int r = ensure_split();
       if (r) return r;
@@ -1013,6 +1049,7 @@ struct Solver final : public sv_ctx {
     float best_ms = 1e30f;
     for (int v = 0; v < svk::kNumVariants; ++v) {
       if (datum && !svk::variant_is_sweep(v)) continue;
+      if (svk::variant_is_pair(v) && sizeof(T) != 4) continue;
       P.nblk = svk::variant_partials(v, (long long)mesh.nx, (long long)mesh.ny);
       if (!batch_path(v)) {
         int rs = ensure_strips(v);
@@ -1121,6 +1158,7 @@ struct sv_batch_base {
   virtual int advance_steps(int, const int*, const sv_forcing*, sv_stats*, int) = 0;
   virtual int kernel_variant() const = 0;
   virtual int set_persistent(int, unsigned long long, double) = 0;
+  virtual int adopt(sv_ctx*, int*) = 0;
 };
 
 template <typename T>
@@ -1203,6 +1241,26 @@ struct Batch final : public sv_batch_base {
     dirty = true;
     return SV_OK;
   }
+  // a solver created and filled on its own (sv_create, then its fields) joins as a member:
+  // its device memory and stream move into the batch
+  int adopt(sv_ctx* c, int* id) override {
+    auto* s = dynamic_cast<Solver<T>*>(c);
+    if (!s || s->prm.precision != precision || s->prm.rk_method != rk_method)
+      return fail(SV_E_ARG, "the solver's precision and tableau must match the batch");
+    if (s->device != device) return fail(SV_E_ARG, "the solver is on another device");
+    for (auto* m : members)
+      if (m == s) return fail(SV_E_ARG, "the solver is already a member");
+    int r = s->set_variant(member_variant());
+    if (r != SV_OK) return fail(r, s->err);
+    int slot = -1;
+    for (size_t i = 0; i < members.size(); ++i)
+      if (!members[i]) { slot = int(i); break; }
+    if (slot < 0) { slot = int(members.size()); members.push_back(nullptr); }
+    members[slot] = s;
+    if (id) *id = slot;
+    dirty = true;
+    return SV_OK;
+  }
   int remove(int id) override {
     if (id < 0 || id >= int(members.size()) || !members[id]) return fail(SV_E_ARG, "no such batch member");
     delete members[id];
@@ -1255,6 +1313,10 @@ struct Batch final : public sv_batch_base {
       Solver<T>* m = members[active[k]];
       // the tile prefix and the partials follow the batch kernel's decomposition
       if (m->variant != member_variant()) m->set_variant(member_variant());
+      if (persistent) {  // the persistent kernel runs each member's interior strips in the interior sweep
+        int rs = m->ensure_strips(member_variant());
+        if (rs) return fail(rs, "member " + std::to_string(active[k]) + ": " + m->err);
+      }
       ht[k + 1] = ht[k] + m->nblk;
       int e2;
       p2 = p2 && std::frexp(m->mesh.dx, &e2) == 0.5 && std::frexp(m->mesh.dy, &e2) == 0.5;
@@ -1588,6 +1650,12 @@ void sv_batch_destroy(sv_batch* b) { delete b; }
 int sv_batch_add(sv_batch* b, const sv_mesh_desc* m, const sv_params* p, int* id) {
   if (!b) return SV_E_ARG;
   int r = b->impl->add(m, p, id);
+  if (r) g_create_err = b->impl->err;
+  return r;
+}
+int sv_batch_adopt(sv_batch* b, sv_ctx* solver, int* id) {
+  if (!b || !solver) return SV_E_ARG;
+  int r = b->impl->adopt(solver, id);
   if (r) g_create_err = b->impl->err;
   return r;
 }

@@ -80,12 +80,25 @@ template <> cudaError_t launch_stage<SV_T>(const StageParams<SV_T>& P, int tile,
   }
 }
 
-template <typename T, int TY, int MINB> static cudaError_t launch_sweep_t(const StageParams<T>& P, int variant,
-                                                                          cudaStream_t s) {
+template <typename T, int TY, int MINB, bool PAIR = false>
+static cudaError_t launch_sweep_t(const StageParams<T>& P, int variant, cudaStream_t s) {
   constexpr int WPB = 4;
   const long long ntiles = variant_partials(variant, P.nx, P.ny);
   dim3 block(32, WPB);
   const bool p2 = pow2_mesh(P.dx, P.dy);
+  // interior strip pairs (FP32, if listed) two cells per lane
+  if constexpr (PAIR && sizeof(T) == 4) {
+    if (P.ipairs && P.n_ipairs > 0) {
+      dim3 grid(unsigned((P.n_ipairs + WPB - 1) / WPB));
+      if (P.eddy) {
+        if (p2) sweep_pair_kernel<TY, WPB, MINB, true, true><<<grid, block, 0, s>>>(P);
+        else sweep_pair_kernel<TY, WPB, MINB, false, true><<<grid, block, 0, s>>>(P);
+      } else {
+        if (p2) sweep_pair_kernel<TY, WPB, MINB, true, false><<<grid, block, 0, s>>>(P);
+        else sweep_pair_kernel<TY, WPB, MINB, false, false><<<grid, block, 0, s>>>(P);
+      }
+    }
+  }
   // interior strips (if listed) in the interior kernel, the rest in the general one
   if (P.istrips && P.n_istrips > 0) {
     dim3 grid(unsigned((P.n_istrips + WPB - 1) / WPB));
@@ -110,6 +123,12 @@ template <typename T, int TY, int MINB> static cudaError_t launch_sweep_t(const 
   return cudaGetLastError();
 }
 
+// the two-cells-per-lane variants (FP32): 32-row strips, register caps for 3 and 4 blocks per SM
+template <typename T> static cudaError_t v12_13(const StageParams<T>& P, int variant, cudaStream_t s) {
+  if (variant == 12) return launch_sweep_t<T, 32, 3, true>(P, variant, s);
+  return launch_sweep_t<T, 32, 4, true>(P, variant, s);
+}
+
 template <> cudaError_t launch_variant<SV_T>(const StageParams<SV_T>& P, int variant, cudaStream_t s) {
   switch (variant) {
     case 4: return launch_sweep_t<SV_T, 16, 1>(P, variant, s);
@@ -120,6 +139,10 @@ template <> cudaError_t launch_variant<SV_T>(const StageParams<SV_T>& P, int var
     case 9: return launch_sweep_t<SV_T, 32, 5>(P, variant, s);
     case 10: return launch_sweep_t<SV_T, 32, 6>(P, variant, s);
     case kSplitVariant: return launch_split_t<SV_T>(P, s);
+    case 12:
+    case 13:
+      if (sizeof(SV_T) != 4) return cudaErrorInvalidValue;  // two cells per lane: FP32 only
+      return v12_13<SV_T>(P, variant, s);
     default: return launch_stage<SV_T>(P, variant, s);
   }
 }

@@ -103,6 +103,10 @@ template <typename T> struct StageParams {
   const int* istrips;
   const int* bstrips;
   int n_istrips, n_bstrips;
+  // two-cells-per-lane variants: pairs of adjacent interior strips (the first strip of each);
+  // istrips then lists the interior strips left out of a pair
+  const int* ipairs;
+  int n_ipairs;
   // split schedule: the stage input's slopes dh/dx, du/dx, dv/dx, dh/dy, du/dy, dv/dy as
   // written by slopes_kernel (read by the stage kernel instead of computing them), or null
   T* pslp[6];
@@ -984,7 +988,7 @@ __global__ void strip_flags_kernel(const T* __restrict__ z, int nx, int ny, int 
 // arithmetic is the general path's, operation for operation; in FP32 the tangential
 // finiteness tests are dropped (they only matter for slopes that are not finite, which an
 // interior window without coded-out beds produces only from a non-finite state).
-template <typename T, int TY, bool P2, bool EDDY>
+template <typename T, int TY, bool P2, bool EDDY, bool COH = false>
 __device__ __forceinline__ void sweep_strip_interior(const StageParams<T>& P, long long gw) {
   using DX = DivX<T, P2>;
   constexpr bool TCHK = sizeof(T) == 8;
@@ -1021,7 +1025,7 @@ __device__ __forceinline__ void sweep_strip_interior(const StageParams<T>& P, lo
   auto load_row = [&](int r) {
     const long long g = (long long)r * nx + gx;
     RowV<T> v;
-    v.h = ld(Yh, g); v.u = ld(Yu, g); v.v = ld(Yv, g);
+    v.h = ldst<COH>(Yh, g); v.u = ldst<COH>(Yu, g); v.v = ldst<COH>(Yv, g);
     v.z = ld(P.z, g);
     v.zx = ld(P.zx, g); v.zy = ld(P.zy, g);
     return v;
@@ -1135,7 +1139,7 @@ __device__ __forceinline__ void sweep_strip_interior(const StageParams<T>& P, lo
       const FaceF<T> FE{dn1(FW.h), dn1(FW.u), dn1(FW.v), dn1(FW.z)};
       if (out_lane) {
         const long long g = (long long)r * nx + gx;
-        finish_cell<T, CellCtx<T, DX>, EDDY, false>(P, fc, c, g, gx, r, me.h, me.u, me.v, me.dhdx, me.dhdy,
+        finish_cell<T, CellCtx<T, DX>, EDDY, false, COH>(P, fc, c, g, gx, r, me.h, me.u, me.v, me.dhdx, me.dhdy,
                                                     me.dzdx, me.dzdy, FW, FE, FS, FN, first, last, cur, dt_d, rain,
                                                     removed, walls, xcfl, xmin, vol, &ed);
       }
@@ -1183,6 +1187,231 @@ __global__ void __launch_bounds__(32 * WPB, MINB) sweep_interior_kernel(const __
   const long long i = (long long)blockIdx.x * WPB + threadIdx.y;
   if (i >= P.n_istrips) return;  // whole warp
   sweep_strip_interior<T, TY, P2, EDDY>(P, P.istrips[i]);
+}
+
+// ---------------------------------------------------------------------------------------
+// Interior column sweep with two cells per lane (FP32). One warp sweeps a pair of adjacent
+// interior strips, 2 x kSweepOut = 56 output columns: lane l holds columns gx0 + 2l and
+// gx0 + 2l + 1 (gx0 = the pair's first output column - 2) and loads both as one 8-byte
+// vector per field. Lanes 1-28 write output; lanes 0 and 29 hold the two-column halo; lanes
+// 30-31 hold nothing that is used (their loads are clamped into the mesh). Per pair of cells
+// the x neighbours take three shuffles per field (the left lane's second cell, the right
+// lane's first cell and the left lane's right difference quotient) and the vertical faces
+// eight (the left lane's east face side, the right lane's west face flux), half of what the
+// one-cell sweep needs; the face between a lane's two cells needs none. The arithmetic per
+// face and per cell is the interior sweep's.
+// ---------------------------------------------------------------------------------------
+template <int TY, bool P2, bool EDDY>
+__device__ __forceinline__ void sweep_pair_interior(const StageParams<float>& P, long long gw) {
+  using T = float;
+  using DX = DivX<T, P2>;
+  const Ctl* ctl = P.ctl;
+  const int nx = P.nx, ny = P.ny;
+  const int tiles_x = (nx + kSweepOut - 1) / kSweepOut;
+  const int lane = threadIdx.x;
+  const int tile_x = int(gw % tiles_x), tile_y = int(gw / tiles_x);  // the pair's first strip
+  const int ca = tile_x * kSweepOut - 2 + 2 * lane;                    // columns ca, ca + 1
+  const int lc = min(ca, nx - 2);  // load column: even (nx is even for pairs), inside the mesh
+  const bool out_lane = lane >= 1 && lane <= kSweepOut;
+  const int y0 = tile_y * TY;
+
+  const int cur = ctl->cur;
+  const double dt_d = ctl->dt;
+  const double tsub = ctl->t_local + P.c_s * dt_d;
+  const bool first = P.mode & M_FIRST, last = P.mode & M_LAST;
+  const T* Yh = first ? P.S[cur][0] : P.Yin[0];
+  const T* Yu = first ? P.S[cur][1] : P.Yin[1];
+  const T* Yv = first ? P.S[cur][2] : P.Yin[2];
+  const DX divx = MkDivX<DX>::make(P.dx), divy = MkDivX<DX>::make(P.dy);
+  const T hdx = T(0.5) * T(P.dx), hdy = T(0.5) * T(P.dy);
+  CellCtx<T, DX> c;
+  c.divx = divx; c.divy = divy;
+  c.divdt = mkdiv<T>(dt_d);
+  c.divL = mkdiv<T>(P.L);
+  c.dt = T(dt_d); c.dt_d = dt_d; c.tsub_d = tsub;
+  c.manning = P.manning; c.rain_mode = P.rain_mode; c.head_first = P.head_first;
+  const DevForcing fc = *P.fc;
+  // tile datums: the first cell of a lane can start a datum tile column (the second one, at an
+  // odd column, never does), so only the west face of the first cell crosses tiles in x
+  const bool xcross = P.zdat != nullptr && (ca % kDatumTX) == 0;
+
+  auto ld2 = [&](const T* p, long long g) { return __ldg(reinterpret_cast<const float2*>(p + g)); };
+  auto load_row = [&](int r, RowV<T>& A, RowV<T>& B) {
+    const long long g = (long long)r * nx + lc;
+    float2 t;
+    t = ld2(Yh, g); A.h = t.x; B.h = t.y;
+    t = ld2(Yu, g); A.u = t.x; B.u = t.y;
+    t = ld2(Yv, g); A.v = t.x; B.v = t.y;
+    t = ld2(P.z, g); A.z = t.x; B.z = t.y;
+    t = ld2(P.zx, g); A.zx = t.x; B.zx = t.y;
+    t = ld2(P.zy, g); A.zy = t.x; B.zy = t.y;
+  };
+  auto prefetch_rows = [&](int k) {
+    {
+      const int r = min(k + 1 + kSweepPfWindow, ny - 1);
+      const long long g = (long long)r * nx + lc;
+      prefetch_l1(Yh + g); prefetch_l1(Yu + g); prefetch_l1(Yv + g);
+      prefetch_l1(P.z + g); prefetch_l1(P.zx + g); prefetch_l1(P.zy + g);
+    }
+    const int r = min(k - 2 + kSweepPfCell, ny - 1);
+    const long long g = (long long)r * nx + lc;
+    if (!first) {
+      for (int f = 0; f < 3; ++f) { prefetch_l1(P.S[cur][f] + g); prefetch_l1(P.S[cur ^ 1][f] + g); }
+    }
+    if (P.manning) {
+      for (int f = 0; f < 4; ++f)
+        if (P.man_p[f]) prefetch_l1(P.man_p[f] + g);
+    }
+    if (P.irate) { prefetch_l1(P.irate + g); prefetch_l1(P.icap + g); }
+    if (P.efx) { prefetch_l1(P.efx + g); prefetch_l1(P.efy + g); }
+    if (fc.rain_kind == 3) prefetch_l1(P.pat + g);
+    if (fc.rain_kind == 2) { prefetch_l1(P.q0p + g); prefetch_l1(P.q1p + g); }
+    if (fc.head_kind == 2) { prefetch_l1(P.hb0p + g); prefetch_l1(P.hb1p + g); }
+  };
+  // x slopes of a lane's two cells (values A, B) from their neighbours in the adjacent lanes
+  auto xslopes = [&](T A, T B, T& sa, T& sb) {
+    const T Bl = up1(B);          // column ca - 1
+    const T Ar = dn1(A);          // column ca + 2
+    const T qab = divx(B - A);
+    const T qbr = divx(Ar - B);
+    const T qla = up1(qbr);       // (A - Bl) / dx, formed by the left lane
+    sa = minmod3q<T>(qla, true, qab, true, divx(B - Bl));
+    sb = minmod3q<T>(qab, true, qbr, true, divx(Ar - A));
+  };
+
+  RowV<T> Rm[2] = {}, R0[2] = {}, Rp[2] = {};
+  SlopeV<T> Sm[2] = {}, S0[2] = {};
+  T Smm_uy[2] = {}, Smm_vy[2] = {};
+  T fyA[2][3] = {}, fyB[2][3] = {};
+  FaceF<T> FS[2] = {}, FN[2] = {};
+  double rain = 0.0, removed = 0.0, walls = 0.0, vol = 0.0;
+  T xcfl = T(0), xmin = T(1.0 / 0.0);
+
+  for (int k = y0 - 2; k <= y0 + TY + 1; ++k) {
+    prefetch_rows(k);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) { Rm[j] = R0[j]; R0[j] = Rp[j]; }
+    load_row(k, Rp[0], Rp[1]);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      if constexpr (EDDY) { Smm_uy[j] = Sm[j].uy; Smm_vy[j] = Sm[j].vy; }
+      Sm[j] = S0[j];
+      fyA[j][0] = fyB[j][0]; fyA[j][1] = fyB[j][1]; fyA[j][2] = fyB[j][2];
+      if (k >= y0 - 1) {
+        fyB[j][0] = divy(Rp[j].h - R0[j].h);
+        fyB[j][1] = divy(Rp[j].u - R0[j].u);
+        fyB[j][2] = divy(Rp[j].v - R0[j].v);
+      }
+    }
+    // slopes of row k-1 (State.cpp:187-192), two-sided; the Y axis uses north as the left side
+    if (k >= y0) {
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        S0[j].hy = minmod3q<T>(-fyB[j][0], true, -fyA[j][0], true, divy(Rm[j].h - Rp[j].h));
+        S0[j].uy = minmod3q<T>(-fyB[j][1], true, -fyA[j][1], true, divy(Rm[j].u - Rp[j].u));
+        S0[j].vy = minmod3q<T>(-fyB[j][2], true, -fyA[j][2], true, divy(Rm[j].v - Rp[j].v));
+      }
+      xslopes(R0[0].h, R0[1].h, S0[0].hx, S0[1].hx);
+      xslopes(R0[0].u, R0[1].u, S0[0].ux, S0[1].ux);
+      xslopes(R0[0].v, R0[1].v, S0[0].vx, S0[1].vx);
+    }
+    // horizontal faces between rows k-2 and k-1 (face row fy = k-1), Fluxes.cpp:55-64
+    if (k >= y0 + 1 && out_lane) {
+      const int fy = k - 1;
+      double dz = 0.0;
+      const bool ycross = P.zdat != nullptr && (fy % kDatumTY) == 0;
+      if (ycross) {  // both cells of the lane lie in one datum tile column
+        const long long tb = datum_tile(ca, fy, P.dtiles_x);
+        dz = P.zdat[tb] - P.zdat[tb - P.dtiles_x];
+      }
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const CellV<T> lo = mkcell(Rm[j], Sm[j]);
+        CellV<T> hi = mkcell(R0[j], S0[j]);
+        if (ycross) hi.z = T(double(hi.z) + dz);
+        face_combine<T, 1>(side_m<T, 1, false>(lo, hdy), side_p<T, 1, false>(hi, hdy), divy, FN[j]);
+      }
+    }
+    // output row k-2
+    if (k >= y0 + 2) {
+      const int r = k - 2;
+      const CellV<T> meA = mkcell(Rm[0], Sm[0]), meB = mkcell(Rm[1], Sm[1]);
+      EddyIn<T> ed[2] = {};
+      if constexpr (EDDY) {
+        if (P.eddy) {  // second derivatives of row r: x from the lanes' slopes, y from rows r+1, r, r-1
+#pragma unroll
+          for (int j = 0; j < 2; ++j) {
+            ed[j].ux = Sm[j].ux; ed[j].uy = Sm[j].uy; ed[j].vx = Sm[j].vx; ed[j].vy = Sm[j].vy;
+            ed[j].uyy = minmod3q<T>(divy(Sm[j].uy - S0[j].uy), true, divy(Smm_uy[j] - Sm[j].uy), true,
+                                    divy(Smm_uy[j] - S0[j].uy));
+            ed[j].vyy = minmod3q<T>(divy(Sm[j].vy - S0[j].vy), true, divy(Smm_vy[j] - Sm[j].vy), true,
+                                    divy(Smm_vy[j] - S0[j].vy));
+          }
+          xslopes(Sm[0].ux, Sm[1].ux, ed[0].uxx, ed[1].uxx);
+          xslopes(Sm[0].vx, Sm[1].vx, ed[0].vxx, ed[1].vxx);
+        }
+      }
+      // west face of the first cell: the left lane's second cell's east side against it
+      const Side<T> eB = side_m<T, 0, false>(meB, hdx);
+      const Side<T> wA{up1(eB.zb), up1(eB.h), up1(eB.un), up1(eB.ut)};
+      CellV<T> meAW = meA;
+      if (xcross) {
+        const long long tb = datum_tile(ca, r, P.dtiles_x);
+        meAW.z = T(double(meA.z) + (P.zdat[tb] - P.zdat[tb - 1]));
+      }
+      FaceF<T> FWa, Fab;
+      face_combine<T, 0>(wA, side_p<T, 0, false>(meAW, hdx), divx, FWa);
+      // the face between the lane's two cells
+      face_combine<T, 0>(side_m<T, 0, false>(meA, hdx), side_p<T, 0, false>(meB, hdx), divx, Fab);
+      // east face of the second cell: the right lane's west face
+      const FaceF<T> FEb{dn1(FWa.h), dn1(FWa.u), dn1(FWa.v), dn1(FWa.z)};
+      if (out_lane) {
+        const long long g = (long long)r * nx + ca;
+        finish_cell<T, CellCtx<T, DX>, EDDY, false>(P, fc, c, g, ca, r, meA.h, meA.u, meA.v, meA.dhdx, meA.dhdy,
+                                                    meA.dzdx, meA.dzdy, FWa, Fab, FS[0], FN[0], first, last, cur,
+                                                    dt_d, rain, removed, walls, xcfl, xmin, vol, &ed[0]);
+        finish_cell<T, CellCtx<T, DX>, EDDY, false>(P, fc, c, g + 1, ca + 1, r, meB.h, meB.u, meB.v, meB.dhdx,
+                                                    meB.dhdy, meB.dzdx, meB.dzdy, Fab, FEb, FS[1], FN[1], first, last,
+                                                    cur, dt_d, rain, removed, walls, xcfl, xmin, vol, &ed[1]);
+      }
+    }
+    FS[0] = FN[0];
+    FS[1] = FN[1];
+  }
+  // the pair's partials go to its first strip's slot; the second strip's slot gets the
+  // identities (max 0, min +inf, sums 0)
+  if (last && !(P.mode & M_DEBUGK)) {
+    double mx = warp_max(double(xcfl)), mn = warp_min(double(xmin)), vs = warp_sum<T>(vol);
+    if (lane == 0) {
+      P.part[gw] = mx;
+      P.part[P.nblk + gw] = mn;
+      P.part[2 * P.nblk + gw] = vs;
+      P.part[gw + 1] = 0.0;
+      P.part[P.nblk + gw + 1] = 1.0 / 0.0;
+      P.part[2 * P.nblk + gw + 1] = 0.0;
+    }
+  }
+  if (P.mode & M_TALLY) {
+    double rs = warp_sum<T>(rain), os = warp_sum<T>(removed), ws = warp_sum<T>(walls);
+    if (lane == 0) {
+      P.part[(3 + 3LL * P.stage) * P.nblk + gw] = rs;
+      P.part[(4 + 3LL * P.stage) * P.nblk + gw] = os;
+      P.part[(5 + 3LL * P.stage) * P.nblk + gw] = ws;
+      P.part[(3 + 3LL * P.stage) * P.nblk + gw + 1] = 0.0;
+      P.part[(4 + 3LL * P.stage) * P.nblk + gw + 1] = 0.0;
+      P.part[(5 + 3LL * P.stage) * P.nblk + gw + 1] = 0.0;
+    }
+  }
+}
+
+// The two-cells-per-lane interior sweep over the strip pairs in P.ipairs (each entry the
+// pair's first strip).
+template <int TY, int WPB, int MINB, bool P2, bool EDDY>
+__global__ void __launch_bounds__(32 * WPB, MINB) sweep_pair_kernel(const __grid_constant__ StageParams<float> P) {
+  if (P.ctl->done) return;
+  const long long i = (long long)blockIdx.x * WPB + threadIdx.y;
+  if (i >= P.n_ipairs) return;  // whole warp
+  sweep_pair_interior<TY, P2, EDDY>(P, P.ipairs[i]);
 }
 
 // Batched column sweep: the strips of every instance of a batch, warp_start[i] being the
@@ -1645,7 +1874,15 @@ __global__ void __launch_bounds__(32 * kPersistWarps, 4) persist_batch_kernel(co
         unsigned* dst = reinterpret_cast<unsigned*>(&Psh[wib]);
         for (int i = lane; i < int(sizeof(StageParams<T>) / 4); i += 32) dst[i] = src[i];
         __syncwarp();
-        sweep_strip<T, kPersistRows, P2, EDDY, true>(Psh[wib], (long long)(t - base));
+        // the member's interior strips (listed first) run the interior sweep
+        const StageParams<T>& SP = Psh[wib];
+        const long long item = (long long)(t - base);
+        if (SP.istrips && item < SP.n_istrips)
+          sweep_strip_interior<T, kPersistRows, P2, EDDY, true>(SP, SP.istrips[item]);
+        else if (SP.bstrips)
+          sweep_strip<T, kPersistRows, P2, EDDY, true>(SP, SP.bstrips[item - SP.n_istrips]);
+        else
+          sweep_strip<T, kPersistRows, P2, EDDY, true>(SP, item);
         __syncwarp();
       } else {
         finalize_warp(PP.Fs[k], red[wib]);

@@ -20,24 +20,30 @@ template <typename T> cudaError_t launch_stage(const StageParams<T>& P, int tile
 // Stage-kernel variants, in two schedules:
 //  fused (one pass per RK stage): 0..3 the tiled shared-memory kernel with kTiles[v]; 4..10
 //   the column-sweep kernel with 16 / 32 / 64 / 32 / 32 / 32 / 32 output rows per warp, the
-//   last four with register caps for 3, 4, 5 and 6 resident 4-warp blocks per SM;
+//   last four with register caps for 3, 4, 5 and 6 resident 4-warp blocks per SM; 12, 13
+//   (FP32 only) the column sweep of 32-row strips whose interior strip pairs run two cells
+//   per lane (sweep_pair_kernel), with register caps for 3 and 4 blocks per SM;
 //  split (two passes per RK stage): 11 the slopes pass (slopes_kernel) then the tiled 32 x 8
 //   kernel at 3 CTAs/SM reading those slopes.
-constexpr int kNumVariants = 12;
+constexpr int kNumVariants = 14;
 constexpr int kSplitVariant = 11;
 constexpr int kSweepRows[7] = {16, 32, 64, 32, 32, 32, 32};
-inline bool variant_is_sweep(int v) { return v >= 4 && v <= 10; }
+inline bool variant_is_pair(int v) { return v == 12 || v == 13; }
+inline bool variant_is_sweep(int v) { return (v >= 4 && v <= 10) || variant_is_pair(v); }
 inline bool variant_is_split(int v) { return v == kSplitVariant; }
+// column-sweep variants: output rows per strip (0 for the other variants)
+inline int variant_sweep_rows(int v) {
+  if (v >= 4 && v <= 10) return kSweepRows[v - 4];
+  return variant_is_pair(v) ? 32 : 0;
+}
 // per-CTA (tiled) or per-warp (sweep) partial count
 inline long long variant_partials(int v, long long nx, long long ny) {
   if (v == kSplitVariant) v = 1;  // the split schedule's stage pass is the tiled 32 x 8 kernel
   if (v < 4) return ((nx + kTiles[v].tx - 1) / kTiles[v].tx) * ((ny + kTiles[v].ty - 1) / kTiles[v].ty);
-  const long long ty = kSweepRows[v - 4];
+  const long long ty = variant_sweep_rows(v);
   return ((nx + kSweepOut - 1) / kSweepOut) * ((ny + ty - 1) / ty);
 }
 template <typename T> cudaError_t launch_variant(const StageParams<T>& P, int variant, cudaStream_t s);
-// column-sweep variants: output rows per strip (0 for the other variants)
-inline int variant_sweep_rows(int v) { return variant_is_sweep(v) ? kSweepRows[v - 4] : 0; }
 // per-strip interior flags of the column sweep with `ty` output rows (strip_flags_kernel)
 template <typename T> cudaError_t launch_strip_flags(const T* z, int nx, int ny, int ty, long long nstrips,
                                                      unsigned char* flags, cudaStream_t s);

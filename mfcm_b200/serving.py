@@ -1,12 +1,14 @@
 """Continuous-batching flood-solve server.
 
 Requests (a catchment, its rainfall and a simulated horizon) arrive at wall-clock times. Each
-request is admitted into one running batch (mfcm_b200.batch) as soon as a slot and its device
-memory fit under the budget. The batch advances every running request by a few steps per
-call (`steps_per_advance`), each request at its own pace; admission happens between calls,
-so requests that arrive while others are on the GPU join the same launches. A request leaves the batch when its
-horizon is reached, freeing its memory for the queue. Each request's results are
-bit-identical whether it runs alone or in the mix (members never share state).
+request is prepared as soon as a slot and its device memory fit under the budget: a thread
+creates its solver and uploads its bed while the batch (mfcm_b200.batch) advances the others.
+The batch advances every running request by a few steps per call (`steps_per_advance`), each
+request at its own pace; prepared requests join it between calls (sv_batch_adopt), so
+requests that arrive while others are on the GPU join the next launches without waiting for
+their own set-up. A request leaves the batch when its horizon is reached, freeing its memory
+for the queue. Each request's results are bit-identical whether it runs alone or in the mix
+(members never share state).
 
 A request whose solve fails is failed alone: a member whose time turns NaN, or which takes
 more than `step_limit` timesteps within one step (the reference's thin-film velocity
@@ -16,13 +18,15 @@ while the rest of the batch completes the same step.
 The reference has no serving layer; this is a production serving pattern built on the same
 step (one `step()` of TypedTemporalScheme per batch advance, per member).
 """
+import collections
 import math
+import threading
 import time
 from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import synth, TimeSeries, start_new_step_forcing, RAIN_UNIFORM
+from . import synth, SaintVenantSolver, TimeSeries, start_new_step_forcing, RAIN_UNIFORM
 from .batch import SaintVenantBatch
 from ._abi import SV_E_NONFINITE
 
@@ -112,9 +116,13 @@ def at_rate(requests, rate, seed=0):
 
 
 class FloodServer:
-    """persistent: each batch advance is one persistent cooperative launch (every running
-    request at its own dt, idle warps taking work from any request); else one launch per RK
-    stage and one per timestep's reductions, replayed as a graph."""
+    """Requests are prepared off the batch's path: a preparation thread creates each arriving
+    request's solver and uploads its bed and roughness on the solver's own stream while the
+    batch advances; between advances the main loop adopts every prepared solver into the
+    batch (sv_batch_adopt), so an arrival waits for the current advance to end, not for its
+    own preparation. persistent: each batch advance is one persistent cooperative launch
+    (every running request at its own dt, idle warps taking work from any request); else one
+    launch per RK stage and one per timestep's reductions, replayed as a graph."""
 
     def __init__(self, budget_bytes=150e9, max_slots=512, precision="f32", step_duration=60.0, cn_target=0.5,
                  device=0, step_limit=20000, steps_per_advance=4, persistent=False):
@@ -122,8 +130,10 @@ class FloodServer:
         self.batch.set_step_limit(step_limit)
         if persistent:
             self.batch.set_persistent(True)
+        self.precision = precision
+        self.device = int(device)
         # steps each running request advances per batched launch sequence: members run them
-        # back to back at their own pace; new arrivals are admitted between sequences
+        # back to back at their own pace; new arrivals are adopted between sequences
         self.steps_per_advance = int(steps_per_advance)
         self.budget = float(budget_bytes)
         self.max_slots = int(max_slots)
@@ -140,87 +150,135 @@ class FloodServer:
         tiles = math.ceil(req.nx / 32) * math.ceil(req.ny / 8)
         return cells * self.value_bytes * 16 + tiles * 11 * 8 + 4096
 
-    def _admit(self, req, now):
-        m = self.batch.add(req.nx, req.ny, req.dx, cn_target=self.cn_target, step_duration=self.L,
-                           rain_mode="physical")
-        m.set_field("Z", req.z)
-        zero = np.zeros((req.ny, req.nx))
-        m.set_field("H", zero)
-        m.set_field("U", zero)
-        m.set_field("V", zero)
-        m.set_manning(req.n, req.n, 0.1, 0.3)
-        req.admitted = now
-        return m
+    def _prepare(self, req):
+        """The request as a solver of its own: bed and roughness uploaded on its own stream; the
+        state starts dry and still (the library zeroes it)."""
+        s = SaintVenantSolver(req.nx, req.ny, req.dx, precision=self.precision, cn_target=self.cn_target,
+                              step_duration=self.L, rain_mode="physical", device=self.device)
+        s.set_field("Z", req.z)
+        s.set_manning(req.n, req.n, 0.1, 0.3)
+        return s
 
     def run(self, requests, time_limit=None):
         """Serve `requests` (sorted by arrival). Returns a summary dict; the requests carry
         their own timings and results."""
-        pending = sorted(requests, key=lambda r: r.arrival)
-        active = {}   # slot -> (request, member, simulated time)
-        used = 0.0
+        pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
+        ready = []                     # (request, solver) prepared, waiting for adoption
+        lock = threading.Lock()
+        wake, freed, stop = threading.Event(), threading.Event(), threading.Event()
+        shared = {"used": 0.0, "slots": 0, "error": None}
         t0 = time.perf_counter()
+
+        def preparer():
+            try:
+                while pending and not stop.is_set():
+                    req = pending[0]
+                    delay = req.arrival - (time.perf_counter() - t0)
+                    if delay > 0:
+                        stop.wait(min(delay, 0.05))
+                        continue
+                    need = self.estimate_bytes(req)
+                    with lock:  # a request larger than the budget still runs once nothing else holds memory
+                        fits = shared["slots"] < self.max_slots and (
+                            shared["used"] + need <= self.budget or shared["slots"] == 0)
+                        if fits:
+                            shared["used"] += need
+                            shared["slots"] += 1
+                    if not fits:
+                        freed.wait(0.05)
+                        freed.clear()
+                        continue
+                    pending.popleft()
+                    solver = self._prepare(req)
+                    with lock:
+                        ready.append((req, solver))
+                    wake.set()
+            except Exception as e:  # reported by the main loop
+                shared["error"] = e
+                wake.set()
+
+        worker = threading.Thread(target=preparer, daemon=True)
+        worker.start()
+        active = {}   # slot -> [request, member, simulated time]
         total_updates = 0
         max_active = 0
-        while pending or active:
-            now = time.perf_counter() - t0
-            if time_limit is not None and now > time_limit:
-                break
-            while pending and pending[0].arrival <= now and len(active) < self.max_slots:
-                need = self.estimate_bytes(pending[0])
-                if used + need > self.budget and active:
-                    break  # wait for memory to free up
-                req = pending.pop(0)
-                m = self._admit(req, now)
-                active[m.slot] = [req, m, 0.0]
-                used += need
-            max_active = max(max_active, len(active))
-            if not active:
-                time.sleep(max(0.0, min(0.05, pending[0].arrival - now)))
-                continue
-            queued = {}
-            for slot, (req, m, t) in active.items():
-                left = max(1, math.ceil((req.horizon - t) / self.L - 1e-9))
-                queued[m] = [start_new_step_forcing(t + i * self.L, self.L, rain=req.rain, rain_kind=RAIN_UNIFORM,
-                                                    head=0.0, head_edges=req.head_edges)
-                             for i in range(min(self.steps_per_advance, left))]
-            res = self.batch.advance_steps(queued, raise_on_error=False)
-            now = time.perf_counter() - t0
-            done = []
-            for slot, entry in active.items():
-                req, m, t = entry
-                r = res[slot]
-                for st in r["steps"]:
-                    req.cell_updates += st["accepted"] * req.nx * req.ny
-                    total_updates += st["accepted"] * req.nx * req.ny
-                req.steps += len(r["steps"])
-                entry[2] = t + self.L * len(r["steps"])
-                if r["status"] != 0:
-                    req.error = ("time became NaN" if r["status"] == SV_E_NONFINITE else
-                                 "step limit reached (dt collapsed)")
-                    req.stats = m.stats()
-                    req.finished = time.perf_counter() - t0
-                    done.append(slot)
-                elif entry[2] >= req.horizon - 1e-9:
-                    req.result_h = m.get_field("H")
-                    req.stats = m.stats()
-                    req.finished = time.perf_counter() - t0
-                    done.append(slot)
-            for slot in done:
-                req, m, _ = active.pop(slot)
-                self.batch.remove(m)
-                used -= self.estimate_bytes(req)
+        try:
+            while True:
+                now = time.perf_counter() - t0
+                if time_limit is not None and now > time_limit:
+                    break
+                if shared["error"] is not None:
+                    raise shared["error"]
+                with lock:
+                    joining = list(ready)
+                    ready.clear()
+                for req, solver in joining:
+                    m = self.batch.adopt(solver)
+                    req.admitted = now
+                    active[m.slot] = [req, m, 0.0]
+                max_active = max(max_active, len(active))
+                if not active:
+                    if not pending and not ready and not worker.is_alive():
+                        break
+                    wake.wait(0.05)
+                    wake.clear()
+                    continue
+                queued = {}
+                for slot, (req, m, t) in active.items():
+                    left = max(1, math.ceil((req.horizon - t) / self.L - 1e-9))
+                    queued[m] = [start_new_step_forcing(t + i * self.L, self.L, rain=req.rain,
+                                                        rain_kind=RAIN_UNIFORM, head=0.0, head_edges=req.head_edges)
+                                 for i in range(min(self.steps_per_advance, left))]
+                res = self.batch.advance_steps(queued, raise_on_error=False)
+                done = []
+                for slot, entry in active.items():
+                    req, m, t = entry
+                    r = res[slot]
+                    for st in r["steps"]:
+                        req.cell_updates += st["accepted"] * req.nx * req.ny
+                        total_updates += st["accepted"] * req.nx * req.ny
+                    req.steps += len(r["steps"])
+                    entry[2] = t + self.L * len(r["steps"])
+                    if r["status"] != 0:
+                        req.error = ("time became NaN" if r["status"] == SV_E_NONFINITE else
+                                     "step limit reached (dt collapsed)")
+                        req.stats = m.stats()
+                        req.finished = time.perf_counter() - t0
+                        done.append(slot)
+                    elif entry[2] >= req.horizon - 1e-9:
+                        req.result_h = m.get_field("H")
+                        req.stats = m.stats()
+                        req.finished = time.perf_counter() - t0
+                        done.append(slot)
+                for slot in done:
+                    req, m, _ = active.pop(slot)
+                    self.batch.remove(m)
+                    with lock:
+                        shared["used"] -= self.estimate_bytes(req)
+                        shared["slots"] -= 1
+                    freed.set()
+        finally:
+            stop.set()
+            worker.join()
+            with lock:
+                leftover = list(ready)
+                ready.clear()
+            for _, solver in leftover:  # prepared but never adopted (time limit)
+                solver.close()
         wall = time.perf_counter() - t0
         lat = np.array([r.latency for r in requests if not math.isnan(r.finished) and r.error is None])
         failures = {}
         for r in requests:
             if r.error is not None:
                 failures[r.error] = failures.get(r.error, 0) + 1
+        admit_wait = [r.admitted - r.arrival for r in requests if not math.isnan(r.admitted)]
         return {
             "requests": len(requests), "completed": int(lat.size),
             "failed": sum(1 for r in requests if r.error is not None), "wall_s": wall,
             "p50_s": float(np.percentile(lat, 50)) if lat.size else None,
             "p95_s": float(np.percentile(lat, 95)) if lat.size else None,
             "p99_s": float(np.percentile(lat, 99)) if lat.size else None,
+            "admission_wait_p50_s": float(np.percentile(admit_wait, 50)) if admit_wait else None,
             "cell_updates_per_s": total_updates / wall if wall > 0 else 0.0,
             "max_concurrent": max_active, "failures": failures,
         }

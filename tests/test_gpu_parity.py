@@ -139,7 +139,7 @@ def test_interior_strips_every_sweep_variant(variant, nan_cells):
 
 
 @pytest.mark.parametrize("precision", ["f32", "f32_datum64"])
-@pytest.mark.parametrize("variant", [4, 5, 9])
+@pytest.mark.parametrize("variant", [4, 5, 9, 12, 13])
 def test_fp32_interior_strips_close_to_fp64(precision, variant):
     """The FP32 interior kernel (no tangential finiteness tests) against the FP64 oracle."""
     nx, ny, dx = 200, 180, 5.0
@@ -215,7 +215,7 @@ def test_autotune_keeps_state_and_bits():
         setup(b, z, h, u, v)
     before = g.get_field("H")
     best = g.autotune()
-    assert 0 <= best < 9
+    assert 0 <= best < 12  # FP64 solvers never take the FP32-only variants 12-13
     assert same(before, g.get_field("H"))
     g.advance(); o.advance()
     for f in ("H", "U", "V"):
@@ -246,3 +246,62 @@ def test_mass_balance_closure_and_tallies(precision, tol):
         so = res[1][0]
         for k in ("rain_in", "outflow", "wall_in"):
             assert abs(s[k] - so[k]) <= 1e-12 * max(abs(so[k]), 1e-300), (k, s[k], so[k])
+
+
+@pytest.mark.parametrize("precision", ["f32", "f32_datum64"])
+@pytest.mark.parametrize("shape", [(232, 170), (231, 170), (290, 97), (58, 40)])
+@pytest.mark.parametrize("eddy,nan_cells", [(False, 0), (True, 0), (False, 5)])
+def test_fp32_two_cells_per_lane_matches_one_cell_sweep(precision, shape, eddy, nan_cells):
+    """Variants 12-13 sweep pairs of interior strips with two cells per lane and 8-byte loads;
+    the arithmetic per face and cell is the one-cell interior sweep's (variants 7-8, same strip
+    height and register caps), so the fields after a timestep agree to FP32 rounding. Odd row
+    lengths and meshes too narrow for a pair have no pairs and give the one-cell results bit for
+    bit. Coded-out cells move strips out of pairs. The pairs' reductions (CFL, volume,
+    tallies) are checked through the controller and the mass balance of a whole step."""
+    nx, ny = shape
+    z, h, u, v = wet_dry_state(nx, ny, 2.0, seed=nx + ny + nan_cells, nan_cells=nan_cells)
+    out = {}
+    for variant in (7, 12, 8, 13):
+        g = SaintVenantSolver(nx, ny, 2.0, precision=precision, cn_target=0.5, step_duration=3.0,
+                              rain_mode="physical")
+        g.set_kernel_variant(variant)
+        setup(g, z, h, u, v, n=(0.03, 0.06, 0.1, 0.3))
+        if eddy:
+            g.set_eddy_viscosity("smagorinsky", mu=1.0, mu_const=0.05, mu_smag=0.5)
+        g.set_forcing(forcing((2e-5, 1e-5), head=(0.01, 0.0), edges=EDGE_XMIN | EDGE_YMAX))
+        v0 = g.stats()["volume"]
+        cn, rep, nd = g.do_timestep(0.5, 0.02)
+        fields = [g.get_field(100 + 12 + f) for f in range(3)]
+        st = None
+        if not nan_cells:  # coded-out beds make the step non-finite in the reference arithmetic
+            g.accept()
+            g.advance()
+            st = g.stats()
+        out[variant] = (cn, fields, st, v0)
+        g.close()
+    no_pairs = nx % 2 == 1 or nx < 2 * 28 + 32
+    for single, pair_v in ((7, 12), (8, 13)):
+        cn1, f1, s1, v0 = out[single]
+        cn2, f2, s2, _ = out[pair_v]
+        for a, b in zip(f1, f2):
+            if no_pairs:
+                assert np.array_equal(a, b, equal_nan=True)
+            else:
+                fin = np.isfinite(a)
+                assert np.array_equal(fin, np.isfinite(b))
+                np.testing.assert_allclose(b[fin], a[fin], rtol=2e-6, atol=2e-7)
+        if nan_cells:
+            continue
+        assert abs(cn2 - cn1) <= 1e-5 * abs(cn1)
+        # the pair kernel's tallies close its mass balance like the one-cell sweep's
+        for st in (s1, s2):
+            closure = st["volume"] - (v0 + st["rain_in"] - st["outflow"] + st["wall_in"])
+            assert abs(closure) <= 1e-5 * abs(st["volume"]), (closure, st)
+
+
+def test_two_cells_per_lane_variants_are_fp32_only():
+    g = SaintVenantSolver(64, 40, 2.0)
+    for variant in (12, 13):
+        with pytest.raises(Exception):
+            g.set_kernel_variant(variant)
+    g.close()

@@ -69,3 +69,29 @@ def test_persistent_serving_matches_solo_runs():
     assert summary["max_concurrent"] >= 2
     for r in reqs[:4]:
         assert same(r.result_h, _alone(r, 1, precision="f64")), f"request {r.rid} differs from its solo run"
+
+
+def test_adopted_solver_matches_its_solo_run():
+    """A solver filled on its own and adopted by a batch (the server's preparation path) runs
+    as a member bit for bit like its solo run; precision mismatches are refused."""
+    from mfcm_b200.batch import SaintVenantBatch
+    req = make_requests(rate=1.0, count=1, seed=3, side=(48, 48), horizon=(120.0, 120.0))[0]
+    b = SaintVenantBatch("f64")
+    wrong = SaintVenantSolver(16, 16, 1.0, precision="f32")
+    with pytest.raises(ValueError):
+        b.adopt(wrong)
+    wrong.close()
+    s = SaintVenantSolver(req.nx, req.ny, req.dx, precision="f64", cn_target=0.5, step_duration=60.0,
+                          rain_mode="physical")
+    s.set_field("Z", req.z)
+    s.set_manning(req.n, req.n, 0.1, 0.3)
+    m = b.adopt(s)
+    assert s._h is None and b.size()[0] == 1
+    t = 0.0
+    while t < req.horizon - 1e-9:
+        b.advance_steps({m: [start_new_step_forcing(t, 60.0, rain=req.rain, rain_kind=RAIN_UNIFORM, head=0.0,
+                                                    head_edges=req.head_edges)]})
+        t += 60.0
+    h = m.get_field("H")
+    b.close()
+    assert same(h, _alone(req, 1, precision="f64"))
