@@ -3,6 +3,7 @@
 #pragma once
 #include <atomic>
 #include <cmath>
+#include <utility>
 
 #include "sv_launch.h"
 
@@ -80,45 +81,66 @@ template <> cudaError_t launch_stage<SV_T>(const StageParams<SV_T>& P, int tile,
   }
 }
 
+// A sweep launch of a stage after the first: allowed to start while the one before it runs
+// (programmatic dependent launch; the sweeps of one stage touch disjoint outputs)
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_overlapped(void (*kern)(KArgs...), dim3 grid, dim3 block, cudaStream_t s, bool overlap,
+                                     Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = overlap ? attr : nullptr;
+  cfg.numAttrs = overlap ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
 template <typename T, int TY, int MINB, bool PAIR = false>
 static cudaError_t launch_sweep_t(const StageParams<T>& P, int variant, cudaStream_t s) {
   constexpr int WPB = 4;
   const long long ntiles = variant_partials(variant, P.nx, P.ny);
   dim3 block(32, WPB);
   const bool p2 = pow2_mesh(P.dx, P.dy);
+  bool overlap = false;  // the first launch of the stage waits for the previous stage
+  cudaError_t e = cudaSuccess;
+  // the general sweep over the edge and coded-out strips (every strip without lists) first:
+  // few warps, each slower than an interior one, so it runs beside the interior launches
+  const long long ngen = P.bstrips ? P.n_bstrips : ntiles;
+  if (ngen > 0) {
+    dim3 grid(unsigned((ngen + WPB - 1) / WPB));
+    void (*k)(const StageParams<T>) =
+        P.eddy ? (p2 ? sweep_kernel<T, TY, WPB, MINB, true, true> : sweep_kernel<T, TY, WPB, MINB, false, true>)
+               : (p2 ? sweep_kernel<T, TY, WPB, MINB, true, false> : sweep_kernel<T, TY, WPB, MINB, false, false>);
+    e = launch_overlapped(k, grid, block, s, overlap, P);
+    if (e != cudaSuccess) return e;
+    overlap = true;
+  }
   // interior strip pairs (FP32, if listed) two cells per lane
   if constexpr (PAIR && sizeof(T) == 4) {
     if (P.ipairs && P.n_ipairs > 0) {
       dim3 grid(unsigned((P.n_ipairs + WPB - 1) / WPB));
-      if (P.eddy) {
-        if (p2) sweep_pair_kernel<TY, WPB, MINB, true, true><<<grid, block, 0, s>>>(P);
-        else sweep_pair_kernel<TY, WPB, MINB, false, true><<<grid, block, 0, s>>>(P);
-      } else {
-        if (p2) sweep_pair_kernel<TY, WPB, MINB, true, false><<<grid, block, 0, s>>>(P);
-        else sweep_pair_kernel<TY, WPB, MINB, false, false><<<grid, block, 0, s>>>(P);
-      }
+      void (*k)(const StageParams<float>) =
+          P.eddy ? (p2 ? sweep_pair_kernel<TY, WPB, MINB, true, true> : sweep_pair_kernel<TY, WPB, MINB, false, true>)
+                 : (p2 ? sweep_pair_kernel<TY, WPB, MINB, true, false> : sweep_pair_kernel<TY, WPB, MINB, false, false>);
+      e = launch_overlapped(k, grid, block, s, overlap, P);
+      if (e != cudaSuccess) return e;
+      overlap = true;
     }
   }
-  // interior strips (if listed) in the interior kernel, the rest in the general one
+  // interior strips (if listed) in the interior kernel
   if (P.istrips && P.n_istrips > 0) {
     dim3 grid(unsigned((P.n_istrips + WPB - 1) / WPB));
-    if (P.eddy) {
-      if (p2) sweep_interior_kernel<T, TY, WPB, MINB, true, true><<<grid, block, 0, s>>>(P);
-      else sweep_interior_kernel<T, TY, WPB, MINB, false, true><<<grid, block, 0, s>>>(P);
-    } else {
-      if (p2) sweep_interior_kernel<T, TY, WPB, MINB, true, false><<<grid, block, 0, s>>>(P);
-      else sweep_interior_kernel<T, TY, WPB, MINB, false, false><<<grid, block, 0, s>>>(P);
-    }
-  }
-  const long long ngen = P.bstrips ? P.n_bstrips : ntiles;
-  if (ngen <= 0) return cudaGetLastError();
-  dim3 grid(unsigned((ngen + WPB - 1) / WPB));
-  if (P.eddy) {
-    if (p2) sweep_kernel<T, TY, WPB, MINB, true, true><<<grid, block, 0, s>>>(P);
-    else sweep_kernel<T, TY, WPB, MINB, false, true><<<grid, block, 0, s>>>(P);
-  } else {
-    if (p2) sweep_kernel<T, TY, WPB, MINB, true, false><<<grid, block, 0, s>>>(P);
-    else sweep_kernel<T, TY, WPB, MINB, false, false><<<grid, block, 0, s>>>(P);
+    void (*k)(const StageParams<T>) =
+        P.eddy ? (p2 ? sweep_interior_kernel<T, TY, WPB, MINB, true, true>
+                     : sweep_interior_kernel<T, TY, WPB, MINB, false, true>)
+               : (p2 ? sweep_interior_kernel<T, TY, WPB, MINB, true, false>
+                     : sweep_interior_kernel<T, TY, WPB, MINB, false, false>);
+    e = launch_overlapped(k, grid, block, s, overlap, P);
+    if (e != cudaSuccess) return e;
   }
   return cudaGetLastError();
 }

@@ -690,29 +690,8 @@ constexpr unsigned kFull = 0xffffffffu;
 template <typename T> __device__ __forceinline__ T up1(T v) { return __shfl_up_sync(kFull, v, 1); }
 template <typename T> __device__ __forceinline__ T dn1(T v) { return __shfl_down_sync(kFull, v, 1); }
 
-// Minmod3 (Minmod3.hpp:22-84) from difference quotients qL = (Uc-Ul)/d, qR = (Ur-Uc)/d and
-// qC = (Ur-Ul)/d of a uniform axis (see minmod3 in sv_device.cuh for the exactness notes).
-template <typename T>
-__device__ __forceinline__ T minmod3q(T qL, bool hasL, T qR, bool hasR, T qC) {
-  T outer, central;
-  if (hasL && hasR) {
-    T lhs = T(2) * qL, rhs = T(2) * qR;
-    central = qC * T(0.5);
-    if (lhs != lhs) outer = rhs;
-    else if (rhs != rhs) outer = lhs;
-    else outer = T(0.5) * (ssign(lhs) + ssign(rhs)) * smin(sfabs(lhs), sfabs(rhs));
-  } else if (hasR) {
-    outer = T(2) * qR;
-    central = qR;
-  } else if (hasL) {
-    outer = T(2) * qL;
-    central = qL;
-  } else {
-    return T(0);
-  }
-  if (outer != outer) return central;
-  return T(0.5) * (ssign(outer) + ssign(central)) * smin(sfabs(outer), sfabs(central));
-}
+// The sweeps form slopes with svd::minmod3q (sv_device.cuh): Minmod3 from difference
+// quotients, its sign and NaN tests on the integer pipe.
 
 template <typename T> struct RowV { T h, u, v, z, zx, zy; };
 template <typename T> struct SlopeV { T hx, ux, vx, hy, uy, vy; };
@@ -1164,9 +1143,18 @@ __device__ __forceinline__ void sweep_strip_interior(const StageParams<T>& P, lo
   }
 }
 
+// The column sweeps of one stage are split over disjoint strip lists (general, interior,
+// interior pairs) that read the same inputs and write disjoint cells and partial slots. Each
+// of them lets the launch queued after it start at once (programmatic dependent launch: the
+// launcher marks the next sweep of the same stage as allowed to overlap), so the small
+// general launch over the edge strips runs beside the interior ones instead of as a tail. A
+// launch not marked that way (the next stage, the finalize) still waits for all of them.
+__device__ __forceinline__ void allow_overlap() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // The general column sweep over the strips in P.bstrips (every strip when the list is null).
 template <typename T, int TY, int WPB, int MINB, bool P2, bool EDDY>
 __global__ void __launch_bounds__(32 * WPB, MINB) sweep_kernel(const __grid_constant__ StageParams<T> P) {
+  allow_overlap();
   if (P.ctl->done) return;
   const long long i = (long long)blockIdx.x * WPB + threadIdx.y;
   long long gw = i;
@@ -1183,6 +1171,7 @@ __global__ void __launch_bounds__(32 * WPB, MINB) sweep_kernel(const __grid_cons
 // The interior column sweep over the strips in P.istrips.
 template <typename T, int TY, int WPB, int MINB, bool P2, bool EDDY>
 __global__ void __launch_bounds__(32 * WPB, MINB) sweep_interior_kernel(const __grid_constant__ StageParams<T> P) {
+  allow_overlap();
   if (P.ctl->done) return;
   const long long i = (long long)blockIdx.x * WPB + threadIdx.y;
   if (i >= P.n_istrips) return;  // whole warp
@@ -1408,6 +1397,7 @@ __device__ __forceinline__ void sweep_pair_interior(const StageParams<float>& P,
 // pair's first strip).
 template <int TY, int WPB, int MINB, bool P2, bool EDDY>
 __global__ void __launch_bounds__(32 * WPB, MINB) sweep_pair_kernel(const __grid_constant__ StageParams<float> P) {
+  allow_overlap();
   if (P.ctl->done) return;
   const long long i = (long long)blockIdx.x * WPB + threadIdx.y;
   if (i >= P.n_ipairs) return;  // whole warp

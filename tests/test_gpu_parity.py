@@ -253,15 +253,15 @@ def test_mass_balance_closure_and_tallies(precision, tol):
 @pytest.mark.parametrize("eddy,nan_cells", [(False, 0), (True, 0), (False, 5)])
 def test_fp32_two_cells_per_lane_matches_one_cell_sweep(precision, shape, eddy, nan_cells):
     """Variants 12-13 sweep pairs of interior strips with two cells per lane and 8-byte loads;
-    the arithmetic per face and cell is the one-cell interior sweep's (variants 7-8, same strip
-    height and register caps), so the fields after a timestep agree to FP32 rounding. Odd row
-    lengths and meshes too narrow for a pair have no pairs and give the one-cell results bit for
-    bit. Coded-out cells move strips out of pairs. The pairs' reductions (CFL, volume,
+    the arithmetic per face and cell is the one-cell interior sweep's (variant 7: the same strip
+    height and variant 12's register cap), so the fields after a timestep agree to FP32 rounding.
+    Odd row lengths and meshes too narrow for a pair have no pairs, and variant 12 then gives
+    variant 7's results bit for bit. Coded-out cells move strips out of pairs. The pairs' reductions (CFL, volume,
     tallies) are checked through the controller and the mass balance of a whole step."""
     nx, ny = shape
     z, h, u, v = wet_dry_state(nx, ny, 2.0, seed=nx + ny + nan_cells, nan_cells=nan_cells)
     out = {}
-    for variant in (7, 12, 8, 13):
+    for variant in (7, 12, 13):
         g = SaintVenantSolver(nx, ny, 2.0, precision=precision, cn_target=0.5, step_duration=3.0,
                               rain_mode="physical")
         g.set_kernel_variant(variant)
@@ -280,11 +280,12 @@ def test_fp32_two_cells_per_lane_matches_one_cell_sweep(precision, shape, eddy, 
         out[variant] = (cn, fields, st, v0)
         g.close()
     no_pairs = nx % 2 == 1 or nx < 2 * 28 + 32
-    for single, pair_v in ((7, 12), (8, 13)):
+    # variant 12 has variant 7's register cap, so without pairs it runs variant 7's kernels
+    for single, pair_v in ((7, 12), (7, 13)):
         cn1, f1, s1, v0 = out[single]
         cn2, f2, s2, _ = out[pair_v]
         for a, b in zip(f1, f2):
-            if no_pairs:
+            if no_pairs and pair_v == 12:
                 assert np.array_equal(a, b, equal_nan=True)
             else:
                 fin = np.isfinite(a)
