@@ -28,7 +28,8 @@ def test_reference_arm_line():
     assert "from its FP64 state after 60 s from dry" in line["cpu_baseline"]["sample"]
 
 
-@pytest.mark.parametrize("name", ["sweep_kernel_f32_datum64", "sweep_batch_kernel_f32_datum64", "stage_kernel_f64"])
+@pytest.mark.parametrize("name", ["sweep_interior_kernel_f32_datum64", "sweep_interior_kernel_f64", "sweep_kernel_f32_datum64",
+                                  "sweep_batch_kernel_f32_datum64", "stage_kernel_f64"])
 def test_profile_files_carry_what_the_bench_reads(name):
     sys.path.insert(0, ROOT)
     import bench
