@@ -1706,13 +1706,17 @@ template <int NT> __global__ void __launch_bounds__(NT) finalize_batch_kernel(co
 // its queued steps (TypedTemporalScheme::solve / step for each member, TemporalScheme.hpp:
 // 112-149, 244-276), each member at its own dt. A member's timestep is N stage phases of
 // column-sweep strips followed by one finalize phase (reductions and the dt controller).
-// Warps claim work items from any member whose current phase has unclaimed items; the warp
-// that completes the last item of a phase opens the member's next phase. Phases are ordered by
-// release fences before each completion count and acquire fences after each claim, and the
-// state buffers are read with coherent loads (ldst<true>). Every wait is bounded twice: a warp
-// that finds no work gives up after spin_limit polls during which no warp completed an item
-// (a global progress count), and every warp gives up once the launch has run max_ns; either
-// records SV_E_TIMEOUT in the launch status, and every warp returns at its next poll.
+// A warp looks at 32 members at once (one per lane) for one whose open phase has unclaimed
+// items and takes that member's next ticket with one atomicAdd (no retry loop, so claims do
+// not serialise when many warps work on one member). Tickets number a member's work items in
+// order; a ticket past the end of the open phase belongs to a later phase, whose opening its
+// warp waits for. The warp that completes the last item of a phase opens the member's next
+// phase. Phases are ordered by release fences before each completion count and acquire
+// fences before each item, and the state buffers are read with coherent loads (ldst<true>).
+// Every wait is bounded twice: a waiting warp gives up after spin_limit polls during which no
+// warp completed an item (a global progress count), and every warp gives up once the launch
+// has run max_ns; either records SV_E_TIMEOUT in the launch status, and every warp returns at
+// its next poll.
 // ---------------------------------------------------------------------------------------
 struct PersistMember {
   unsigned long long phase;   // phases opened so far: stage = phase % (N + 1), N = the finalize
@@ -1825,90 +1829,129 @@ __global__ void __launch_bounds__(32 * kPersistWarps, 4) persist_batch_kernel(co
   volatile unsigned long long* progress = PP.progress;
   const unsigned long long t_start = global_ns();
   unsigned long long idle = 0, seen = *progress;
+  // one poll of a waiting warp; true when the warp must return (another warp gave up, the
+  // launch ran out of time, or spin_limit polls passed with no item completed anywhere)
+  auto poll_gives_up = [&]() -> bool {
+    if (*status != 0) return true;
+    if (global_ns() - t_start > PP.max_ns) {
+      if (lane == 0) atomicExch((int*)PP.status, -6);
+      return true;
+    }
+    const unsigned long long now = *progress;
+    if (now != seen) {
+      idle = 0;
+      seen = now;
+    } else if (++idle > PP.spin_limit) {
+      if (lane == 0) atomicExch((int*)PP.status, -6);
+      return true;
+    } else {
+      __nanosleep(256);
+    }
+    return false;
+  };
   while (true) {
     if (*status != 0) return;  // whole warp: another warp gave up
     if (global_ns() - t_start > PP.max_ns) {
       if (lane == 0) atomicExch((int*)PP.status, -6);
       return;
     }
-    bool worked = false, active = false;
-    for (int j = 0; j < nact && !worked; ++j) {
-      const int k = (k0 + j) % nact;
-      PersistMember* m = PP.mem + k;
-      if (*(volatile int*)&m->finished) continue;
-      active = true;
-      const unsigned long long p = *(volatile unsigned long long*)&m->phase;
-      const int s = int(p % (N + 1));
-      const long long ns = m->nstrips;
-      const unsigned long long base = (p / (N + 1)) * (unsigned long long)(N * ns + 1) + (unsigned long long)s * ns;
-      const unsigned long long nwork = s < N ? (unsigned long long)ns : 1ull;
-      // claim one item of phase p (a claim can only succeed while phase p is open)
-      unsigned long long t = 0;
-      int ok = 0;
-      if (lane == 0) {
-        unsigned long long cur = *(volatile unsigned long long*)&m->ticket;
-        while (cur >= base && cur < base + nwork) {
-          const unsigned long long prev = atomicCAS(&m->ticket, cur, cur + 1);
-          if (prev == cur) { ok = 1; t = cur; break; }
-          cur = prev;
+    // a member whose open phase has unclaimed items: the lanes look at 32 members at once,
+    // starting from this warp's own member so that warps spread over the members
+    int pick = -1;
+    bool any_active = false;
+    for (int j0 = 0; j0 < nact && pick < 0; j0 += 32) {
+      const int j = j0 + lane;
+      bool act = false, open = false;
+      if (j < nact) {
+        const PersistMember* m = PP.mem + (k0 + j) % nact;
+        if (!*(volatile const int*)&m->finished) {
+          act = true;
+          const unsigned long long p = *(volatile const unsigned long long*)&m->phase;
+          const int s = int(p % (N + 1));
+          const long long ns = m->nstrips;
+          const unsigned long long end = (p / (N + 1)) * (unsigned long long)(N * ns + 1) +
+                                         (unsigned long long)s * ns + (s < N ? (unsigned long long)ns : 1ull);
+          open = *(volatile const unsigned long long*)&m->ticket < end;
         }
       }
-      ok = __shfl_sync(kFull, ok, 0);
-      if (!ok) continue;
-      t = __shfl_sync(kFull, t, 0);
-      __threadfence();  // acquire: the previous phases' writes of every warp
-      if (s < N) {
-        // stage s, strip t - base: the member's parameters to shared memory, then the sweep
-        static_assert(sizeof(StageParams<T>) % 4 == 0, "parameter block copied as 32-bit words");
-        const unsigned* src = reinterpret_cast<const unsigned*>(PP.Ps + size_t(s) * nact + k);
-        unsigned* dst = reinterpret_cast<unsigned*>(&Psh[wib]);
-        for (int i = lane; i < int(sizeof(StageParams<T>) / 4); i += 32) dst[i] = src[i];
-        __syncwarp();
-        // the member's interior strips (listed first) run the interior sweep
-        const StageParams<T>& SP = Psh[wib];
-        const long long item = (long long)(t - base);
-        if (SP.istrips && item < SP.n_istrips)
-          sweep_strip_interior<T, kPersistRows, P2, EDDY, true>(SP, SP.istrips[item]);
-        else if (SP.bstrips)
-          sweep_strip<T, kPersistRows, P2, EDDY, true>(SP, SP.bstrips[item - SP.n_istrips]);
-        else
-          sweep_strip<T, kPersistRows, P2, EDDY, true>(SP, item);
-        __syncwarp();
-      } else {
-        finalize_warp(PP.Fs[k], red[wib]);
-      }
-      __threadfence();  // release this item's writes before counting it
-      int last = 0;
-      if (lane == 0) {
-        last = atomicAdd(&m->done, 1u) + 1u == (unsigned)nwork;
-        atomicAdd(PP.progress, 1ull);
-      }
-      last = __shfl_sync(kFull, last, 0);
-      if (last) {
-        __threadfence();  // acquire the other items of the phase
-        if (lane == 0) {
-          m->done = 0;
-          // after a finalize the member goes on while its controller has a step running
-          const bool more = s < N || (*(volatile int*)&PP.Fs[k].ctl->done == 0);
-          __threadfence();
-          if (more) atomicExch(&m->phase, p + 1);
-          else atomicExch(&m->finished, 1);
-        }
-        __syncwarp();
-      }
-      worked = true;
+      any_active = __any_sync(kFull, act) || any_active;
+      const unsigned b = __ballot_sync(kFull, open);
+      if (b) pick = (k0 + j0 + __ffs(b) - 1) % nact;
     }
-    if (!active) return;  // every member has finished
-    const unsigned long long now = *progress;
-    if (worked || now != seen) {  // this warp or another completed an item
-      idle = 0;
-      seen = now;
-    } else if (++idle > PP.spin_limit) {
-      if (lane == 0) atomicExch((int*)PP.status, -6);
-      return;
+    if (!any_active) return;  // every member has finished
+    if (pick < 0) {
+      if (poll_gives_up()) return;
+      continue;
+    }
+    // take the member's next ticket. Tickets number the member's work items in order: per
+    // timestep N stage phases of nstrips items, then one finalize item. Warps that saw the
+    // same open phase may take tickets past its end; such a ticket belongs to a later phase
+    // and its warp waits for that phase to open (or drops it if the member finishes first)
+    PersistMember* m = PP.mem + pick;
+    const long long ns = m->nstrips;
+    unsigned long long t = 0;
+    if (lane == 0) t = atomicAdd(&m->ticket, 1ull);
+    t = __shfl_sync(kFull, t, 0);
+    const unsigned long long per = (unsigned long long)N * ns + 1;
+    const unsigned long long r = t % per;
+    const int s = r < (unsigned long long)N * ns ? int(r / ns) : N;
+    const unsigned long long q = (t / per) * (N + 1) + s;  // the ticket's phase
+    const unsigned long long nwork = s < N ? (unsigned long long)ns : 1ull;
+    bool dropped = false, stop = false;
+    while (*(volatile unsigned long long*)&m->phase < q) {
+      if (*(volatile int*)&m->finished) {
+        dropped = true;
+        break;
+      }
+      if (poll_gives_up()) {
+        stop = true;
+        break;
+      }
+    }
+    if (stop) return;
+    if (dropped) continue;
+    __threadfence();  // acquire: the previous phases' writes of every warp
+    if (s < N) {
+      // stage s, strip item r % ns: the member's parameters to shared memory, then the sweep
+      static_assert(sizeof(StageParams<T>) % 4 == 0, "parameter block copied as 32-bit words");
+      const unsigned* src = reinterpret_cast<const unsigned*>(PP.Ps + size_t(s) * nact + pick);
+      unsigned* dst = reinterpret_cast<unsigned*>(&Psh[wib]);
+      for (int i = lane; i < int(sizeof(StageParams<T>) / 4); i += 32) dst[i] = src[i];
+      __syncwarp();
+      // the member's interior strips (listed first) run the interior sweep
+      const StageParams<T>& SP = Psh[wib];
+      const long long item = (long long)(r % ns);
+      if (SP.istrips && item < SP.n_istrips)
+        sweep_strip_interior<T, kPersistRows, P2, EDDY, true>(SP, SP.istrips[item]);
+      else if (SP.bstrips)
+        sweep_strip<T, kPersistRows, P2, EDDY, true>(SP, SP.bstrips[item - SP.n_istrips]);
+      else
+        sweep_strip<T, kPersistRows, P2, EDDY, true>(SP, item);
+      __syncwarp();
     } else {
-      __nanosleep(256);
+      finalize_warp(PP.Fs[pick], red[wib]);
     }
+    __threadfence();  // release this item's writes before counting it
+    int last = 0;
+    if (lane == 0) {
+      last = atomicAdd(&m->done, 1u) + 1u == (unsigned)nwork;
+      atomicAdd(PP.progress, 1ull);
+    }
+    last = __shfl_sync(kFull, last, 0);
+    if (last) {
+      __threadfence();  // acquire the other items of the phase
+      if (lane == 0) {
+        m->done = 0;
+        // after a finalize the member goes on while its controller has a step running
+        const bool more = s < N || (*(volatile int*)&PP.Fs[pick].ctl->done == 0);
+        __threadfence();
+        if (more) atomicExch(&m->phase, q + 1);
+        else atomicExch(&m->finished, 1);
+      }
+      __syncwarp();
+    }
+    idle = 0;
+    seen = *progress;
   }
 }
 
