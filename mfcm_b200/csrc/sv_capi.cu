@@ -998,8 +998,8 @@ struct Solver final : public sv_ctx {
     if (v < 0 || v >= svk::kNumVariants) return fail(SV_E_ARG, "unknown kernel variant");
     // with tile datums only the column sweep evaluates each face in one frame (face_frame)
     if (datum && !svk::variant_is_sweep(v))
-      return fail(SV_E_ARG, "tile datums need a column-sweep variant (4-10, 12-13)");
-    if (svk::variant_is_pair(v) && sizeof(T) != 4) return fail(SV_E_ARG, "variants 12-13 are FP32 only");
+      return fail(SV_E_ARG, "tile datums need a column-sweep variant (4-10, 12-15)");
+    if (svk::variant_is_fp32_only(v) && sizeof(T) != 4) return fail(SV_E_ARG, "variants 12-15 are FP32 only");
     if (svk::variant_is_split(v)) {
       int r = ensure_split();
       if (r) return r;
@@ -1049,7 +1049,7 @@ struct Solver final : public sv_ctx {
     float best_ms = 1e30f;
     for (int v = 0; v < svk::kNumVariants; ++v) {
       if (datum && !svk::variant_is_sweep(v)) continue;
-      if (svk::variant_is_pair(v) && sizeof(T) != 4) continue;
+      if (svk::variant_is_fp32_only(v) && sizeof(T) != 4) continue;
       P.nblk = svk::variant_partials(v, (long long)mesh.nx, (long long)mesh.ny);
       if (!batch_path(v)) {
         int rs = ensure_strips(v);

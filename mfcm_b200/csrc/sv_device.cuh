@@ -254,7 +254,9 @@ __device__ __forceinline__ Side<T> side_p(const CellV<T>& c, T hd) {
 // The flux of a face from its two reconstructed sides (FluxKernel.cpp:189-291): the face bed,
 // the wet/dry branch and the Rusanov-type fluxes of h, the normal and the tangential momentum,
 // and the bed-step (z) term. Returns the branch code (1, 2.25, 2.75, 3 or 4).
-template <typename T, int DIR, typename DV>
+// TCHK = false drops the tangential finiteness terms (u_t * 0, g h * 0), which only matter
+// when a side's value is not finite (the FP32 interior sweeps; a non-finite state).
+template <typename T, int DIR, bool TCHK = true, typename DV>
 __device__ __forceinline__ T face_combine(Side<T> m, Side<T> p, const DV& divd, FaceF<T>& F) {
   const T g = T(kG);
   const T zb_m = m.zb, zb_p = p.zb, un_m = m.un, un_p = p.un, ut_m = m.ut, ut_p = p.ut;
@@ -279,13 +281,14 @@ __device__ __forceinline__ T face_combine(Side<T> m, Side<T> p, const DV& divd, 
     // evaluated without divergence: each side's terms, then the branch's own combination of
     // them selected per face.
     const T c_m = ssqrt(g * h_m), c_p = ssqrt(g * h_p);
-    const T spd_m = add_tangential(un_m, ut_m), spd_p = add_tangential(un_p, ut_p);
+    const T spd_m = TCHK ? add_tangential(un_m, ut_m) : un_m;
+    const T spd_p = TCHK ? add_tangential(un_p, ut_p) : un_p;
     const T hf_m = h_m * spd_m, hf_p = h_p * spd_p;
     const T gh_m = g * h_m, gh_p = g * h_p;
     const T nf_m = un_m * (T(0.5) * spd_m) + gh_m;
     const T nf_p = both ? un_p * (T(0.5) * spd_p) - gh_p : un_p * (T(0.5) * spd_p) + gh_p;
-    const T tf_m = add_tangential(ut_m * spd_m, gh_m);
-    const T tf_p = add_tangential(ut_p * spd_p, gh_p);
+    const T tf_m = TCHK ? add_tangential(ut_m * spd_m, gh_m) : ut_m * spd_m;
+    const T tf_p = TCHK ? add_tangential(ut_p * spd_p, gh_p) : ut_p * spd_p;
     // |spd + sign(spd) c| = |spd| + c, or 0 when spd is an exact zero (sign(0) = 0)
     const T a_m = iszero_b(spd_m) ? T(0) : abs_b(spd_m) + c_m;
     const T a_p = iszero_b(spd_p) ? T(0) : abs_b(spd_p) + c_p;

@@ -145,10 +145,18 @@ static cudaError_t launch_sweep_t(const StageParams<T>& P, int variant, cudaStre
   return cudaGetLastError();
 }
 
-// the two-cells-per-lane variants (FP32): 32-row strips, register caps for 3 and 4 blocks per SM
-template <typename T> static cudaError_t v12_13(const StageParams<T>& P, int variant, cudaStream_t s) {
-  if (variant == 12) return launch_sweep_t<T, 32, 3, true>(P, variant, s);
-  return launch_sweep_t<T, 32, 4, true>(P, variant, s);
+// the FP32-only variants: two cells per lane with register caps for 3 and 4 blocks per SM
+// (12, 13), one cell per lane capped for 7 and 8 blocks per SM (14, 15); 32-row strips
+template <typename T> static cudaError_t v12_15(const StageParams<T>& P, int variant, cudaStream_t s) {
+  if constexpr (sizeof(T) == 4) {
+    switch (variant) {
+      case 12: return launch_sweep_t<T, 32, 3, true>(P, variant, s);
+      case 13: return launch_sweep_t<T, 32, 4, true>(P, variant, s);
+      case 14: return launch_sweep_t<T, 32, 7>(P, variant, s);
+      default: return launch_sweep_t<T, 32, 8>(P, variant, s);
+    }
+  }
+  return cudaErrorInvalidValue;
 }
 
 template <> cudaError_t launch_variant<SV_T>(const StageParams<SV_T>& P, int variant, cudaStream_t s) {
@@ -163,8 +171,10 @@ template <> cudaError_t launch_variant<SV_T>(const StageParams<SV_T>& P, int var
     case kSplitVariant: return launch_split_t<SV_T>(P, s);
     case 12:
     case 13:
-      if (sizeof(SV_T) != 4) return cudaErrorInvalidValue;  // two cells per lane: FP32 only
-      return v12_13<SV_T>(P, variant, s);
+    case 14:
+    case 15:
+      if (sizeof(SV_T) != 4) return cudaErrorInvalidValue;  // FP32-only variants
+      return v12_15<SV_T>(P, variant, s);
     default: return launch_stage<SV_T>(P, variant, s);
   }
 }

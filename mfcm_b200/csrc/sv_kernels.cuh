@@ -692,6 +692,22 @@ template <typename T> __device__ __forceinline__ T dn1(T v) { return __shfl_down
 
 // The sweeps form slopes with svd::minmod3q (sv_device.cuh): Minmod3 from difference
 // quotients, its sign and NaN tests on the integer pipe.
+//
+// Two-sided Minmod3 of the FP32 interior sweeps: for finite quotients the reference's nested
+// pair minmods (Minmod3.hpp:66-80) reduce to sign * min(|2 qL|, |2 qR|, |qC / 2|) when the
+// three agree in sign and zero otherwise (up to the sign of a zero result). The NaN rules
+// only matter for a non-finite state, as for the dropped tangential terms.
+__device__ __forceinline__ float minmod3_finite(float qL, float qR, float qC) {
+  const float a = 2.0f * qL, b = 2.0f * qR, c = 0.5f * qC;
+  const int ia = __float_as_int(a), ib = __float_as_int(b), ic = __float_as_int(c);
+  const float m = fminf(fminf(fabsf(a), fabsf(b)), fabsf(c));
+  return ((ia ^ ib) | (ia ^ ic)) >= 0 ? __int_as_float(__float_as_int(m) | (ia & 0x80000000)) : 0.0f;
+}
+// the interior sweeps' two-sided slope: exact reference rules in FP64, the finite form in FP32
+template <typename T> __device__ __forceinline__ T slope2s(T qL, T qR, T qC) {
+  if constexpr (sizeof(T) == 4) return minmod3_finite(qL, qR, qC);
+  return minmod3q<T>(qL, true, qR, true, qC);
+}
 
 template <typename T> struct RowV { T h, u, v, z, zx, zy; };
 template <typename T> struct SlopeV { T hx, ux, vx, hy, uy, vy; };
@@ -1053,23 +1069,23 @@ __device__ __forceinline__ void sweep_strip_interior(const StageParams<T>& P, lo
     }
     // slopes of row k-1 (State.cpp:187-192), two-sided; the Y axis uses north as the left side
     if (k >= y0) {
-      S0.hy = minmod3q<T>(-fyB[0], true, -fyA[0], true, divy(Rm.h - Rp.h));
-      S0.uy = minmod3q<T>(-fyB[1], true, -fyA[1], true, divy(Rm.u - Rp.u));
-      S0.vy = minmod3q<T>(-fyB[2], true, -fyA[2], true, divy(Rm.v - Rp.v));
+      S0.hy = slope2s<T>(-fyB[0], -fyA[0], divy(Rm.h - Rp.h));
+      S0.uy = slope2s<T>(-fyB[1], -fyA[1], divy(Rm.u - Rp.u));
+      S0.vy = slope2s<T>(-fyB[2], -fyA[2], divy(Rm.v - Rp.v));
       {
         T r_ = dn1(R0.h), l_ = up1(R0.h);
         T fq = divx(r_ - R0.h);
-        S0.hx = minmod3q<T>(up1(fq), true, fq, true, divx(r_ - l_));
+        S0.hx = slope2s<T>(up1(fq), fq, divx(r_ - l_));
       }
       {
         T r_ = dn1(R0.u), l_ = up1(R0.u);
         T fq = divx(r_ - R0.u);
-        S0.ux = minmod3q<T>(up1(fq), true, fq, true, divx(r_ - l_));
+        S0.ux = slope2s<T>(up1(fq), fq, divx(r_ - l_));
       }
       {
         T r_ = dn1(R0.v), l_ = up1(R0.v);
         T fq = divx(r_ - R0.v);
-        S0.vx = minmod3q<T>(up1(fq), true, fq, true, divx(r_ - l_));
+        S0.vx = slope2s<T>(up1(fq), fq, divx(r_ - l_));
       }
     }
     // horizontal face between rows k-2 and k-1 (face row fy = k-1), Fluxes.cpp:55-64
@@ -1081,7 +1097,7 @@ __device__ __forceinline__ void sweep_strip_interior(const StageParams<T>& P, lo
         const long long tb = datum_tile(gx, fy, P.dtiles_x);
         hi.z = T(double(hi.z) + (P.zdat[tb] - P.zdat[tb - P.dtiles_x]));
       }
-      face_combine<T, 1>(side_m<T, 1, TCHK>(lo, hdy), side_p<T, 1, TCHK>(hi, hdy), divy, FN);
+      face_combine<T, 1, TCHK>(side_m<T, 1, TCHK>(lo, hdy), side_p<T, 1, TCHK>(hi, hdy), divy, FN);
     }
     // output row k-2
     if (k >= y0 + 2) {
@@ -1094,15 +1110,15 @@ __device__ __forceinline__ void sweep_strip_interior(const StageParams<T>& P, lo
           {
             T r_ = dn1(Sm.ux), l_ = up1(Sm.ux);
             T fq = divx(r_ - Sm.ux);
-            ed.uxx = minmod3q<T>(up1(fq), true, fq, true, divx(r_ - l_));
+            ed.uxx = slope2s<T>(up1(fq), fq, divx(r_ - l_));
           }
           {
             T r_ = dn1(Sm.vx), l_ = up1(Sm.vx);
             T fq = divx(r_ - Sm.vx);
-            ed.vxx = minmod3q<T>(up1(fq), true, fq, true, divx(r_ - l_));
+            ed.vxx = slope2s<T>(up1(fq), fq, divx(r_ - l_));
           }
-          ed.uyy = minmod3q<T>(divy(Sm.uy - S0.uy), true, divy(Smm_uy - Sm.uy), true, divy(Smm_uy - S0.uy));
-          ed.vyy = minmod3q<T>(divy(Sm.vy - S0.vy), true, divy(Smm_vy - Sm.vy), true, divy(Smm_vy - S0.vy));
+          ed.uyy = slope2s<T>(divy(Sm.uy - S0.uy), divy(Smm_uy - Sm.uy), divy(Smm_uy - S0.uy));
+          ed.vyy = slope2s<T>(divy(Sm.vy - S0.vy), divy(Smm_vy - Sm.vy), divy(Smm_vy - S0.vy));
         }
       }
       // west face: the left lane's east side against this lane's west side
@@ -1114,7 +1130,7 @@ __device__ __forceinline__ void sweep_strip_interior(const StageParams<T>& P, lo
         meW.z = T(double(me.z) + (P.zdat[tb] - P.zdat[tb - 1]));
       }
       FaceF<T> FW;
-      face_combine<T, 0>(mW, side_p<T, 0, TCHK>(meW, hdx), divx, FW);
+      face_combine<T, 0, TCHK>(mW, side_p<T, 0, TCHK>(meW, hdx), divx, FW);
       const FaceF<T> FE{dn1(FW.h), dn1(FW.u), dn1(FW.v), dn1(FW.z)};
       if (out_lane) {
         const long long g = (long long)r * nx + gx;
@@ -1264,8 +1280,8 @@ __device__ __forceinline__ void sweep_pair_interior(const StageParams<float>& P,
     const T qab = divx(B - A);
     const T qbr = divx(Ar - B);
     const T qla = up1(qbr);       // (A - Bl) / dx, formed by the left lane
-    sa = minmod3q<T>(qla, true, qab, true, divx(B - Bl));
-    sb = minmod3q<T>(qab, true, qbr, true, divx(Ar - A));
+    sa = minmod3_finite(qla, qab, divx(B - Bl));
+    sb = minmod3_finite(qab, qbr, divx(Ar - A));
   };
 
   RowV<T> Rm[2] = {}, R0[2] = {}, Rp[2] = {};
@@ -1296,9 +1312,9 @@ __device__ __forceinline__ void sweep_pair_interior(const StageParams<float>& P,
     if (k >= y0) {
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
-        S0[j].hy = minmod3q<T>(-fyB[j][0], true, -fyA[j][0], true, divy(Rm[j].h - Rp[j].h));
-        S0[j].uy = minmod3q<T>(-fyB[j][1], true, -fyA[j][1], true, divy(Rm[j].u - Rp[j].u));
-        S0[j].vy = minmod3q<T>(-fyB[j][2], true, -fyA[j][2], true, divy(Rm[j].v - Rp[j].v));
+        S0[j].hy = minmod3_finite(-fyB[j][0], -fyA[j][0], divy(Rm[j].h - Rp[j].h));
+        S0[j].uy = minmod3_finite(-fyB[j][1], -fyA[j][1], divy(Rm[j].u - Rp[j].u));
+        S0[j].vy = minmod3_finite(-fyB[j][2], -fyA[j][2], divy(Rm[j].v - Rp[j].v));
       }
       xslopes(R0[0].h, R0[1].h, S0[0].hx, S0[1].hx);
       xslopes(R0[0].u, R0[1].u, S0[0].ux, S0[1].ux);
@@ -1318,7 +1334,7 @@ __device__ __forceinline__ void sweep_pair_interior(const StageParams<float>& P,
         const CellV<T> lo = mkcell(Rm[j], Sm[j]);
         CellV<T> hi = mkcell(R0[j], S0[j]);
         if (ycross) hi.z = T(double(hi.z) + dz);
-        face_combine<T, 1>(side_m<T, 1, false>(lo, hdy), side_p<T, 1, false>(hi, hdy), divy, FN[j]);
+        face_combine<T, 1, false>(side_m<T, 1, false>(lo, hdy), side_p<T, 1, false>(hi, hdy), divy, FN[j]);
       }
     }
     // output row k-2
@@ -1331,10 +1347,10 @@ __device__ __forceinline__ void sweep_pair_interior(const StageParams<float>& P,
 #pragma unroll
           for (int j = 0; j < 2; ++j) {
             ed[j].ux = Sm[j].ux; ed[j].uy = Sm[j].uy; ed[j].vx = Sm[j].vx; ed[j].vy = Sm[j].vy;
-            ed[j].uyy = minmod3q<T>(divy(Sm[j].uy - S0[j].uy), true, divy(Smm_uy[j] - Sm[j].uy), true,
-                                    divy(Smm_uy[j] - S0[j].uy));
-            ed[j].vyy = minmod3q<T>(divy(Sm[j].vy - S0[j].vy), true, divy(Smm_vy[j] - Sm[j].vy), true,
-                                    divy(Smm_vy[j] - S0[j].vy));
+            ed[j].uyy = minmod3_finite(divy(Sm[j].uy - S0[j].uy), divy(Smm_uy[j] - Sm[j].uy),
+                                       divy(Smm_uy[j] - S0[j].uy));
+            ed[j].vyy = minmod3_finite(divy(Sm[j].vy - S0[j].vy), divy(Smm_vy[j] - Sm[j].vy),
+                                       divy(Smm_vy[j] - S0[j].vy));
           }
           xslopes(Sm[0].ux, Sm[1].ux, ed[0].uxx, ed[1].uxx);
           xslopes(Sm[0].vx, Sm[1].vx, ed[0].vxx, ed[1].vxx);
@@ -1349,9 +1365,9 @@ __device__ __forceinline__ void sweep_pair_interior(const StageParams<float>& P,
         meAW.z = T(double(meA.z) + (P.zdat[tb] - P.zdat[tb - 1]));
       }
       FaceF<T> FWa, Fab;
-      face_combine<T, 0>(wA, side_p<T, 0, false>(meAW, hdx), divx, FWa);
+      face_combine<T, 0, false>(wA, side_p<T, 0, false>(meAW, hdx), divx, FWa);
       // the face between the lane's two cells
-      face_combine<T, 0>(side_m<T, 0, false>(meA, hdx), side_p<T, 0, false>(meB, hdx), divx, Fab);
+      face_combine<T, 0, false>(side_m<T, 0, false>(meA, hdx), side_p<T, 0, false>(meB, hdx), divx, Fab);
       // east face of the second cell: the right lane's west face
       const FaceF<T> FEb{dn1(FWa.h), dn1(FWa.u), dn1(FWa.v), dn1(FWa.z)};
       if (out_lane) {
