@@ -94,6 +94,12 @@ __device__ __forceinline__ float mm2(float a, float b) {
 template <typename T> __device__ __forceinline__ T ssign(T x) {
   return x > T(0) ? T(1) : (x < T(0) ? T(-1) : (x == x ? x : T(0)));
 }
+// sign(f) != sign(u) for an f with |f| > |u| (so f is neither zero nor NaN, and u is not
+// NaN): u is a zero, or the two have opposite signs. The same truth value as comparing the
+// sycl::sign results, without forming them.
+template <typename T> __device__ __forceinline__ bool opposes(T f, T u) {
+  return u == T(0) || ((f < T(0)) != (u < T(0)));
+}
 // sycl::min(x, y): y if y < x, else x
 template <typename T> __device__ __forceinline__ T smin(T x, T y) { return (y < x) ? y : x; }
 // fmax: IEEE maxNum
@@ -461,8 +467,8 @@ __device__ __forceinline__ bool manning_term(T h, T u, T v, T ns, T nd, T ds, T 
     fu = -T(kG) * sf * u;
     fv = -T(kG) * sf * v;
     T fudt = fu * c.dt, fvdt = fv * c.dt;
-    if (sfabs(fudt) > sfabs(u) && ssign(fudt) != ssign(u)) fu = -c.divdt(u);
-    if (sfabs(fvdt) > sfabs(v) && ssign(fvdt) != ssign(v)) fv = -c.divdt(v);
+    if (sfabs(fudt) > sfabs(u) && opposes(fudt, u)) fu = -c.divdt(u);
+    if (sfabs(fvdt) > sfabs(v) && opposes(fvdt, v)) fv = -c.divdt(v);
     return true;
   }
   if (sf_out) *sf_out = T(0);
@@ -487,8 +493,8 @@ __device__ __forceinline__ void manning_apply(T h, T u, T v, T ns, T nd, T ds, T
     T fu = -T(kG) * sf * u;
     T fv = -T(kG) * sf * v;
     T fudt = fu * c.dt, fvdt = fv * c.dt;
-    if (sfabs(fudt) > sfabs(u) && ssign(fudt) != ssign(u)) fu = -c.divdt(u);
-    if (sfabs(fvdt) > sfabs(v) && ssign(fvdt) != ssign(v)) fv = -c.divdt(v);
+    if (sfabs(fudt) > sfabs(u) && opposes(fudt, u)) fu = -c.divdt(u);
+    if (sfabs(fvdt) > sfabs(v) && opposes(fvdt, v)) fv = -c.divdt(v);
     du = du + fu;
     dv = dv + fv;
   } else if (sf_out) {
@@ -505,8 +511,8 @@ __device__ __forceinline__ bool energy_loss_term(T h, T u, T v, T fx, T fy, cons
   eu = T(-0.5) * u * fx * hyp;
   ev = T(-0.5) * v * fy * hyp;
   T eudt = eu * c.dt, evdt = ev * c.dt;
-  if (sfabs(eudt) > sfabs(u) && ssign(eudt) != ssign(u)) eu = -c.divdt(u);
-  if (sfabs(evdt) > sfabs(v) && ssign(evdt) != ssign(v)) ev = -c.divdt(v);
+  if (sfabs(eudt) > sfabs(u) && opposes(eudt, u)) eu = -c.divdt(u);
+  if (sfabs(evdt) > sfabs(v) && opposes(evdt, v)) ev = -c.divdt(v);
   return true;
 }
 template <typename T, typename CC>
@@ -516,8 +522,8 @@ __device__ __forceinline__ void energy_loss_apply(T h, T u, T v, T fx, T fy, con
   T eu = T(-0.5) * u * fx * hyp;
   T ev = T(-0.5) * v * fy * hyp;
   T eudt = eu * c.dt, evdt = ev * c.dt;
-  if (sfabs(eudt) > sfabs(u) && ssign(eudt) != ssign(u)) eu = -c.divdt(u);
-  if (sfabs(evdt) > sfabs(v) && ssign(evdt) != ssign(v)) ev = -c.divdt(v);
+  if (sfabs(eudt) > sfabs(u) && opposes(eudt, u)) eu = -c.divdt(u);
+  if (sfabs(evdt) > sfabs(v) && opposes(evdt, v)) ev = -c.divdt(v);
   du = du + eu;
   dv = dv + ev;
 }
@@ -546,8 +552,8 @@ __device__ __forceinline__ bool eddy_term(T h, T u, T v, T mu, const EddyIn<T>& 
   fu = -mu * (e.uxx + e.uyy);
   fv = -mu * (e.vxx + e.vyy);
   T fudt = fu * c.dt, fvdt = fv * c.dt;
-  if (sfabs(fudt) > sfabs(u) && ssign(fudt) != ssign(u)) fu = -c.divdt(u);
-  if (sfabs(fvdt) > sfabs(v) && ssign(fvdt) != ssign(v)) fv = -c.divdt(v);
+  if (sfabs(fudt) > sfabs(u) && opposes(fudt, u)) fu = -c.divdt(u);
+  if (sfabs(fvdt) > sfabs(v) && opposes(fvdt, v)) fv = -c.divdt(v);
   return true;
 }
 
