@@ -252,8 +252,7 @@ int sv_run_timesteps(sv_ctx* ctx, uint64_t max_timesteps, int begin, sv_stats* o
  * from coded-out cells run an interior form of it), 12-13 (FP32 solvers only) the 32-row
  * column sweep whose pairs of adjacent interior strips run two cells per lane with 8-byte
  * loads (capped for 3 and 4 CTAs/SM; meshes with an odd row length have no pairs), 14-15
- * (FP32 solvers only) the one-cell 32-row sweep capped for 7 and 8 CTAs/SM, 16-17 (FP32
- * solvers only) the one-cell sweep at 7 CTAs/SM with 48- and 24-row strips. Split
+ * (FP32 solvers only) the one-cell 32-row sweep capped for 7 and 8 CTAs/SM. Split
  * schedule, two passes per RK stage: 11 a slopes pass, then the tiled 32x8 kernel reading
  * those slopes. Every variant computes bit-identical FP64 results; FP32 results are
  * reproducible per variant. SV_F32_DATUM64 solvers take the column-sweep variants only. */

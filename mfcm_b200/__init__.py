@@ -233,7 +233,7 @@ class SaintVenantSolver(_Backend):
             raise SvError(r, self.last_error())
         return v.value
 
-    def autotune_ms(self, n=32):
+    def autotune_ms(self, n=16):
         """Per-variant stage-kernel times (ms) measured by the last autotune (0 = untimed)."""
         a = (C.c_float * n)()
         self._lib.sv_get_autotune_ms(self._h, a, n)

@@ -208,12 +208,9 @@ struct Solver final : public sv_ctx {
     int np = 0, npi = 0;
     bool valid = false;
   };
-  Strips strips_[5];
+  Strips strips_[3];
   unsigned char* d_sflags = nullptr;
-  // one list per strip height of the sweep variants: 16, 24, 32, 48, 64 rows
-  static int strips_slot(int rows) {
-    return rows == 16 ? 0 : (rows == 24 ? 1 : (rows == 32 ? 2 : (rows == 48 ? 3 : 4)));
-  }
+  static int strips_slot(int rows) { return rows == 16 ? 0 : (rows == 32 ? 1 : 2); }
   void invalidate_strips() {
     for (Strips& x : strips_) x.valid = false;
     graph_dirty = true; ++pversion;
@@ -1001,8 +998,8 @@ struct Solver final : public sv_ctx {
     if (v < 0 || v >= svk::kNumVariants) return fail(SV_E_ARG, "unknown kernel variant");
     // with tile datums only the column sweep evaluates each face in one frame (face_frame)
     if (datum && !svk::variant_is_sweep(v))
-      return fail(SV_E_ARG, "tile datums need a column-sweep variant (4-10, 12-17)");
-    if (svk::variant_is_fp32_only(v) && sizeof(T) != 4) return fail(SV_E_ARG, "variants 12-17 are FP32 only");
+      return fail(SV_E_ARG, "tile datums need a column-sweep variant (4-10, 12-15)");
+    if (svk::variant_is_fp32_only(v) && sizeof(T) != 4) return fail(SV_E_ARG, "variants 12-15 are FP32 only");
     if (svk::variant_is_split(v)) {
       int r = ensure_split();
       if (r) return r;

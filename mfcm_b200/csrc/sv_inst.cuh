@@ -146,17 +146,14 @@ static cudaError_t launch_sweep_t(const StageParams<T>& P, int variant, cudaStre
 }
 
 // the FP32-only variants: two cells per lane with register caps for 3 and 4 blocks per SM
-// (12, 13), one cell per lane capped for 7 and 8 blocks per SM (14, 15), all with 32-row
-// strips; 48- and 24-row strips at 7 blocks per SM (16, 17)
+// (12, 13), one cell per lane capped for 7 and 8 blocks per SM (14, 15); 32-row strips
 template <typename T> static cudaError_t v12_15(const StageParams<T>& P, int variant, cudaStream_t s) {
   if constexpr (sizeof(T) == 4) {
     switch (variant) {
       case 12: return launch_sweep_t<T, 32, 3, true>(P, variant, s);
       case 13: return launch_sweep_t<T, 32, 4, true>(P, variant, s);
       case 14: return launch_sweep_t<T, 32, 7>(P, variant, s);
-      case 15: return launch_sweep_t<T, 32, 8>(P, variant, s);
-      case 16: return launch_sweep_t<T, 48, 7>(P, variant, s);
-      default: return launch_sweep_t<T, 24, 7>(P, variant, s);
+      default: return launch_sweep_t<T, 32, 8>(P, variant, s);
     }
   }
   return cudaErrorInvalidValue;
@@ -176,8 +173,6 @@ template <> cudaError_t launch_variant<SV_T>(const StageParams<SV_T>& P, int var
     case 13:
     case 14:
     case 15:
-    case 16:
-    case 17:
       if (sizeof(SV_T) != 4) return cudaErrorInvalidValue;  // FP32-only variants
       return v12_15<SV_T>(P, variant, s);
     default: return launch_stage<SV_T>(P, variant, s);

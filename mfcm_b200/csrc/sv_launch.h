@@ -23,24 +23,21 @@ template <typename T> cudaError_t launch_stage(const StageParams<T>& P, int tile
 //   last four with register caps for 3, 4, 5 and 6 resident 4-warp blocks per SM; 12, 13
 //   (FP32 only) the column sweep of 32-row strips whose interior strip pairs run two cells
 //   per lane (sweep_pair_kernel), with register caps for 3 and 4 blocks per SM; 14, 15 (FP32
-//   only) the one-cell sweep of 32-row strips capped for 7 and 8 blocks per SM; 16, 17 (FP32
-//   only) the same at 7 blocks per SM with 48- and 24-row strips (other strip counts, so the
-//   last wave of blocks fills differently);
+//   only) the one-cell sweep of 32-row strips capped for 7 and 8 blocks per SM;
 //  split (two passes per RK stage): 11 the slopes pass (slopes_kernel) then the tiled 32 x 8
 //   kernel at 3 CTAs/SM reading those slopes.
-constexpr int kNumVariants = 18;
+constexpr int kNumVariants = 16;
 constexpr int kSplitVariant = 11;
 constexpr int kSweepRows[7] = {16, 32, 64, 32, 32, 32, 32};
 inline bool variant_is_pair(int v) { return v == 12 || v == 13; }
 // variants compiled for FP32 solvers only (the two-cells-per-lane sweep, the tightest caps)
-inline bool variant_is_fp32_only(int v) { return v >= 12 && v <= 17; }
-inline bool variant_is_sweep(int v) { return (v >= 4 && v <= 10) || (v >= 12 && v <= 17); }
+inline bool variant_is_fp32_only(int v) { return v >= 12 && v <= 15; }
+inline bool variant_is_sweep(int v) { return (v >= 4 && v <= 10) || (v >= 12 && v <= 15); }
 inline bool variant_is_split(int v) { return v == kSplitVariant; }
 // column-sweep variants: output rows per strip (0 for the other variants)
 inline int variant_sweep_rows(int v) {
   if (v >= 4 && v <= 10) return kSweepRows[v - 4];
-  if (v >= 12 && v <= 15) return 32;
-  return v == 16 ? 48 : (v == 17 ? 24 : 0);
+  return (v >= 12 && v <= 15) ? 32 : 0;
 }
 // per-CTA (tiled) or per-warp (sweep) partial count
 inline long long variant_partials(int v, long long nx, long long ny) {

@@ -139,7 +139,7 @@ def test_interior_strips_every_sweep_variant(variant, nan_cells):
 
 
 @pytest.mark.parametrize("precision", ["f32", "f32_datum64"])
-@pytest.mark.parametrize("variant", [4, 5, 9, 12, 13, 14, 15, 16, 17])
+@pytest.mark.parametrize("variant", [4, 5, 9, 12, 13, 14, 15])
 def test_fp32_interior_strips_close_to_fp64(precision, variant):
     """The FP32 interior kernel (no tangential finiteness tests) against the FP64 oracle."""
     nx, ny, dx = 200, 180, 5.0
@@ -261,7 +261,7 @@ def test_fp32_two_cells_per_lane_matches_one_cell_sweep(precision, shape, eddy, 
     nx, ny = shape
     z, h, u, v = wet_dry_state(nx, ny, 2.0, seed=nx + ny + nan_cells, nan_cells=nan_cells)
     out = {}
-    for variant in (7, 12, 13, 14, 15, 16, 17):
+    for variant in (7, 12, 13, 14, 15):
         g = SaintVenantSolver(nx, ny, 2.0, precision=precision, cn_target=0.5, step_duration=3.0,
                               rain_mode="physical")
         g.set_kernel_variant(variant)
@@ -281,7 +281,7 @@ def test_fp32_two_cells_per_lane_matches_one_cell_sweep(precision, shape, eddy, 
         g.close()
     no_pairs = nx % 2 == 1 or nx < 2 * 28 + 32
     # variant 12 has variant 7's register cap, so without pairs it runs variant 7's kernels
-    for single, pair_v in ((7, 12), (7, 13), (7, 14), (7, 15), (7, 16), (7, 17)):
+    for single, pair_v in ((7, 12), (7, 13), (7, 14), (7, 15)):
         cn1, f1, s1, v0 = out[single]
         cn2, f2, s2, _ = out[pair_v]
         for a, b in zip(f1, f2):
@@ -302,7 +302,7 @@ def test_fp32_two_cells_per_lane_matches_one_cell_sweep(precision, shape, eddy, 
 
 def test_fp32_only_variants_refused_by_fp64_solvers():
     g = SaintVenantSolver(64, 40, 2.0)
-    for variant in (12, 13, 14, 15, 16, 17):
+    for variant in (12, 13, 14, 15):
         with pytest.raises(Exception):
             g.set_kernel_variant(variant)
     g.close()
