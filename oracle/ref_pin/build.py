@@ -28,6 +28,10 @@ a clang extension the reference relies on):
 
 Everything else is compiled as the reference wrote it. Without the reference tree (the GPU
 machines do not have it) `available()` is False and the pin tests skip.
+
+A second library, oracle/_ref/libsv_refpin_nimrod.so, holds the reference's NIMROD raster reader
+(src/Raster/RasterFormats/NIMROD.cpp with src/Raster/RasterFormat.hpp, copied unchanged) and
+oracle/ref_pin/nimrod_pin.cpp, the driver that runs it on a file and copies out what it read.
 """
 import os
 import re
@@ -66,6 +70,8 @@ COPY = [
     "Config/TimeParameters.hpp", "Config/TimeParameters.cpp",
     "TemporalScheme/TemporalScheme.hpp", "TemporalScheme/RungeKutta.hpp", "TemporalScheme/RungeKutta.cpp",
 ]
+# the NIMROD reader, compiled into its own library
+NIMROD_COPY = ["Raster/RasterFormat.hpp", "Raster/RasterFormats/NIMROD.hpp", "Raster/RasterFormats/NIMROD.cpp"]
 # stand-ins, by the path the reference includes them from
 STUBS = {
     "Config/Config.hpp": "Config.hpp",
@@ -77,13 +83,16 @@ STUBS = {
     "Output/OutputFile.hpp": "OutputFile.hpp",
 }
 INCLUDE_DIRS = ["", "DataArray", "Mesh", "Field", "SpatialDerivative", "SaintVenant", "SaintVenant/SourceTerms",
-                "SaintVenant/Boundaries", "Config", "Geometry", "Input", "Output", "TemporalScheme"]
+                "SaintVenant/Boundaries", "Config", "Geometry", "Input", "Output", "TemporalScheme",
+                "Raster", "Raster/RasterFormats"]
 FLAGS = ["-std=c++17", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared", "-w"]
 DRIVER = os.path.join(HERE, "ref_pin.cpp")
+NIMROD_DRIVER = os.path.join(HERE, "nimrod_pin.cpp")
+NIMROD_LIB = os.path.join(OUT, "libsv_refpin_nimrod.so")
 
 
 def available():
-    return os.path.isdir(REF_SRC) and all(os.path.exists(os.path.join(REF_SRC, f)) for f in COPY)
+    return os.path.isdir(REF_SRC) and all(os.path.exists(os.path.join(REF_SRC, f)) for f in COPY + NIMROD_COPY)
 
 
 def _block_end(text, start):
@@ -180,7 +189,7 @@ def patch(rel, text):
 def prepare():
     if os.path.isdir(TREE):
         shutil.rmtree(TREE)
-    for rel in COPY:
+    for rel in COPY + NIMROD_COPY:
         dst = os.path.join(TREE, rel)
         os.makedirs(os.path.dirname(dst), exist_ok=True)
         with open(os.path.join(REF_SRC, rel)) as f:
@@ -193,31 +202,41 @@ def prepare():
         shutil.copy(os.path.join(HERE, "stubs", stub), dst)
 
 
-def _stale():
-    if not os.path.exists(LIB):
+def _stale(lib, driver, copied):
+    if not os.path.exists(lib):
         return True
-    t = os.path.getmtime(LIB)
-    deps = [DRIVER, os.path.join(HERE, "shim", "CL", "sycl.hpp"), __file__]
+    t = os.path.getmtime(lib)
+    deps = [driver, os.path.join(HERE, "shim", "CL", "sycl.hpp"), __file__]
     deps += [os.path.join(HERE, "stubs", s) for s in STUBS.values()]
-    deps += [os.path.join(REF_SRC, f) for f in COPY]
+    deps += [os.path.join(REF_SRC, f) for f in copied]
     return any(os.path.getmtime(d) > t for d in deps)
 
 
 def build(force=False, verbose=False):
+    """Build both pin libraries (when stale); returns the path of the kernels' library."""
     if not available():
         raise RuntimeError(f"reference sources not found under {REF_SRC}")
-    if not (force or _stale()):
+    targets = [(LIB, DRIVER, COPY), (NIMROD_LIB, NIMROD_DRIVER, COPY + NIMROD_COPY)]
+    todo = [t for t in targets if force or _stale(*t)]
+    if not todo:
         return LIB
     os.makedirs(OUT, exist_ok=True)
     prepare()
     inc = ["-I", os.path.join(HERE, "shim")]
     for d in INCLUDE_DIRS:
         inc += ["-I", os.path.join(TREE, d)]
-    cmd = ["g++"] + FLAGS + inc + [DRIVER, "-o", LIB]
-    if verbose:
-        print(" ".join(cmd), flush=True)
-    subprocess.check_call(cmd)
+    for lib, driver, _ in todo:
+        cmd = ["g++"] + FLAGS + inc + [driver, "-o", lib]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.check_call(cmd)
     return LIB
+
+
+def build_nimrod(force=False, verbose=False):
+    """Build (when stale) and return the path of the NIMROD reader's library."""
+    build(force=force, verbose=verbose)
+    return NIMROD_LIB
 
 
 if __name__ == "__main__":

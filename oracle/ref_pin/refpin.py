@@ -157,3 +157,55 @@ def solve(z, h, u, v, dx, dy=None, manning=None, rain=None, head_edges=0, head_v
     if r != 0:
         raise RuntimeError("reference solve failed")
     return out[0], out[1], out[2], n.value
+
+
+class RefReaderError(RuntimeError):
+    """The reference's reader threw; the message is its exception's."""
+
+
+_nimrod = None
+
+
+def _load_nimrod():
+    global _nimrod
+    if _nimrod is None:
+        _nimrod = C.CDLL(_build_module().build_nimrod())
+        f = _nimrod.refpin_nimrod_read
+        f.restype = C.c_int
+        D = C.POINTER(C.c_double)
+        f.argtypes = [C.c_char_p, D, C.POINTER(C.c_int16), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_char_p,
+                      C.POINTER(C.c_int16), C.POINTER(C.c_uint64), D, D, D, D, C.c_uint64, D, C.c_uint64, C.c_char_p,
+                      C.c_uint64]
+    return _nimrod
+
+
+def nimrod_read(path, bbox=None):
+    """The reference's NIMRODRasterFormat<double> on the file at `path` (bbox = xmin, ymin, xmax,
+    ymax or None). Returns a dict: h1..h5 (header arrays), nxpx, nypx, ulc (x, y) and lrc (x, y)
+    pixel corners, ncols, nrows (of the crop), buffer (the whole grid, nypx x nxpx, file order,
+    north row first), values (values_, flat, the crop row by row from the north), geo (the
+    geotransform), llc (the reader's llc()) and nodata. Raises RefReaderError when the reader
+    throws."""
+    lib = _load_nimrod()
+    bb = None if bbox is None else (C.c_double * 4)(*[float(b) for b in bbox])
+    err = C.create_string_buffer(512)
+    dims = (C.c_uint64 * 9)()
+    h1, h5 = (C.c_int16 * 31)(), (C.c_int16 * 51)()
+    h2, h3 = (C.c_float * 28)(), (C.c_float * 45)()
+    h4 = C.create_string_buffer(56)
+    geo, llc, nod = (C.c_double * 6)(), (C.c_double * 2)(), (C.c_double * 1)()
+    r = lib.refpin_nimrod_read(os.fsencode(path), bb, h1, h2, h3, h4, h5, dims, geo, llc, nod, None, 0, None, 0,
+                               err, len(err))
+    if r == 1:
+        raise RefReaderError(err.value.decode(errors="replace"))
+    nxpx, nypx, nval = int(dims[0]), int(dims[1]), int(dims[8])
+    buf = np.empty(nxpx * nypx, dtype=np.float64)
+    val = np.empty(max(1, nval), dtype=np.float64)
+    r = lib.refpin_nimrod_read(os.fsencode(path), bb, None, None, None, None, None, None, None, None, None,
+                               _ptr(buf, C.c_double), buf.size, _ptr(val, C.c_double), val.size, err, len(err))
+    if r != 0:
+        raise RefReaderError(f"second read failed ({r}): {err.value.decode(errors='replace')}")
+    return {"h1": list(h1), "h2": list(h2), "h3": list(h3), "h4": h4.raw, "h5": list(h5), "nxpx": nxpx, "nypx": nypx,
+            "ulc": (int(dims[2]), int(dims[3])), "lrc": (int(dims[4]), int(dims[5])), "ncols": int(dims[6]),
+            "nrows": int(dims[7]), "buffer": buf.reshape(nypx, nxpx), "values": val[:nval], "geo": list(geo),
+            "llc": (llc[0], llc[1]), "nodata": nod[0]}

@@ -3,7 +3,7 @@
 // oracle/ref_pin builds the reference's hot-path kernels. It holds string key/value pairs; the
 // pin driver fills the mesh section ("cell count", "cell size", "origin") so that the
 // reference's own Cartesian2DMesh constructor reads its geometry from it. Nothing else of the
-// configuration is used on the path.
+// configuration is used on the path. The NIMROD reader's driver sets "bbox" (and reads count()).
 #pragma once
 #include <array>
 #include <filesystem>
@@ -13,11 +13,14 @@
 #include <utility>
 #include <vector>
 
+namespace stdfs = std::filesystem;
+
 struct ConfigChild;
 class Config {
  public:
   std::map<std::string, std::string> kv;
   Config() {}
+  size_t count(const std::string& key) const { return kv.count(key); }
   template <typename T>
   T get(const std::string& key, const T& def = T()) const {
     auto it = kv.find(key);

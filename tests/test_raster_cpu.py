@@ -50,6 +50,8 @@ def test_malformed_files():
         nimrod_bytes(_grid(2, 3), 0.5, 1.5, 1.0, 1.0, h1={12: 2}),   # float with 2 bytes
         nimrod_bytes(_grid(2, 3), 0.5, 1.5, 1.0, 1.0, h1={11: 7}),   # unknown type
         nimrod_bytes(_grid(2, 3), 0.5, 1.5, 1.0, 1.0, h1={23: 1}),   # bottom-left origin
+        nimrod_bytes(_grid(2, 3), 0.5, 1.5, 1.0, 1.0, h1={15: -2}),  # negative row count
+        nimrod_bytes(_grid(2, 3), 0.5, 1.5, 1.0, 1.0, h1={16: 0}),   # no columns
     ]
     for b in bad:
         with pytest.raises(RasterError):
