@@ -748,6 +748,63 @@ constexpr int kSweepOut = 28;  // output columns per warp
 constexpr int kSweepPfWindow = 2, kSweepPfCell = 4;
 __device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
 
+// Prefetch plan of the interior sweeps. A warp's row of one field is 32 consecutive values of
+// an interior strip (columns gx0 .. gx0+31, all inside the mesh): at most two 128-byte lines
+// in FP32 and three in FP64. The plan gives each lane kPfSlots (field, line) pairs of the
+// fields the stage reads -- the window fields (stage input, bed, bed slopes) first, then the
+// per-cell fields -- so that a row ahead costs kPfSlots prefetch instructions per warp instead
+// of one per field with its address arithmetic. Pairs beyond 32 * kPfSlots are not prefetched.
+constexpr int kPfSlots = 2;
+template <typename T> struct PfPlan {
+  const T* p[kPfSlots];  // the lane's line in row 0 of its field, or null
+  int d[kPfSlots];       // rows ahead of the loop row: the window's or the per-cell fields'
+  __device__ __forceinline__ void init(const StageParams<T>& P, const DevForcing& fc, const T* Yh, const T* Yu,
+                                       const T* Yv, bool first, int cur, int gx0, int lane) {
+    constexpr int kLines = sizeof(T) == 4 ? 2 : 3;
+    constexpr int kLineCols = 128 / int(sizeof(T));
+    int fi[kPfSlots];
+#pragma unroll
+    for (int s = 0; s < kPfSlots; ++s) {
+      fi[s] = (lane + 32 * s) / kLines;
+      p[s] = nullptr;
+      d[s] = fi[s] < 6 ? 1 + kSweepPfWindow : kSweepPfCell - 2;
+    }
+    int n = 0;
+    auto add = [&](const T* f) {
+#pragma unroll
+      for (int s = 0; s < kPfSlots; ++s)
+        if (fi[s] == n) p[s] = f;
+      ++n;
+    };
+    add(Yh); add(Yu); add(Yv); add(P.z); add(P.zx); add(P.zy);
+    if (!first) {
+      for (int f = 0; f < 3; ++f) { add(P.S[cur][f]); add(P.S[cur ^ 1][f]); }
+    }
+    if (P.manning) {
+      for (int f = 0; f < 4; ++f) {
+        const T* m = P.man_p[f];
+        bool dup = false;
+        for (int e = 0; e < f; ++e) dup = dup || (P.man_p[e] == m);
+        if (m && !dup) add(m);
+      }
+    }
+    if (P.irate) { add(P.irate); add(P.icap); }
+    if (P.efx) { add(P.efx); add(P.efy); }
+    if (fc.rain_kind == 3) add(P.pat);
+    if (fc.rain_kind == 2) { add(P.q0p); add(P.q1p); }
+    if (fc.head_kind == 2) { add(P.hb0p); add(P.hb1p); }
+#pragma unroll
+    for (int s = 0; s < kPfSlots; ++s)
+      if (p[s]) p[s] += gx0 + min(((lane + 32 * s) % kLines) * kLineCols, 31);
+  }
+  // the rows k + d of every slot, clamped into the mesh
+  __device__ __forceinline__ void rows(int k, int nx, int ny) const {
+#pragma unroll
+    for (int s = 0; s < kPfSlots; ++s)
+      if (p[s]) prefetch_l1(p[s] + (long long)min(max(k + d[s], 0), ny - 1) * nx);
+  }
+};
+
 // One warp's strip `gw` (row-major over strips of kSweepOut columns x TY rows) of one
 // solver's stage. Called by the single-solver kernel (P in parameter space) and by the
 // batched kernel (P in shared memory).
@@ -1025,28 +1082,8 @@ __device__ __forceinline__ void sweep_strip_interior(const StageParams<T>& P, lo
     v.zx = ld(P.zx, g); v.zy = ld(P.zy, g);
     return v;
   };
-  auto prefetch_rows = [&](int k) {
-    {
-      const int r = min(k + 1 + kSweepPfWindow, ny - 1);
-      const long long g = (long long)r * nx + gx;
-      prefetch_l1(Yh + g); prefetch_l1(Yu + g); prefetch_l1(Yv + g);
-      prefetch_l1(P.z + g); prefetch_l1(P.zx + g); prefetch_l1(P.zy + g);
-    }
-    const int r = min(k - 2 + kSweepPfCell, ny - 1);
-    const long long g = (long long)r * nx + gx;
-    if (!first) {
-      for (int f = 0; f < 3; ++f) { prefetch_l1(P.S[cur][f] + g); prefetch_l1(P.S[cur ^ 1][f] + g); }
-    }
-    if (P.manning) {
-      for (int f = 0; f < 4; ++f)
-        if (P.man_p[f]) prefetch_l1(P.man_p[f] + g);
-    }
-    if (P.irate) { prefetch_l1(P.irate + g); prefetch_l1(P.icap + g); }
-    if (P.efx) { prefetch_l1(P.efx + g); prefetch_l1(P.efy + g); }
-    if (fc.rain_kind == 3) prefetch_l1(P.pat + g);
-    if (fc.rain_kind == 2) { prefetch_l1(P.q0p + g); prefetch_l1(P.q1p + g); }
-    if (fc.head_kind == 2) { prefetch_l1(P.hb0p + g); prefetch_l1(P.hb1p + g); }
-  };
+  PfPlan<T> pf;
+  pf.init(P, fc, Yh, Yu, Yv, first, cur, gx - lane, lane);
 
   RowV<T> Rm{}, R0{}, Rp{};
   SlopeV<T> Sm{}, S0{};
@@ -1057,7 +1094,7 @@ __device__ __forceinline__ void sweep_strip_interior(const StageParams<T>& P, lo
   T xcfl = T(0), xmin = T(1.0 / 0.0);
 
   for (int k = y0 - 2; k <= y0 + TY + 1; ++k) {
-    prefetch_rows(k);
+    pf.rows(k, nx, ny);
     Rm = R0; R0 = Rp; Rp = load_row(k);
     if constexpr (EDDY) { Smm_uy = Sm.uy; Smm_vy = Sm.vy; }
     Sm = S0;
