@@ -108,10 +108,15 @@ __device__ __forceinline__ float sfmax(float x, float y) { return fmaxf(x, y); }
 __device__ __forceinline__ double sfmin(double x, double y) { return fmin(x, y); }
 __device__ __forceinline__ float sfmin(float x, float y) { return fminf(x, y); }
 __device__ __forceinline__ double ssqrt(double x) { return sqrt(x); }
-// FP32 path: the hardware reciprocal square root (about 2 ulp) instead of the correctly
-// rounded square root; 0, infinity and NaN pass through unchanged. The FP32 path is held to
-// a depth tolerance, not to bit parity, and this saves about 8 instructions per root.
-__device__ __forceinline__ float ssqrt(float x) { return (x > 0.0f && x < INFINITY) ? x * rsqrtf(x) : x; }
+// FP32 path: the hardware's approximate square root (sqrt.approx, a relative error of a few
+// ulp) instead of the correctly rounded one; 0, infinity and NaN pass through, subnormal
+// arguments (depths below 1e-39 m, speeds below 1e-19 m/s) count as 0. The FP32 path is held
+// to a depth tolerance, not to bit parity. The arguments here are never negative.
+__device__ __forceinline__ float ssqrt(float x) {
+  float r;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
 __device__ __forceinline__ double sfabs(double x) { return fabs(x); }
 __device__ __forceinline__ float sfabs(float x) { return fabsf(x); }
 

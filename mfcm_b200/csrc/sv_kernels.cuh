@@ -384,7 +384,9 @@ __device__ __forceinline__ void finish_cell(const StageParams<T>& P, const DevFo
 #pragma unroll
       for (int f = 0; f < 3; ++f) {
         T y = u0v[f] + k[f] * cA;
-        if (!first && finite_(u0v[f]) && !finite_(accv[f])) y = Lim<T>::nan();
+        // FP32 leaves this out: a non-finite accumulator reaches U_N at the last stage anyway
+        if constexpr (sizeof(T) == 8)
+          if (!first && finite_(u0v[f]) && !finite_(accv[f])) y = Lim<T>::nan();
         P.Yout[f][g] = y;
       }
     }
@@ -1092,6 +1094,7 @@ __device__ __forceinline__ void sweep_strip_interior(const StageParams<T>& P, lo
   FaceF<T> FS{}, FN{};
   double rain = 0.0, removed = 0.0, walls = 0.0, vol = 0.0;
   T xcfl = T(0), xmin = T(1.0 / 0.0);
+  T xstep = T(0);  // datum step of the west face in the current tile row (xcross lanes)
 
   for (int k = y0 - 2; k <= y0 + TY + 1; ++k) {
     pf.rows(k, nx, ny);
@@ -1163,8 +1166,20 @@ __device__ __forceinline__ void sweep_strip_interior(const StageParams<T>& P, lo
       const Side<T> mW{up1(mE.zb), up1(mE.h), up1(mE.un), up1(mE.ut)};
       CellV<T> meW = me;
       if (xcross) {
-        const long long tb = datum_tile(gx, r, P.dtiles_x);
-        meW.z = T(double(me.z) + (P.zdat[tb] - P.zdat[tb - 1]));
+        // the datum step across the tile column edge, read once per tile row: datums are
+        // multiples of 2^-10 m, so the step is exact in FP32 (below 2^14 m) and me.z + step
+        // rounds as the FP64 sum does; an inexact step (NaN here) takes the FP64 sum
+        if (r == y0 || (r % kDatumTY) == 0) {
+          const long long tb = datum_tile(gx, r, P.dtiles_x);
+          const double st = P.zdat[tb] - P.zdat[tb - 1];
+          xstep = double(T(st)) == st ? T(st) : Lim<T>::nan();
+        }
+        if (xstep == xstep) {
+          meW.z = me.z + xstep;
+        } else {
+          const long long tb = datum_tile(gx, r, P.dtiles_x);
+          meW.z = T(double(me.z) + (P.zdat[tb] - P.zdat[tb - 1]));
+        }
       }
       FaceF<T> FW;
       face_combine<T, 0, TCHK>(mW, side_p<T, 0, TCHK>(meW, hdx), divx, FW);
