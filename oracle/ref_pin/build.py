@@ -67,6 +67,10 @@ COPY = [
     "SaintVenant/Boundaries/DischargeBoundarySourceTerm.cpp",
     "SaintVenant/Boundaries/HeadBoundarySourceTerm.hpp",
     "SaintVenant/Boundaries/HeadBoundarySourceTerm.cpp",
+    "SaintVenant/SourceTerms/EnergyLossSourceTerm.hpp", "SaintVenant/SourceTerms/EnergyLossSourceTerm.cpp",
+    "SaintVenant/SourceTerms/InfiltrationSourceTerm.hpp", "SaintVenant/SourceTerms/InfiltrationSourceTerm.cpp",
+    "SaintVenant/SourceTerms/EddyViscositySourceTerm.hpp", "SaintVenant/SourceTerms/EddyViscositySourceTerm.cpp",
+    "SaintVenant/Boundaries/StageBoundarySourceTerm.hpp", "SaintVenant/Boundaries/StageBoundarySourceTerm.cpp",
     "Config/TimeParameters.hpp", "Config/TimeParameters.cpp",
     "TemporalScheme/TemporalScheme.hpp", "TemporalScheme/RungeKutta.hpp", "TemporalScheme/RungeKutta.cpp",
 ]

@@ -15,6 +15,12 @@
 //   Manning roughness                     ManningRoughnessSourceKernel (:44-88)
 //   discharge and head boundaries         DischargeBoundarySourceKernel (:39-69),
 //                                         HeadBoundarySourceKernel (:39-67)
+//   further source and boundary terms     EnergyLossSourceKernel (EnergyLossSourceTerm.cpp),
+//                                         InfiltrationSourceKernel (InfiltrationSourceTerm.cpp),
+//                                         EddyViscositySourceKernel and SmagorinskyCoefficientKernel
+//                                         with the second derivatives of EddyViscositySourceTerm::
+//                                         apply (EddyViscositySourceTerm.hpp:222-257),
+//                                         StageBoundarySourceKernel (StageBoundarySourceTerm.cpp)
 //   control number                        SaintVenantState::max_control_number (State.cpp:195-230)
 //   stage combination                     the SaintVenantState operators (State.cpp:88-174) in
 //                                         the order of RungeKuttaSolver::update_y
@@ -57,6 +63,14 @@
 #include "DischargeBoundarySourceTerm.cpp"
 #include "HeadBoundarySourceTerm.hpp"
 #include "HeadBoundarySourceTerm.cpp"
+#include "EnergyLossSourceTerm.hpp"
+#include "EnergyLossSourceTerm.cpp"
+#include "InfiltrationSourceTerm.hpp"
+#include "InfiltrationSourceTerm.cpp"
+#include "EddyViscositySourceTerm.hpp"
+#include "EddyViscositySourceTerm.cpp"
+#include "StageBoundarySourceTerm.hpp"
+#include "StageBoundarySourceTerm.cpp"
 #include "TimeParameters.hpp"
 #include "TimeParameters.cpp"
 #include "RungeKutta.hpp"
@@ -275,6 +289,127 @@ int dudt(uint64_t nx, uint64_t ny, double dx, double dy, const T* z, const T* h,
     for (FF* f : faces) { read(*f, o); o += nf; }
     CF<T>* ks[] = {&dUdt.h(), &dUdt.u(), &dUdt.v()};
     for (CF<T>* f : ks) { read(*f, o); o += nc; }
+    return 0;
+  } catch (const std::exception& e) {
+    std::cerr << "ref_pin: " << e.what() << std::endl;
+    return -1;
+  }
+}
+
+// One update_dUdt with the further source and boundary terms. f[] holds the optional per-cell
+// arrays (null = term off): 0-3 Manning n_shallow, n_deep, d_shallow, d_deep; 4-5 energy-loss
+// fx, fy; 6 infiltration rate (icap, the capacity, is read and written back); 7 the eddy-
+// viscosity coefficient mu (eddy mode 1); 8-9 discharge q0, q1; 10-11 stage levels l0, l1.
+// iopt: eddy mode (0 off, 1 coefficient field, 2 Smagorinsky with dopt[0], dopt[1]), head_first
+// (the stage boundary before the discharge), and the configured order of the momentum terms
+// (three codes: 1 roughness, 2 energy loss, 3 eddy viscosity). Infiltration, which touches
+// dh/dt only, runs after them. dopt: mu_const, mu_smag, time_now, timestep, step_length.
+// out: dh/dt, du/dt, dv/dt.
+template <typename T>
+int dudt_terms(uint64_t nx, uint64_t ny, double dx, double dy, const T* z, const T* h, const T* u, const T* v,
+               const T* const* f, T* icap, const int* iopt, const double* dopt, T* out) {
+  try {
+    using TT = T;
+    const TT tnow = TT(dopt[2]), tstep = TT(dopt[3]), tlen = TT(dopt[4]);
+    auto q = get_sycl_queue();
+    auto mesh = make_mesh(q, nx, ny, dx, dy);
+    const size_t nc = nx * ny;
+    PinBed<T>::z = vec(z, nc);
+    SaintVenantConstants<T, Cartesian2DMesh> K(mesh, true);
+    State<T> U(T(0), mesh), dUdx(T(0), mesh), dUdy(T(0), mesh), dUdt(T(0), mesh);
+    set_state(U, q, mesh, h, u, v, nc);
+    SaintVenantFluxes<T, Cartesian2DMesh> F(mesh);
+    U.calculate_spatial_derivatives(dUdx, dUdy);
+    F.update(U, K, dUdx, dUdy);
+    using TDKernel = SaintVenantTemporalDerivativeKernel<T, Cartesian2DMesh>;
+    q->submit([&](sycl::handler& cgh) {
+      auto kernel = TDKernel(cgh, U, K, dUdx, dUdy, F, dUdt, tnow, tstep);
+      cgh.parallel_for(sycl::range<1>(nc), kernel);
+    });
+    auto manning = [&]() {
+      if (!f[0]) return;
+      CF<T> fns(q, "n_shallow", mesh, vec(f[0], nc), true), fnd(q, "n_deep", mesh, vec(f[1], nc), true);
+      CF<T> fds(q, "d_shallow", mesh, vec(f[2], nc), true), fdd(q, "d_deep", mesh, vec(f[3], nc), true);
+      CF<T> nh(q, "mannings_n", mesh, 0.0f, true), Sf(q, "friction_slope", mesh, 0.0f, true);
+      using Kernel = ManningRoughnessSourceKernel<TT, T, Cartesian2DMesh>;
+      q->submit([&](sycl::handler& cgh) {
+        auto kernel = Kernel(cgh, U, K, fns, fnd, fds, fdd, nh, Sf, dUdt, tstep);
+        cgh.parallel_for(sycl::range<1>(nc), kernel);
+      });
+    };
+    auto eloss = [&]() {
+      if (!f[4]) return;
+      CF<T> fx(q, "fx", mesh, vec(f[4], nc), true), fy(q, "fy", mesh, vec(f[5], nc), true);
+      using Kernel = EnergyLossSourceKernel<TT, T, Cartesian2DMesh>;
+      q->submit([&](sycl::handler& cgh) {
+        auto kernel = Kernel(cgh, U, K, fx, fy, dUdt, tstep);
+        cgh.parallel_for(sycl::range<1>(nc), kernel);
+      });
+    };
+    auto eddy = [&]() {
+      if (iopt[0] == 0) return;
+      // EddyViscositySourceTerm::apply (EddyViscositySourceTerm.hpp:222-257)
+      using SpatialDerivative = SpatialDerivativeOperator<T, Cartesian2DMesh, MeshComponent::Cell, Minmod3<T>>;
+      CF<T> d2udx2(q, "d2udx2", mesh, 0.0, true), d2udy2(q, "d2udy2", mesh, 0.0, true);
+      CF<T> d2vdx2(q, "d2vdx2", mesh, 0.0, true), d2vdy2(q, "d2vdy2", mesh, 0.0, true);
+      SpatialDerivative::template apply<SpatialDerivativeAxis::X>(dUdx.u(), d2udx2);
+      SpatialDerivative::template apply<SpatialDerivativeAxis::Y>(dUdy.u(), d2udy2);
+      SpatialDerivative::template apply<SpatialDerivativeAxis::X>(dUdx.v(), d2vdx2);
+      SpatialDerivative::template apply<SpatialDerivativeAxis::Y>(dUdy.v(), d2vdy2);
+      const T mu_const = T(iopt[0] == 2 ? dopt[0] : std::nan("")), mu_smag = T(iopt[0] == 2 ? dopt[1] : std::nan(""));
+      CF<T> mu(q, "mu", mesh, iopt[0] == 1 ? vec(f[7], nc) : std::vector<T>(nc, T(0)), true);
+      if (!(mu_const != mu_const) && !(mu_smag != mu_smag)) {
+        q->submit([&](sycl::handler& cgh) {
+          auto kernel = SmagorinskyCoefficientKernel<T, Cartesian2DMesh>(cgh, mu_const, mu_smag, dUdx.u(), dUdy.u(),
+                                                                         dUdx.v(), dUdy.v(), mu);
+          cgh.parallel_for(sycl::range<1>(nc), kernel);
+        });
+      }
+      using Kernel = EddyViscositySourceKernel<TT, T, Cartesian2DMesh>;
+      q->submit([&](sycl::handler& cgh) {
+        auto kernel = Kernel(cgh, U, K, mu, d2udx2, d2udy2, d2vdx2, d2vdy2, dUdt, tstep);
+        cgh.parallel_for(sycl::range<1>(nc), kernel);
+      });
+    };
+    for (int i = 0; i < 3; ++i) {
+      const int t = iopt[2 + i];
+      if (t == 1) manning();
+      else if (t == 2) eloss();
+      else if (t == 3) eddy();
+    }
+    CF<T> cap(q, "infiltration_capacity", mesh, icap ? vec(icap, nc) : std::vector<T>(nc, T(0)), true);
+    if (f[6]) {
+      CF<T> rate(q, "infiltration_rate", mesh, vec(f[6], nc), true);
+      using Kernel = InfiltrationSourceKernel<TT, T, Cartesian2DMesh>;
+      q->submit([&](sycl::handler& cgh) {
+        auto kernel = Kernel(cgh, U, K, rate, cap, dUdt, tstep);
+        cgh.parallel_for(sycl::range<1>(nc), kernel);
+      });
+    }
+    auto discharge = [&]() {
+      if (!f[8]) return;
+      CF<T> f0(q, "qbdy0", mesh, vec(f[8], nc), true), f1(q, "qbdy1", mesh, vec(f[9], nc), true);
+      using Kernel = DischargeBoundarySourceKernel<T, Cartesian2DMesh>;
+      q->submit([&](sycl::handler& cgh) {
+        auto kernel = Kernel(cgh, U, K, f0, f1, dUdt, tstep, tnow, tlen);
+        cgh.parallel_for(sycl::range<1>(nc), kernel);
+      });
+    };
+    auto stage = [&]() {
+      if (!f[10]) return;
+      CF<T> f0(q, "hbdy0", mesh, vec(f[10], nc), true), f1(q, "hbdy1", mesh, vec(f[11], nc), true);
+      using Kernel = StageBoundarySourceKernel<T, Cartesian2DMesh>;
+      q->submit([&](sycl::handler& cgh) {
+        auto kernel = Kernel(cgh, U, K, f0, f1, dUdt, double(tstep), double(tnow), double(tlen));
+        cgh.parallel_for(sycl::range<1>(nc), kernel);
+      });
+    };
+    if (iopt[1]) { stage(); discharge(); }
+    else { discharge(); stage(); }
+    T* o = out;
+    CF<T>* ks[] = {&dUdt.h(), &dUdt.u(), &dUdt.v()};
+    for (CF<T>* k : ks) { read(*k, o); o += nc; }
+    if (icap) read(cap, icap);
     return 0;
   } catch (const std::exception& e) {
     std::cerr << "ref_pin: " << e.what() << std::endl;
@@ -557,6 +692,16 @@ int refpin_dudt_f32(uint64_t nx, uint64_t ny, double dx, double dy, const float*
                     double timestep, double step_length, float* out) {
   return dudt<float>(nx, ny, dx, dy, z, h, u, v, ns, nd, ds, dd, q0, q1, hb0, hb1, head_first, time_now, timestep,
                      step_length, out);
+}
+int refpin_dudt_terms_f64(uint64_t nx, uint64_t ny, double dx, double dy, const double* z, const double* h,
+                          const double* u, const double* v, const double* const* f, double* icap, const int* iopt,
+                          const double* dopt, double* out) {
+  return dudt_terms<double>(nx, ny, dx, dy, z, h, u, v, f, icap, iopt, dopt, out);
+}
+int refpin_dudt_terms_f32(uint64_t nx, uint64_t ny, double dx, double dy, const float* z, const float* h,
+                          const float* u, const float* v, const float* const* f, float* icap, const int* iopt,
+                          const double* dopt, float* out) {
+  return dudt_terms<float>(nx, ny, dx, dy, z, h, u, v, f, icap, iopt, dopt, out);
 }
 int refpin_control_number_f64(uint64_t nx, uint64_t ny, double dx, double dy, const double* h, const double* u,
                               const double* v, double timestep, double* cn) {

@@ -44,6 +44,10 @@ def load():
             f.argtypes = [C.c_uint64, C.c_uint64, C.c_double, C.c_double, P, P, P, P, D, D, D, C.c_int, C.c_uint,
                           C.c_double, C.c_int, C.c_char_p, C.c_double, C.c_double, C.c_double, C.c_double, P,
                           C.POINTER(C.c_uint64)]
+            f = getattr(_lib, f"refpin_dudt_terms_{t}")
+            f.restype = C.c_int
+            f.argtypes = [C.c_uint64, C.c_uint64, C.c_double, C.c_double] + [P] * 4 + \
+                         [C.POINTER(P), P, C.POINTER(C.c_int), C.POINTER(C.c_double), P]
             f = getattr(_lib, f"refpin_update_y_{t}")
             f.restype = C.c_int
             f.argtypes = [C.c_uint64, C.c_uint64, C.c_double, C.c_double, P, P, C.c_int,
@@ -96,6 +100,61 @@ def dudt(z, h, u, v, dx, dy=None, manning=None, q=None, head=None, head_first=Fa
     for name in KS:
         res[name] = out[o:o + nc].reshape(ny, nx)
         o += nc
+    return res
+
+
+def dudt_terms(z, h, u, v, dx, dy=None, manning=None, eloss=None, infil=None, eddy=None, q=None, stage=None,
+               stage_first=False, order=(1, 2, 3), time_now=0.0, timestep=1.0, step_length=60.0, precision="f64"):
+    """One update_dUdt with the further source and boundary terms through the reference's
+    kernels: manning = (ns, nd, ds, dd) cell arrays, eloss = (fx, fy), infil = (rate, capacity),
+    eddy = ("field", mu) or ("smagorinsky", mu_const, mu_smag), q = (q0, q1) discharge values,
+    stage = (l0, l1) water levels (NaN = not selected); `order` the configured order of the
+    momentum terms (1 roughness, 2 energy loss, 3 eddy viscosity). Returns dh/dt, du/dt, dv/dt
+    and the infiltration capacity after the evaluation (None without infiltration)."""
+    lib = load()
+    dt_, ct = _np(precision)
+    dy = dx if dy is None else dy
+    ny, nx = h.shape
+    nc = nx * ny
+    arr = lambda a: None if a is None else np.ascontiguousarray(a, dtype=dt_)
+    keep = []
+    slots = [None] * 12
+
+    def put(i, a):
+        a = arr(a)
+        keep.append(a)
+        slots[i] = a
+
+    for i, a in enumerate(manning or ()):
+        put(i, a)
+    if eloss:
+        put(4, eloss[0]); put(5, eloss[1])
+    cap = None
+    if infil:
+        put(6, infil[0])
+        cap = arr(infil[1]).copy()
+    mode, mu_c, mu_s = 0, 0.0, 0.0
+    if eddy:
+        if eddy[0] == "field":
+            mode = 1
+            put(7, eddy[1])
+        else:
+            mode, mu_c, mu_s = 2, float(eddy[1]), float(eddy[2])
+    if q:
+        put(8, q[0]); put(9, q[1])
+    if stage:
+        put(10, stage[0]); put(11, stage[1])
+    F = (C.POINTER(ct) * 12)(*[_ptr(a, ct) if a is not None else None for a in slots])
+    iopt = (C.c_int * 5)(mode, 1 if stage_first else 0, *list(order))
+    dopt = (C.c_double * 5)(mu_c, mu_s, time_now, timestep, step_length)
+    ins = [arr(a) for a in (z, h, u, v)]
+    out = np.empty(3 * nc, dtype=dt_)
+    r = getattr(lib, f"refpin_dudt_terms_{precision}")(nx, ny, dx, dy, *[_ptr(a, ct) for a in ins], F, _ptr(cap, ct),
+                                                       iopt, dopt, _ptr(out, ct))
+    if r != 0:
+        raise RuntimeError("reference kernels failed")
+    res = {name: out[i * nc:(i + 1) * nc].reshape(ny, nx) for i, name in enumerate(KS)}
+    res["INFIL_CAP"] = None if cap is None else cap.reshape(ny, nx)
     return res
 
 

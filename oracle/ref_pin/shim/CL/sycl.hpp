@@ -14,7 +14,8 @@
 //     min/max by comparison, mix, smoothstep, clamp). pow(x, 4/3) -- the only pow of the hot
 //     path, whose accuracy SYCL leaves to the implementation -- is, in FP64, the shared
 //     division-free sv_math::pow43 that both the oracle and the CUDA path use; FP32 and
-//     other exponents go to std::pow, as in the oracle.
+//     other exponents go to std::pow, as in the oracle, except an integer exponent of 2,
+//     which is the correctly rounded square x * x.
 #pragma once
 
 #include <algorithm>
@@ -277,6 +278,13 @@ T pow(T x, T y) {
   if constexpr (std::is_same<T, double>::value)
     if (y == 4.0 / 3.0) return sv_math::pow43(x);
   return std::pow(x, y);
+}
+// an integer exponent (the Smagorinsky coefficient's pow(..., 2)) converts to the value type;
+// the square is the correctly rounded x * x, which is within any accuracy bound SYCL allows
+template <typename T, typename I, typename std::enable_if<std::is_integral<I>::value, int>::type = 0>
+T pow(T x, I n) {
+  if (n == 2) return x * x;
+  return pow(x, T(n));
 }
 
 }  // namespace sycl

@@ -647,14 +647,16 @@ class Solver final : public SolverBase {
   // SmagorinskyCoefficientKernel::operator() (EddyViscositySourceTerm.cpp:97-110) when
   // Smagorinsky, else the coefficient field (or its default); then
   // EddyViscositySourceKernel::operator() (EddyViscositySourceTerm.cpp:46-78). The square
-  // pow(x, 2) is taken as x * x.
+  // pow(x, 2) is taken as x * x. The reference's 0.5 is a double literal, so in FP32 the sum
+  // under the root, the root and the products and sum after it are formed in FP64 and the
+  // coefficient is rounded once (EddyViscositySourceTerm.cpp:104-108).
   void eddy_cell(size_t c, const State& S, State& D, double timestep) {
     T mu;
     if (p.eddy == 2) {
       T cell_area = T(m.cell_area());
       T a = std::fabs(dUdy.u[c]) + std::fabs(dUdx.v[c]);
-      mu = T(p.eddy_c) + T(p.eddy_s) * cell_area *
-           std::sqrt(dUdx.u[c] * dUdx.u[c] + dUdy.v[c] * dUdy.v[c] + T(0.5) * (a * a));
+      T s = dUdx.u[c] * dUdx.u[c] + dUdy.v[c] * dUdy.v[c];
+      mu = T(T(p.eddy_c) + T(p.eddy_s) * cell_area * std::sqrt(s + 0.5 * (a * a)));
     } else {
       mu = emu_set ? emu[c] : T(p.eddy_mu);
     }

@@ -11,7 +11,7 @@ import os
 import numpy as np
 import pytest
 
-from mfcm_b200 import solve, Forcing, RAIN_FIELDS, HEAD_FIELDS
+from mfcm_b200 import solve, Forcing, RAIN_FIELDS, HEAD_FIELDS, STAGE_FIELDS
 from oracle.sv_oracle_py import OracleSolver
 from tests.scenarios import setup, forcing, rain_series, same
 
@@ -93,6 +93,33 @@ def check_ref_dudt(kind, prec="f64"):
         assert same(b.get_field(f), g[f].astype(np.float64)), f
 
 
+def check_ref_dudt_terms(kind, prec="f64"):
+    """One update_dUdt of the reference's kernels with every further term (energy loss,
+    infiltration, Smagorinsky eddy viscosity, a stage boundary): dU/dt and the infiltration
+    capacity left."""
+    g = load(f"ref_dudt_terms_23x17_{prec}")
+    nx, ny = int(g["nx"]), int(g["ny"])
+    b = backend(kind, nx, ny, float(g["dx"]), dy=float(g["dy"]), precision=prec, rain_mode="reference",
+                step_duration=float(g["step_duration"]), head_first=bool(g["stage_first"]))
+    setup(b, *(g[k].astype(np.float64) for k in ("z", "h", "u", "v")))
+    f = Forcing()
+    f.rain_kind, f.head_kind = RAIN_FIELDS, STAGE_FIELDS
+    per_cell = ("n_shallow", "n_deep", "d_shallow", "d_deep", "qbdy0", "qbdy1", "hbdy0", "hbdy1")
+    for name in per_cell:
+        b.set_field(name.upper(), g[name].astype(np.float64))
+    b.set_forcing(f)
+    for name in ("qbdy0", "qbdy1", "hbdy0", "hbdy1"):
+        b.set_field(name.upper(), g[name].astype(np.float64))
+    for field, key in (("ELOSS_FX", "eloss_fx"), ("ELOSS_FY", "eloss_fy"), ("INFIL_RATE", "infil_rate"),
+                       ("INFIL_CAP", "infil_cap0")):
+        b.set_field(field, g[key].astype(np.float64))
+    b.set_eddy_viscosity("smagorinsky", mu_const=float(g["mu_const"]), mu_smag=float(g["mu_smag"]))
+    b.set_source_order([{1: "manning", 2: "energy loss", 3: "eddy viscosity"}[int(k)] for k in g["order"]])
+    b.eval_dudt(0, float(g["t_sub"]), float(g["dt"]))
+    for f in KS + ["INFIL_CAP"]:
+        assert same(b.get_field(f), g[f].astype(np.float64)), f
+
+
 def check_ref_solve(kind, name):
     """Two steps through the reference's RungeKuttaSolver::solve (control-number target 1.0):
     the number of timesteps taken and the final state."""
@@ -115,6 +142,9 @@ REF_CPU = [lambda k: check_ref_dudt(k, "f64"), lambda k: check_ref_dudt(k, "f32"
            lambda k: check_ref_solve(k, "ref_solve_45x30_classic_f32")]
 # the CUDA FP32 path is held to a depth tolerance against FP64, not to the reference's FP32 bits
 REF_GPU = REF_CPU[:1] + REF_CPU[2:4]
+# the further terms: the oracle against the reference (the CUDA path meets the oracle bit for
+# bit on them in tests/test_gpu_source_terms.py and tests/test_gpu_eddy.py)
+REF_TERMS_CPU = [lambda k: check_ref_dudt_terms(k, "f64"), lambda k: check_ref_dudt_terms(k, "f32")]
 
 
 @pytest.mark.parametrize("check", [check_dudt, check_timestep, check_steps])
@@ -125,6 +155,11 @@ def test_oracle_matches_golden(check):
 @pytest.mark.parametrize("check", REF_CPU, ids=["dudt_f64", "dudt_f32", "solve_classic_f64", "solve_kutta3_f64",
                                                 "solve_classic_f32"])
 def test_oracle_matches_reference_golden(check):
+    check("cpu")
+
+
+@pytest.mark.parametrize("check", REF_TERMS_CPU, ids=["dudt_terms_f64", "dudt_terms_f32"])
+def test_oracle_matches_reference_golden_further_terms(check):
     check("cpu")
 
 

@@ -11,7 +11,7 @@ fixtures made from it (tests/golden/make_ref_golden.py) carry the same checks ev
 import numpy as np
 import pytest
 
-from mfcm_b200 import synth, solve, Forcing, TimeSeries, RK_METHODS, RAIN_FIELDS, HEAD_FIELDS
+from mfcm_b200 import synth, solve, Forcing, TimeSeries, RK_METHODS, RAIN_FIELDS, HEAD_FIELDS, STAGE_FIELDS
 from oracle.ref_pin import refpin
 from oracle.sv_oracle_py import OracleSolver
 from tests.scenarios import wet_dry_state, setup, first_diff
@@ -171,3 +171,72 @@ TABLEAUX = {
     "3/8rule": [[0.0], [1.0 / 3.0, 1.0 / 3.0], [2.0 / 3.0, -1.0 / 3.0, 1.0], [1.0, 1.0, -1.0, 1.0],
                 [0.0, 1.0 / 8.0, 3.0 / 8.0, 3.0 / 8.0, 1.0 / 8.0]],
 }
+
+
+TERM_NAMES = {1: "manning", 2: "energy loss", 3: "eddy viscosity"}
+
+
+def _oracle_terms(prec, nx, ny, dx, dy, z, h, u, v, man, eloss, infil, eddy, q, stage, stage_first, order, t, dt, L):
+    o = OracleSolver(nx, ny, dx, dy, precision=prec, rain_mode="reference", step_duration=L, head_first=stage_first,
+                     manning=man is not None)
+    for name, a in (("Z", z), ("H", h), ("U", u), ("V", v)):
+        o.set_field(name, a)
+    f = Forcing()
+    f.rain_kind = RAIN_FIELDS if q else 0
+    f.head_kind = STAGE_FIELDS if stage else 0
+    o.set_forcing(f)  # per-cell boundary values are uploaded after the forcing
+    fields = []
+    if man:
+        fields += list(zip(("N_SHALLOW", "N_DEEP", "D_SHALLOW", "D_DEEP"), man))
+    if q:
+        fields += [("QBDY0", q[0]), ("QBDY1", q[1])]
+    if stage:
+        fields += [("HBDY0", stage[0]), ("HBDY1", stage[1])]
+    if eloss:
+        fields += [("ELOSS_FX", eloss[0]), ("ELOSS_FY", eloss[1])]
+    if infil:
+        fields += [("INFIL_RATE", infil[0]), ("INFIL_CAP", infil[1])]
+    for name, a in fields:
+        o.set_field(name, a)
+    if eddy and eddy[0] == "field":
+        o.set_eddy_viscosity("constant", mu=0.7)
+        o.set_field("EDDY_MU", eddy[1])
+    elif eddy:
+        o.set_eddy_viscosity("smagorinsky", mu_const=eddy[1], mu_smag=eddy[2])
+    o.set_source_order([TERM_NAMES[k] for k in order])
+    o.eval_dudt(0, t, dt)
+    return o
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+@pytest.mark.parametrize("shape,dxy,nan_cells,eddy_mode,order,stage_first", [
+    ((23, 17), (3.0, 3.0), 0, "smagorinsky", (1, 2, 3), False),
+    ((23, 17), (3.0, 3.0), 6, "field", (3, 1, 2), True),
+    ((19, 12), (2.0, 5.0), 0, "smagorinsky", (2, 3, 1), False),
+    ((1, 9), (1.5, 1.5), 0, "field", (2, 1, 3), True),
+    ((9, 1), (1.5, 1.5), 0, "smagorinsky", (3, 2, 1), False),
+    ((40, 3), (0.5, 0.25), 4, "smagorinsky", (1, 3, 2), True)])
+def test_further_terms_match_reference_kernels(prec, shape, dxy, nan_cells, eddy_mode, order, stage_first):
+    """dU/dt with energy loss, infiltration (and its capacity, consumed in place), eddy
+    viscosity (a coefficient field or the Smagorinsky coefficient) and a stage boundary, beside
+    Manning roughness and the discharge boundary, in the configured order of the momentum terms:
+    the reference's EnergyLoss, Infiltration, EddyViscosity, SmagorinskyCoefficient and
+    StageBoundary kernels against the oracle."""
+    nx, ny = shape
+    dx, dy = dxy
+    z, h, u, v = wet_dry_state(nx, ny, dx, seed=nx * 5 + ny, nan_cells=nan_cells)
+    man, q, _ = boundary_fields(nx, ny, seed=nx + ny + 1)
+    rng = np.random.default_rng(nx * ny)
+    eloss = (rng.uniform(0.0, 0.5, (ny, nx)), rng.uniform(0.0, 0.5, (ny, nx)))
+    infil = (rng.uniform(0.0, 2e-5, (ny, nx)), rng.uniform(0.0, 2e-3, (ny, nx)) * (rng.uniform(size=(ny, nx)) > 0.2))
+    eddy = ("field", rng.uniform(0.0, 2.0, (ny, nx))) if eddy_mode == "field" else ("smagorinsky", 0.05, 0.5)
+    sel = rng.uniform(size=(ny, nx)) > 0.7
+    zf = np.nan_to_num(z, nan=0.0)
+    stage = (np.where(sel, zf + rng.uniform(-0.05, 0.2, (ny, nx)), np.nan), np.where(sel, zf + 0.03, np.nan))
+    t, dt, L = 7.5, 0.37, 60.0
+    ref = refpin.dudt_terms(z, h, u, v, dx, dy, manning=man, eloss=eloss, infil=infil, eddy=eddy, q=q, stage=stage,
+                            stage_first=stage_first, order=order, time_now=t, timestep=dt, step_length=L,
+                            precision=prec)
+    o = _oracle_terms(prec, nx, ny, dx, dy, z, h, u, v, man, eloss, infil, eddy, q, stage, stage_first, order, t, dt, L)
+    for name, a in ref.items():
+        assert_same(a, o.get_field(name), name)
