@@ -832,6 +832,8 @@ class Model:
         With `write_outputs` false, no file is written."""
         outs = self.outputs() if write_outputs else []
         meas = self.measures() if write_outputs else []
+        for m in meas:  # the measures' values (and times) are written in the solver's value type
+            m.value_type = np.float64 if getattr(solver, "precision", "f64") == "f64" else np.float32
         n = num_steps(self.start_time, self.end_time, self.step_duration)
         per_step = []
         for i in range(n):

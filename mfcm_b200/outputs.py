@@ -3,9 +3,10 @@
 - Timed multi-field CSV files (MultiFieldOutputFile, src/Output/OutputFile.hpp:159-224): one file
   `<name>_<std::to_string(t)>.csv` whenever t reaches start + every * n. Each file has a header
   `X, Y, "f1", "f2", ` and one row per cell `x, y, v1, v2, `, the delimiter ", " ending every
-  entry (CSVOutput, src/Output/OutputFormat.hpp:78-122). Coordinates are written as a C++
-  ostream writes a double (precision 6, %g); values as std::to_string does (%f,
-  OutputFunction.hpp:88-92).
+  entry (CSVOutput, src/Output/OutputFormat.hpp:78-122). Names are quoted as std::quoted
+  quotes them. Coordinates are written as a C++ ostream writes a double (precision 6, %g);
+  values as std::to_string does (%f, OutputFunction.hpp:88-92), a NaN with its sign bit set
+  as glibc's "-nan".
 - Raw binary (RawBinaryOutput, OutputFormat.hpp:47-76): three 64-bit unsigned integers
   (rows, columns, bytes per value), then the values row by row in the value type.
 - Measures (src/SaintVenant/Measure.hpp:57-177): the volume of the wetted domain and the depth
@@ -35,14 +36,27 @@ _NAMES = {"h": "H", "u": "U", "v": "V", "z_bed": "Z", "IR": "INFIL_RATE", "IC": 
           "fx": "ELOSS_FX", "fy": "ELOSS_FY", "fdx": "ELOSS_FX", "fdy": "ELOSS_FY", "h_comp": "H_COMP"}
 
 
+def _signed_nan(x, text):
+    """glibc's printf writes a NaN with its sign bit set as "-nan"."""
+    if x != x and math.copysign(1.0, x) < 0.0:
+        return "-" + text
+    return text
+
+
 def fmt_value(x):
     """std::to_string(double): printf %f."""
-    return "%f" % x
+    return _signed_nan(x, "%f" % x)
 
 
 def fmt_coord(x):
     """operator<<(std::ostream&, double) with the default precision 6: printf %g."""
-    return "%g" % x
+    return _signed_nan(x, "%g" % x)
+
+
+def quoted(name):
+    """std::quoted(name) on output: the name in double quotes, with every double quote and
+    backslash preceded by a backslash; everything else, non-ASCII text included, as is."""
+    return '"' + name.replace("\\", "\\\\").replace('"', '\\"') + '"'
 
 
 def cell_locations(nx, ny, dx, dy, origin_x=0.0, origin_y=0.0):
@@ -57,7 +71,7 @@ def cell_locations(nx, ny, dx, dy, origin_x=0.0, origin_y=0.0):
 def csv_text(names, columns, locations=None, delimiter=", "):
     """CSVOutput::output as text. `columns` are equal-length 1-D arrays; `locations` an
     (x, y) pair of arrays or None."""
-    q = [json.dumps(n) for n in names]  # std::quoted: double quotes, escaped quotes
+    q = [quoted(n) for n in names]
     head = (["X", "Y"] if locations is not None else []) + q
     lines = ["".join(h + delimiter for h in head)]
     cols = [np.asarray(c).ravel() for c in columns]
@@ -75,7 +89,7 @@ def write_csv(path, names, columns, locations=None, delimiter=", "):
     d = os.path.dirname(path)
     if d:
         os.makedirs(d, exist_ok=True)
-    with open(path, "w") as f:
+    with open(path, "w", encoding="utf-8", newline="\n") as f:
         f.write(csv_text(names, columns, locations, delimiter))
 
 
@@ -147,22 +161,27 @@ class VolumeMeasure:
 class DepthPointMeasure:
     """SaintVenantHPointMeasure (Measure.hpp:57-135): the depth of the cell nearest `location`
     (Cartesian2DMesh::get_nearest_object_index<Cell>, Cartesian2DMesh.hpp:179-188); a location
-    outside the mesh is an error (the reference would read past the field)."""
+    outside the mesh is an error (the reference would read past the field). `value_type` is the
+    solver's: the reference's time series output writes the times in it too
+    (TimeSeriesOutputFunction::at, Output/OutputFunction.hpp:373-383)."""
 
-    def __init__(self, location, nx, ny, dx, dy, origin=(0.0, 0.0), name="h_point"):
+    def __init__(self, location, nx, ny, dx, dy, origin=(0.0, 0.0), name="h_point", value_type=np.float64):
         cx = (location[0] - origin[0]) / dx
         cy = (location[1] - origin[1]) / dy
         if not (0.0 <= cx < nx and 0.0 <= cy < ny):
             raise ValueError(f"location {location} is outside the mesh")
         self.index = int(math.floor(cy)) * nx + int(math.floor(cx))
         self.name = name
+        self.value_type = value_type
         self.points = []
 
     def update(self, t, solver):
         self.points.append((float(t), float(solver.get_field("H").ravel()[self.index])))
 
     def write(self, path):
-        write_csv(path, ["ID", self.name], [[p[0] for p in self.points], [p[1] for p in self.points]])
+        vt = self.value_type
+        write_csv(path, ["ID", self.name], [np.array([p[0] for p in self.points], dtype=vt),
+                                             np.array([p[1] for p in self.points], dtype=vt)])
 
 
 _CKPT_MAGIC = b"SVCKPT01"
@@ -206,6 +225,6 @@ def load_checkpoint(solver, path):
     return meta
 
 
-__all__ = ["fmt_value", "fmt_coord", "cell_locations", "csv_text", "write_csv", "raw_binary_bytes",
+__all__ = ["fmt_value", "fmt_coord", "quoted", "cell_locations", "csv_text", "write_csv", "raw_binary_bytes",
            "read_raw_binary", "solver_field", "MultiFieldOutput", "VolumeMeasure", "DepthPointMeasure",
            "save_checkpoint", "load_checkpoint", "FIELD"]

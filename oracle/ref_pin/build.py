@@ -71,6 +71,7 @@ COPY = [
     "SaintVenant/SourceTerms/InfiltrationSourceTerm.hpp", "SaintVenant/SourceTerms/InfiltrationSourceTerm.cpp",
     "SaintVenant/SourceTerms/EddyViscositySourceTerm.hpp", "SaintVenant/SourceTerms/EddyViscositySourceTerm.cpp",
     "SaintVenant/Boundaries/StageBoundarySourceTerm.hpp", "SaintVenant/Boundaries/StageBoundarySourceTerm.cpp",
+    "Output/OutputFunction.hpp", "Output/OutputFormat.hpp",
     "Config/TimeParameters.hpp", "Config/TimeParameters.cpp",
     "TemporalScheme/TemporalScheme.hpp", "TemporalScheme/RungeKutta.hpp", "TemporalScheme/RungeKutta.cpp",
 ]

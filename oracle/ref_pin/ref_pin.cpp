@@ -21,6 +21,10 @@
 //                                         with the second derivatives of EddyViscositySourceTerm::
 //                                         apply (EddyViscositySourceTerm.hpp:222-257),
 //                                         StageBoundarySourceKernel (StageBoundarySourceTerm.cpp)
+//   output file formats                   CSVOutput and RawBinaryOutput (src/Output/OutputFormat.hpp)
+//                                         over FieldOutputFunction (cell fields with their
+//                                         locations) and TimeSeriesOutputFunction (measures),
+//                                         src/Output/OutputFunction.hpp
 //   control number                        SaintVenantState::max_control_number (State.cpp:195-230)
 //   stage combination                     the SaintVenantState operators (State.cpp:88-174) in
 //                                         the order of RungeKuttaSolver::update_y
@@ -75,6 +79,8 @@
 #include "TimeParameters.cpp"
 #include "RungeKutta.hpp"
 #include "RungeKutta.cpp"
+#include "OutputFunction.hpp"
+#include "OutputFormat.hpp"
 
 #include <cstdint>
 #include <cstring>
@@ -417,6 +423,79 @@ int dudt_terms(uint64_t nx, uint64_t ny, double dx, double dy, const T* z, const
   }
 }
 
+// The cell fields `values[k]` named `names[k]` on an nx x ny mesh of cell size dx, dy with its
+// origin at (ox, oy), written by the reference's formatter for a FieldOutputFunction (as
+// MultiFieldOutputFile::timed_output does, OutputFile.hpp:195-223): CSVOutput with `delimiter`,
+// or RawBinaryOutput when `binary`.
+template <typename T>
+int write_fields(uint64_t nx, uint64_t ny, double dx, double dy, double ox, double oy, int nfields,
+                 const char* const* names, const T* const* values, const char* delimiter, int binary,
+                 const char* path) {
+  try {
+    auto q = get_sycl_queue();
+    Config& c = GlobalConfig::instance().mesh;
+    auto mesh = make_mesh(q, nx, ny, dx, dy);
+    {
+      std::ostringstream o;
+      o.precision(17);
+      o << ox << ", " << oy;
+      c.kv["origin"] = o.str();
+      mesh = std::make_shared<Cartesian2DMesh>(q, true);
+      c.kv.erase("origin");
+    }
+    const size_t nc = nx * ny;
+    std::vector<std::unique_ptr<CF<T>>> fields;
+    std::vector<CF<T>*> ptrs;
+    for (int k = 0; k < nfields; ++k) {
+      fields.emplace_back(new CF<T>(q, names[k], mesh, vec(values[k], nc), true));
+      ptrs.push_back(fields.back().get());
+    }
+    auto of = std::make_shared<FieldOutputFunction<CF<T>>>(ptrs);
+    if (binary) {
+      RawBinaryOutput(of).output(path);
+    } else {
+      CSVOutput(of, delimiter).output(path);
+    }
+    return 0;
+  } catch (const std::exception& e) {
+    std::cerr << "ref_pin: " << e.what() << std::endl;
+    return -1;
+  }
+}
+
+// A measure's points (times t, values v) as the reference writes them (Measure::output,
+// src/Output/Measure.hpp:82-97): CSVOutput over TimeSeriesOutputFunction, whose first column
+// "ID" holds the times in the value type. PinSeries stands in for the reference's TimeSeries
+// with the two arrays the output function reads.
+template <typename TT, typename T>
+struct PinSeries {
+  using TimeType = TT;
+  using ValueType = T;
+  struct Array {
+    std::vector<T> v;
+    const std::vector<T>& host_vector() const { return v; }
+  };
+  Array t, x;
+  const Array& get_time_array() const { return t; }
+  const Array& get_value_array() const { return x; }
+};
+template <typename T>
+int write_series(uint64_t n, const double* t, const T* v, const char* name, const char* path) {
+  try {
+    auto ts = std::make_shared<PinSeries<T, T>>();
+    for (uint64_t i = 0; i < n; ++i) {
+      ts->t.v.push_back(T(t[i]));
+      ts->x.v.push_back(v[i]);
+    }
+    auto of = std::make_shared<TimeSeriesOutputFunction<PinSeries<T, T>>>(name, ts);
+    CSVOutput(of).output(path);
+    return 0;
+  } catch (const std::exception& e) {
+    std::cerr << "ref_pin: " << e.what() << std::endl;
+    return -1;
+  }
+}
+
 // SaintVenantState::max_control_number (State.cpp:195-230) of (h, u, v) for `timestep`
 template <typename T>
 int control_number(uint64_t nx, uint64_t ny, double dx, double dy, const T* h, const T* u, const T* v, double timestep,
@@ -702,6 +781,22 @@ int refpin_dudt_terms_f32(uint64_t nx, uint64_t ny, double dx, double dy, const 
                           const float* u, const float* v, const float* const* f, float* icap, const int* iopt,
                           const double* dopt, float* out) {
   return dudt_terms<float>(nx, ny, dx, dy, z, h, u, v, f, icap, iopt, dopt, out);
+}
+int refpin_write_fields_f64(uint64_t nx, uint64_t ny, double dx, double dy, double ox, double oy, int nfields,
+                            const char* const* names, const double* const* values, const char* delimiter, int binary,
+                            const char* path) {
+  return write_fields<double>(nx, ny, dx, dy, ox, oy, nfields, names, values, delimiter, binary, path);
+}
+int refpin_write_fields_f32(uint64_t nx, uint64_t ny, double dx, double dy, double ox, double oy, int nfields,
+                            const char* const* names, const float* const* values, const char* delimiter, int binary,
+                            const char* path) {
+  return write_fields<float>(nx, ny, dx, dy, ox, oy, nfields, names, values, delimiter, binary, path);
+}
+int refpin_write_series_f64(uint64_t n, const double* t, const double* v, const char* name, const char* path) {
+  return write_series<double>(n, t, v, name, path);
+}
+int refpin_write_series_f32(uint64_t n, const double* t, const float* v, const char* name, const char* path) {
+  return write_series<float>(n, t, v, name, path);
 }
 int refpin_control_number_f64(uint64_t nx, uint64_t ny, double dx, double dy, const double* h, const double* u,
                               const double* v, double timestep, double* cn) {

@@ -48,6 +48,13 @@ def load():
             f.restype = C.c_int
             f.argtypes = [C.c_uint64, C.c_uint64, C.c_double, C.c_double] + [P] * 4 + \
                          [C.POINTER(P), P, C.POINTER(C.c_int), C.POINTER(C.c_double), P]
+            f = getattr(_lib, f"refpin_write_fields_{t}")
+            f.restype = C.c_int
+            f.argtypes = [C.c_uint64, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+                          C.POINTER(C.c_char_p), C.POINTER(P), C.c_char_p, C.c_int, C.c_char_p]
+            f = getattr(_lib, f"refpin_write_series_{t}")
+            f.restype = C.c_int
+            f.argtypes = [C.c_uint64, C.POINTER(C.c_double), P, C.c_char_p, C.c_char_p]
             f = getattr(_lib, f"refpin_update_y_{t}")
             f.restype = C.c_int
             f.argtypes = [C.c_uint64, C.c_uint64, C.c_double, C.c_double, P, P, C.c_int,
@@ -156,6 +163,34 @@ def dudt_terms(z, h, u, v, dx, dy=None, manning=None, eloss=None, infil=None, ed
     res = {name: out[i * nc:(i + 1) * nc].reshape(ny, nx) for i, name in enumerate(KS)}
     res["INFIL_CAP"] = None if cap is None else cap.reshape(ny, nx)
     return res
+
+
+def write_fields(path, nx, ny, dx, dy, origin, names, values, delimiter=", ", binary=False, precision="f64"):
+    """Write cell fields (arrays of nx * ny values, names as str) the way the reference's
+    MultiFieldOutputFile does: CSVOutput (or RawBinaryOutput) over a FieldOutputFunction on a
+    mesh with the given cell size and origin."""
+    lib = load()
+    dt_, ct = _np(precision)
+    vals = [np.ascontiguousarray(np.asarray(v).ravel(), dtype=dt_) for v in values]
+    nm = (C.c_char_p * len(names))(*[n.encode() for n in names])
+    vp = (C.POINTER(ct) * len(vals))(*[_ptr(v, ct) for v in vals])
+    r = getattr(lib, f"refpin_write_fields_{precision}")(nx, ny, dx, dy, origin[0], origin[1], len(vals), nm, vp,
+                                                         delimiter.encode(), 1 if binary else 0,
+                                                         os.fsencode(path))
+    if r != 0:
+        raise RuntimeError("reference output failed")
+
+
+def write_series(path, times, values, name, precision="f64"):
+    """Write a measure's points the way the reference's Measure::output does."""
+    lib = load()
+    dt_, ct = _np(precision)
+    t = np.ascontiguousarray(times, dtype=np.float64)
+    v = np.ascontiguousarray(values, dtype=dt_)
+    r = getattr(lib, f"refpin_write_series_{precision}")(len(t), t.ctypes.data_as(C.POINTER(C.c_double)),
+                                                         _ptr(v, ct), name.encode(), os.fsencode(path))
+    if r != 0:
+        raise RuntimeError("reference output failed")
 
 
 def control_number(h, u, v, dx, dy=None, timestep=1.0, precision="f64"):
