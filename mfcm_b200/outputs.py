@@ -166,8 +166,11 @@ class DepthPointMeasure:
     (TimeSeriesOutputFunction::at, Output/OutputFunction.hpp:373-383)."""
 
     def __init__(self, location, nx, ny, dx, dy, origin=(0.0, 0.0), name="h_point", value_type=np.float64):
-        cx = (location[0] - origin[0]) / dx
-        cy = (location[1] - origin[1]) / dy
+        # Cartesian2DMesh::get_coordinate (Cartesian2DMesh.hpp:112-121) on an unrotated mesh:
+        # the offset times the stored reciprocal of the cell size, which rounds differently from
+        # a division on cell edges
+        cx = (location[0] - origin[0]) * (1.0 / dx)
+        cy = (location[1] - origin[1]) * (1.0 / dy)
         if not (0.0 <= cx < nx and 0.0 <= cy < ny):
             raise ValueError(f"location {location} is outside the mesh")
         self.index = int(math.floor(cy)) * nx + int(math.floor(cx))

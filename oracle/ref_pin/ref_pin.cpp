@@ -496,6 +496,38 @@ int write_series(uint64_t n, const double* t, const T* v, const char* name, cons
   }
 }
 
+// Cartesian2DMesh::get_nearest_object_index<Cell> (Cartesian2DMesh.hpp:179-188) of n locations
+// xy (x0, y0, x1, y1, ...) on an nx x ny mesh of cell size dx, dy with its origin at (ox, oy):
+// the cell containing each location, nx * ny outside the mesh; and, when loc is not null, the
+// cell centres get_object_location<Cell> (x, y per cell) of every cell.
+int nearest_cells(uint64_t nx, uint64_t ny, double dx, double dy, double ox, double oy, uint64_t n,
+                  const double* xy, uint64_t* out, double* loc) {
+  try {
+    auto q = get_sycl_queue();
+    Config& c = GlobalConfig::instance().mesh;
+    make_mesh(q, nx, ny, dx, dy);  // sets the cell count and size
+    std::ostringstream o;
+    o.precision(17);
+    o << ox << ", " << oy;
+    c.kv["origin"] = o.str();
+    auto mesh = std::make_shared<Cartesian2DMesh>(q, false);
+    c.kv.erase("origin");
+    for (uint64_t i = 0; i < n; ++i)
+      out[i] = mesh->get_nearest_object_index<MeshComponent::Cell>({xy[2 * i], xy[2 * i + 1]});
+    if (loc) {
+      for (uint64_t i = 0; i < nx * ny; ++i) {
+        const std::array<double, 2> p = mesh->get_object_location<MeshComponent::Cell>(i);
+        loc[2 * i] = p[0];
+        loc[2 * i + 1] = p[1];
+      }
+    }
+    return 0;
+  } catch (const std::exception& e) {
+    std::cerr << "ref_pin: " << e.what() << std::endl;
+    return -1;
+  }
+}
+
 // SaintVenantState::max_control_number (State.cpp:195-230) of (h, u, v) for `timestep`
 template <typename T>
 int control_number(uint64_t nx, uint64_t ny, double dx, double dy, const T* h, const T* u, const T* v, double timestep,
@@ -797,6 +829,10 @@ int refpin_write_series_f64(uint64_t n, const double* t, const double* v, const 
 }
 int refpin_write_series_f32(uint64_t n, const double* t, const float* v, const char* name, const char* path) {
   return write_series<float>(n, t, v, name, path);
+}
+int refpin_nearest_cells(uint64_t nx, uint64_t ny, double dx, double dy, double ox, double oy, uint64_t n,
+                         const double* xy, uint64_t* out, double* loc) {
+  return nearest_cells(nx, ny, dx, dy, ox, oy, n, xy, out, loc);
 }
 int refpin_control_number_f64(uint64_t nx, uint64_t ny, double dx, double dy, const double* h, const double* u,
                               const double* v, double timestep, double* cn) {

@@ -59,7 +59,29 @@ def load():
             f.restype = C.c_int
             f.argtypes = [C.c_uint64, C.c_uint64, C.c_double, C.c_double, P, P, C.c_int,
                           C.POINTER(C.c_double), C.c_double, P]
+    if not getattr(_lib, "_nearest_set", False):
+        f = _lib.refpin_nearest_cells
+        f.restype = C.c_int
+        D = C.POINTER(C.c_double)
+        f.argtypes = [C.c_uint64, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64, D,
+                      C.POINTER(C.c_uint64), D]
+        _lib._nearest_set = True
     return _lib
+
+
+def nearest_cells(nx, ny, dx, dy, origin, x, y):
+    """Cartesian2DMesh::get_nearest_object_index<Cell> of the locations (x, y) (nx * ny when
+    outside the mesh) and get_object_location<Cell> of every cell, as (index array, (cx, cy))."""
+    lib = load()
+    xy = np.ascontiguousarray(np.stack([np.ravel(x), np.ravel(y)], axis=1), dtype=np.float64)
+    n = xy.shape[0]
+    out = np.empty(n, dtype=np.uint64)
+    loc = np.empty(2 * nx * ny, dtype=np.float64)
+    r = lib.refpin_nearest_cells(nx, ny, dx, dy, origin[0], origin[1], n, _ptr(xy, C.c_double),
+                                 out.ctypes.data_as(C.POINTER(C.c_uint64)), _ptr(loc, C.c_double))
+    if r != 0:
+        raise RuntimeError("reference mesh failed")
+    return out.astype(np.int64), (loc[0::2], loc[1::2])
 
 
 def _np(precision):
