@@ -830,6 +830,25 @@ int refpin_write_series_f64(uint64_t n, const double* t, const double* v, const 
 int refpin_write_series_f32(uint64_t n, const double* t, const float* v, const char* name, const char* path) {
   return write_series<float>(n, t, v, name, path);
 }
+// TimeParameters::num_steps (TimeParameters.cpp:40-58) for start, end and step duration in
+// seconds, TimeType double
+int refpin_num_steps(double start, double end, double step, uint64_t* n) {
+  try {
+    Config conf;
+    std::ostringstream s;
+    s.precision(17);
+    auto put = [&](const char* k, double x) { s.str(""); s << x; conf.kv[k] = s.str(); };
+    put("start time", start);
+    put("end time", end);
+    put("step duration seconds", step);
+    TimeParameters<double> tp(conf);
+    *n = tp.num_steps();
+    return 0;
+  } catch (const std::exception& e) {
+    std::cerr << "ref_pin: " << e.what() << std::endl;
+    return -1;
+  }
+}
 int refpin_nearest_cells(uint64_t nx, uint64_t ny, double dx, double dy, double ox, double oy, uint64_t n,
                          const double* xy, uint64_t* out, double* loc) {
   return nearest_cells(nx, ny, dx, dy, ox, oy, n, xy, out, loc);

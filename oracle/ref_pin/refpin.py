@@ -65,8 +65,19 @@ def load():
         D = C.POINTER(C.c_double)
         f.argtypes = [C.c_uint64, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64, D,
                       C.POINTER(C.c_uint64), D]
+        f = _lib.refpin_num_steps
+        f.restype = C.c_int
+        f.argtypes = [C.c_double, C.c_double, C.c_double, C.POINTER(C.c_uint64)]
         _lib._nearest_set = True
     return _lib
+
+
+def num_steps(start, end, step):
+    """TimeParameters::num_steps of the reference (TimeType double)."""
+    n = C.c_uint64()
+    if load().refpin_num_steps(start, end, step, C.byref(n)) != 0:
+        raise RuntimeError("reference time parameters failed")
+    return n.value
 
 
 def nearest_cells(nx, ny, dx, dy, origin, x, y):

@@ -240,3 +240,21 @@ def test_further_terms_match_reference_kernels(prec, shape, dxy, nan_cells, eddy
     o = _oracle_terms(prec, nx, ny, dx, dy, z, h, u, v, man, eloss, infil, eddy, q, stage, stage_first, order, t, dt, L)
     for name, a in ref.items():
         assert_same(a, o.get_field(name), name)
+
+
+def test_num_steps_matches_reference():
+    """TimeParameters::num_steps: whole steps within 1e-6 s of the duration count as whole, any
+    other remainder adds a step; the package's restatement (used by solve() and the decks)."""
+    from mfcm_b200 import num_steps
+    rng = np.random.default_rng(3)
+    cases = [(0.0, 3600.0, 60.0), (0.0, 3600.0000001, 60.0), (0.0, 3600.000002, 60.0), (0.0, 3601.0, 60.0),
+             (0.0, 59.9999995, 60.0), (10.0, 70.0, 60.0), (0.0, 0.3, 0.1), (0.0, 1.0, 0.1), (0.0, 7200.0, 7.0),
+             (5.5, 5.5, 60.0), (0.0, 1e9, 60.0)]
+    for _ in range(300):
+        step = float(rng.choice([0.1, 1.0, 7.5, 30.0, 60.0, 600.0, 3600.0, 0.37]))
+        k = int(rng.integers(0, 500))
+        start = float(rng.choice([0.0, rng.uniform(0, 1e5)]))
+        end = start + k * step + float(rng.choice([0.0, 1e-7, -1e-7, 2e-6, -2e-6, rng.uniform(0, step)]))
+        cases.append((start, end, step))
+    for start, end, step in cases:
+        assert num_steps(start, end, step) == refpin.num_steps(start, end, step), (start, end, step)
