@@ -41,6 +41,88 @@ from . import (TimeSeries, Forcing, num_steps, RAIN_NONE, RAIN_UNIFORM, RAIN_FIE
                STAGE_FIELDS)
 
 
+
+_SPACE = " \t\n\v\f\r"   # isspace in the C locale
+
+
+def rapidcsv_rows(data, sep=",", comment="#"):
+    """rapidcsv 8.51's Document::ParseCsv (the reader the reference vendors in src/rapidcsv/)
+    with the reference's settings: cells split at `sep` outside quotes, a quote opening a quoted
+    cell only at the cell's first character, carriage returns dropped, cells trimmed of
+    whitespace and then unquoted (outer quotes removed, doubled quotes halved), empty lines
+    skipped (a line of blanks is a row of one empty cell), lines whose first cell starts with
+    `comment` skipped except a last line without a line break, a UTF-8 byte-order mark
+    ignored. Bytes map one to one onto the characters of the returned cells (latin-1)."""
+    if data[:3] == b"\xef\xbb\xbf":
+        data = data[3:]
+    text = data.decode("latin-1")
+
+    def finish(cell):
+        cell = cell.strip(_SPACE)
+        if len(cell) >= 2 and cell[0] == '"' and cell[-1] == '"':
+            cell = cell[1:-1].replace('""', '"')
+        return cell
+
+    rows, row, cell, quoted = [], [], "", False
+    for ch in text:
+        if ch == '"':
+            if cell == "" or cell[0] == '"':
+                quoted = not quoted
+            cell += ch
+        elif ch == sep:
+            if quoted:
+                cell += ch
+            else:
+                row.append(finish(cell))
+                cell = ""
+        elif ch == "\r":
+            pass
+        elif ch == "\n":
+            if not row and cell == "":
+                continue
+            row.append(finish(cell))
+            if not (row[0] != "" and row[0][0] == comment):
+                rows.append(row)
+            row, cell, quoted = [], "", False
+        else:
+            cell += ch
+    if cell != "" or row:
+        row.append(finish(cell))
+        rows.append(row)
+    return rows
+
+
+_STRTOD = re.compile(r"[ \t\n\v\f\r]*[+-]?(?:(?P<inf>inf(?:inity)?)|(?P<nan>nan(?:\([0-9A-Za-z_]*\))?)"
+                     r"|(?P<hex>0x(?:[0-9a-f]+\.?[0-9a-f]*|\.[0-9a-f]+)(?:p[+-]?[0-9]+)?)"
+                     r"|(?P<dec>(?:[0-9]+\.?[0-9]*|\.[0-9]+)(?:e[+-]?[0-9]+)?))", re.IGNORECASE)
+
+
+def stod_or_nan(cell):
+    """rapidcsv's default converter for double: std::stod, i.e. strtod in the C locale on the
+    longest valid prefix (leading blanks, a sign, decimal or hexadecimal digits, inf, nan), and
+    NaN where std::stod throws: no number at the start, or a result out of range (overflow to
+    infinity, or underflow below the smallest normal double)."""
+    m = _STRTOD.match(cell)
+    if not m:
+        return float("nan")
+    text = m.group(0).strip(_SPACE)
+    if m.group("inf") or m.group("nan"):
+        return float(text.lower().split("(")[0])
+    try:
+        v = float.fromhex(text) if m.group("hex") else float(text)
+    except OverflowError:
+        return float("nan")
+    if math.isinf(v):
+        return float("nan")
+    if v == 0.0:
+        digits = re.sub(r"[eEpP].*$", "", text)
+        digits = re.sub(r"^[+-]?(0[xX])?", "", digits)
+        if re.search(r"[1-9a-fA-F]", digits):
+            return float("nan")  # a non-zero number that underflowed to zero
+    elif abs(v) < 2.2250738585072014e-308:
+        return float("nan")  # a subnormal result
+    return v
+
 class ConfigError(ValueError):
     pass
 
@@ -634,44 +716,54 @@ class Model:
             times, values = self._csv(conf, TimeParser(conf, self.parser))
         else:
             raise ConfigError(f"unknown time series source {src!r}")
+        # TimeSeries::apply_transform (TimeSeries.cpp:81-105) with the `transform` section
+        tr = conf.child("transform")
+        if tr is not None:
+            tf, to = float(tr.get("time factor", "1.0")), float(tr.get("time offset", "0.0"))
+            vf, vo = float(tr.get("value factor", "1.0")), float(tr.get("value offset", "0.0"))
+            times = [(t + to) * tf for t in times]
+            values = [(v + vo) * vf for v in values]
         ts = TimeSeries(times, values)
         self._series[name] = ts
         return ts
 
     def _csv(self, conf, tp):
-        """TimeSeries::load_csv (TimeSeries.cpp:209-259): rapidcsv's label row is `skip rows`
-        (+1 with headers, so the first row by default) and its row-name column `skip cols`
-        (-1: none); named or 1-based numbered time and value columns."""
+        """TimeSeries::load_csv (TimeSeries.cpp:209-259) through rapidcsv 8.51 as the reference
+        configures it (trimmed cells, comment and empty lines skipped, the default converter):
+        the label row is `skip rows` (+1 with headers, so the first row by default), the row-name
+        column `skip cols` (-1: none); named or 1-based numbered time and value columns."""
         fn = conf.get("filename")
         path = fn if os.path.isabs(fn) else os.path.join(self.base, fn)
-        sep = conf.get("separator", ",")
-        comment = conf.get("comment character", "#")
+        sep = conf.get("separator", ",")[:1] or ","
+        comment = conf.get("comment character", "#")[:1] or "#"
         headers = conf.get("headers", "true").lower() in ("true", "1", "yes")
         label_row = int(conf.get("skip rows", "-1")) + (1 if headers else 0)
         name_col = int(conf.get("skip cols", "-1"))
-        rows = []
-        for line in open(path):
-            line = line.rstrip("\r\n")
-            if not line.strip() or line.lstrip().startswith(comment):
-                continue
-            cells = [c.strip() for c in line.split(sep)]
-            if name_col >= 0:
-                del cells[name_col]
-            rows.append(cells)
-        if label_row >= 0:
-            head, body = rows[label_row], rows[label_row + 1:]
-        else:
-            head, body = None, rows
+        with open(path, "rb") as f:
+            rows = rapidcsv_rows(f.read(), sep, comment)
         if headers:
-            try:
-                tcol = head.index(conf.get("time column"))
-                vcol = head.index(conf.get("value column"))
-            except ValueError as e:
-                raise ConfigError(f"{fn}: {e}") from None
+            labels = {}
+            if 0 <= label_row < len(rows):
+                for i, name in enumerate(rows[label_row]):
+                    labels[name] = i  # a repeated label: the last one counts
+            cols = []
+            for key in ("time column", "value column"):
+                name = conf.get(key, "").encode("utf-8").decode("latin-1")
+                if name not in labels:
+                    raise ConfigError(f"{fn}: no column {conf.get(key, '')!r}")
+                cols.append(labels[name])
+            tcol, vcol = cols
         else:
-            tcol = int(conf.get("time column", "1")) - 1
-            vcol = int(conf.get("value column", "2")) - 1
-        return [tp.parse(r[tcol]) for r in body], [float(r[vcol]) for r in body]
+            tcol = int(conf.get("time column", "1")) - 1 + name_col + 1
+            vcol = int(conf.get("value column", "2")) - 1 + name_col + 1
+        body = rows[label_row + 1:] if label_row >= 0 else rows
+        times, values = [], []
+        for r in body:
+            if not (0 <= tcol < len(r) and 0 <= vcol < len(r)):
+                raise ConfigError(f"{fn}: a row has no column {max(tcol, vcol) + 1}")
+            times.append(tp.parse(r[tcol]))
+            values.append(stod_or_nan(r[vcol]))
+        return times, values
 
     # --- building and running
     def build(self, solver_cls, precision="f64", **kw):

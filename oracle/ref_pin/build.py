@@ -32,6 +32,9 @@ machines do not have it) `available()` is False and the pin tests skip.
 A second library, oracle/_ref/libsv_refpin_nimrod.so, holds the reference's NIMROD raster reader
 (src/Raster/RasterFormats/NIMROD.cpp with src/Raster/RasterFormat.hpp, copied unchanged) and
 oracle/ref_pin/nimrod_pin.cpp, the driver that runs it on a file and copies out what it read.
+A third, oracle/_ref/libsv_refpin_ts.so, holds the reference's time-series reader
+(src/Input/TimeSeries.cpp and .hpp with the rapidcsv header the reference vendors, copied
+unchanged into a tree of their own) and oracle/ref_pin/ts_pin.cpp, its driver.
 """
 import os
 import re
@@ -77,6 +80,10 @@ COPY = [
 ]
 # the NIMROD reader, compiled into its own library
 NIMROD_COPY = ["Raster/RasterFormat.hpp", "Raster/RasterFormats/NIMROD.hpp", "Raster/RasterFormats/NIMROD.cpp"]
+# the time-series reader, compiled into its own library from a tree of its own (the kernels'
+# tree has a stand-in at Input/TimeSeries.hpp): destination -> reference source file
+TS_COPY = {"tsreal/Input/TimeSeries.hpp": "Input/TimeSeries.hpp", "tsreal/Input/TimeSeries.cpp": "Input/TimeSeries.cpp",
+           "tsreal/rapidcsv/rapidcsv.h": "rapidcsv/rapidcsv.h"}
 # stand-ins, by the path the reference includes them from
 STUBS = {
     "Config/Config.hpp": "Config.hpp",
@@ -94,10 +101,13 @@ FLAGS = ["-std=c++17", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-
 DRIVER = os.path.join(HERE, "ref_pin.cpp")
 NIMROD_DRIVER = os.path.join(HERE, "nimrod_pin.cpp")
 NIMROD_LIB = os.path.join(OUT, "libsv_refpin_nimrod.so")
+TS_DRIVER = os.path.join(HERE, "ts_pin.cpp")
+TS_LIB = os.path.join(OUT, "libsv_refpin_ts.so")
 
 
 def available():
-    return os.path.isdir(REF_SRC) and all(os.path.exists(os.path.join(REF_SRC, f)) for f in COPY + NIMROD_COPY)
+    return os.path.isdir(REF_SRC) and all(os.path.exists(os.path.join(REF_SRC, f))
+                                          for f in COPY + NIMROD_COPY + list(TS_COPY.values()))
 
 
 def _block_end(text, start):
@@ -205,6 +215,14 @@ def prepare():
         dst = os.path.join(TREE, rel)
         os.makedirs(os.path.dirname(dst), exist_ok=True)
         shutil.copy(os.path.join(HERE, "stubs", stub), dst)
+    # the time-series tree: the reference's reader and rapidcsv unchanged, the check-file stand-in
+    for dst_rel, src_rel in TS_COPY.items():
+        dst = os.path.join(TREE, dst_rel)
+        os.makedirs(os.path.dirname(dst), exist_ok=True)
+        shutil.copy(os.path.join(REF_SRC, src_rel), dst)
+    dst = os.path.join(TREE, "tsreal", "Output", "CheckFile.hpp")
+    os.makedirs(os.path.dirname(dst), exist_ok=True)
+    shutil.copy(os.path.join(HERE, "stubs", "CheckFile.hpp"), dst)
 
 
 def _stale(lib, driver, copied):
@@ -221,7 +239,8 @@ def build(force=False, verbose=False):
     """Build both pin libraries (when stale); returns the path of the kernels' library."""
     if not available():
         raise RuntimeError(f"reference sources not found under {REF_SRC}")
-    targets = [(LIB, DRIVER, COPY), (NIMROD_LIB, NIMROD_DRIVER, COPY + NIMROD_COPY)]
+    targets = [(LIB, DRIVER, COPY), (NIMROD_LIB, NIMROD_DRIVER, COPY + NIMROD_COPY),
+               (TS_LIB, TS_DRIVER, COPY + list(TS_COPY.values()))]
     todo = [t for t in targets if force or _stale(*t)]
     if not todo:
         return LIB
@@ -231,11 +250,18 @@ def build(force=False, verbose=False):
     for d in INCLUDE_DIRS:
         inc += ["-I", os.path.join(TREE, d)]
     for lib, driver, _ in todo:
-        cmd = ["g++"] + FLAGS + inc + [driver, "-o", lib]
+        first = ["-I", os.path.join(TREE, "tsreal", "Input")] if lib == TS_LIB else []
+        cmd = ["g++"] + FLAGS + inc[:2] + first + inc[2:] + [driver, "-o", lib]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.check_call(cmd)
     return LIB
+
+
+def build_ts(force=False, verbose=False):
+    """Build (when stale) and return the path of the time-series reader's library."""
+    build(force=force, verbose=verbose)
+    return TS_LIB
 
 
 def build_nimrod(force=False, verbose=False):

@@ -336,3 +336,68 @@ def nimrod_read(path, bbox=None):
             "ulc": (int(dims[2]), int(dims[3])), "lrc": (int(dims[4]), int(dims[5])), "ncols": int(dims[6]),
             "nrows": int(dims[7]), "buffer": buf.reshape(nypx, nxpx), "values": val[:nval], "geo": list(geo),
             "llc": (llc[0], llc[1]), "nodata": nod[0]}
+
+
+_ts = None
+
+
+def _load_ts():
+    global _ts
+    if _ts is None:
+        _ts = C.CDLL(_build_module().build_ts())
+        S = C.POINTER(C.c_char_p)
+        D = C.POINTER(C.c_double)
+        f = _ts.refpin_ts_load
+        f.restype = C.c_int
+        f.argtypes = [S, S, C.c_int, S, S, C.c_int, S, S, C.c_int, D, D, C.c_uint64, C.POINTER(C.c_uint64),
+                      C.c_char_p, C.c_uint64]
+        f = _ts.refpin_ts_at
+        f.restype = C.c_int
+        f.argtypes = [D, D, C.c_uint64, D, C.c_uint64, D]
+    return _ts
+
+
+def _strings(items):
+    items = list(items)
+    return (C.c_char_p * max(1, len(items)))(*[str(x).encode() for x in items]), len(items)
+
+
+def ts_load(section, data=None, transform=None):
+    """TimeSeries<double, double>::load of the reference on a "time series" section given as
+    key -> value strings (`source`, `filename`, `separator`, `headers`, ...), the inline data
+    as (time string, value string) pairs, and the transform section's keys. Returns (times,
+    values); raises RefReaderError when the reader throws."""
+    lib = _load_ts()
+    k, nk = _strings(section.keys())
+    v, _ = _strings(section.values())
+    data = list(data or [])
+    dk, nd = _strings(d[0] for d in data)
+    dv, _ = _strings(d[1] for d in data)
+    transform = dict(transform or {})
+    tk, nt = _strings(transform.keys())
+    tv, _ = _strings(transform.values())
+    err = C.create_string_buffer(512)
+    n = C.c_uint64()
+    cap = 1 << 16
+    t = np.empty(cap)
+    x = np.empty(cap)
+    r = lib.refpin_ts_load(k, v, nk, dk, dv, nd, tk, tv, nt, _ptr(t, C.c_double), _ptr(x, C.c_double), cap,
+                           C.byref(n), err, len(err))
+    if r != 0:
+        raise RefReaderError(err.value.decode(errors="replace"))
+    m = min(n.value, cap)
+    return t[:m].copy(), x[:m].copy()
+
+
+def ts_at(times, values, queries):
+    """TimeSeries<double, double>::at (ts_linterp) of the reference at each query time (each
+    below the last knot)."""
+    lib = _load_ts()
+    t = np.ascontiguousarray(times, dtype=np.float64)
+    v = np.ascontiguousarray(values, dtype=np.float64)
+    q = np.ascontiguousarray(queries, dtype=np.float64)
+    out = np.empty_like(q)
+    if lib.refpin_ts_at(_ptr(t, C.c_double), _ptr(v, C.c_double), len(t), _ptr(q, C.c_double), len(q),
+                        _ptr(out, C.c_double)) != 0:
+        raise RuntimeError("reference time series failed")
+    return out

@@ -3,6 +3,7 @@
 #pragma once
 #include <filesystem>
 #include <initializer_list>
+#include <string>
 template <typename F>
 class FieldCheckFile {
  public:
@@ -15,4 +16,10 @@ class MeshSelectionCheckFile {
  public:
   MeshSelectionCheckFile(const char*) {}
   void output(const S&) {}
+};
+template <typename TS>
+class TimeSeriesCheckFile {
+ public:
+  TimeSeriesCheckFile(const char*) {}
+  void output(const std::string&) {}
 };

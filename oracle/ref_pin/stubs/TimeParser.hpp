@@ -7,5 +7,6 @@ template <typename T>
 class TimeParser {
  public:
   TimeParser(const Config&) {}
+  TimeParser(const TimeParser&, const Config&) {}
   T parse(const std::string& s) const { return s.empty() ? T(0) : T(std::stod(s)); }
 };
