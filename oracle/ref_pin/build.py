@@ -53,7 +53,7 @@ LIB = os.path.join(OUT, "libsv_refpin.so")
 COPY = [
     "sycl.hpp",
     "DataArray/DataArray.hpp", "DataArray/DataArray.cpp",
-    "Mesh/Mesh.hpp", "Mesh/Cartesian2DMesh.hpp", "Mesh/MeshSelection.hpp",
+    "Mesh/Mesh.hpp", "Mesh/Cartesian2DMesh.hpp", "Mesh/Cartesian2DMesh.cpp", "Mesh/MeshSelection.hpp",
     "Field/Field.hpp", "Field/Field.cpp", "Field/FieldOperators.hpp", "Field/FieldOperators.cpp",
     "Field/BinaryFieldOperator_impl.hpp",
     "SpatialDerivative/Minmod3.hpp", "SpatialDerivative/SpatialDerivative.hpp",

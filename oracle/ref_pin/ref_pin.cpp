@@ -87,53 +87,9 @@
 #include <iostream>
 
 // ---- glue the reference defines in files that read its configuration --------------------
-// Cartesian2DMesh's configured constructor and device moves are compiled from the reference
-// only through src/Mesh/Cartesian2DMesh.cpp, which also defines the raster constructor whose
-// cell count is lost (it copies the count vector); the configured constructor is restated
-// here from Cartesian2DMesh.cpp:24-61 with the same geo-transform layout and arithmetic.
-Cartesian2DMesh::Cartesian2DMesh(const std::shared_ptr<sycl::queue>& queue, bool on_device)
-    : ncells_(queue, 2), geotrans_(queue, 12) {
-  const Config& conf = GlobalConfig::instance().mesh_configuration();
-  std::array<size_t, 2> user_ncells = split_string<size_t, 2>(conf.get<std::string>("cell count"));
-  ncells_.host_vector() = {user_ncells[0], user_ncells[1]};
-  std::array<double, 2> user_origin = split_string<double, 2>(conf.get<std::string>("origin", "0.0, 0.0"));
-  std::array<double, 2> user_cellsize = split_string<double, 2>(conf.get<std::string>("cell size"));
-  double rotation = conf.get<double>("angle", 0.0);
-  std::vector<double>& gt = geotrans_.host_vector();
-  gt[0] = user_origin[0];
-  gt[1] = user_cellsize[0] * std::cos(rotation);
-  gt[2] = user_cellsize[0] * std::sin(rotation);
-  gt[3] = user_origin[1];
-  gt[4] = user_cellsize[1] * std::sin(rotation);
-  gt[5] = user_cellsize[1] * std::cos(rotation);
-  gt[6] = 1.0 / gt.at(1);
-  gt[7] = 1.0 / gt.at(5);
-  gt[8] = 1.0 / (gt.at(1) * gt.at(5));
-  gt[9] = 1.0 - (gt.at(2) * gt.at(4)) * gt.at(8);
-  gt[10] = std::sqrt(gt[1] * gt[1] + gt[2] * gt[2]);
-  gt[11] = std::sqrt(gt[4] * gt[4] + gt[5] * gt[5]);
-  if (on_device) {
-    ncells_.move_to_device();
-    geotrans_.move_to_device();
-  }
-}
-void Cartesian2DMesh::move_to_device(void) {
-  ncells_.move_to_device();
-  geotrans_.move_to_device();
-}
-void Cartesian2DMesh::move_to_host(void) {
-  ncells_.move_to_host();
-  geotrans_.move_to_host();
-}
-Cartesian2DMeshAccessor::Cartesian2DMeshAccessor(const Cartesian2DMesh& c2m)
-    : ncells_ro_(c2m.ncells_data()
-                     .template get_placeholder_accessor<sycl::access::mode::read, sycl::access::target::global_buffer>()),
-      geotrans_ro_(c2m.geotrans_data()
-                       .template get_placeholder_accessor<sycl::access::mode::read, sycl::access::target::global_buffer>()) {}
-void Cartesian2DMeshAccessor::bind(sycl::handler& cgh) {
-  cgh.require(ncells_ro_);
-  cgh.require(geotrans_ro_);
-}
+// Cartesian2DMesh's configured constructor, device moves and accessor are the reference's own
+// (src/Mesh/Cartesian2DMesh.cpp, compiled below with the configuration stand-in).
+#include "Cartesian2DMesh.cpp"
 
 // MeshSelection, global selections only (MeshSelection.cpp:22-33, 146-157, 196-214): a global
 // selection is a two-entry list holding the object count twice.
