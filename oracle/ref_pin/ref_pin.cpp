@@ -3,8 +3,9 @@
 // into oracle/_ref/libsv_refpin.so from the reference's sources; only tests/ load it.
 //
 // What runs here is the reference's code, compiled unchanged:
-//   mesh, field and data-array classes    src/Mesh/Cartesian2DMesh.hpp, src/Field/Field.cpp,
-//                                         src/DataArray/DataArray.cpp
+//   mesh, field and data-array classes    src/Mesh/Cartesian2DMesh.hpp and .cpp (the configured
+//                                         constructor, cell centres and cell lookups),
+//                                         src/Field/Field.cpp, src/DataArray/DataArray.cpp
 //   slopes                                SaintVenantState::calculate_spatial_derivatives
 //                                         (src/SaintVenant/State.cpp:176-193) with
 //                                         SpatialDerivativeOperator<Minmod3> (SpatialDerivative.cpp)
